@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark of the GNSS particle-filter step on B200.
+
+One step = one epoch of predict -> weight -> (ESS-conditional) resample ->
+estimate for every particle of the workload.  Default workload: the
+1,000,000-particle x 32-satellite plain filter with four clock states
+(7-D FP32 state about an FP64 anchor), systematic resampling when
+ESS < N/2, synthetic seeded observations (cfg "drop-in at scale").
+
+Prints ONE JSON line (rank 0).  Multi-GPU: one process per GPU, each an
+independent replica of the workload (the path shards across independent
+filters with no exchange), timed on the device, max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--workload cfg1-systematic|cfg1-megopolis|cfg2-batched]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "PF particle-steps/s (1M particles x 32 satellites, predict+weight+resample+estimate)"
+UNIT = "particle-steps/s"
+L2_FLUSH_BYTES = 512 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="cfg1-systematic",
+                    choices=["cfg1-systematic", "cfg1-megopolis", "cfg2-batched"])
+    ap.add_argument("--n-particles", type=int, default=1_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------- process set
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reduce_max(pg, value: float) -> float:
+    if pg is None:
+        return value
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[4], parts[5], parts[6], parts[7], parts[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = np.array([r[0] for r in rows])
+        mx = max(r[1] for r in rows)
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[3:]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        load = sm[sm >= 0.5 * sm.max()] if sm.max() > 0 else sm
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------------- workloads
+def cfg1_inputs(n_epochs: int, seed: int):
+    from gnss_gpu_b200 import scenario as S
+    return S.config1(n_epochs=n_epochs, seed=seed)
+
+
+def epoch_record(tr, t, flags):
+    return {"disp": tr.disp_enu[t], "sats": tr.sats[t], "pr": tr.pr[t], "clk": tr.clk_idx[t], "flags": flags}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(kernel: str):
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get(kernel)
+    return None
+
+
+def cpu_baseline_cfg1(n: int, epochs: int, seed: int):
+    """The oracle (FP64 C port of the reference's step, OpenMP on all host
+    cores) on the same workload: predict, weight, ESS, systematic resample,
+    estimate."""
+    from oracle import oracle as O
+    from gnss_gpu_b200 import scenario as S
+    import ctypes as C
+    tr = cfg1_inputs(epochs + 1, seed)
+    D = 7
+    x = O.init_state(n, D, 10.0, 30.0, 4242)
+    x = np.ascontiguousarray(x.reshape(-1))
+    xt = np.zeros_like(x)
+    lw = np.zeros(n)
+    lw32 = np.zeros(n, np.float32)
+    anc = np.zeros(n, np.int32)
+    anchor = np.ascontiguousarray(tr.truth_ecef[0])
+    clk = np.ascontiguousarray(tr.truth_clk[0], dtype=np.float64)
+    ca = np.zeros(4)
+    ca[:4] = clk
+    rot = np.ascontiguousarray(tr.rot.ravel())
+    sigma = np.array([1, 1, 0.5, 0.5, 0.5, 0.5, 0.5, 0], np.float32)
+    stats = np.zeros(24)
+    L = O.lib()
+    t0 = time.perf_counter()
+    for t in range(epochs):
+        rows = np.ascontiguousarray(np.column_stack([tr.sats[t], tr.pr[t], np.ones(len(tr.pr[t]))]).ravel())
+        ci = np.ascontiguousarray(tr.clk_idx[t], np.int32)
+        L.orc_epoch(n, D, x, xt, lw, lw32, anc, anchor, ca, rot, np.ascontiguousarray(tr.disp_enu[t]), sigma,
+                    4242, 0, t + 1, len(tr.pr[t]), rows, ci, 3.0, 0.5, stats)
+    dt = time.perf_counter() - t0
+    return n * epochs / dt, O.num_threads(), dt
+
+
+# ------------------------------------------------------------ b200 arm
+def run_b200(args, world, rank, local, pg):
+    import torch
+    from gnss_gpu_b200 import _native as N
+    from gnss_gpu_b200.engine import Engine, EngineOptions, FilterSpec
+    from gnss_gpu_b200 import scenario as S
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    W, K = args.warmup, args.steps
+    n = args.n_particles
+    resampler = "megopolis" if args.workload == "cfg1-megopolis" else "systematic"
+    E = W + K + 1
+    tr = cfg1_inputs(E + K + 2, seed=1 + rank)
+    opts = EngineOptions(n_clk=4, resampler=resampler, megopolis_iters=32, ess_threshold=0.5,
+                         sys_offset="random", max_sats=32, obs_slots=E, covariance=True, recenter=True)
+    spec = FilterSpec(n_particles=n, seed=1234 + rank, sigma_pos=(1.0, 1.0, 0.5), sigma_clk=0.5, sigma_pr=3.0)
+    eng = Engine([spec], opts, device=local)
+    eng.initialize(0, tr.truth_ecef[0], tr.truth_clk[0], 10.0, 30.0)
+    flags = N.PF_EP_PREDICT | N.PF_EP_WEIGHT
+    for t in range(E):  # every input resident in HBM before timing
+        fe, sv = eng.pack_epoch([epoch_record(tr, t, flags)])
+        eng.upload(t, fe, sv)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    eng.enable_timing(K + W + 4)
+
+    def one_step(t):
+        with torch.cuda.stream(eng.stream):
+            flush.fill_(t & 0xFF)  # evict the working set from L2 between steps
+        eng.step()
+
+    for t in range(W):
+        one_step(t)
+    eng.read_timing()
+    eng.synchronize()
+    barrier(pg)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    resampled = []
+    errs = []
+    for i in range(K):
+        one_step(W + i)
+        r = eng.results()[0]  # host read between steps (outside the device intervals)
+        resampled.append(r["resampled"])
+        truth = tr.truth_ecef[W + i]
+        errs.append(float(np.linalg.norm((r["est_ecef"] - truth) @ tr.rot[:2].T)))
+    torch.cuda.synchronize()
+    barrier(pg)
+    clk = clocks.stop()
+    k_ms, step_ms = eng.read_timing()
+    assert len(step_ms) == K, (len(step_ms), K)
+    total_s = float(np.sum(step_ms)) / 1e3
+    total_s = reduce_max(pg, total_s)
+    kern_ms = float(np.mean(k_ms))
+    value = n * K * world / total_s
+    launches = K * eng.last_launch_count()
+
+    # -------- e2e through the public API, host buffers, per step H2D + D2H
+    e2e = None
+    if not args.no_e2e:
+        eng2 = Engine([spec], EngineOptions(n_clk=4, resampler=resampler, megopolis_iters=32, ess_threshold=0.5,
+                                            max_sats=32, obs_slots=1), device=local)
+        eng2.initialize(0, tr.truth_ecef[0], tr.truth_clk[0], 10.0, 30.0)
+        s_ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + W)]
+        e_ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + W)]
+        h2d = 0
+        for i in range(K + W):
+            t = i % len(tr.pr)
+            with torch.cuda.stream(eng2.stream):
+                flush.fill_(i & 0xFF)
+                s_ev[i].record(eng2.stream)
+            fe, sv = eng2.pack_epoch([epoch_record(tr, t, flags)])  # host inputs
+            eng2.upload(0, fe, sv)                                   # pinned H2D
+            eng2.step()
+            eng2.results()                                           # D2H + sync
+            with torch.cuda.stream(eng2.stream):
+                e_ev[i].record(eng2.stream)
+            h2d = fe.nbytes + sv.nbytes
+        torch.cuda.synchronize()
+        e2e_s = sum(s_ev[i].elapsed_time(e_ev[i]) for i in range(W, W + K)) / 1e3
+        e2e_s = reduce_max(pg, e2e_s)
+        e2e = {"value": n * K * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(eng2.result_bytes()), "ms_per_step": e2e_s / K * 1e3,
+               "api": "gnss_gpu_b200.Engine pack_epoch/upload/step/results per step"}
+        eng2.close()
+
+    peak, peak_kind = peaks()
+    D = 7
+    alg_k1 = (2 * D * 4 + 4) * n  # state read + write, log-weight write
+    achieved = alg_k1 / (kern_ms / 1e3) / 1e9
+    b_alg = 2 * D * 4 + 2 * 4  # 64 B per particle-step
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": total_s / K * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 state / f64 anchor+scan-free int64 CDF", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: 1 filter x {n} particles x 32 satellites (4 constellations x 8), "
+                               f"D=7 (E,N,U + 4 clocks), sigma_pr 3 m, 25% NLOS Exp(15 m), ESS<N/2 "
+                               f"{resampler} resampling" + (" (32 iterations)" if resampler == "megopolis" else ""),
+                   "particles": n, "satellites": 32, "state_dim": D, "parallelism": f"replicas x{world}",
+                   "l2": "flushed between steps (512 MiB device write outside the per-step event intervals)",
+                   "inputs": "all epochs resident in HBM before timing"},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "k_step (fused predict+weight+statistics)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": alg_k1,
+                     "kernel_ms": kern_ms, "traffic": committed_traffic("k_step")},
+        "step_roofline": {"b_alg_bytes_per_particle_step": b_alg,
+                          "achieved_gbs": value / world * b_alg / 1e9,
+                          "frac_of_measured_peak": value / world * b_alg / 1e9 / peak,
+                          "frac_of_nominal_8tbs": value / world * b_alg / 1e9 / 8000.0},
+        "resampled_fraction": float(np.mean(resampled)),
+        "p50_2d_error_m": float(np.median(errs)),
+        "clocks": clk,
+    }
+    if e2e:
+        out["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        n_cpu = 200_000
+        v, cores, dt = cpu_baseline_cfg1(n_cpu, 3, 7)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                               "sample": f"oracle FP64 C port (OpenMP), {n_cpu} particles x 32 satellites, "
+                                         f"3 epochs, {dt:.1f} s"}
+    eng.close()
+    return out
+
+
+# ------------------------------------------------------- reference arm
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    W, K = args.warmup, args.steps
+    n = args.n_particles
+    from oracle import oracle as O
+    # bounded sample: the full workload, at most a few seconds per step
+    t0 = time.perf_counter()
+    v_w, cores, _ = cpu_baseline_cfg1(n, max(1, min(W, 1)), 11)
+    per_step = (time.perf_counter() - t0)
+    k_eff = max(1, min(K, int(60.0 / max(per_step, 1e-3))))
+    v, cores, dt = cpu_baseline_cfg1(n, k_eff, 12)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": k_eff,
+        "warmup": 1, "ms_per_step": dt / k_eff * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: 1 filter x {n} particles x 32 satellites, D=7, "
+                               "systematic resampling when ESS<N/2 (CPU restatement of the reference step)",
+                   "parallelism": "host cores (OpenMP)"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{n} particles x {k_eff} epochs, {dt:.1f} s"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    return out
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args)
+    if args.impl == "reference":
+        out = run_reference(args, world, rank)
+    else:
+        out = run_b200(args, world, rank, local, pg)
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

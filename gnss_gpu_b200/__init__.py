@@ -1,0 +1,10 @@
+"""B200 (sm_100a) implementation of the gnss_gpu particle-filter step.
+
+`ParticleFilter` is the drop-in for gnss_gpu.particle_filter.ParticleFilter;
+`_gnss_gpu_pf` mirrors the reference's pybind11 module; `Engine` advances many
+filters together.  All compute runs in libgnsspf_b200.so (hand-written CUDA).
+"""
+from .particle_filter import ParticleFilter
+from .engine import Engine, EngineOptions, FilterSpec
+
+__all__ = ["ParticleFilter", "Engine", "EngineOptions", "FilterSpec"]

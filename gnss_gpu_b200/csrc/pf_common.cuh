@@ -1,0 +1,197 @@
+// pf_common.cuh -- arithmetic shared by the engine and the stateless kernels.
+//
+// * Philox4x32-10 counter-based RNG, written from Salmon, Moraes, Dror, Shaw,
+//   "Parallel random numbers: as easy as 1, 2, 3" (SC'11).  It replaces the
+//   reference's cuRAND Philox states (src/particle_filter/predict.cu:14-20,
+//   resampling.cu:183-205).
+// * Box-Muller normals.
+// * Deterministic weight quantisation: exp(lw - max) evaluated with IEEE
+//   single-precision operations that round identically on host and device,
+//   then scaled to a 64-bit integer.  The systematic resampler's CDF is an
+//   exact integer prefix sum of these values, so the ancestor indices are a
+//   function of (log-weights, offset) alone, independent of scan order.
+// * The systematic predicate of resampling.cu:69-77,
+//       cdf[i] < (u + k) / N
+//   evaluated exactly as  C_i * N * 2^32  <  (k * 2^32 + u32) * W
+//   with C the integer inclusive CDF and W its total.
+#pragma once
+#include <stdint.h>
+#include <math.h>
+#include <cuda_runtime.h>
+
+#define PF_HD __host__ __device__ __forceinline__
+
+namespace pfb {
+
+// ---------------------------------------------------------------- Philox
+struct U4 {
+  uint32_t x, y, z, w;
+};
+
+PF_HD void mulhilo32(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo) {
+#ifdef __CUDA_ARCH__
+  lo = a * b;
+  hi = __umulhi(a, b);
+#else
+  uint64_t p = (uint64_t)a * (uint64_t)b;
+  lo = (uint32_t)p;
+  hi = (uint32_t)(p >> 32);
+#endif
+}
+
+// Ten rounds; round multipliers and Weyl key increments from the paper.
+PF_HD U4 philox10(U4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    uint32_t hi0, lo0, hi1, lo1;
+    mulhilo32(0xD2511F53u, c.x, hi0, lo0);
+    mulhilo32(0xCD9E8D57u, c.z, hi1, lo1);
+    U4 n;
+    n.x = hi1 ^ c.y ^ k0;
+    n.y = lo1;
+    n.z = hi0 ^ c.w ^ k1;
+    n.w = lo0;
+    c = n;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// Stream tags (third counter word, high byte) keep the draws of different
+// purposes disjoint for the same (particle, epoch, filter).
+enum : uint32_t {
+  TAG_INIT = 0x01000000u,
+  TAG_PREDICT = 0x02000000u,
+  TAG_SYS_U = 0x03000000u,
+  TAG_MEGO_OFF = 0x04000000u,
+  TAG_MEGO_U = 0x05000000u,
+  TAG_COMPAT_INIT = 0x11000000u,
+  TAG_COMPAT_PREDICT = 0x12000000u,
+  TAG_COMPAT_MEGO = 0x13000000u,
+};
+
+#ifdef __CUDACC__
+// Two standard normals from two 32-bit words (Box-Muller).  u1 lies in
+// (0, 1]; the angle is 2*pi*(b * 2^-32 - 1/2), inside [-pi, pi) where the
+// fast sine/cosine are accurate to about 2^-21.
+__device__ __forceinline__ float2 box_muller_f32(uint32_t a, uint32_t b) {
+  const float two_m32 = 2.3283064365386963e-10f;  // 2^-32
+  float u1 = fmaf((float)a, two_m32, 1.1641532182693481e-10f);  // (a+1/2) 2^-32
+  float u2 = fmaf((float)b, two_m32, -0.5f);
+  float r = sqrtf(fmaxf(-2.0f * __logf(u1), 0.0f));
+  float s, c;
+  __sincosf(6.283185307179586f * u2, &s, &c);
+  return make_float2(r * c, r * s);
+}
+
+__device__ __forceinline__ double2 box_muller_f64(uint32_t a, uint32_t b) {
+  const double two_m32 = 2.3283064365386963e-10;
+  double u1 = ((double)a + 0.5) * two_m32;
+  double u2 = (double)b * two_m32 - 0.5;
+  double r = sqrt(-2.0 * log(u1));
+  double s, c;
+  sincospi(2.0 * u2, &s, &c);
+  return make_double2(r * c, r * s);
+}
+#endif
+
+// ------------------------------------------------ deterministic quantiser
+// Single-precision operations with round-to-nearest that neither the host
+// compiler nor nvcc may contract or reorder.
+PF_HD float det_sub(float a, float b) {
+#ifdef __CUDA_ARCH__
+  return __fsub_rn(a, b);
+#else
+  volatile float r = a - b;
+  return r;
+#endif
+}
+PF_HD float det_mul(float a, float b) {
+#ifdef __CUDA_ARCH__
+  return __fmul_rn(a, b);
+#else
+  volatile float r = a * b;
+  return r;
+#endif
+}
+PF_HD float det_fma(float a, float b, float c) {
+#ifdef __CUDA_ARCH__
+  return __fmaf_rn(a, b, c);
+#else
+  return fmaf(a, b, c);
+#endif
+}
+
+// Exponent K of the fixed-point scale: the largest weight maps to about
+// 2^K, and N * 2^(K+1) stays below 2^63.
+PF_HD int quant_exponent(int n) {
+  int lg = 0;
+  while ((1ll << lg) < (long long)n) ++lg;
+  int k = 62 - lg;
+  return k < 40 ? k : 40;
+}
+
+// q = floor(2^K * 2^x) with x = (lw - max) * log2(e), 2^frac(x) from its
+// Taylor series (coefficients (ln 2)^j / j!), Horner form with fma.
+// Weights below 2^-40 of the largest quantise to zero.
+PF_HD uint64_t quantize_weight(float lw, float max_lw, int K) {
+  float d = det_sub(lw, max_lw);
+  float x = det_mul(d, 1.44269504088896341f);
+  if (!(x > -40.0f)) return 0ull;  // also catches NaN
+  float n = floorf(x);
+  float f = det_sub(x, n);         // exact: f in [0, 1)
+  float p = 1.0178086009239699e-07f;
+  p = det_fma(p, f, 1.3215486790144307e-06f);
+  p = det_fma(p, f, 1.5252733804059840e-05f);
+  p = det_fma(p, f, 1.5403530393381606e-04f);
+  p = det_fma(p, f, 1.3333558146428443e-03f);
+  p = det_fma(p, f, 9.6181291076284772e-03f);
+  p = det_fma(p, f, 5.5504108664821580e-02f);
+  p = det_fma(p, f, 2.4022650695910071e-01f);
+  p = det_fma(p, f, 6.9314718055994531e-01f);
+  p = det_fma(p, f, 1.0f);
+  uint32_t P = (uint32_t)det_mul(p, 8388608.0f);  // p * 2^23, p in [1, 2]
+  int sh = K - 23 + (int)n;
+  return sh >= 0 ? ((uint64_t)P << sh) : ((uint64_t)P >> (-sh));
+}
+
+// ------------------------------------------------ 128-bit exact compare
+PF_HD void mul_64x64(uint64_t a, uint64_t b, uint64_t& hi, uint64_t& lo) {
+#ifdef __CUDA_ARCH__
+  lo = a * b;
+  hi = __umul64hi(a, b);
+#else
+  unsigned __int128 p = (unsigned __int128)a * b;
+  lo = (uint64_t)p;
+  hi = (uint64_t)(p >> 64);
+#endif
+}
+
+// (k * 2^32 + u) * W  <=  C * N * 2^32 ?
+PF_HD bool slot_at_or_below(uint64_t k, uint32_t u, uint64_t W, uint64_t C,
+                            uint32_t N) {
+  uint64_t T = (k << 32) | (uint64_t)u;
+  uint64_t lh, ll;
+  mul_64x64(T, W, lh, ll);
+  uint64_t ch, cl;
+  mul_64x64(C, (uint64_t)N, ch, cl);  // < 2^94
+  uint64_t rh = (ch << 32) | (cl >> 32);
+  uint64_t rl = cl << 32;
+  return (lh < rh) || (lh == rh && ll <= rl);
+}
+
+// F(C) = #{k in [0, N) : (k * 2^32 + u) * W <= C * N * 2^32}.
+// Slots [F(C_{i-1}), F(C_i)) are the offspring of particle i; equivalently
+// the lower-bound search of resampling.cu:72-77 returns i for those slots.
+PF_HD uint32_t offspring_end(uint64_t C, uint64_t W, uint32_t N, uint32_t u) {
+  double est = (double)C / (double)W * (double)N - (double)u * 2.3283064365386963e-10;
+  long long k = (long long)floor(est);
+  if (k < -1) k = -1;
+  if (k > (long long)N - 1) k = (long long)N - 1;
+  while (k >= 0 && !slot_at_or_below((uint64_t)k, u, W, C, N)) --k;
+  while (k + 1 < (long long)N && slot_at_or_below((uint64_t)(k + 1), u, W, C, N)) ++k;
+  return (uint32_t)(k + 1);
+}
+
+}  // namespace pfb

@@ -1,0 +1,560 @@
+// pf_compat.cu -- the stateless host-array API (pf_*), one function per
+// entry of the reference's _gnss_gpu_pf module
+// (python/gnss_gpu/_particle_filter_bindings.cpp:10-145 ->
+//  include/gnss_gpu/particle_filter.h:15-64).
+//
+// Each call copies the caller's FP64 host arrays to the device, runs FP64
+// kernels with the reference's arithmetic, and copies the results back, as
+// the reference does (predict.cu:70-113, weight.cu:222-368,
+// resampling.cu:85-272).  Unlike the reference it keeps one grow-only device
+// workspace per device instead of cudaMalloc/cudaFree on every call, frees
+// everything it uses, and finishes its reductions on the device.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <mutex>
+#include <vector>
+
+#include "pf_common.cuh"
+#include "pf_status.h"
+
+namespace pfb {
+size_t systematic_scratch_bytes(int n);
+int systematic_ancestors(const float* d_lw32, int n, uint32_t u, int* d_anc, void* d_scratch,
+                         cudaStream_t st);
+}  // namespace pfb
+
+using namespace pfb;
+
+namespace {
+
+constexpr int kB = 256;  // threads per block of the stateless kernels
+
+struct Workspace {
+  void* buf = nullptr;
+  size_t bytes = 0;
+  cudaStream_t stream = nullptr;
+};
+
+std::mutex g_mu;
+std::vector<Workspace> g_ws;  // indexed by device
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+int cuda_status(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) return set_err(PF_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+  return PF_OK;
+}
+
+#define CK(call)                                  \
+  do {                                            \
+    int _s = cuda_status((call), #call);          \
+    if (_s != PF_OK) return _s;                   \
+  } while (0)
+
+// Grow-only workspace of the current device (caller holds g_mu).
+int workspace(size_t bytes, Workspace** out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if ((int)g_ws.size() <= dev) g_ws.resize(dev + 1);
+  Workspace& w = g_ws[dev];
+  if (!w.stream) CK(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking));
+  if (w.bytes < bytes) {
+    if (w.buf) CK(cudaFree(w.buf));
+    w.buf = nullptr;
+    w.bytes = 0;
+    size_t want = align_up(bytes, 1 << 20);
+    CK(cudaMalloc(&w.buf, want));
+    w.bytes = want;
+  }
+  *out = &w;
+  return PF_OK;
+}
+
+struct Carve {
+  unsigned char* base;
+  size_t off = 0;
+  template <typename T>
+  T* take(size_t count) {
+    T* p = (T*)(base + off);
+    off = align_up(off + count * sizeof(T), 256);
+    return p;
+  }
+};
+
+inline int grid_of(int n) { return (n + kB - 1) / kB; }
+
+// --------------------------------------------------------------- kernels
+__global__ void c_init(double* px, double* py, double* pz, double* pcb, double ix, double iy,
+                       double iz, double icb, double sp, double scb, int n, uint32_t k0,
+                       uint32_t k1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  U4 r = philox10(U4{(uint32_t)i, 0u, TAG_COMPAT_INIT, 0u}, k0, k1);
+  double2 a = box_muller_f64(r.x, r.y), b = box_muller_f64(r.z, r.w);
+  px[i] = ix + a.x * sp;
+  py[i] = iy + a.y * sp;
+  pz[i] = iz + b.x * sp;
+  pcb[i] = icb + b.y * scb;
+}
+
+__global__ void c_predict(double* px, double* py, double* pz, double* pcb, double vx, double vy,
+                          double vz, double dt, double sp, double scb, int n, uint32_t k0,
+                          uint32_t k1, uint32_t step) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  U4 r = philox10(U4{(uint32_t)i, step, TAG_COMPAT_PREDICT, 0u}, k0, k1);
+  double2 a = box_muller_f64(r.x, r.y), b = box_muller_f64(r.z, r.w);
+  px[i] += vx * dt + a.x * sp;
+  py[i] += vy * dt + a.y * sp;
+  pz[i] += vz * dt + b.x * sp;
+  pcb[i] += b.y * scb;
+}
+
+// weight.cu:13-57: Gaussian pseudorange log-likelihood, overwriting lw.
+__global__ void c_weight(const double* px, const double* py, const double* pz, const double* pcb,
+                         const double* sat, const double* pr, const double* ws, double* lw, int n,
+                         int n_sat, double sigma_pr) {
+  extern __shared__ double s[];
+  double* s_sat = s;
+  double* s_pr = s + 3 * n_sat;
+  double* s_ws = s + 4 * n_sat;
+  for (int k = threadIdx.x; k < n_sat; k += blockDim.x) {
+    s_sat[3 * k] = sat[3 * k];
+    s_sat[3 * k + 1] = sat[3 * k + 1];
+    s_sat[3 * k + 2] = sat[3 * k + 2];
+    s_pr[k] = pr[k];
+    s_ws[k] = ws[k];
+  }
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double x = px[i], y = py[i], z = pz[i], cb = pcb[i];
+  const double inv_s2 = 1.0 / (sigma_pr * sigma_pr);
+  double acc = 0.0;
+  for (int k = 0; k < n_sat; ++k) {
+    const double dx = x - s_sat[3 * k], dy = y - s_sat[3 * k + 1], dz = z - s_sat[3 * k + 2];
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    const double res = s_pr[k] - (r + cb);
+    acc += -0.5 * s_ws[k] * res * res * inv_s2;
+  }
+  lw[i] = acc;
+}
+
+// Max-shifted sums of one block: max, sum w, sum w^2, sum w x (4 arrays);
+// the last block merges all block rows (weight.cu:61-160,163-328, with the
+// host merge moved onto the device).  out: [0..3] weighted mean, [4] sum w,
+// [5] sum w^2, [6] ESS, [7] max log-weight.
+__global__ void c_stats(const double* lw, const double* px, const double* py, const double* pz,
+                        const double* pcb, int n, double* rows, unsigned* ticket, double* out) {
+  __shared__ double s_v[kB];
+  __shared__ double s_r[7][kB / 32];
+  __shared__ bool s_last;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool ok = i < n;
+  const double l = ok ? lw[i] : -INFINITY;
+  // block max
+  double m = l;
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) s_v[threadIdx.x >> 5] = m;
+  __syncthreads();
+  double bm = s_v[0];
+  for (int w = 1; w < kB / 32; ++w) bm = fmax(bm, s_v[w]);
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  if (ok && bm > -INFINITY) {
+    const double w = exp(l - bm);
+    v[0] = w;
+    v[1] = w * w;
+    if (px) {
+      v[2] = w * px[i];
+      v[3] = w * py[i];
+      v[4] = w * pz[i];
+      v[5] = w * pcb[i];
+    }
+  }
+  for (int k = 0; k < 6; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 6; ++k) s_r[k][threadIdx.x >> 5] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double* row = rows + (size_t)blockIdx.x * 8;
+    row[0] = bm;
+    for (int k = 0; k < 6; ++k) {
+      double t = 0;
+      for (int w = 0; w < kB / 32; ++w) t += s_r[k][w];
+      row[1 + k] = t;
+    }
+    __threadfence();
+    s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const int nb = gridDim.x;
+  double gm = -INFINITY;
+  for (int b = threadIdx.x; b < nb; b += kB) gm = fmax(gm, __ldcg(rows + (size_t)b * 8));
+  for (int o = 16; o > 0; o >>= 1) gm = fmax(gm, __shfl_xor_sync(0xffffffffu, gm, o));
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) s_v[threadIdx.x >> 5] = gm;
+  __syncthreads();
+  gm = s_v[0];
+  for (int w = 1; w < kB / 32; ++w) gm = fmax(gm, s_v[w]);
+  double a[6] = {0, 0, 0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nb; b += kB) {
+    const double* row = rows + (size_t)b * 8;
+    const double rm = __ldcg(row);
+    if (!(rm > -INFINITY)) continue;
+    const double c = exp(rm - gm);
+    a[0] += __ldcg(row + 1) * c;
+    a[1] += __ldcg(row + 2) * c * c;
+    for (int k = 2; k < 6; ++k) a[k] += __ldcg(row + 1 + k) * c;
+  }
+  for (int k = 0; k < 6; ++k)
+    for (int o = 16; o > 0; o >>= 1) a[k] += __shfl_xor_sync(0xffffffffu, a[k], o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 6; ++k) s_r[k][threadIdx.x >> 5] = a[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t[6];
+    for (int k = 0; k < 6; ++k) {
+      t[k] = 0;
+      for (int w = 0; w < kB / 32; ++w) t[k] += s_r[k][w];
+    }
+    out[0] = t[2] / t[0];
+    out[1] = t[3] / t[0];
+    out[2] = t[4] / t[0];
+    out[3] = t[5] / t[0];
+    out[4] = t[0];
+    out[5] = t[1];
+    out[6] = (t[0] * t[0]) / t[1];
+    out[7] = gm;
+    *ticket = 0u;
+  }
+}
+
+__global__ void c_shift_f32(const double* lw, const double* stats, float* lw32, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  lw32[i] = (float)(lw[i] - stats[7]);
+}
+
+__global__ void c_gather4(const double* ix, const double* iy, const double* iz, const double* icb,
+                          double* ox, double* oy, double* oz, double* ocb, const int* anc, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int a = anc[k];
+  ox[k] = ix[a];
+  oy[k] = iy[a];
+  oz[k] = iz[a];
+  ocb[k] = icb[a];
+}
+
+__global__ void c_iota(int* a, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) a[k] = k;
+}
+
+// resampling.cu:175-219: one Megopolis iteration of the reference chain on
+// ancestor indices.  Slot k proposes j = (k + 1 + floor(U (N-1))) mod N and
+// copies the previous iteration's occupant of j with probability
+// min(1, exp(lw[j] - lw[k])).
+__device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
+  return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+__global__ void c_mego_iter(const double* lw, const int* src, int* dst, int n, uint32_t k0,
+                            uint32_t k1, uint32_t iter) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  U4 r = philox10(U4{(uint32_t)k, iter, TAG_COMPAT_MEGO, 0u}, k0, k1);
+  const double U1 = u53(r.x, r.y), U2 = u53(r.z, r.w);
+  const long long off = (long long)(U1 * (double)(n - 1)) + 1;
+  const int j = (int)(((long long)k + off) % n);
+  const double alpha = fmin(1.0, exp(lw[j] - lw[k]));
+  dst[k] = (U2 < alpha) ? src[j] : src[k];
+}
+
+__global__ void c_interleave(const double* px, const double* py, const double* pz, const double* pcb,
+                             double* out, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  out[4 * (size_t)k] = px[k];
+  out[4 * (size_t)k + 1] = py[k];
+  out[4 * (size_t)k + 2] = pz[k];
+  out[4 * (size_t)k + 3] = pcb[k];
+}
+
+int check_n(int n) {
+  if (n <= 0) return set_err(PF_EINVAL, "n_particles must be > 0 (got %d)", n);
+  return PF_OK;
+}
+
+int finish(Workspace* w) {
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(w->stream));
+  return PF_OK;
+}
+
+uint32_t sys_u_reference(unsigned long long seed, int n) {
+  double u0 = (double)(seed % 1000000ull) / (1000000.0 * (double)n);
+  double v = floor(u0 * 4294967296.0);
+  return (uint32_t)(v < 0 ? 0 : (v > 4294967295.0 ? 4294967295.0 : v));
+}
+
+}  // namespace
+
+extern "C" {
+
+int pf_initialize(double* px, double* py, double* pz, double* pcb, double init_x, double init_y,
+                  double init_z, double init_cb, double spread_pos, double spread_cb, int n_particles,
+                  unsigned long long seed) {
+  clear_err();
+  int s = check_n(n_particles);
+  if (s != PF_OK) return s;
+  if (!px || !py || !pz || !pcb) return set_err(PF_EINVAL, "null particle array");
+  std::lock_guard<std::mutex> lk(g_mu);
+  const size_t nb = (size_t)n_particles * 8;
+  Workspace* w;
+  if ((s = workspace(4 * align_up(nb, 256), &w)) != PF_OK) return s;
+  Carve c{(unsigned char*)w->buf};
+  double *dx = c.take<double>(n_particles), *dy = c.take<double>(n_particles),
+         *dz = c.take<double>(n_particles), *dcb = c.take<double>(n_particles);
+  c_init<<<grid_of(n_particles), kB, 0, w->stream>>>(dx, dy, dz, dcb, init_x, init_y, init_z, init_cb,
+                                                     spread_pos, spread_cb, n_particles,
+                                                     (uint32_t)seed, (uint32_t)(seed >> 32));
+  CK(cudaMemcpyAsync(px, dx, nb, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(py, dy, nb, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(pz, dz, nb, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(pcb, dcb, nb, cudaMemcpyDeviceToHost, w->stream));
+  return finish(w);
+}
+
+int pf_predict(double* px, double* py, double* pz, double* pcb, const double* vx, const double* vy,
+               const double* vz, double dt, double sigma_pos, double sigma_cb, int n_particles,
+               unsigned long long seed, int step) {
+  clear_err();
+  int s = check_n(n_particles);
+  if (s != PF_OK) return s;
+  if (!px || !py || !pz || !pcb || !vx || !vy || !vz) return set_err(PF_EINVAL, "null array");
+  std::lock_guard<std::mutex> lk(g_mu);
+  const size_t nb = (size_t)n_particles * 8;
+  Workspace* w;
+  if ((s = workspace(4 * align_up(nb, 256), &w)) != PF_OK) return s;
+  Carve c{(unsigned char*)w->buf};
+  double *dx = c.take<double>(n_particles), *dy = c.take<double>(n_particles),
+         *dz = c.take<double>(n_particles), *dcb = c.take<double>(n_particles);
+  CK(cudaMemcpyAsync(dx, px, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dy, py, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dz, pz, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dcb, pcb, nb, cudaMemcpyHostToDevice, w->stream));
+  c_predict<<<grid_of(n_particles), kB, 0, w->stream>>>(dx, dy, dz, dcb, vx[0], vy[0], vz[0], dt, sigma_pos,
+                                                        sigma_cb, n_particles, (uint32_t)seed,
+                                                        (uint32_t)(seed >> 32), (uint32_t)step);
+  CK(cudaMemcpyAsync(px, dx, nb, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(py, dy, nb, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(pz, dz, nb, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(pcb, dcb, nb, cudaMemcpyDeviceToHost, w->stream));
+  return finish(w);
+}
+
+int pf_weight(const double* px, const double* py, const double* pz, const double* pcb,
+              const double* sat_ecef, const double* pseudoranges, const double* weights_sat,
+              double* log_weights, int n_particles, int n_sat, double sigma_pr) {
+  clear_err();
+  int s = check_n(n_particles);
+  if (s != PF_OK) return s;
+  if (n_sat <= 0) return set_err(PF_EINVAL, "n_sat must be > 0 (got %d)", n_sat);
+  if (n_sat > 1024) return set_err(PF_ECAP, "n_sat %d above the 1024 satellites staged in shared memory", n_sat);
+  if (!px || !py || !pz || !pcb || !sat_ecef || !pseudoranges || !weights_sat || !log_weights)
+    return set_err(PF_EINVAL, "null array");
+  if (!(sigma_pr > 0.0) || !isfinite(sigma_pr)) return set_err(PF_EINVAL, "sigma_pr must be finite and > 0");
+  std::lock_guard<std::mutex> lk(g_mu);
+  const size_t nb = (size_t)n_particles * 8;
+  Workspace* w;
+  if ((s = workspace(5 * align_up(nb, 256) + align_up((size_t)n_sat * 40, 256) * 2, &w)) != PF_OK) return s;
+  Carve c{(unsigned char*)w->buf};
+  double *dx = c.take<double>(n_particles), *dy = c.take<double>(n_particles),
+         *dz = c.take<double>(n_particles), *dcb = c.take<double>(n_particles),
+         *dlw = c.take<double>(n_particles);
+  double *dsat = c.take<double>(3 * (size_t)n_sat), *dpr = c.take<double>(n_sat), *dws = c.take<double>(n_sat);
+  CK(cudaMemcpyAsync(dx, px, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dy, py, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dz, pz, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dcb, pcb, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dsat, sat_ecef, (size_t)n_sat * 24, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dpr, pseudoranges, (size_t)n_sat * 8, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dws, weights_sat, (size_t)n_sat * 8, cudaMemcpyHostToDevice, w->stream));
+  c_weight<<<grid_of(n_particles), kB, (size_t)n_sat * 40, w->stream>>>(dx, dy, dz, dcb, dsat, dpr, dws, dlw,
+                                                                        n_particles, n_sat, sigma_pr);
+  CK(cudaMemcpyAsync(log_weights, dlw, nb, cudaMemcpyDeviceToHost, w->stream));
+  return finish(w);
+}
+
+int pf_compute_ess(const double* log_weights, int n_particles, double* ess_out) {
+  clear_err();
+  int s = check_n(n_particles);
+  if (s != PF_OK) return s;
+  if (!log_weights || !ess_out) return set_err(PF_EINVAL, "null array");
+  std::lock_guard<std::mutex> lk(g_mu);
+  const size_t nb = (size_t)n_particles * 8;
+  const int g = grid_of(n_particles);
+  Workspace* w;
+  if ((s = workspace(align_up(nb, 256) + align_up((size_t)g * 64, 256) + 512, &w)) != PF_OK) return s;
+  Carve c{(unsigned char*)w->buf};
+  double* dlw = c.take<double>(n_particles);
+  double* rows = c.take<double>((size_t)g * 8);
+  double* out = c.take<double>(8);
+  unsigned* ticket = c.take<unsigned>(4);
+  CK(cudaMemcpyAsync(dlw, log_weights, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemsetAsync(ticket, 0, 16, w->stream));
+  c_stats<<<g, kB, 0, w->stream>>>(dlw, nullptr, nullptr, nullptr, nullptr, n_particles, rows, ticket, out);
+  double h[8];
+  CK(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, w->stream));
+  if ((s = finish(w)) != PF_OK) return s;
+  *ess_out = h[6];
+  return PF_OK;
+}
+
+int pf_estimate(const double* px, const double* py, const double* pz, const double* pcb,
+                const double* log_weights, double* result, int n_particles) {
+  clear_err();
+  int s = check_n(n_particles);
+  if (s != PF_OK) return s;
+  if (!px || !py || !pz || !pcb || !log_weights || !result) return set_err(PF_EINVAL, "null array");
+  std::lock_guard<std::mutex> lk(g_mu);
+  const size_t nb = (size_t)n_particles * 8;
+  const int g = grid_of(n_particles);
+  Workspace* w;
+  if ((s = workspace(5 * align_up(nb, 256) + align_up((size_t)g * 64, 256) + 512, &w)) != PF_OK) return s;
+  Carve c{(unsigned char*)w->buf};
+  double *dx = c.take<double>(n_particles), *dy = c.take<double>(n_particles),
+         *dz = c.take<double>(n_particles), *dcb = c.take<double>(n_particles),
+         *dlw = c.take<double>(n_particles);
+  double* rows = c.take<double>((size_t)g * 8);
+  double* out = c.take<double>(8);
+  unsigned* ticket = c.take<unsigned>(4);
+  CK(cudaMemcpyAsync(dx, px, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dy, py, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dz, pz, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dcb, pcb, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dlw, log_weights, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemsetAsync(ticket, 0, 16, w->stream));
+  c_stats<<<g, kB, 0, w->stream>>>(dlw, dx, dy, dz, dcb, n_particles, rows, ticket, out);
+  double h[8];
+  CK(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, w->stream));
+  if ((s = finish(w)) != PF_OK) return s;
+  for (int i = 0; i < 4; ++i) result[i] = h[i];
+  return PF_OK;
+}
+
+int pf_get_particles(const double* px, const double* py, const double* pz, const double* pcb,
+                     double* output, int n_particles) {
+  clear_err();
+  int s = check_n(n_particles);
+  if (s != PF_OK) return s;
+  if (!px || !py || !pz || !pcb || !output) return set_err(PF_EINVAL, "null array");
+  std::lock_guard<std::mutex> lk(g_mu);
+  const size_t nb = (size_t)n_particles * 8;
+  Workspace* w;
+  if ((s = workspace(8 * align_up(nb, 256), &w)) != PF_OK) return s;
+  Carve c{(unsigned char*)w->buf};
+  double *dx = c.take<double>(n_particles), *dy = c.take<double>(n_particles),
+         *dz = c.take<double>(n_particles), *dcb = c.take<double>(n_particles),
+         *dout = c.take<double>(4 * (size_t)n_particles);
+  CK(cudaMemcpyAsync(dx, px, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dy, py, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dz, pz, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dcb, pcb, nb, cudaMemcpyHostToDevice, w->stream));
+  c_interleave<<<grid_of(n_particles), kB, 0, w->stream>>>(dx, dy, dz, dcb, dout, n_particles);
+  CK(cudaMemcpyAsync(output, dout, 4 * nb, cudaMemcpyDeviceToHost, w->stream));
+  return finish(w);
+}
+
+int pf_resample_systematic(double* px, double* py, double* pz, double* pcb, const double* log_weights,
+                           int n_particles, unsigned long long seed) {
+  clear_err();
+  int s = check_n(n_particles);
+  if (s != PF_OK) return s;
+  if (!px || !py || !pz || !pcb || !log_weights) return set_err(PF_EINVAL, "null array");
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int n = n_particles;
+  const size_t nb = (size_t)n * 8;
+  const int g = grid_of(n);
+  const size_t need = 9 * align_up(nb, 256) + align_up((size_t)n * 4, 256) * 2 +
+                      align_up((size_t)g * 64, 256) + 512 + pfb::systematic_scratch_bytes(n) + 256;
+  Workspace* w;
+  if ((s = workspace(need, &w)) != PF_OK) return s;
+  Carve c{(unsigned char*)w->buf};
+  double *ix = c.take<double>(n), *iy = c.take<double>(n), *iz = c.take<double>(n), *icb = c.take<double>(n);
+  double *ox = c.take<double>(n), *oy = c.take<double>(n), *oz = c.take<double>(n), *ocb = c.take<double>(n);
+  double* dlw = c.take<double>(n);
+  float* lw32 = c.take<float>(align_up(n, 4));
+  int* anc = c.take<int>(n);
+  double* rows = c.take<double>((size_t)g * 8);
+  double* out = c.take<double>(8);
+  unsigned* ticket = c.take<unsigned>(4);
+  unsigned char* scratch = c.take<unsigned char>(pfb::systematic_scratch_bytes(n));
+  CK(cudaMemcpyAsync(ix, px, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(iy, py, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(iz, pz, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(icb, pcb, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dlw, log_weights, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemsetAsync(ticket, 0, 16, w->stream));
+  c_stats<<<g, kB, 0, w->stream>>>(dlw, nullptr, nullptr, nullptr, nullptr, n, rows, ticket, out);
+  c_shift_f32<<<g, kB, 0, w->stream>>>(dlw, out, lw32, n);
+  CK(cudaGetLastError());
+  if ((s = pfb::systematic_ancestors(lw32, n, sys_u_reference(seed, n), anc, scratch, w->stream)) != PF_OK)
+    return s;
+  c_gather4<<<g, kB, 0, w->stream>>>(ix, iy, iz, icb, ox, oy, oz, ocb, anc, n);
+  CK(cudaMemcpyAsync(px, ox, nb, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(py, oy, nb, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(pz, oz, nb, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(pcb, ocb, nb, cudaMemcpyDeviceToHost, w->stream));
+  return finish(w);
+}
+
+int pf_resample_megopolis(double* px, double* py, double* pz, double* pcb, const double* log_weights,
+                          int n_particles, int n_iterations, unsigned long long seed) {
+  clear_err();
+  int s = check_n(n_particles);
+  if (s != PF_OK) return s;
+  if (n_iterations < 0) return set_err(PF_EINVAL, "n_iterations must be >= 0");
+  if (!px || !py || !pz || !pcb || !log_weights) return set_err(PF_EINVAL, "null array");
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int n = n_particles;
+  const size_t nb = (size_t)n * 8;
+  const int g = grid_of(n);
+  Workspace* w;
+  if ((s = workspace(9 * align_up(nb, 256) + 2 * align_up((size_t)n * 4, 256), &w)) != PF_OK) return s;
+  Carve c{(unsigned char*)w->buf};
+  double *ix = c.take<double>(n), *iy = c.take<double>(n), *iz = c.take<double>(n), *icb = c.take<double>(n);
+  double *ox = c.take<double>(n), *oy = c.take<double>(n), *oz = c.take<double>(n), *ocb = c.take<double>(n);
+  double* dlw = c.take<double>(n);
+  int* a0 = c.take<int>(n);
+  int* a1 = c.take<int>(n);
+  CK(cudaMemcpyAsync(ix, px, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(iy, py, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(iz, pz, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(icb, pcb, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dlw, log_weights, nb, cudaMemcpyHostToDevice, w->stream));
+  c_iota<<<g, kB, 0, w->stream>>>(a0, n);
+  int* src = a0;
+  int* dst = a1;
+  for (int it = 0; it < n_iterations; ++it) {
+    c_mego_iter<<<g, kB, 0, w->stream>>>(dlw, src, dst, n, (uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)it);
+    int* t = src;
+    src = dst;
+    dst = t;
+  }
+  c_gather4<<<g, kB, 0, w->stream>>>(ix, iy, iz, icb, ox, oy, oz, ocb, src, n);
+  CK(cudaMemcpyAsync(px, ox, nb, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(py, oy, nb, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(pz, oz, nb, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(pcb, ocb, nb, cudaMemcpyDeviceToHost, w->stream));
+  return finish(w);
+}
+
+}  // extern "C"

@@ -1,0 +1,1022 @@
+// pf_engine.cu -- host side of the resident engine (the pfe_* C ABI).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "pf_engine_kernels.cuh"
+#include "pf_status.h"
+
+using namespace pfb;
+
+struct pf_engine {
+  pf_engine_config_t cfg;
+  std::vector<pf_filter_params_t> params;
+  std::vector<FilterDesc> hdesc;
+  std::vector<int> tile_filter;
+  int D = 0;
+  int T = 0;
+  long long P = 0;
+  int max_n = 0;
+  EngineDev dev;
+  unsigned char* ws = nullptr;
+  size_t ws_bytes = 0;
+  double* export_buf = nullptr;
+  FilterCtrl* ctrl_dev = nullptr;
+  FilterDesc* desc_dev = nullptr;
+  cudaStream_t stream = nullptr;
+  unsigned char* pinned[2] = {nullptr, nullptr};
+  cudaEvent_t pin_ev[2] = {nullptr, nullptr};
+  int pin_cur = 0;
+  FilterCtrl* ctrl_host = nullptr;  // pinned mirror
+  size_t obs_slot_bytes = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int resident[Q_COUNT];
+  int sm_count = 0;
+  int last_launches = 0;
+  std::vector<int> initialized;
+  // timing ring (pfe_enable_timing)
+  std::vector<cudaEvent_t> tev;  // 3 per slot
+  int t_slots = 0;
+  int t_next = 0;
+  int t_pending = 0;
+};
+
+namespace {
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct Layout {
+  size_t off_state0, off_state1, off_lw, off_anc, off_offs, off_mp, off_part, off_agg, off_inc,
+      off_flag, off_excl, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
+      total;
+  size_t obs_slot_bytes;
+  long long P;
+  int T, D, max_n;
+};
+
+int validate_config(const pf_engine_config_t* cfg, const pf_filter_params_t* fp) {
+  if (!cfg || !fp) return set_err(PF_EINVAL, "null config");
+  if (cfg->n_filters <= 0) return set_err(PF_EINVAL, "n_filters must be > 0");
+  if (cfg->n_clk < 1 || cfg->n_clk > PF_MAX_CLK) return set_err(PF_EINVAL, "n_clk must be 1..%d", PF_MAX_CLK);
+  if (cfg->resampler != PF_RESAMPLE_SYSTEMATIC && cfg->resampler != PF_RESAMPLE_MEGOPOLIS)
+    return set_err(PF_EINVAL, "unknown resampler %d", cfg->resampler);
+  if (cfg->resampler == PF_RESAMPLE_MEGOPOLIS && (cfg->megopolis_iters < 1 || cfg->megopolis_iters > 128))
+    return set_err(PF_EINVAL, "megopolis_iters must be 1..128");
+  if (cfg->weight_mode != PF_WEIGHT_GAUSSIAN && cfg->weight_mode != PF_WEIGHT_HUBER)
+    return set_err(PF_EINVAL, "unknown weight_mode %d", cfg->weight_mode);
+  if (cfg->lw_mode != PF_LW_OVERWRITE && cfg->lw_mode != PF_LW_ACCUMULATE)
+    return set_err(PF_EINVAL, "unknown lw_mode %d", cfg->lw_mode);
+  if (cfg->sys_offset != PF_SYS_OFFSET_RANDOM && cfg->sys_offset != PF_SYS_OFFSET_REFERENCE)
+    return set_err(PF_EINVAL, "unknown sys_offset %d", cfg->sys_offset);
+  if (cfg->max_sats < 1 || cfg->max_sats > PF_MAX_SATS)
+    return set_err(PF_ECAP, "max_sats must be 1..%d", PF_MAX_SATS);
+  if (cfg->obs_slots < 1) return set_err(PF_EINVAL, "obs_slots must be >= 1");
+  if (!(cfg->ess_threshold >= 0.0) || !isfinite(cfg->ess_threshold))
+    return set_err(PF_EINVAL, "ess_threshold must be finite and >= 0");
+  if (cfg->weight_mode == PF_WEIGHT_HUBER && !(cfg->huber_k > 0.0))
+    return set_err(PF_EINVAL, "huber_k must be > 0");
+  for (int f = 0; f < cfg->n_filters; ++f) {
+    const pf_filter_params_t& p = fp[f];
+    if (p.n_particles <= 0 || p.n_particles > (1 << 30))
+      return set_err(PF_EINVAL, "filter %d: n_particles must be 1..2^30", f);
+    for (int a = 0; a < 3; ++a)
+      if (!(p.sigma_pos[a] >= 0.0) || !isfinite(p.sigma_pos[a]))
+        return set_err(PF_EINVAL, "filter %d: sigma_pos must be finite and >= 0", f);
+    if (!(p.sigma_clk >= 0.0) || !isfinite(p.sigma_clk))
+      return set_err(PF_EINVAL, "filter %d: sigma_clk must be finite and >= 0", f);
+    if (!(p.sigma_pr > 0.0) || !isfinite(p.sigma_pr))
+      return set_err(PF_EINVAL, "filter %d: sigma_pr must be finite and > 0", f);
+  }
+  return PF_OK;
+}
+
+Layout make_layout(const pf_engine_config_t* cfg, const pf_filter_params_t* fp) {
+  Layout L{};
+  L.D = 3 + cfg->n_clk;
+  long long P = 0;
+  int T = 0, max_n = 0;
+  for (int f = 0; f < cfg->n_filters; ++f) {
+    int n = fp[f].n_particles;
+    P += (long long)align_up((size_t)n, 4);
+    T += (n + PF_TILE - 1) / PF_TILE;
+    max_n = std::max(max_n, n);
+  }
+  P = (long long)align_up((size_t)P, 64);
+  L.P = P;
+  L.T = T;
+  L.max_n = max_n;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = o;
+    o = align_up(o + bytes, 256);
+    return at;
+  };
+  L.off_state0 = take((size_t)L.D * P * 4);
+  L.off_state1 = take((size_t)L.D * P * 4);
+  L.off_lw = take((size_t)P * 4);
+  L.off_anc = take((size_t)P * 4);
+  L.off_offs = take((size_t)P * 4);
+  L.off_mp = take((size_t)T * 4);
+  L.off_part = take((size_t)T * kPartStride * 4);
+  L.off_agg = take((size_t)T * 8);
+  L.off_inc = take((size_t)T * 8);
+  L.off_flag = take((size_t)T * 4);
+  L.off_excl = take((size_t)T * 8);
+  L.off_desc = take(sizeof(FilterDesc) * cfg->n_filters);
+  L.off_ctrl = take(sizeof(FilterCtrl) * cfg->n_filters);
+  L.off_tf = take((size_t)T * 4);
+  L.off_queue = take(sizeof(unsigned) * 2 * Q_COUNT);
+  L.off_err = take(sizeof(unsigned) * 4);
+  L.obs_slot_bytes = align_up(sizeof(pf_filter_epoch_t) * cfg->n_filters +
+                                  sizeof(pf_sat_t) * (size_t)cfg->n_filters * cfg->max_sats,
+                              256);
+  L.off_obs = take(L.obs_slot_bytes * cfg->obs_slots);
+  L.off_export = take((size_t)max_n * L.D * 8);
+  L.total = o;
+  return L;
+}
+
+// ECEF -> local E/N/U rotation at an ECEF point (geodetic latitude from the
+// WGS-84 ellipsoid by Bowring's iteration).
+void enu_rotation(const double* p, double* rot) {
+  const double a = 6378137.0, f = 1.0 / 298.257223563;
+  const double e2 = f * (2.0 - f);
+  const double x = p[0], y = p[1], z = p[2];
+  const double lon = atan2(y, x);
+  const double rho = sqrt(x * x + y * y);
+  double lat = atan2(z, rho * (1.0 - e2));
+  for (int it = 0; it < 8; ++it) {
+    const double s = sin(lat);
+    const double Nr = a / sqrt(1.0 - e2 * s * s);
+    const double h = (fabs(cos(lat)) > 1e-12) ? rho / cos(lat) - Nr : fabs(z) - Nr * (1.0 - e2);
+    lat = atan2(z, rho * (1.0 - e2 * Nr / (Nr + h)));
+  }
+  if (rho < 1e-6) lat = z >= 0 ? M_PI / 2 : -M_PI / 2;
+  const double sl = sin(lat), cl = cos(lat), so = sin(lon), co = cos(lon);
+  rot[0] = -so;      rot[1] = co;       rot[2] = 0.0;
+  rot[3] = -sl * co; rot[4] = -sl * so; rot[5] = cl;
+  rot[6] = cl * co;  rot[7] = cl * so;  rot[8] = sl;
+}
+
+uint32_t reference_sys_offset(unsigned long long seed, int n) {
+  // resampling.cu:152 sets u0 = (seed % 1e6) / (1e6 * N) and searches for the
+  // target (u0 + k) / N (resampling.cu:69).  In units of one slot the target
+  // of slot k is k + u0, so the slot fraction is u0 itself, kept here as a
+  // 32-bit fixed-point fraction.
+  double u0 = (double)(seed % 1000000ull) / (1000000.0 * (double)n);
+  double v = floor(u0 * 4294967296.0);
+  if (v < 0) v = 0;
+  if (v > 4294967295.0) v = 4294967295.0;
+  return (uint32_t)v;
+}
+
+void fill_desc(pf_engine* eng, int f) {
+  const pf_filter_params_t& p = eng->params[f];
+  FilterDesc& d = eng->hdesc[f];
+  for (int i = 0; i < 8; ++i) d.sigma[i] = 0.f;
+  d.sigma[0] = (float)p.sigma_pos[0];
+  d.sigma[1] = (float)p.sigma_pos[1];
+  d.sigma[2] = (float)p.sigma_pos[2];
+  for (int c = 0; c < eng->cfg.n_clk; ++c) d.sigma[3 + c] = (float)p.sigma_clk;
+  d.sigma_pr = (float)p.sigma_pr;
+  d.inv_sigma_pr = (float)(1.0 / p.sigma_pr);
+  d.wscale = (float)(-0.5 / (p.sigma_pr * p.sigma_pr));
+  d.huber_k = (float)eng->cfg.huber_k;
+  d.key0 = (uint32_t)(p.seed & 0xffffffffull);
+  d.key1 = (uint32_t)(p.seed >> 32);
+  d.sys_ref_u = reference_sys_offset(p.seed, p.n_particles);
+}
+
+int check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) return set_err(PF_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+  return PF_OK;
+}
+
+#define CK(call)                                   \
+  do {                                             \
+    int _s = check_cuda((call), #call);            \
+    if (_s != PF_OK) return _s;                    \
+  } while (0)
+
+template <typename K>
+int occupancy(K kernel, int sm_count, int* out) {
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0);
+  if (e != cudaSuccess) return set_err(PF_ECUDA, "occupancy: %s", cudaGetErrorString(e));
+  *out = std::max(1, per_sm) * sm_count;
+  return PF_OK;
+}
+
+inline int grid_for(const pf_engine* eng, int slot, int count) {
+  return std::max(1, std::min(count, eng->resident[slot]));
+}
+
+template <int NCLK>
+int launch_step_t(pf_engine* eng, int t0, int count) {
+  const int g = grid_for(eng, Q_STEP, count);
+  if (eng->cfg.weight_mode == PF_WEIGHT_GAUSSIAN)
+    k_step<NCLK, PF_WEIGHT_GAUSSIAN><<<g, kThreads, 0, eng->stream>>>(eng->dev, t0, count);
+  else
+    k_step<NCLK, PF_WEIGHT_HUBER><<<g, kThreads, 0, eng->stream>>>(eng->dev, t0, count);
+  return check_cuda(cudaGetLastError(), "k_step launch");
+}
+
+int launch_step(pf_engine* eng, int t0, int count) {
+  switch (eng->cfg.n_clk) {
+    case 1: return launch_step_t<1>(eng, t0, count);
+    case 2: return launch_step_t<2>(eng, t0, count);
+    case 3: return launch_step_t<3>(eng, t0, count);
+    default: return launch_step_t<4>(eng, t0, count);
+  }
+}
+
+int launch_resample(pf_engine* eng, int t0, int count, int* n_launch) {
+  if (eng->cfg.resampler == PF_RESAMPLE_SYSTEMATIC) {
+    k_scan<<<grid_for(eng, Q_SCAN, count), kThreads, 0, eng->stream>>>(eng->dev, t0, count);
+    k_offs<<<grid_for(eng, Q_OFFS, count), kThreads, 0, eng->stream>>>(eng->dev, t0, count);
+    k_merge<<<grid_for(eng, Q_MERGE, count), kThreads, 0, eng->stream>>>(eng->dev, t0, count);
+    *n_launch += 3;
+  } else {
+    k_mego<<<grid_for(eng, Q_MEGO, count), kThreads, 0, eng->stream>>>(eng->dev, t0, count);
+    *n_launch += 1;
+  }
+  return check_cuda(cudaGetLastError(), "resample launch");
+}
+
+template <template <int> class Kn>
+struct DSwitch;
+
+int sync_and_check(pf_engine* eng) {
+  CK(cudaStreamSynchronize(eng->stream));
+  unsigned w = 0;
+  CK(cudaMemcpy(&w, eng->dev.err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (w & ERR_LOOKBACK_TIMEOUT) return set_err(PF_ETIMEOUT, "device look-back spin limit reached (error word 0x%x)", w);
+  if (w & ERR_SAT_CAP) return set_err(PF_ECAP, "n_sat above max_sats (error word 0x%x)", w);
+  if (w & ERR_BAD_WEIGHTS) return set_err(PF_EINVAL, "all log-weights non-finite (error word 0x%x)", w);
+  return PF_OK;
+}
+
+int read_ctrl(pf_engine* eng) {
+  CK(cudaMemcpyAsync(eng->ctrl_host, eng->ctrl_dev, sizeof(FilterCtrl) * eng->cfg.n_filters,
+                     cudaMemcpyDeviceToHost, eng->stream));
+  return sync_and_check(eng);
+}
+
+int check_filter(pf_engine* eng, int f) {
+  if (!eng) return set_err(PF_EINVAL, "null engine");
+  if (f < 0 || f >= eng->cfg.n_filters) return set_err(PF_EINVAL, "filter index %d out of range", f);
+  return PF_OK;
+}
+
+int filter_dims(pf_engine* eng, int f, int* n, long long* base, int* tb, int* nt) {
+  const FilterDesc& d = eng->hdesc[f];
+  *n = d.n;
+  *base = d.p_off;
+  *tb = d.tile_begin;
+  *nt = d.n_tiles;
+  return PF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pfe_workspace_bytes(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
+                        size_t* bytes) {
+  clear_err();
+  int s = validate_config(cfg, filters);
+  if (s != PF_OK) return s;
+  if (!bytes) return set_err(PF_EINVAL, "null bytes");
+  *bytes = make_layout(cfg, filters).total;
+  return PF_OK;
+}
+
+int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
+               void* dev_workspace, size_t workspace_bytes, void* stream, pf_engine_t** out) {
+  clear_err();
+  int s = validate_config(cfg, filters);
+  if (s != PF_OK) return s;
+  if (!out) return set_err(PF_EINVAL, "null out");
+  Layout L = make_layout(cfg, filters);
+  if (!dev_workspace) return set_err(PF_EINVAL, "null workspace");
+  if (workspace_bytes < L.total)
+    return set_err(PF_ENOMEM, "workspace %zu bytes < required %zu", workspace_bytes, L.total);
+  if (((uintptr_t)dev_workspace & 255u) != 0) return set_err(PF_EINVAL, "workspace must be 256-byte aligned");
+
+  pf_engine* eng = new pf_engine();
+  eng->cfg = *cfg;
+  eng->params.assign(filters, filters + cfg->n_filters);
+  eng->D = L.D;
+  eng->T = L.T;
+  eng->P = L.P;
+  eng->max_n = L.max_n;
+  eng->ws = (unsigned char*)dev_workspace;
+  eng->ws_bytes = workspace_bytes;
+  eng->stream = (cudaStream_t)stream;
+  eng->obs_slot_bytes = L.obs_slot_bytes;
+  eng->initialized.assign(cfg->n_filters, 0);
+
+  eng->hdesc.assign(cfg->n_filters, FilterDesc{});
+  eng->tile_filter.resize(L.T);
+  long long poff = 0;
+  int tb = 0;
+  for (int f = 0; f < cfg->n_filters; ++f) {
+    FilterDesc& d = eng->hdesc[f];
+    d.n = filters[f].n_particles;
+    d.tile_begin = tb;
+    d.n_tiles = (d.n + PF_TILE - 1) / PF_TILE;
+    d.K = quant_exponent(d.n);
+    d.p_off = poff;
+    d.filter_id = f;
+    for (int i = 0; i < 9; ++i) d.rot[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    fill_desc(eng, f);
+    for (int t = 0; t < d.n_tiles; ++t) eng->tile_filter[tb + t] = f;
+    tb += d.n_tiles;
+    poff += (long long)align_up((size_t)d.n, 4);
+  }
+
+  unsigned char* w = eng->ws;
+  EngineDev& e = eng->dev;
+  e.state0 = (float*)(w + L.off_state0);
+  e.state1 = (float*)(w + L.off_state1);
+  e.lw = (float*)(w + L.off_lw);
+  e.anc = (int*)(w + L.off_anc);
+  e.offs = (uint32_t*)(w + L.off_offs);
+  e.mp_part = (uint32_t*)(w + L.off_mp);
+  e.part = (float*)(w + L.off_part);
+  e.lb_agg = (unsigned long long*)(w + L.off_agg);
+  e.lb_inc = (unsigned long long*)(w + L.off_inc);
+  e.lb_flag = (unsigned*)(w + L.off_flag);
+  e.tile_excl = (unsigned long long*)(w + L.off_excl);
+  eng->desc_dev = (FilterDesc*)(w + L.off_desc);
+  eng->ctrl_dev = (FilterCtrl*)(w + L.off_ctrl);
+  e.desc = eng->desc_dev;
+  e.ctrl = eng->ctrl_dev;
+  e.tile_filter = (const int*)(w + L.off_tf);
+  e.queue = (unsigned*)(w + L.off_queue);
+  e.err = (unsigned*)(w + L.off_err);
+  e.obs = w + L.off_obs;
+  e.obs_slot_bytes = L.obs_slot_bytes;
+  e.spin_limit = 1ull << 24;
+  e.p_total = L.P;
+  e.obs_slots = cfg->obs_slots;
+  e.n_filters = cfg->n_filters;
+  e.max_sats = cfg->max_sats;
+  e.resampler = cfg->resampler;
+  e.mego_iters = cfg->megopolis_iters;
+  e.lw_mode = cfg->lw_mode;
+  e.sys_offset = cfg->sys_offset;
+  e.flags = cfg->flags;
+  e.ess_threshold = (float)cfg->ess_threshold;
+  e.lookback_poison = 0;
+  eng->export_buf = (double*)(w + L.off_export);
+
+  auto fail = [&](int st) {
+    pfe_destroy(eng);
+    return st;
+  };
+  int dev = 0;
+  if (check_cuda(cudaGetDevice(&dev), "cudaGetDevice") != PF_OK) return fail(PF_ECUDA);
+  if (check_cuda(cudaDeviceGetAttribute(&eng->sm_count, cudaDevAttrMultiProcessorCount, dev), "sm count") != PF_OK)
+    return fail(PF_ECUDA);
+  int st = PF_OK;
+  if (cfg->n_clk == 1) st = occupancy(k_step<1, PF_WEIGHT_GAUSSIAN>, eng->sm_count, &eng->resident[Q_STEP]);
+  else if (cfg->n_clk == 2) st = occupancy(k_step<2, PF_WEIGHT_GAUSSIAN>, eng->sm_count, &eng->resident[Q_STEP]);
+  else if (cfg->n_clk == 3) st = occupancy(k_step<3, PF_WEIGHT_GAUSSIAN>, eng->sm_count, &eng->resident[Q_STEP]);
+  else st = occupancy(k_step<4, PF_WEIGHT_GAUSSIAN>, eng->sm_count, &eng->resident[Q_STEP]);
+  if (st != PF_OK) return fail(st);
+  if ((st = occupancy(k_scan, eng->sm_count, &eng->resident[Q_SCAN])) != PF_OK) return fail(st);
+  if ((st = occupancy(k_offs, eng->sm_count, &eng->resident[Q_OFFS])) != PF_OK) return fail(st);
+  if ((st = occupancy(k_merge, eng->sm_count, &eng->resident[Q_MERGE])) != PF_OK) return fail(st);
+  if ((st = occupancy(k_mego, eng->sm_count, &eng->resident[Q_MEGO])) != PF_OK) return fail(st);
+  if ((st = occupancy(k_init<7>, eng->sm_count, &eng->resident[Q_INIT])) != PF_OK) return fail(st);
+  if ((st = occupancy(k_estimate<7>, eng->sm_count, &eng->resident[Q_EST])) != PF_OK) return fail(st);
+  if ((st = occupancy(k_export<7>, eng->sm_count, &eng->resident[Q_EXPORT])) != PF_OK) return fail(st);
+
+  for (int i = 0; i < 2; ++i) {
+    if (check_cuda(cudaHostAlloc((void**)&eng->pinned[i], L.obs_slot_bytes, cudaHostAllocDefault), "pinned staging") != PF_OK)
+      return fail(PF_ENOMEM);
+    if (check_cuda(cudaEventCreateWithFlags(&eng->pin_ev[i], cudaEventDisableTiming), "event") != PF_OK)
+      return fail(PF_ECUDA);
+  }
+  if (check_cuda(cudaHostAlloc((void**)&eng->ctrl_host, sizeof(FilterCtrl) * cfg->n_filters, cudaHostAllocDefault),
+                 "pinned ctrl") != PF_OK)
+    return fail(PF_ENOMEM);
+
+  // Device tables and zeroed control blocks.
+  std::vector<FilterCtrl> hc(cfg->n_filters);
+  memset(hc.data(), 0, sizeof(FilterCtrl) * hc.size());
+  for (auto& c : hc) {
+    c.lw_zero = 1;
+    c.rs_seq = 1;
+  }
+  if (check_cuda(cudaMemsetAsync(w + L.off_flag, 0, (size_t)L.T * 4, eng->stream), "memset flags") != PF_OK ||
+      check_cuda(cudaMemsetAsync(w + L.off_queue, 0, sizeof(unsigned) * 2 * Q_COUNT, eng->stream), "memset queue") != PF_OK ||
+      check_cuda(cudaMemsetAsync(w + L.off_err, 0, sizeof(unsigned) * 4, eng->stream), "memset err") != PF_OK ||
+      check_cuda(cudaMemsetAsync(w + L.off_obs, 0, L.obs_slot_bytes * cfg->obs_slots, eng->stream), "memset obs") != PF_OK ||
+      check_cuda(cudaMemsetAsync(w + L.off_state0, 0, (size_t)L.D * L.P * 4, eng->stream), "memset state") != PF_OK ||
+      check_cuda(cudaMemsetAsync(w + L.off_lw, 0, (size_t)L.P * 4, eng->stream), "memset lw") != PF_OK)
+    return fail(PF_ECUDA);
+  if (check_cuda(cudaMemcpyAsync(eng->desc_dev, eng->hdesc.data(), sizeof(FilterDesc) * cfg->n_filters,
+                                 cudaMemcpyHostToDevice, eng->stream), "desc upload") != PF_OK ||
+      check_cuda(cudaMemcpyAsync(eng->ctrl_dev, hc.data(), sizeof(FilterCtrl) * cfg->n_filters,
+                                 cudaMemcpyHostToDevice, eng->stream), "ctrl upload") != PF_OK ||
+      check_cuda(cudaMemcpyAsync((void*)e.tile_filter, eng->tile_filter.data(), sizeof(int) * L.T,
+                                 cudaMemcpyHostToDevice, eng->stream), "tile table upload") != PF_OK ||
+      check_cuda(cudaStreamSynchronize(eng->stream), "create sync") != PF_OK)
+    return fail(PF_ECUDA);
+  *out = eng;
+  return PF_OK;
+}
+
+int pfe_destroy(pf_engine_t* eng) {
+  if (!eng) return PF_OK;
+  if (eng->stream) cudaStreamSynchronize(eng->stream);
+  if (eng->gexec) cudaGraphExecDestroy(eng->gexec);
+  if (eng->graph) cudaGraphDestroy(eng->graph);
+  for (int i = 0; i < 2; ++i) {
+    if (eng->pinned[i]) cudaFreeHost(eng->pinned[i]);
+    if (eng->pin_ev[i]) cudaEventDestroy(eng->pin_ev[i]);
+  }
+  if (eng->ctrl_host) cudaFreeHost(eng->ctrl_host);
+  for (cudaEvent_t e : eng->tev) cudaEventDestroy(e);
+  delete eng;
+  return PF_OK;
+}
+
+int pfe_set_stream(pf_engine_t* eng, void* stream) {
+  clear_err();
+  if (!eng) return set_err(PF_EINVAL, "null engine");
+  eng->stream = (cudaStream_t)stream;
+  return PF_OK;
+}
+
+int pfe_set_filter_params(pf_engine_t* eng, int filter, const pf_filter_params_t* params) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!params) return set_err(PF_EINVAL, "null params");
+  if (params->n_particles != eng->params[filter].n_particles)
+    return set_err(PF_EINVAL, "n_particles cannot change after pfe_create");
+  pf_engine_config_t one = eng->cfg;
+  one.n_filters = 1;
+  if ((s = validate_config(&one, params)) != PF_OK) return s;
+  eng->params[filter] = *params;
+  fill_desc(eng, filter);
+  CK(cudaMemcpyAsync(eng->desc_dev + filter, &eng->hdesc[filter], sizeof(FilterDesc), cudaMemcpyHostToDevice,
+                     eng->stream));
+  CK(cudaStreamSynchronize(eng->stream));
+  return PF_OK;
+}
+
+int pfe_initialize(pf_engine_t* eng, int filter, const double anchor_ecef[3], const double* clk0,
+                   double spread_pos, double spread_clk) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!anchor_ecef) return set_err(PF_EINVAL, "null anchor");
+  for (int i = 0; i < 3; ++i)
+    if (!isfinite(anchor_ecef[i])) return set_err(PF_EINVAL, "anchor must be finite");
+  if (!(spread_pos >= 0.0) || !(spread_clk >= 0.0) || !isfinite(spread_pos) || !isfinite(spread_clk))
+    return set_err(PF_EINVAL, "spreads must be finite and >= 0");
+  FilterDesc& d = eng->hdesc[filter];
+  enu_rotation(anchor_ecef, d.rot);
+  CK(cudaMemcpyAsync(eng->desc_dev + filter, &d, sizeof(FilterDesc), cudaMemcpyHostToDevice, eng->stream));
+  // The control block goes through the pinned mirror so the copy is truly
+  // asynchronous-safe.
+  CK(cudaStreamSynchronize(eng->stream));
+  FilterCtrl c;
+  memset(&c, 0, sizeof(c));
+  CK(cudaMemcpy(&c, eng->ctrl_dev + filter, sizeof(FilterCtrl), cudaMemcpyDeviceToHost));
+  const unsigned rs_seq = c.rs_seq;
+  memset(&c, 0, sizeof(c));
+  for (int i = 0; i < 3; ++i) c.anchor[i] = anchor_ecef[i];
+  for (int k = 0; k < eng->cfg.n_clk; ++k) {
+    double v = clk0 ? clk0[k] : 0.0;
+    if (!isfinite(v)) return set_err(PF_EINVAL, "clock anchor must be finite");
+    c.clk_anchor[k] = v;
+  }
+  c.lw_zero = 1;
+  c.rs_seq = rs_seq + 1u;
+  c.initialized = 1;
+  eng->ctrl_host[filter] = c;
+  CK(cudaMemcpyAsync(eng->ctrl_dev + filter, &eng->ctrl_host[filter], sizeof(FilterCtrl), cudaMemcpyHostToDevice,
+                     eng->stream));
+  const int g = grid_for(eng, Q_INIT, d.n_tiles);
+  switch (eng->D) {
+    case 4: k_init<4><<<g, kThreads, 0, eng->stream>>>(eng->dev, d.tile_begin, d.n_tiles, (float)spread_pos, (float)spread_clk); break;
+    case 5: k_init<5><<<g, kThreads, 0, eng->stream>>>(eng->dev, d.tile_begin, d.n_tiles, (float)spread_pos, (float)spread_clk); break;
+    case 6: k_init<6><<<g, kThreads, 0, eng->stream>>>(eng->dev, d.tile_begin, d.n_tiles, (float)spread_pos, (float)spread_clk); break;
+    default: k_init<7><<<g, kThreads, 0, eng->stream>>>(eng->dev, d.tile_begin, d.n_tiles, (float)spread_pos, (float)spread_clk); break;
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(eng->stream));
+  eng->initialized[filter] = 1;
+  return PF_OK;
+}
+
+int pfe_get_frame(pf_engine_t* eng, int filter, double rot[9], double anchor_ecef[3]) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (rot) memcpy(rot, eng->hdesc[filter].rot, sizeof(double) * 9);
+  if (anchor_ecef) {
+    if ((s = read_ctrl(eng)) != PF_OK) return s;
+    memcpy(anchor_ecef, eng->ctrl_host[filter].anchor, sizeof(double) * 3);
+  }
+  return PF_OK;
+}
+
+int pfe_obs_slot_bytes(pf_engine_t* eng, size_t* bytes) {
+  clear_err();
+  if (!eng || !bytes) return set_err(PF_EINVAL, "null argument");
+  *bytes = eng->obs_slot_bytes;
+  return PF_OK;
+}
+
+int pfe_upload_obs(pf_engine_t* eng, int slot, const pf_filter_epoch_t* fe, const pf_sat_t* sats,
+                   int n_sats_total) {
+  clear_err();
+  if (!eng || !fe) return set_err(PF_EINVAL, "null argument");
+  if (slot < 0 || slot >= eng->cfg.obs_slots) return set_err(PF_EINVAL, "slot %d out of range", slot);
+  const int F = eng->cfg.n_filters;
+  const int cap = F * eng->cfg.max_sats;
+  if (n_sats_total < 0 || n_sats_total > cap) return set_err(PF_ECAP, "n_sats_total %d above capacity %d", n_sats_total, cap);
+  if (n_sats_total > 0 && !sats) return set_err(PF_EINVAL, "null sats");
+  for (int f = 0; f < F; ++f) {
+    const pf_filter_epoch_t& r = fe[f];
+    if (r.n_sat < 0 || r.n_sat > eng->cfg.max_sats)
+      return set_err(PF_ECAP, "filter %d: n_sat %d above max_sats %d", f, r.n_sat, eng->cfg.max_sats);
+    if (r.sat_offset < 0 || r.sat_offset + r.n_sat > n_sats_total)
+      return set_err(PF_EINVAL, "filter %d: satellite range out of bounds", f);
+    for (int i = 0; i < 3; ++i)
+      if (!isfinite(r.disp[i])) return set_err(PF_EINVAL, "filter %d: displacement must be finite", f);
+    if ((r.flags & PF_EP_WEIGHT)) {
+      for (int k = 0; k < r.n_sat; ++k) {
+        const pf_sat_t& sv = sats[r.sat_offset + k];
+        if (!isfinite(sv.x) || !isfinite(sv.y) || !isfinite(sv.z) || !isfinite(sv.pr) || !isfinite(sv.w) || sv.w < 0)
+          return set_err(PF_EINVAL, "filter %d: satellite %d has non-finite position/pseudorange/weight", f, k);
+        if (sv.clk < 0 || sv.clk >= eng->cfg.n_clk)
+          return set_err(PF_EINVAL, "filter %d: satellite %d clock index %d out of range", f, k, sv.clk);
+      }
+    }
+  }
+  const int b = eng->pin_cur;
+  eng->pin_cur ^= 1;
+  CK(cudaEventSynchronize(eng->pin_ev[b]));
+  unsigned char* h = eng->pinned[b];
+  const size_t fe_bytes = sizeof(pf_filter_epoch_t) * F;
+  memcpy(h, fe, fe_bytes);
+  if (n_sats_total > 0) memcpy(h + fe_bytes, sats, sizeof(pf_sat_t) * n_sats_total);
+  const size_t bytes = fe_bytes + sizeof(pf_sat_t) * (size_t)n_sats_total;
+  CK(cudaMemcpyAsync((void*)(eng->dev.obs + (size_t)slot * eng->obs_slot_bytes), h, bytes, cudaMemcpyHostToDevice,
+                     eng->stream));
+  CK(cudaEventRecord(eng->pin_ev[b], eng->stream));
+  return PF_OK;
+}
+
+int pfe_step(pf_engine_t* eng) {
+  clear_err();
+  if (!eng) return set_err(PF_EINVAL, "null engine");
+  for (int f = 0; f < eng->cfg.n_filters; ++f)
+    if (!eng->initialized[f]) return set_err(PF_ENOTINIT, "filter %d not initialized", f);
+  int n = 1;
+  cudaEvent_t* ev = nullptr;
+  if (eng->t_slots > 0) {
+    ev = &eng->tev[3 * (size_t)eng->t_next];
+    eng->t_next = (eng->t_next + 1) % eng->t_slots;
+    eng->t_pending = std::min(eng->t_pending + 1, eng->t_slots);
+    CK(cudaEventRecord(ev[0], eng->stream));
+  }
+  int s = launch_step(eng, 0, eng->T);
+  if (s != PF_OK) return s;
+  if (ev) CK(cudaEventRecord(ev[1], eng->stream));
+  s = launch_resample(eng, 0, eng->T, &n);
+  if (s != PF_OK) return s;
+  if (ev) CK(cudaEventRecord(ev[2], eng->stream));
+  eng->last_launches = n;
+  return PF_OK;
+}
+
+int pfe_enable_timing(pf_engine_t* eng, int slots) {
+  clear_err();
+  if (!eng) return set_err(PF_EINVAL, "null engine");
+  if (slots < 0) return set_err(PF_EINVAL, "slots must be >= 0");
+  if (eng->gexec || eng->graph) return set_err(PF_EINVAL, "timing applies to eager steps, not captured graphs");
+  CK(cudaStreamSynchronize(eng->stream));
+  for (cudaEvent_t e : eng->tev) cudaEventDestroy(e);
+  eng->tev.clear();
+  eng->t_slots = 0;
+  eng->t_next = 0;
+  eng->t_pending = 0;
+  if (slots == 0) return PF_OK;
+  eng->tev.resize(3 * (size_t)slots, nullptr);
+  for (auto& e : eng->tev) CK(cudaEventCreate(&e));
+  eng->t_slots = slots;
+  return PF_OK;
+}
+
+int pfe_read_timing(pf_engine_t* eng, float* step_kernel_ms, float* whole_step_ms, int max_entries,
+                    int* count) {
+  clear_err();
+  if (!eng || !count) return set_err(PF_EINVAL, "null argument");
+  *count = 0;
+  if (eng->t_slots == 0) return set_err(PF_EINVAL, "timing is not enabled");
+  CK(cudaStreamSynchronize(eng->stream));
+  const int n = std::min(eng->t_pending, max_entries);
+  const int first = (eng->t_next - eng->t_pending + eng->t_slots) % eng->t_slots;
+  for (int i = 0; i < n; ++i) {
+    const cudaEvent_t* ev = &eng->tev[3 * (size_t)((first + i) % eng->t_slots)];
+    float a = 0.f, b = 0.f;
+    CK(cudaEventElapsedTime(&a, ev[0], ev[1]));
+    CK(cudaEventElapsedTime(&b, ev[0], ev[2]));
+    if (step_kernel_ms) step_kernel_ms[i] = a;
+    if (whole_step_ms) whole_step_ms[i] = b;
+  }
+  *count = n;
+  eng->t_pending = 0;
+  return PF_OK;
+}
+
+int pfe_step_per_filter(pf_engine_t* eng) {
+  clear_err();
+  if (!eng) return set_err(PF_EINVAL, "null engine");
+  int n = 0;
+  for (int f = 0; f < eng->cfg.n_filters; ++f) {
+    if (!eng->initialized[f]) return set_err(PF_ENOTINIT, "filter %d not initialized", f);
+    const FilterDesc& d = eng->hdesc[f];
+    int s = launch_step(eng, d.tile_begin, d.n_tiles);
+    if (s != PF_OK) return s;
+    ++n;
+    s = launch_resample(eng, d.tile_begin, d.n_tiles, &n);
+    if (s != PF_OK) return s;
+  }
+  eng->last_launches = n;
+  return PF_OK;
+}
+
+int pfe_graph_capture(pf_engine_t* eng, int per_filter) {
+  clear_err();
+  if (!eng) return set_err(PF_EINVAL, "null engine");
+  if (!eng->stream) return set_err(PF_EINVAL, "graph capture needs a non-default stream (pfe_set_stream)");
+  if (eng->gexec) {
+    cudaGraphExecDestroy(eng->gexec);
+    eng->gexec = nullptr;
+  }
+  if (eng->graph) {
+    cudaGraphDestroy(eng->graph);
+    eng->graph = nullptr;
+  }
+  CK(cudaStreamBeginCapture(eng->stream, cudaStreamCaptureModeThreadLocal));
+  const int saved_slots = eng->t_slots;  // no timing events inside a graph
+  eng->t_slots = 0;
+  int s = per_filter ? pfe_step_per_filter(eng) : pfe_step(eng);
+  eng->t_slots = saved_slots;
+  cudaGraph_t g = nullptr;
+  cudaError_t ce = cudaStreamEndCapture(eng->stream, &g);
+  if (s != PF_OK) {
+    if (g) cudaGraphDestroy(g);
+    return s;
+  }
+  CK(ce);
+  eng->graph = g;
+  CK(cudaGraphInstantiate(&eng->gexec, g, 0));
+  return PF_OK;
+}
+
+int pfe_graph_launch(pf_engine_t* eng, int n_epochs) {
+  clear_err();
+  if (!eng || !eng->gexec) return set_err(PF_EINVAL, "no captured graph");
+  for (int i = 0; i < n_epochs; ++i) CK(cudaGraphLaunch(eng->gexec, eng->stream));
+  return PF_OK;
+}
+
+int pfe_read_results(pf_engine_t* eng, pf_filter_result_t* out) {
+  clear_err();
+  if (!eng || !out) return set_err(PF_EINVAL, "null argument");
+  int s = read_ctrl(eng);
+  if (s != PF_OK) return s;
+  for (int f = 0; f < eng->cfg.n_filters; ++f) {
+    const FilterCtrl& c = eng->ctrl_host[f];
+    pf_filter_result_t& r = out[f];
+    memset(&r, 0, sizeof(r));
+    for (int i = 0; i < 3; ++i) r.est_ecef[i] = c.est_ecef[i];
+    for (int k = 0; k < PF_MAX_CLK; ++k) r.est_clk[k] = c.est_clk[k];
+    for (int i = 0; i < 6; ++i) r.cov_enu[i] = c.cov[i];
+    r.ess = c.ess;
+    r.sum_w = c.sum_w;
+    r.max_lw = c.max_lw;
+    r.resampled = c.resample_flag;
+    r.epoch = c.epoch;
+    r.initialized = eng->initialized[f];
+  }
+  return PF_OK;
+}
+
+int pfe_result_bytes(pf_engine_t* eng, size_t* bytes) {
+  clear_err();
+  if (!eng || !bytes) return set_err(PF_EINVAL, "null argument");
+  *bytes = sizeof(FilterCtrl) * (size_t)eng->cfg.n_filters;
+  return PF_OK;
+}
+
+int pfe_estimate(pf_engine_t* eng, int filter, double* out) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!out) return set_err(PF_EINVAL, "null out");
+  if (!eng->initialized[filter]) return set_err(PF_ENOTINIT, "filter %d not initialized", filter);
+  const FilterDesc& d = eng->hdesc[filter];
+  const int g = grid_for(eng, Q_EST, d.n_tiles);
+  switch (eng->D) {
+    case 4: k_estimate<4><<<g, kThreads, 0, eng->stream>>>(eng->dev, d.tile_begin, d.n_tiles); break;
+    case 5: k_estimate<5><<<g, kThreads, 0, eng->stream>>>(eng->dev, d.tile_begin, d.n_tiles); break;
+    case 6: k_estimate<6><<<g, kThreads, 0, eng->stream>>>(eng->dev, d.tile_begin, d.n_tiles); break;
+    default: k_estimate<7><<<g, kThreads, 0, eng->stream>>>(eng->dev, d.tile_begin, d.n_tiles); break;
+  }
+  CK(cudaGetLastError());
+  if ((s = read_ctrl(eng)) != PF_OK) return s;
+  for (int i = 0; i < eng->D; ++i) out[i] = eng->ctrl_host[filter].api_est[i];
+  return PF_OK;
+}
+
+int pfe_get_ess(pf_engine_t* eng, int filter, double* out) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!out) return set_err(PF_EINVAL, "null out");
+  if (!eng->initialized[filter]) return set_err(PF_ENOTINIT, "filter %d not initialized", filter);
+  if ((s = read_ctrl(eng)) != PF_OK) return s;
+  const FilterCtrl& c = eng->ctrl_host[filter];
+  *out = c.lw_zero ? (double)eng->hdesc[filter].n : c.ess;
+  return PF_OK;
+}
+
+int pfe_get_particles(pf_engine_t* eng, int filter, double* out_host) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!out_host) return set_err(PF_EINVAL, "null out");
+  if (!eng->initialized[filter]) return set_err(PF_ENOTINIT, "filter %d not initialized", filter);
+  const FilterDesc& d = eng->hdesc[filter];
+  const int g = grid_for(eng, Q_EXPORT, d.n_tiles);
+  switch (eng->D) {
+    case 4: k_export<4><<<g, kThreads, 0, eng->stream>>>(eng->dev, d.tile_begin, d.n_tiles, eng->export_buf); break;
+    case 5: k_export<5><<<g, kThreads, 0, eng->stream>>>(eng->dev, d.tile_begin, d.n_tiles, eng->export_buf); break;
+    case 6: k_export<6><<<g, kThreads, 0, eng->stream>>>(eng->dev, d.tile_begin, d.n_tiles, eng->export_buf); break;
+    default: k_export<7><<<g, kThreads, 0, eng->stream>>>(eng->dev, d.tile_begin, d.n_tiles, eng->export_buf); break;
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out_host, eng->export_buf, sizeof(double) * (size_t)d.n * eng->D, cudaMemcpyDeviceToHost,
+                     eng->stream));
+  return sync_and_check(eng);
+}
+
+int pfe_get_anchor(pf_engine_t* eng, int filter, double anchor_ecef[3], double clk_anchor[PF_MAX_CLK],
+                   float shift[8]) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if ((s = read_ctrl(eng)) != PF_OK) return s;
+  const FilterCtrl& c = eng->ctrl_host[filter];
+  if (anchor_ecef) memcpy(anchor_ecef, c.anchor, sizeof(double) * 3);
+  if (clk_anchor) memcpy(clk_anchor, c.clk_anchor, sizeof(double) * PF_MAX_CLK);
+  if (shift) memcpy(shift, c.shift, sizeof(float) * 8);
+  return PF_OK;
+}
+
+int pfe_get_state_f32(pf_engine_t* eng, int filter, float* out_state, float* out_lw, int raw) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if ((s = read_ctrl(eng)) != PF_OK) return s;
+  const FilterCtrl& c = eng->ctrl_host[filter];
+  int n, tb, nt;
+  long long base;
+  filter_dims(eng, filter, &n, &base, &tb, &nt);
+  const float* src = c.parity ? eng->dev.state1 : eng->dev.state0;
+  const bool gather = c.resample_flag && !raw;
+  std::vector<int> anc;
+  if (gather) {
+    anc.resize(n);
+    CK(cudaMemcpy(anc.data(), eng->dev.anc + base, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  }
+  if (out_state) {
+    std::vector<float> tmp(n);
+    for (int dd = 0; dd < eng->D; ++dd) {
+      CK(cudaMemcpy(tmp.data(), src + (size_t)dd * eng->P + base, sizeof(float) * n, cudaMemcpyDeviceToHost));
+      float* o = out_state + (size_t)dd * n;
+      if (gather)
+        for (int k = 0; k < n; ++k) o[k] = tmp[anc[k]];
+      else
+        memcpy(o, tmp.data(), sizeof(float) * n);
+    }
+  }
+  if (out_lw) {
+    if (c.lw_zero && !raw)
+      memset(out_lw, 0, sizeof(float) * n);
+    else
+      CK(cudaMemcpy(out_lw, eng->dev.lw + base, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  }
+  return PF_OK;
+}
+
+int pfe_set_state_f32(pf_engine_t* eng, int filter, const float* state, const float* lw) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!state) return set_err(PF_EINVAL, "null state");
+  if (!eng->initialized[filter]) return set_err(PF_ENOTINIT, "filter %d not initialized", filter);
+  if ((s = read_ctrl(eng)) != PF_OK) return s;
+  FilterCtrl& c = eng->ctrl_host[filter];
+  int n, tb, nt;
+  long long base;
+  filter_dims(eng, filter, &n, &base, &tb, &nt);
+  float* dst = c.parity ? eng->dev.state1 : eng->dev.state0;
+  for (int dd = 0; dd < eng->D; ++dd)
+    CK(cudaMemcpy(dst + (size_t)dd * eng->P + base, state + (size_t)dd * n, sizeof(float) * n,
+                  cudaMemcpyHostToDevice));
+  if (lw) {
+    for (int k = 0; k < n; ++k)
+      if (!isfinite(lw[k])) return set_err(PF_EINVAL, "log-weights must be finite");
+    CK(cudaMemcpy(eng->dev.lw + base, lw, sizeof(float) * n, cudaMemcpyHostToDevice));
+  }
+  c.resample_flag = 0;
+  c.lw_zero = lw ? 0 : 1;
+  for (int d = 0; d < 8; ++d) c.shift[d] = 0.f;
+  CK(cudaMemcpy(eng->ctrl_dev + filter, &c, sizeof(FilterCtrl), cudaMemcpyHostToDevice));
+  return PF_OK;
+}
+
+int pfe_get_ancestors(pf_engine_t* eng, int filter, int* out_host) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!out_host) return set_err(PF_EINVAL, "null out");
+  if ((s = sync_and_check(eng)) != PF_OK) return s;
+  int n, tb, nt;
+  long long base;
+  filter_dims(eng, filter, &n, &base, &tb, &nt);
+  CK(cudaMemcpy(out_host, eng->dev.anc + base, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  return PF_OK;
+}
+
+int pfe_get_resample_info(pf_engine_t* eng, int filter, uint32_t* u32, uint64_t* wq_total, float* max_lw) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if ((s = read_ctrl(eng)) != PF_OK) return s;
+  const FilterCtrl& c = eng->ctrl_host[filter];
+  if (u32) *u32 = c.sys_u;
+  if (wq_total) *wq_total = c.wq_total;
+  if (max_lw) *max_lw = c.max_lw;
+  return PF_OK;
+}
+
+int pfe_error_word(pf_engine_t* eng, unsigned* word) {
+  clear_err();
+  if (!eng || !word) return set_err(PF_EINVAL, "null argument");
+  CK(cudaStreamSynchronize(eng->stream));
+  CK(cudaMemcpy(word, eng->dev.err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  return PF_OK;
+}
+
+int pfe_set_spin_limit(pf_engine_t* eng, unsigned long long limit) {
+  clear_err();
+  if (!eng) return set_err(PF_EINVAL, "null engine");
+  eng->dev.spin_limit = limit ? limit : (1ull << 24);
+  return PF_OK;
+}
+
+int pfe_last_launch_count(pf_engine_t* eng, int* count) {
+  clear_err();
+  if (!eng || !count) return set_err(PF_EINVAL, "null argument");
+  *count = eng->last_launches;
+  return PF_OK;
+}
+
+// Test hook: make the next look-back wait for a tag that is never published
+// (on != 0), so its bounded spin runs out and sets the error word; clears
+// the error word when switched off.
+int pfe_test_poison_lookback(pf_engine_t* eng, int on) {
+  clear_err();
+  if (!eng) return set_err(PF_EINVAL, "null engine");
+  eng->dev.lookback_poison = on ? 1 : 0;
+  if (!on) {
+    CK(cudaStreamSynchronize(eng->stream));
+    CK(cudaMemset(eng->dev.err, 0, sizeof(unsigned)));
+  }
+  return PF_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Internal hook for the stateless API: systematic ancestors of one weight
+// vector, with the engine's look-back scan and merge-path kernels.  lw32 holds
+// log-weights already shifted by their maximum (so the maximum is 0).
+namespace pfb {
+
+size_t systematic_scratch_bytes(int n) {
+  const int T = (n + PF_TILE - 1) / PF_TILE;
+  size_t o = 0;
+  auto take = [&](size_t b) { o = align_up(o + b, 256); };
+  take(sizeof(FilterDesc));
+  take(sizeof(FilterCtrl));
+  take((size_t)T * 4);                 // tile table
+  take((size_t)align_up(n, 4) * 4);    // offs
+  take((size_t)T * 4);                 // mp_part
+  take((size_t)T * 8 * 3);             // agg, inc, excl
+  take((size_t)T * 4);                 // flags
+  take(sizeof(unsigned) * 2 * Q_COUNT + 16);
+  return o;
+}
+
+int systematic_ancestors(const float* d_lw32, int n, uint32_t u, int* d_anc, void* d_scratch,
+                         cudaStream_t st) {
+  const int T = (n + PF_TILE - 1) / PF_TILE;
+  unsigned char* w = (unsigned char*)d_scratch;
+  size_t o = 0;
+  auto take = [&](size_t b) {
+    unsigned char* p = w + o;
+    o = align_up(o + b, 256);
+    return p;
+  };
+  FilterDesc* desc = (FilterDesc*)take(sizeof(FilterDesc));
+  FilterCtrl* ctrl = (FilterCtrl*)take(sizeof(FilterCtrl));
+  int* tf = (int*)take((size_t)T * 4);
+  uint32_t* offs = (uint32_t*)take((size_t)align_up(n, 4) * 4);
+  uint32_t* mp = (uint32_t*)take((size_t)T * 4);
+  unsigned long long* agg = (unsigned long long*)take((size_t)T * 8);
+  unsigned long long* inc = (unsigned long long*)take((size_t)T * 8);
+  unsigned long long* excl = (unsigned long long*)take((size_t)T * 8);
+  unsigned* flag = (unsigned*)take((size_t)T * 4);
+  unsigned* queue = (unsigned*)take(sizeof(unsigned) * 2 * Q_COUNT + 16);
+  unsigned* err = queue + 2 * Q_COUNT;
+
+  FilterDesc hd;
+  memset(&hd, 0, sizeof(hd));
+  hd.n = n;
+  hd.tile_begin = 0;
+  hd.n_tiles = T;
+  hd.K = quant_exponent(n);
+  hd.p_off = 0;
+  FilterCtrl hc;
+  memset(&hc, 0, sizeof(hc));
+  hc.resample_flag = 1;
+  hc.rs_seq = 1;
+  hc.max_lw = 0.0f;
+  hc.sys_u = u;
+  std::vector<int> htf(T, 0);
+  CK(cudaMemcpyAsync(desc, &hd, sizeof(hd), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctrl, &hc, sizeof(hc), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(tf, htf.data(), sizeof(int) * T, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(flag, 0, (size_t)T * 4, st));
+  CK(cudaMemsetAsync(queue, 0, sizeof(unsigned) * 2 * Q_COUNT + 16, st));
+
+  EngineDev e;
+  memset(&e, 0, sizeof(e));
+  e.desc = desc;
+  e.ctrl = ctrl;
+  e.tile_filter = tf;
+  e.lw = const_cast<float*>(d_lw32);
+  e.anc = d_anc;
+  e.offs = offs;
+  e.mp_part = mp;
+  e.lb_agg = agg;
+  e.lb_inc = inc;
+  e.lb_flag = flag;
+  e.tile_excl = excl;
+  e.queue = queue;
+  e.err = err;
+  e.spin_limit = 1ull << 24;
+  e.n_filters = 1;
+  e.resampler = PF_RESAMPLE_SYSTEMATIC;
+  int dev = 0, sms = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  int r_scan = 0, r_offs = 0, r_merge = 0;
+  int s;
+  if ((s = occupancy(k_scan, sms, &r_scan)) != PF_OK) return s;
+  if ((s = occupancy(k_offs, sms, &r_offs)) != PF_OK) return s;
+  if ((s = occupancy(k_merge, sms, &r_merge)) != PF_OK) return s;
+  k_scan<<<std::min(T, r_scan), kThreads, 0, st>>>(e, 0, T);
+  k_offs<<<std::min(T, r_offs), kThreads, 0, st>>>(e, 0, T);
+  k_merge<<<std::min(T, r_merge), kThreads, 0, st>>>(e, 0, T);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  unsigned hw = 0;
+  CK(cudaMemcpy(&hw, err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (hw & ERR_LOOKBACK_TIMEOUT) return set_err(PF_ETIMEOUT, "device look-back spin limit reached");
+  if (hw) return set_err(PF_EINVAL, "systematic resampling: invalid weights (error word 0x%x)", hw);
+  return PF_OK;
+}
+
+}  // namespace pfb

@@ -1,0 +1,99 @@
+// pf_engine_dev.cuh -- device data structures of the resident engine.
+#pragma once
+#include <stdint.h>
+#include "../../include/gnss_pf_b200.h"
+#include "pf_common.cuh"
+
+namespace pfb {
+
+constexpr int kThreads = 256;        // threads per CTA of the tile kernels
+constexpr int kPerThread = 4;        // particles per thread (one float4)
+constexpr int kTile = kThreads * kPerThread;
+static_assert(kTile == PF_TILE, "tile size mismatch");
+constexpr int kMergeDiag = 2 * kTile;  // merge-path diagonals per tile
+constexpr int kPartStride = 16;        // floats per tile partial
+constexpr int kMaxD = 3 + PF_MAX_CLK;
+
+// Work-queue slots (two words each: next tile, exit ticket).
+enum QueueSlot : int {
+  Q_STEP = 0, Q_SCAN = 1, Q_OFFS = 2, Q_MERGE = 3, Q_MEGO = 4,
+  Q_INIT = 5, Q_EST = 6, Q_EXPORT = 7, Q_COUNT = 8
+};
+
+// Error word bits.
+enum : unsigned { ERR_LOOKBACK_TIMEOUT = 1u, ERR_BAD_WEIGHTS = 2u, ERR_SAT_CAP = 4u };
+
+struct FilterDesc {
+  int n;
+  int tile_begin;
+  int n_tiles;
+  int K;                  // quantisation exponent (quant_exponent(n))
+  long long p_off;        // element offset of particle 0, multiple of 4
+  uint32_t key0, key1;    // Philox key (filter seed)
+  float sigma[8];         // predict noise per state component
+  float sigma_pr;
+  float inv_sigma_pr;
+  float wscale;           // -0.5 / sigma_pr^2
+  float huber_k;
+  uint32_t sys_ref_u;     // (seed % 1e6)/(1e6 N) as a 32-bit slot fraction
+  int filter_id;
+  double rot[9];          // ECEF -> local (rows E, N, U)
+};
+
+struct FilterCtrl {
+  double anchor[3];       // ECEF origin of the stored offsets
+  double clk_anchor[PF_MAX_CLK];
+  double est_ecef[3];     // fused weighted mean of the last step
+  double est_clk[PF_MAX_CLK];
+  double cov[6];
+  double ess;
+  double sum_w;
+  double api_est[8];      // output of the on-demand estimate kernel
+  unsigned long long wq_total;
+  float shift[8];         // pending re-centring, applied by the next predict
+  float max_lw;
+  uint32_t sys_u;
+  unsigned epoch;
+  unsigned ticket;
+  unsigned est_ticket;
+  unsigned rs_seq;        // resample sequence number (look-back tag)
+  int resample_flag;      // resampled in the last step: next read gathers
+  int lw_zero;            // log-weights read as zero
+  int parity;             // which state buffer is current
+  int initialized;
+};
+
+struct EngineDev {
+  const FilterDesc* desc;
+  FilterCtrl* ctrl;
+  const int* tile_filter;
+  float* state0;
+  float* state1;
+  float* lw;
+  int* anc;
+  uint32_t* offs;
+  uint32_t* mp_part;
+  float* part;
+  unsigned long long* lb_agg;
+  unsigned long long* lb_inc;
+  unsigned* lb_flag;
+  unsigned long long* tile_excl;
+  unsigned* queue;
+  unsigned* err;
+  const unsigned char* obs;
+  unsigned long long obs_slot_bytes;
+  unsigned long long spin_limit;
+  long long p_total;      // stride between state components
+  int obs_slots;
+  int n_filters;
+  int max_sats;
+  int resampler;
+  int mego_iters;
+  int lw_mode;
+  int sys_offset;
+  unsigned flags;
+  float ess_threshold;
+  int lookback_poison;    // test hook: wait for a tag nobody publishes
+};
+
+}  // namespace pfb

@@ -1,0 +1,977 @@
+// pf_engine_kernels.cuh -- sm_100a kernels of the resident engine.
+//
+// One epoch of every filter is a short chain of persistent kernels, each a
+// loop over (filter, tile) work items taken from an atomic queue:
+//
+//   k_step   fused predict + likelihood + tile statistics; the last tile of a
+//            filter merges the tile statistics into max log-weight, ESS,
+//            weighted mean and covariance and decides on the device whether
+//            the filter resamples (reference: predict.cu:23-38,
+//            weight.cu:13-57,61-108,163-220, particle_filter.py:153-161).
+//   k_scan   quantised weights, tile sums and a decoupled look-back scan of
+//            the tile sums (systematic only).
+//   k_offs   in-tile scan, offspring end F(i) of every particle and the
+//            merge-path partition points.
+//   k_merge  merge-path offspring assignment: ancestor index of every slot.
+//   k_mego   Megopolis chain per slot, ancestor in registers.
+//
+// The resampled state is never copied here: the next k_step (or the
+// estimate / export kernels) reads state[ancestor[k]].
+#pragma once
+#include "pf_engine_dev.cuh"
+
+namespace pfb {
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 bc(float a) { return make_float2(a, a); }
+
+__device__ __forceinline__ int dequeue(unsigned* q, int* s_slot) {
+  if (threadIdx.x == 0) *s_slot = (int)atomicAdd(q, 1u);
+  __syncthreads();
+  int v = *s_slot;
+  __syncthreads();
+  return v;
+}
+
+// The last CTA to leave resets the queue for the next launch.
+__device__ __forceinline__ void queue_exit(unsigned* q) {
+  if (threadIdx.x == 0) {
+    unsigned old = atomicAdd(q + 1, 1u);
+    if (old == gridDim.x - 1) {
+      q[0] = 0u;
+      q[1] = 0u;
+      __threadfence();
+    }
+  }
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Inclusive warp scan of 64-bit integers.
+__device__ __forceinline__ unsigned long long warp_incl_scan_u64(unsigned long long v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned long long t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  return v;
+}
+
+// Block-wide max over kThreads threads.
+__device__ __forceinline__ float block_max(float v, float* s_tmp) {
+  v = warp_max(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) s_tmp[warp] = v;
+  __syncthreads();
+  float r = s_tmp[0];
+#pragma unroll
+  for (int w = 1; w < kThreads / 32; ++w) r = fmaxf(r, s_tmp[w]);
+  return r;
+}
+
+// Block exclusive scan of one 64-bit value per thread; returns the exclusive
+// prefix and writes the block total to *total.
+__device__ __forceinline__ unsigned long long block_excl_scan_u64(
+    unsigned long long v, unsigned long long* s_tmp, unsigned long long* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long incl = warp_incl_scan_u64(v);
+  __syncthreads();
+  if (lane == 31) s_tmp[warp] = incl;
+  __syncthreads();
+  unsigned long long wpre = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < kThreads / 32; ++w) {
+    unsigned long long x = s_tmp[w];
+    if (w < warp) wpre += x;
+    tot += x;
+  }
+  *total = tot;
+  return wpre + incl - v;
+}
+
+// -------------------------------------------------------------------------
+// Tile statistics: max log-weight, sum w, sum w^2, sum w x_d, sum w x_i x_j
+// (positions) with w = exp(lw - tile max).  Written as one 16-float row.
+template <int D>
+__device__ __forceinline__ void tile_stats(const float (&x)[D][4], const float (&lwv)[4],
+                                           bool cov, float* part_row, float* s_maxtmp,
+                                           float (*s_red)[kPartStride]) {
+  constexpr int NV = 2 + D + 6;  // s, s2, sx[D], cov6
+  float tmax = fmaxf(fmaxf(lwv[0], lwv[1]), fmaxf(lwv[2], lwv[3]));
+  const float bmax = block_max(tmax, s_maxtmp);
+  float acc[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) acc[i] = 0.f;
+  if (bmax > -INFINITY) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      float w = exp2f((lwv[k] - bmax) * 1.4426950408889634f);
+      acc[0] += w;
+      acc[1] = fmaf(w, w, acc[1]);
+#pragma unroll
+      for (int d = 0; d < D; ++d) acc[2 + d] = fmaf(w, x[d][k], acc[2 + d]);
+      if (cov) {
+        float wx = w * x[0][k], wy = w * x[1][k], wz = w * x[2][k];
+        acc[2 + D + 0] = fmaf(wx, x[0][k], acc[2 + D + 0]);
+        acc[2 + D + 1] = fmaf(wx, x[1][k], acc[2 + D + 1]);
+        acc[2 + D + 2] = fmaf(wx, x[2][k], acc[2 + D + 2]);
+        acc[2 + D + 3] = fmaf(wy, x[1][k], acc[2 + D + 3]);
+        acc[2 + D + 4] = fmaf(wy, x[2][k], acc[2 + D + 4]);
+        acc[2 + D + 5] = fmaf(wz, x[2][k], acc[2 + D + 5]);
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) acc[i] = warp_sum(acc[i]);
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) s_red[warp][i] = acc[i];
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    float s = 0.f;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) s += s_red[w][threadIdx.x];
+    part_row[1 + threadIdx.x] = s;
+  }
+  if (threadIdx.x == 0) part_row[0] = bmax;
+  __syncthreads();
+}
+
+struct MergedStats {
+  float max_lw;
+  double w, w2;
+  double sx[kMaxD];
+  double sxx[6];
+};
+
+// Merge the tile rows [tb, tb + nt) of one filter (executed by a whole CTA,
+// result valid in thread 0).  Rows written by other CTAs are read through L2.
+template <int D>
+__device__ __forceinline__ MergedStats merge_tiles(const float* part, int tb, int nt,
+                                                   float* s_maxtmp, double* s_dred) {
+  constexpr int NV = 2 + D + 6;
+  float m = -INFINITY;
+  for (int i = threadIdx.x; i < nt; i += kThreads) m = fmaxf(m, __ldcg(part + (size_t)(tb + i) * kPartStride));
+  const float M = block_max(m, s_maxtmp);
+  double acc[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) acc[i] = 0.0;
+  if (M > -INFINITY) {
+    for (int i = threadIdx.x; i < nt; i += kThreads) {
+      const float* row = part + (size_t)(tb + i) * kPartStride;
+      float pm = __ldcg(row);
+      if (!(pm > -INFINITY)) continue;
+      double sc = exp((double)pm - (double)M);
+      acc[0] += sc * (double)__ldcg(row + 1);
+      acc[1] += sc * sc * (double)__ldcg(row + 2);
+#pragma unroll
+      for (int v = 2; v < NV; ++v) acc[v] += sc * (double)__ldcg(row + 1 + v);
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) acc[i] = warp_sum_d(acc[i]);
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) s_dred[warp * 16 + i] = acc[i];
+  }
+  __syncthreads();
+  MergedStats r;
+  r.max_lw = M;
+  if (threadIdx.x == 0) {
+    double t[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double s = 0.0;
+      for (int w = 0; w < kThreads / 32; ++w) s += s_dred[w * 16 + i];
+      t[i] = s;
+    }
+    r.w = t[0];
+    r.w2 = t[1];
+#pragma unroll
+    for (int d = 0; d < kMaxD; ++d) r.sx[d] = d < D ? t[2 + d] : 0.0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) r.sxx[i] = t[2 + D + i];
+  }
+  return r;
+}
+
+// Local offsets -> ECEF: anchor + R^T v.
+__device__ __forceinline__ void local_to_ecef(const double* rot, const double* anchor,
+                                              double e, double n, double u, double* out) {
+  out[0] = anchor[0] + rot[0] * e + rot[3] * n + rot[6] * u;
+  out[1] = anchor[1] + rot[1] * e + rot[4] * n + rot[7] * u;
+  out[2] = anchor[2] + rot[2] * e + rot[5] * n + rot[8] * u;
+}
+
+// -------------------------------------------------------------------------
+// Load the 4 particles [p0, p0+4) of the current state (gathering through
+// the ancestor array when the last step resampled).
+template <int D>
+__device__ __forceinline__ void load_particles(const EngineDev& e, const float* src,
+                                               long long base, int p0, int n, bool gather,
+                                               float (&x)[D][4]) {
+  if (gather) {
+    int4 a = __ldcg(reinterpret_cast<const int4*>(e.anc + base + p0));
+    int ai[4] = {a.x, a.y, a.z, a.w};
+    // slots past the filter's end hold no ancestor; keep every index in range
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (p0 + k >= n || (unsigned)ai[k] >= (unsigned)n) ai[k] = p0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const float* s = src + (size_t)d * e.p_total + base;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) x[d][k] = __ldcg(s + ai[k]);
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      float4 v = __ldcs(reinterpret_cast<const float4*>(src + (size_t)d * e.p_total + base + p0));
+      x[d][0] = v.x; x[d][1] = v.y; x[d][2] = v.z; x[d][3] = v.w;
+    }
+  }
+}
+
+// -------------------------------------------------------------------------
+// k_step: fused predict + weight + statistics (+ per-filter finalize).
+template <int NCLK, int WMODE>
+__global__ void __launch_bounds__(kThreads, 2) k_step(EngineDev e, int t0, int count) {
+  constexpr int D = 3 + NCLK;
+  __shared__ float4 s_sat[2 * PF_MAX_SATS];
+  __shared__ int s_grp[PF_MAX_CLK + 1];
+  __shared__ float s_red[kThreads / 32][kPartStride];
+  __shared__ float s_maxtmp[kThreads / 32];
+  __shared__ double s_dred[(kThreads / 32) * 16];
+  __shared__ int s_slot, s_last;
+
+  unsigned* q = e.queue + 2 * Q_STEP;
+  int cached = -1;
+  for (;;) {
+    const int tq = dequeue(q, &s_slot);
+    if (tq >= count) break;
+    const int t = t0 + tq;
+    const int f = __ldg(e.tile_filter + t);
+    const FilterDesc* fd = e.desc + f;
+    FilterCtrl* fc = e.ctrl + f;
+    const unsigned epoch = fc->epoch;
+    const int parity = fc->parity;
+    const bool gather = fc->resample_flag != 0;
+    const bool lw_zero = fc->lw_zero != 0;
+    const unsigned char* ob = e.obs + (size_t)(epoch % (unsigned)e.obs_slots) * e.obs_slot_bytes;
+    const pf_filter_epoch_t* fe = reinterpret_cast<const pf_filter_epoch_t*>(ob) + f;
+    const pf_sat_t* sats = reinterpret_cast<const pf_sat_t*>(ob + sizeof(pf_filter_epoch_t) * e.n_filters);
+    const int eflags = fe->flags;
+    int n_sat = fe->n_sat;
+    if (n_sat > e.max_sats) {
+      if (threadIdx.x == 0) atomicOr(e.err, ERR_SAT_CAP);
+      n_sat = e.max_sats;
+    }
+    if (n_sat < 0) n_sat = 0;
+    const bool do_predict = (eflags & PF_EP_PREDICT) != 0;
+    const bool do_weight = (eflags & PF_EP_WEIGHT) != 0;
+
+    // ---- per-filter satellite geometry in FP64, stored as FP32 in smem,
+    //      grouped by clock state.
+    if (f != cached) {
+      if (do_weight && threadIdx.x < n_sat) {
+        const double* rot = fd->rot;
+        const double sh0 = fc->shift[0], sh1 = fc->shift[1], sh2 = fc->shift[2];
+        double A[3];
+        local_to_ecef(rot, fc->anchor, sh0, sh1, sh2, A);
+        const pf_sat_t* sp = sats + fe->sat_offset + threadIdx.x;
+        int c = sp->clk;
+        c = c < 0 ? 0 : (c >= NCLK ? NCLK - 1 : c);
+        const double clkA = fc->clk_anchor[c] + (double)fc->shift[3 + c];
+        double vx = sp->x - A[0], vy = sp->y - A[1], vz = sp->z - A[2];
+        double r0 = sqrt(vx * vx + vy * vy + vz * vz);
+        double inv = 1.0 / r0;
+        vx *= inv; vy *= inv; vz *= inv;
+        double eE = rot[0] * vx + rot[1] * vy + rot[2] * vz;
+        double eN = rot[3] * vx + rot[4] * vy + rot[5] * vz;
+        double eU = rot[6] * vx + rot[7] * vy + rot[8] * vz;
+        float g = (float)inv;
+        float y = (float)(sp->pr - r0 - clkA);
+        float wq = WMODE == PF_WEIGHT_GAUSSIAN ? (float)((double)fd->wscale * sp->w) : (float)sp->w;
+        float4 a4 = make_float4((float)eE, (float)eN, (float)eU, -0.5f * g);
+        float4 b4 = make_float4(0.5f * g * g, 0.5f * g, y, wq);
+        int rank = 0;
+        for (int s2 = 0; s2 < n_sat; ++s2) {
+          int c2 = sats[fe->sat_offset + s2].clk;
+          c2 = c2 < 0 ? 0 : (c2 >= NCLK ? NCLK - 1 : c2);
+          rank += (c2 < c) || (c2 == c && s2 < (int)threadIdx.x);
+        }
+        s_sat[2 * rank] = a4;
+        s_sat[2 * rank + 1] = b4;
+      }
+      if (threadIdx.x <= NCLK) {
+        int cnt = 0;
+        if (do_weight) {
+          for (int s2 = 0; s2 < n_sat; ++s2) {
+            int c2 = sats[fe->sat_offset + s2].clk;
+            c2 = c2 < 0 ? 0 : (c2 >= NCLK ? NCLK - 1 : c2);
+            cnt += c2 < (int)threadIdx.x;
+          }
+        }
+        s_grp[threadIdx.x] = cnt;
+      }
+      cached = f;
+      __syncthreads();
+    }
+
+    const int n = fd->n;
+    const int j = t - fd->tile_begin;
+    const int p0 = j * kTile + (int)threadIdx.x * 4;
+    const bool active = p0 < n;
+    const long long base = fd->p_off;
+    const float* src = parity ? e.state1 : e.state0;
+    float* dst = parity ? e.state0 : e.state1;
+
+    float x[D][4];
+    float lwv[4];
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) x[d][k] = 0.f;
+    if (active) {
+      load_particles<D>(e, src, base, p0, n, gather, x);
+      // predict: x += disp - shift + sigma * N(0,1)
+      float ds[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) ds[d] = -fc->shift[d];
+      if (do_predict) {
+        ds[0] += (float)fe->disp[0];
+        ds[1] += (float)fe->disp[1];
+        ds[2] += (float)fe->disp[2];
+        const uint32_t fid = (uint32_t)fd->filter_id;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          float nz[8];
+          U4 r = philox10(U4{(uint32_t)(p0 + k), epoch, TAG_PREDICT, fid}, fd->key0, fd->key1);
+          float2 a = box_muller_f32(r.x, r.y), b = box_muller_f32(r.z, r.w);
+          nz[0] = a.x; nz[1] = a.y; nz[2] = b.x; nz[3] = b.y;
+          if (D > 4) {
+            U4 r2 = philox10(U4{(uint32_t)(p0 + k), epoch, TAG_PREDICT | 1u, fid}, fd->key0, fd->key1);
+            float2 c = box_muller_f32(r2.x, r2.y), dd = box_muller_f32(r2.z, r2.w);
+            nz[4] = c.x; nz[5] = c.y; nz[6] = dd.x; nz[7] = dd.y;
+          } else {
+            nz[4] = nz[5] = nz[6] = nz[7] = 0.f;
+          }
+#pragma unroll
+          for (int d = 0; d < D; ++d) x[d][k] = fmaf(fd->sigma[d], nz[d], x[d][k] + ds[d]);
+        }
+      } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+#pragma unroll
+          for (int k = 0; k < 4; ++k) x[d][k] += ds[d];
+      }
+#pragma unroll
+      for (int d = 0; d < D; ++d)
+        __stcs(reinterpret_cast<float4*>(dst + (size_t)d * e.p_total + base + p0),
+               make_float4(x[d][0], x[d][1], x[d][2], x[d][3]));
+
+      // previous log-weights (accumulate mode, or statistics of a
+      // predict-only step)
+      float lw0[4] = {0.f, 0.f, 0.f, 0.f};
+      const bool need_prev = !lw_zero && (!do_weight || e.lw_mode == PF_LW_ACCUMULATE);
+      if (need_prev) {
+        float4 v = __ldcs(reinterpret_cast<const float4*>(e.lw + base + p0));
+        lw0[0] = v.x; lw0[1] = v.y; lw0[2] = v.z; lw0[3] = v.w;
+      }
+      if (do_weight) {
+        float2 lwp[2] = {f2(lw0[0], lw0[1]), f2(lw0[2], lw0[3])};
+        float2 dx[2], dy[2], dz[2], bb[2];
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+          dx[p] = f2(x[0][2 * p], x[0][2 * p + 1]);
+          dy[p] = f2(x[1][2 * p], x[1][2 * p + 1]);
+          dz[p] = f2(x[2][2 * p], x[2][2 * p + 1]);
+          bb[p] = __fmul2_rn(dx[p], dx[p]);
+          bb[p] = __ffma2_rn(dy[p], dy[p], bb[p]);
+          bb[p] = __ffma2_rn(dz[p], dz[p], bb[p]);
+        }
+#pragma unroll
+        for (int c = 0; c < NCLK; ++c) {
+          float2 ncb[2] = {f2(-x[3 + c][0], -x[3 + c][1]), f2(-x[3 + c][2], -x[3 + c][3])};
+          const int s_end = s_grp[c + 1];
+          for (int s = s_grp[c]; s < s_end; ++s) {
+            const float4 A = s_sat[2 * s];
+            const float4 B = s_sat[2 * s + 1];
+#pragma unroll
+            for (int p = 0; p < 2; ++p) {
+              float2 ed = __fmul2_rn(bc(A.x), dx[p]);
+              ed = __ffma2_rn(bc(A.y), dy[p], ed);
+              ed = __ffma2_rn(bc(A.z), dz[p], ed);           // e . d
+              float2 nh = __ffma2_rn(bb[p], bc(A.w), ed);     // -h = e.d - |d|^2 g/2
+              float2 ninner = __ffma2_rn(nh, bc(B.x), bc(B.y));
+              float2 hh = __fmul2_rn(nh, nh);
+              float2 ndl = __ffma2_rn(hh, ninner, nh);        // -(|s-d| - r0)
+              float2 r = __fadd2_rn(__fadd2_rn(bc(B.z), ncb[p]), ndl);
+              if (WMODE == PF_WEIGHT_GAUSSIAN) {
+                float2 rw = __fmul2_rn(r, bc(B.w));
+                lwp[p] = __ffma2_rn(rw, r, lwp[p]);
+              } else {
+                const float ks = fd->huber_k;
+                float z0 = fabsf(r.x) * fd->inv_sigma_pr, z1 = fabsf(r.y) * fd->inv_sigma_pr;
+                float rho0 = z0 < ks ? 0.5f * z0 * z0 : fmaf(ks, z0, -0.5f * ks * ks);
+                float rho1 = z1 < ks ? 0.5f * z1 * z1 : fmaf(ks, z1, -0.5f * ks * ks);
+                lwp[p].x = fmaf(-B.w, rho0, lwp[p].x);
+                lwp[p].y = fmaf(-B.w, rho1, lwp[p].y);
+              }
+            }
+          }
+        }
+        lwv[0] = lwp[0].x; lwv[1] = lwp[0].y; lwv[2] = lwp[1].x; lwv[3] = lwp[1].y;
+        __stcs(reinterpret_cast<float4*>(e.lw + base + p0), make_float4(lwv[0], lwv[1], lwv[2], lwv[3]));
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) lwv[k] = lw0[k];
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (p0 + k >= n) lwv[k] = -INFINITY;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) lwv[k] = -INFINITY;
+    }
+
+    float* row = e.part + (size_t)t * kPartStride;
+    tile_stats<D>(x, lwv, (e.flags & PF_FLAG_COVARIANCE) != 0, row, s_maxtmp, s_red);
+
+    if (threadIdx.x == 0) {
+      __threadfence();
+      unsigned old = atomicAdd(&fc->ticket, 1u);
+      s_last = (old == (unsigned)fd->n_tiles - 1u);
+    }
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      MergedStats ms = merge_tiles<D>(e.part, fd->tile_begin, fd->n_tiles, s_maxtmp, s_dred);
+      if (threadIdx.x == 0) {
+        const double W = ms.w;
+        const double ess = (ms.w2 > 0.0) ? (W * W) / ms.w2 : 0.0;
+        double mu[kMaxD];
+#pragma unroll
+        for (int d = 0; d < kMaxD; ++d) mu[d] = (W > 0.0 && d < D) ? ms.sx[d] / W : 0.0;
+        double A[3];
+        local_to_ecef(fd->rot, fc->anchor, fc->shift[0], fc->shift[1], fc->shift[2], A);
+        double est[3];
+        local_to_ecef(fd->rot, A, mu[0], mu[1], mu[2], est);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          fc->anchor[i] = A[i];
+          fc->est_ecef[i] = est[i];
+        }
+#pragma unroll
+        for (int c = 0; c < PF_MAX_CLK; ++c) {
+          if (c < NCLK) {
+            double ca = fc->clk_anchor[c] + (double)fc->shift[3 + c];
+            fc->clk_anchor[c] = ca;
+            fc->est_clk[c] = ca + mu[3 + c];
+          } else {
+            fc->est_clk[c] = 0.0;
+          }
+        }
+        if (e.flags & PF_FLAG_COVARIANCE) {
+          if (W > 0.0) {
+            fc->cov[0] = ms.sxx[0] / W - mu[0] * mu[0];
+            fc->cov[1] = ms.sxx[1] / W - mu[0] * mu[1];
+            fc->cov[2] = ms.sxx[2] / W - mu[0] * mu[2];
+            fc->cov[3] = ms.sxx[3] / W - mu[1] * mu[1];
+            fc->cov[4] = ms.sxx[4] / W - mu[1] * mu[2];
+            fc->cov[5] = ms.sxx[5] / W - mu[2] * mu[2];
+          }
+        }
+        fc->ess = ess;
+        fc->sum_w = W;
+        fc->max_lw = ms.max_lw;
+        const bool recenter = (e.flags & PF_FLAG_RECENTER) != 0 && W > 0.0;
+#pragma unroll
+        for (int d = 0; d < 8; ++d) fc->shift[d] = (recenter && d < D) ? (float)mu[d] : 0.f;
+        bool rs = do_weight && !(eflags & PF_EP_NO_RESAMPLE) &&
+                  ((eflags & PF_EP_FORCE_RESAMPLE) || ess < (double)e.ess_threshold * (double)n);
+        if (!(W > 0.0) || !(ms.max_lw > -INFINITY)) {
+          if (do_weight) atomicOr(e.err, ERR_BAD_WEIGHTS);
+          rs = false;
+        }
+        fc->resample_flag = rs ? 1 : 0;
+        fc->lw_zero = rs ? 1 : (do_weight ? 0 : (lw_zero ? 1 : 0));
+        if (rs) {
+          fc->rs_seq = fc->rs_seq + 1u;
+          uint32_t u = fd->sys_ref_u;
+          if (e.sys_offset == PF_SYS_OFFSET_RANDOM) {
+            U4 r = philox10(U4{0u, epoch, TAG_SYS_U, (uint32_t)fd->filter_id}, fd->key0, fd->key1);
+            u = r.x;
+          }
+          fc->sys_u = u;
+        }
+        fc->parity = parity ^ 1;
+        fc->epoch = epoch + 1u;
+        fc->ticket = 0u;
+        __threadfence();
+      }
+      __syncthreads();
+    }
+  }
+  queue_exit(q);
+}
+
+// -------------------------------------------------------------------------
+// k_scan: quantised weights, tile sums, decoupled look-back over tiles.
+__global__ void __launch_bounds__(kThreads) k_scan(EngineDev e, int t0, int count) {
+  __shared__ unsigned long long s_u64[kThreads / 32];
+  __shared__ int s_slot;
+  unsigned* q = e.queue + 2 * Q_SCAN;
+  for (;;) {
+    const int tq = dequeue(q, &s_slot);
+    if (tq >= count) break;
+    const int t = t0 + tq;
+    const int f = __ldg(e.tile_filter + t);
+    const FilterDesc* fd = e.desc + f;
+    FilterCtrl* fc = e.ctrl + f;
+    if (!fc->resample_flag) continue;
+    const int n = fd->n, K = fd->K;
+    const float M = fc->max_lw;
+    const unsigned tag = (fc->rs_seq & 0x3FFFFFFFu) << 2;
+    const int tb = fd->tile_begin, j = t - tb;
+    const int p0 = j * kTile + (int)threadIdx.x * 4;
+    const long long base = fd->p_off;
+    unsigned long long qs = 0;
+    if (p0 < n) {
+      float4 v = __ldcg(reinterpret_cast<const float4*>(e.lw + base + p0));
+      float l[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (p0 + k < n) qs += quantize_weight(l[k], M, K);
+    }
+    unsigned long long tot;
+    block_excl_scan_u64(qs, s_u64, &tot);
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      unsigned long long excl = 0;
+      if (j == 0) {
+        if (lane == 0) {
+          e.lb_inc[t] = tot;
+          __threadfence();
+          atomicExch(e.lb_flag + t, tag | 2u);
+        }
+      } else {
+        if (lane == 0) {
+          e.lb_agg[t] = tot;
+          __threadfence();
+          atomicExch(e.lb_flag + t, tag | 1u);
+        }
+        const unsigned want = e.lookback_poison ? ((tag + 4u) >> 2) : (tag >> 2);
+        int pred = t - 1;
+        bool done = false;
+        while (!done) {
+          const int idx = pred - lane;
+          const bool inr = idx >= tb;
+          unsigned fl = 0;
+          unsigned long long spins = 0;
+          bool ok = !inr;
+          bool timed_out = false;
+          while (true) {
+            if (!ok) {
+              fl = *(volatile unsigned*)(e.lb_flag + idx);
+              ok = ((fl >> 2) == want) && ((fl & 3u) != 0u);
+            }
+            if (__all_sync(0xffffffffu, ok)) break;
+            if (++spins > e.spin_limit) {
+              timed_out = true;
+              break;
+            }
+            if (spins > 64) __nanosleep(64);
+          }
+          if (__any_sync(0xffffffffu, timed_out)) {
+            if (lane == 0) atomicOr(e.err, ERR_LOOKBACK_TIMEOUT);
+            break;
+          }
+          __threadfence();
+          unsigned long long val = 0;
+          const bool is_inc = inr && ((fl & 3u) == 2u);
+          if (inr) val = is_inc ? *(volatile unsigned long long*)(e.lb_inc + idx)
+                                : *(volatile unsigned long long*)(e.lb_agg + idx);
+          const unsigned inc_mask = __ballot_sync(0xffffffffu, is_inc);
+          if (inc_mask) {
+            const int first = __ffs(inc_mask) - 1;  // closest predecessor with a prefix
+            if (lane > first) val = 0;
+            done = true;
+          }
+          excl += warp_sum_u64(val);
+          pred -= 32;
+          if (pred < tb) done = true;
+        }
+        if (lane == 0) {
+          e.lb_inc[t] = excl + tot;
+          __threadfence();
+          atomicExch(e.lb_flag + t, tag | 2u);
+        }
+      }
+      if (lane == 0) {
+        e.tile_excl[t] = excl;
+        if (j == fd->n_tiles - 1) fc->wq_total = excl + tot;
+      }
+    }
+  }
+  queue_exit(q);
+}
+
+// -------------------------------------------------------------------------
+// k_offs: inclusive CDF of every particle, its offspring end F(i), and the
+// merge-path partition points of the filter's diagonal tiles.
+__global__ void __launch_bounds__(kThreads) k_offs(EngineDev e, int t0, int count) {
+  __shared__ unsigned long long s_u64[kThreads / 32];
+  __shared__ int s_slot;
+  unsigned* q = e.queue + 2 * Q_OFFS;
+  for (;;) {
+    const int tq = dequeue(q, &s_slot);
+    if (tq >= count) break;
+    const int t = t0 + tq;
+    const int f = __ldg(e.tile_filter + t);
+    const FilterDesc* fd = e.desc + f;
+    const FilterCtrl* fc = e.ctrl + f;
+    if (!fc->resample_flag) continue;
+    const int n = fd->n, K = fd->K;
+    const float M = fc->max_lw;
+    const unsigned long long W = fc->wq_total;
+    const uint32_t u = fc->sys_u;
+    const int tb = fd->tile_begin, j = t - tb;
+    const int p0 = j * kTile + (int)threadIdx.x * 4;
+    const long long base = fd->p_off;
+    unsigned long long qv[4] = {0, 0, 0, 0};
+    if (p0 < n) {
+      float4 v = __ldcg(reinterpret_cast<const float4*>(e.lw + base + p0));
+      float l[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (p0 + k < n) qv[k] = quantize_weight(l[k], M, K);
+    }
+    unsigned long long tot;
+    const unsigned long long texcl = block_excl_scan_u64(qv[0] + qv[1] + qv[2] + qv[3], s_u64, &tot);
+    if (p0 < n) {
+      if (W == 0ull) {
+        if (threadIdx.x == 0) atomicOr(e.err, ERR_BAD_WEIGHTS);
+        continue;
+      }
+      unsigned long long C = __ldcg(e.tile_excl + t) + texcl;
+      uint32_t Fprev = (p0 == 0) ? 0u : offspring_end(C, W, (uint32_t)n, u);
+      uint32_t Fk[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        C += qv[k];
+        Fk[k] = (p0 + k < n) ? offspring_end(C, W, (uint32_t)n, u) : (uint32_t)n;
+      }
+      *reinterpret_cast<uint4*>(e.offs + base + p0) = make_uint4(Fk[0], Fk[1], Fk[2], Fk[3]);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const long long i = p0 + k;
+        if (i >= n) break;
+        const long long hprev = i - 1 + (long long)Fprev;
+        const long long h = i + (long long)Fk[k];
+        long long c = (hprev < 0) ? 0 : hprev / kMergeDiag + 1;
+        for (; c * kMergeDiag <= h; ++c) e.mp_part[tb + c] = (uint32_t)i;
+        Fprev = Fk[k];
+      }
+    }
+  }
+  queue_exit(q);
+}
+
+// -------------------------------------------------------------------------
+// k_merge: walk the merge path of (offspring ends F, slots) over a window of
+// 2*kTile diagonals; slot k gets ancestor i when F(i-1) <= k < F(i).
+__global__ void __launch_bounds__(kThreads) k_merge(EngineDev e, int t0, int count) {
+  constexpr int kSteps = kMergeDiag / kThreads;  // 8
+  __shared__ uint32_t s_F[kMergeDiag + 1];
+  __shared__ int s_slot;
+  unsigned* q = e.queue + 2 * Q_MERGE;
+  for (;;) {
+    const int tq = dequeue(q, &s_slot);
+    if (tq >= count) break;
+    const int t = t0 + tq;
+    const int f = __ldg(e.tile_filter + t);
+    const FilterDesc* fd = e.desc + f;
+    const FilterCtrl* fc = e.ctrl + f;
+    if (!fc->resample_flag) continue;
+    const int n = fd->n;
+    const int tb = fd->tile_begin, c = t - tb;
+    const long long base = fd->p_off;
+    const long long d0 = (long long)c * kMergeDiag;
+    const long long dend = min(d0 + kMergeDiag, 2ll * n);
+    const int i0 = (int)__ldcg(e.mp_part + t);
+    if (i0 < 0 || i0 >= n) {  // cannot happen with valid weights; never index with it
+      if (threadIdx.x == 0) atomicOr(e.err, ERR_BAD_WEIGHTS);
+      continue;
+    }
+    const int win = min(kMergeDiag + 1, n - i0);
+    for (int w = threadIdx.x; w < win; w += kThreads) s_F[w] = __ldcg(e.offs + base + i0 + w);
+    __syncthreads();
+    const long long d = d0 + (long long)threadIdx.x * kSteps;
+    if (d < dend) {
+      int lo = 0, hi = (int)min((long long)(win - 1), d - d0);
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if ((long long)(i0 + mid) + (long long)s_F[mid] >= d) hi = mid;
+        else lo = mid + 1;
+      }
+      int i = i0 + lo;
+      long long k = d - i;
+      const int steps = (int)min((long long)kSteps, dend - d);
+      for (int s = 0; s < steps; ++s) {
+        const int wi = i - i0;
+        if (wi >= win) break;
+        if (k < (long long)s_F[wi]) {
+          if (k >= 0 && k < n) e.anc[base + k] = i;
+          ++k;
+        } else {
+          ++i;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  queue_exit(q);
+}
+
+// -------------------------------------------------------------------------
+// k_mego: Megopolis (Chesser et al., arXiv:2109.13504) with the ancestor and
+// its log-weight in registers.  Iteration b proposes j = (k + o_{b,g}) mod N
+// with one random offset per (iteration, 32-slot segment g), so a warp reads
+// 32 consecutive candidate weights, and accepts with probability
+// min(1, w_j / w_ancestor).
+__global__ void __launch_bounds__(kThreads) k_mego(EngineDev e, int t0, int count) {
+  __shared__ int s_slot;
+  unsigned* q = e.queue + 2 * Q_MEGO;
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    const int tq = dequeue(q, &s_slot);
+    if (tq >= count) break;
+    const int t = t0 + tq;
+    const int f = __ldg(e.tile_filter + t);
+    const FilterDesc* fd = e.desc + f;
+    const FilterCtrl* fc = e.ctrl + f;
+    if (!fc->resample_flag) continue;
+    const int n = fd->n;
+    const int j = t - fd->tile_begin;
+    const long long base = fd->p_off;
+    const unsigned epoch = fc->epoch - 1u;  // the step that decided to resample
+    const uint32_t fid = (uint32_t)fd->filter_id;
+    const int B = e.mego_iters;
+    const float* lw = e.lw + base;
+#pragma unroll 1
+    for (int r = 0; r < 4; ++r) {
+      const int seg0 = j * kTile + r * kThreads + ((int)threadIdx.x & ~31);  // warp's first slot
+      if (seg0 >= n) continue;  // whole warp past the filter's end
+      const int k_real = seg0 + lane;
+      const bool valid = k_real < n;
+      const int k = valid ? k_real : seg0;  // lanes past the end shadow a valid slot
+      const uint32_t g = (uint32_t)(seg0 / 32);
+      // lane l draws the offsets of iterations 4l .. 4l+3 of this segment
+      U4 ol = philox10(U4{g, epoch, TAG_MEGO_OFF | (uint32_t)lane, fid}, fd->key0, fd->key1);
+      int a = k;
+      float la = __ldg(lw + k);
+#pragma unroll 1
+      for (int b0 = 0; b0 < B; b0 += 4) {
+        U4 ur = philox10(U4{(uint32_t)k, epoch, TAG_MEGO_U | (uint32_t)(b0 >> 2), fid}, fd->key0, fd->key1);
+        const uint32_t uw[4] = {ur.x, ur.y, ur.z, ur.w};
+#pragma unroll
+        for (int bb = 0; bb < 4; ++bb) {
+          if (b0 + bb >= B) break;
+          const int src_lane = (b0 + bb) >> 2;
+          const uint32_t ow = (bb == 0) ? ol.x : (bb == 1) ? ol.y : (bb == 2) ? ol.z : ol.w;
+          const uint32_t o = __umulhi(__shfl_sync(0xffffffffu, ow, src_lane), (uint32_t)n);
+          int cand = k + (int)o;
+          if (cand >= n) cand -= n;
+          const float lc = __ldg(lw + cand);
+          const float lu = __logf(fmaf((float)uw[bb], 2.3283064365386963e-10f, 1.1641532182693481e-10f));
+          if (lc - la > lu) {
+            a = cand;
+            la = lc;
+          }
+        }
+      }
+      if (valid) e.anc[base + k] = a;
+    }
+  }
+  queue_exit(q);
+}
+
+// -------------------------------------------------------------------------
+// k_init: N(0, spread) offsets about the anchor into state buffer 0.
+template <int D>
+__global__ void __launch_bounds__(kThreads) k_init(EngineDev e, int t0, int count,
+                                                    float spread_pos, float spread_clk) {
+  __shared__ int s_slot;
+  unsigned* q = e.queue + 2 * Q_INIT;
+  for (;;) {
+    const int tq = dequeue(q, &s_slot);
+    if (tq >= count) break;
+    const int t = t0 + tq;
+    const int f = __ldg(e.tile_filter + t);
+    const FilterDesc* fd = e.desc + f;
+    const int n = fd->n, j = t - fd->tile_begin;
+    const int p0 = j * kTile + (int)threadIdx.x * 4;
+    if (p0 >= n) continue;
+    const long long base = fd->p_off;
+    const uint32_t fid = (uint32_t)fd->filter_id;
+    float x[D][4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      float nz[8];
+      U4 r = philox10(U4{(uint32_t)(p0 + k), 0u, TAG_INIT, fid}, fd->key0, fd->key1);
+      float2 a = box_muller_f32(r.x, r.y), b = box_muller_f32(r.z, r.w);
+      nz[0] = a.x; nz[1] = a.y; nz[2] = b.x; nz[3] = b.y;
+      if (D > 4) {
+        U4 r2 = philox10(U4{(uint32_t)(p0 + k), 0u, TAG_INIT | 1u, fid}, fd->key0, fd->key1);
+        float2 c = box_muller_f32(r2.x, r2.y), dd = box_muller_f32(r2.z, r2.w);
+        nz[4] = c.x; nz[5] = c.y; nz[6] = dd.x; nz[7] = dd.y;
+      } else {
+        nz[4] = nz[5] = nz[6] = nz[7] = 0.f;
+      }
+#pragma unroll
+      for (int d = 0; d < D; ++d) x[d][k] = (d < 3 ? spread_pos : spread_clk) * nz[d];
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+      *reinterpret_cast<float4*>(e.state0 + (size_t)d * e.p_total + base + p0) =
+          make_float4(x[d][0], x[d][1], x[d][2], x[d][3]);
+    *reinterpret_cast<float4*>(e.lw + base + p0) = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  queue_exit(q);
+}
+
+// -------------------------------------------------------------------------
+// k_estimate: weighted mean over the current particle set with the current
+// log-weights (zeros after a resample) -- the reference's pf_estimate
+// semantics (weight.cu:163-220,301-321) -- plus the ESS of those weights.
+template <int D>
+__global__ void __launch_bounds__(kThreads) k_estimate(EngineDev e, int t0, int count) {
+  __shared__ float s_red[kThreads / 32][kPartStride];
+  __shared__ float s_maxtmp[kThreads / 32];
+  __shared__ double s_dred[(kThreads / 32) * 16];
+  __shared__ int s_slot, s_last;
+  unsigned* q = e.queue + 2 * Q_EST;
+  for (;;) {
+    const int tq = dequeue(q, &s_slot);
+    if (tq >= count) break;
+    const int t = t0 + tq;
+    const int f = __ldg(e.tile_filter + t);
+    const FilterDesc* fd = e.desc + f;
+    FilterCtrl* fc = e.ctrl + f;
+    const int n = fd->n, j = t - fd->tile_begin;
+    const int p0 = j * kTile + (int)threadIdx.x * 4;
+    const long long base = fd->p_off;
+    const float* src = fc->parity ? e.state1 : e.state0;
+    float x[D][4];
+    float lwv[4];
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) x[d][k] = 0.f;
+    if (p0 < n) {
+      load_particles<D>(e, src, base, p0, n, fc->resample_flag != 0, x);
+      if (fc->lw_zero) {
+        lwv[0] = lwv[1] = lwv[2] = lwv[3] = 0.f;
+      } else {
+        float4 v = __ldcg(reinterpret_cast<const float4*>(e.lw + base + p0));
+        lwv[0] = v.x; lwv[1] = v.y; lwv[2] = v.z; lwv[3] = v.w;
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (p0 + k >= n) lwv[k] = -INFINITY;
+    } else {
+      lwv[0] = lwv[1] = lwv[2] = lwv[3] = -INFINITY;
+    }
+    tile_stats<D>(x, lwv, false, e.part + (size_t)t * kPartStride, s_maxtmp, s_red);
+    if (threadIdx.x == 0) {
+      __threadfence();
+      unsigned old = atomicAdd(&fc->est_ticket, 1u);
+      s_last = (old == (unsigned)fd->n_tiles - 1u);
+    }
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      MergedStats ms = merge_tiles<D>(e.part, fd->tile_begin, fd->n_tiles, s_maxtmp, s_dred);
+      if (threadIdx.x == 0) {
+        const double W = ms.w;
+        double est[3];
+        local_to_ecef(fd->rot, fc->anchor, ms.sx[0] / W, ms.sx[1] / W, ms.sx[2] / W, est);
+        fc->api_est[0] = est[0];
+        fc->api_est[1] = est[1];
+        fc->api_est[2] = est[2];
+#pragma unroll
+        for (int c = 0; c < D - 3; ++c) fc->api_est[3 + c] = fc->clk_anchor[c] + ms.sx[3 + c] / W;
+        fc->api_est[7] = (ms.w2 > 0.0) ? W * W / ms.w2 : 0.0;
+        fc->est_ticket = 0u;
+        __threadfence();
+      }
+      __syncthreads();
+    }
+  }
+  queue_exit(q);
+}
+
+// -------------------------------------------------------------------------
+// k_export: current particles as FP64 ECEF rows [n][D] (x, y, z, clocks),
+// the reference's pf_get_particles layout (weight.cu:331-340).
+template <int D>
+__global__ void __launch_bounds__(kThreads) k_export(EngineDev e, int t0, int count, double* out) {
+  __shared__ int s_slot;
+  unsigned* q = e.queue + 2 * Q_EXPORT;
+  for (;;) {
+    const int tq = dequeue(q, &s_slot);
+    if (tq >= count) break;
+    const int t = t0 + tq;
+    const int f = __ldg(e.tile_filter + t);
+    const FilterDesc* fd = e.desc + f;
+    const FilterCtrl* fc = e.ctrl + f;
+    const int n = fd->n, j = t - fd->tile_begin;
+    const int p0 = j * kTile + (int)threadIdx.x * 4;
+    if (p0 >= n) continue;
+    const long long base = fd->p_off;
+    const float* src = fc->parity ? e.state1 : e.state0;
+    float x[D][4];
+    load_particles<D>(e, src, base, p0, n, fc->resample_flag != 0, x);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (p0 + k >= n) break;
+      double p[3];
+      local_to_ecef(fd->rot, fc->anchor, (double)x[0][k], (double)x[1][k], (double)x[2][k], p);
+      double* o = out + (size_t)(p0 + k) * D;
+      o[0] = p[0];
+      o[1] = p[1];
+      o[2] = p[2];
+#pragma unroll
+      for (int c = 0; c < D - 3; ++c) o[3 + c] = fc->clk_anchor[c] + (double)x[3 + c][k];
+    }
+  }
+  queue_exit(q);
+}
+
+}  // namespace pfb

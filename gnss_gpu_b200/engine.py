@@ -1,0 +1,278 @@
+"""Device-resident particle-filter engine (one or many filters).
+
+Python side of the pfe_* C ABI.  PyTorch supplies the device workspace and the
+CUDA stream; every step runs the library's sm_100a kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+from . import _native as N
+
+
+@dataclass
+class FilterSpec:
+    n_particles: int
+    seed: int = 42
+    sigma_pos: Sequence[float] = (1.0, 1.0, 1.0)
+    sigma_clk: float = 300.0
+    sigma_pr: float = 5.0
+
+
+@dataclass
+class EngineOptions:
+    n_clk: int = 1
+    resampler: str = "systematic"          # "systematic" | "megopolis"
+    megopolis_iters: int = 15
+    weight_mode: str = "gaussian"          # "gaussian" | "huber"
+    huber_k: float = 1.5
+    lw_mode: str = "overwrite"             # "overwrite" (reference) | "accumulate"
+    sys_offset: str = "random"             # "random" | "reference"
+    max_sats: int = 64
+    obs_slots: int = 1
+    covariance: bool = True
+    recenter: bool = True
+    ess_threshold: float = 0.5
+
+
+def _torch():
+    import torch  # noqa: WPS433 (import on use: torch is only the buffer/stream provider)
+    if not torch.cuda.is_available():
+        raise RuntimeError("CUDA is not available: the B200 particle filter has no CPU path")
+    return torch
+
+
+class Engine:
+    """Many independent filters advanced together by fused kernels."""
+
+    def __init__(self, filters: Sequence[FilterSpec], options: EngineOptions | None = None,
+                 stream=None, device=None):
+        torch = _torch()
+        self._torch = torch
+        self.lib = N.load()
+        self.opt = options or EngineOptions()
+        self.filters = list(filters)
+        o = self.opt
+        cfg = N.EngineConfig()
+        cfg.n_filters = len(self.filters)
+        cfg.n_clk = int(o.n_clk)
+        cfg.resampler = {"systematic": N.PF_RESAMPLE_SYSTEMATIC, "megopolis": N.PF_RESAMPLE_MEGOPOLIS}[o.resampler]
+        cfg.megopolis_iters = int(o.megopolis_iters)
+        cfg.weight_mode = {"gaussian": N.PF_WEIGHT_GAUSSIAN, "huber": N.PF_WEIGHT_HUBER}[o.weight_mode]
+        cfg.lw_mode = {"overwrite": N.PF_LW_OVERWRITE, "accumulate": N.PF_LW_ACCUMULATE}[o.lw_mode]
+        cfg.sys_offset = {"random": N.PF_SYS_OFFSET_RANDOM, "reference": N.PF_SYS_OFFSET_REFERENCE}[o.sys_offset]
+        cfg.max_sats = int(o.max_sats)
+        cfg.obs_slots = int(o.obs_slots)
+        cfg.flags = (N.PF_FLAG_COVARIANCE if o.covariance else 0) | (N.PF_FLAG_RECENTER if o.recenter else 0)
+        cfg.ess_threshold = float(o.ess_threshold)
+        cfg.huber_k = float(o.huber_k)
+        self.cfg = cfg
+        self.D = 3 + cfg.n_clk
+        self.params = (N.FilterParams * len(self.filters))()
+        for k, f in enumerate(self.filters):
+            self._fill_params(self.params[k], f)
+        nbytes = C.c_size_t(0)
+        N.check(self.lib.pfe_workspace_bytes(C.byref(cfg), self.params, C.byref(nbytes)))
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        self.workspace = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
+        self.stream = stream if stream is not None else torch.cuda.Stream(device=self.device)
+        h = C.c_void_p()
+        with torch.cuda.device(self.device):
+            N.check(self.lib.pfe_create(C.byref(cfg), self.params, C.c_void_p(self.workspace.data_ptr()),
+                                        nbytes, C.c_void_p(self.stream.cuda_stream), C.byref(h)))
+        self.h = h
+        slot = C.c_size_t(0)
+        N.check(self.lib.pfe_obs_slot_bytes(self.h, C.byref(slot)))
+        self.obs_slot_bytes = int(slot.value)
+        self._results = (N.FilterResult * len(self.filters))()
+
+    @staticmethod
+    def _fill_params(p, f: FilterSpec):
+        p.n_particles = int(f.n_particles)
+        p.seed = int(f.seed) & 0xFFFFFFFFFFFFFFFF
+        sp = list(f.sigma_pos) if np.ndim(f.sigma_pos) else [float(f.sigma_pos)] * 3
+        for a in range(3):
+            p.sigma_pos[a] = float(sp[a])
+        p.sigma_clk = float(f.sigma_clk)
+        p.sigma_pr = float(f.sigma_pr)
+
+    # ------------------------------------------------------------ lifecycle
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pfe_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_filter_params(self, k: int, f: FilterSpec):
+        self.filters[k] = f
+        self._fill_params(self.params[k], f)
+        N.check(self.lib.pfe_set_filter_params(self.h, k, C.byref(self.params[k])))
+
+    def initialize(self, k: int, anchor_ecef, clk0=0.0, spread_pos=100.0, spread_clk=1000.0):
+        a = np.ascontiguousarray(anchor_ecef, dtype=np.float64).ravel()[:3].copy()
+        c = np.zeros(N.PF_MAX_CLK)
+        c[: self.cfg.n_clk] = np.broadcast_to(np.asarray(clk0, dtype=np.float64), (self.cfg.n_clk,))
+        N.check(self.lib.pfe_initialize(self.h, k, N.dptr(a), N.dptr(c), float(spread_pos), float(spread_clk)))
+
+    def frame(self, k: int):
+        rot = np.zeros(9)
+        anchor = np.zeros(3)
+        N.check(self.lib.pfe_get_frame(self.h, k, N.dptr(rot), N.dptr(anchor)))
+        return rot.reshape(3, 3), anchor
+
+    # ---------------------------------------------------------------- inputs
+    def pack_epoch(self, per_filter):
+        """per_filter: list of dicts with keys disp (3,), sats (S,3), pr (S,),
+        w (S,) [optional], clk (S,) [optional], flags (int)."""
+        F = len(self.filters)
+        fe = np.zeros(F, N.FILTER_EPOCH_DTYPE)
+        chunks = []
+        off = 0
+        for k, r in enumerate(per_filter):
+            fe["disp"][k] = np.asarray(r.get("disp", (0.0, 0.0, 0.0)), dtype=np.float64)
+            fe["flags"][k] = int(r.get("flags", N.PF_EP_PREDICT | N.PF_EP_WEIGHT))
+            sats = np.asarray(r.get("sats", np.zeros((0, 3))), dtype=np.float64).reshape(-1, 3)
+            s = len(sats)
+            fe["n_sat"][k] = s
+            fe["sat_offset"][k] = off
+            if s:
+                rec = np.zeros(s, N.SAT_DTYPE)
+                rec["x"], rec["y"], rec["z"] = sats[:, 0], sats[:, 1], sats[:, 2]
+                rec["pr"] = np.asarray(r["pr"], dtype=np.float64).ravel()
+                w = r.get("w")
+                rec["w"] = 1.0 if w is None else np.asarray(w, dtype=np.float64).ravel()
+                clk = r.get("clk")
+                rec["clk"] = 0 if clk is None else np.asarray(clk, dtype=np.int32).ravel()
+                chunks.append(rec)
+            off += s
+        sats_all = np.concatenate(chunks) if chunks else np.zeros(0, N.SAT_DTYPE)
+        return fe, sats_all
+
+    def upload(self, slot: int, fe: np.ndarray, sats: np.ndarray):
+        fe = np.ascontiguousarray(fe, dtype=N.FILTER_EPOCH_DTYPE)
+        sats = np.ascontiguousarray(sats, dtype=N.SAT_DTYPE)
+        N.check(self.lib.pfe_upload_obs(self.h, int(slot), N.vptr(fe), N.vptr(sats) if len(sats) else None,
+                                        len(sats)))
+
+    # ------------------------------------------------------------------ steps
+    def step(self):
+        N.check(self.lib.pfe_step(self.h))
+
+    def step_per_filter(self):
+        N.check(self.lib.pfe_step_per_filter(self.h))
+
+    def capture(self, per_filter: bool = False):
+        N.check(self.lib.pfe_graph_capture(self.h, 1 if per_filter else 0))
+
+    def replay(self, n: int = 1):
+        N.check(self.lib.pfe_graph_launch(self.h, int(n)))
+
+    def last_launch_count(self) -> int:
+        c = C.c_int(0)
+        N.check(self.lib.pfe_last_launch_count(self.h, C.byref(c)))
+        return int(c.value)
+
+    def synchronize(self):
+        self.stream.synchronize()
+
+    # ---------------------------------------------------------------- outputs
+    def results(self):
+        N.check(self.lib.pfe_read_results(self.h, self._results))
+        out = []
+        for r in self._results:
+            out.append({
+                "est_ecef": np.array(r.est_ecef[:]), "est_clk": np.array(r.est_clk[: self.cfg.n_clk]),
+                "cov_enu": np.array(r.cov_enu[:]), "ess": r.ess, "sum_w": r.sum_w, "max_lw": r.max_lw,
+                "resampled": bool(r.resampled), "epoch": r.epoch,
+            })
+        return out
+
+    def result_bytes(self) -> int:
+        b = C.c_size_t(0)
+        N.check(self.lib.pfe_result_bytes(self.h, C.byref(b)))
+        return int(b.value)
+
+    def estimate(self, k: int) -> np.ndarray:
+        out = np.zeros(self.D)
+        N.check(self.lib.pfe_estimate(self.h, k, N.dptr(out)))
+        return out
+
+    def ess(self, k: int) -> float:
+        v = C.c_double(0)
+        N.check(self.lib.pfe_get_ess(self.h, k, C.byref(v)))
+        return float(v.value)
+
+    def particles(self, k: int) -> np.ndarray:
+        n = self.filters[k].n_particles
+        out = np.zeros((n, self.D))
+        N.check(self.lib.pfe_get_particles(self.h, k, N.dptr(out)))
+        return out
+
+    def state_f32(self, k: int, raw: bool = False):
+        """(state [D][N] FP32 local offsets, lw [N] FP32).  raw=True returns
+        the buffers as the last step wrote them (before the resample gather)."""
+        n = self.filters[k].n_particles
+        st = np.zeros((self.D, n), np.float32)
+        lw = np.zeros(n, np.float32)
+        N.check(self.lib.pfe_get_state_f32(self.h, k, N.vptr(st), N.vptr(lw), 1 if raw else 0))
+        return st, lw
+
+    def anchor(self, k: int):
+        """(anchor ECEF (3,), clock anchors (n_clk,), pending shift (D,))."""
+        a = np.zeros(3)
+        c = np.zeros(N.PF_MAX_CLK)
+        sh = np.zeros(8, np.float32)
+        N.check(self.lib.pfe_get_anchor(self.h, k, N.dptr(a), N.dptr(c), sh.ctypes.data_as(C.POINTER(C.c_float))))
+        return a, c[: self.cfg.n_clk].copy(), sh[: self.D].copy()
+
+    def set_state_f32(self, k: int, state, lw=None):
+        st = np.ascontiguousarray(state, dtype=np.float32)
+        assert st.shape == (self.D, self.filters[k].n_particles)
+        lwa = None if lw is None else np.ascontiguousarray(lw, dtype=np.float32)
+        N.check(self.lib.pfe_set_state_f32(self.h, k, N.vptr(st), None if lwa is None else N.vptr(lwa)))
+
+    def ancestors(self, k: int) -> np.ndarray:
+        out = np.zeros(self.filters[k].n_particles, np.int32)
+        N.check(self.lib.pfe_get_ancestors(self.h, k, N.vptr(out)))
+        return out
+
+    def resample_info(self, k: int):
+        u = C.c_uint32(0)
+        w = C.c_uint64(0)
+        m = C.c_float(0)
+        N.check(self.lib.pfe_get_resample_info(self.h, k, C.byref(u), C.byref(w), C.byref(m)))
+        return int(u.value), int(w.value), float(m.value)
+
+    def error_word(self) -> int:
+        w = C.c_uint(0)
+        N.check(self.lib.pfe_error_word(self.h, C.byref(w)))
+        return int(w.value)
+
+    def set_spin_limit(self, limit: int):
+        N.check(self.lib.pfe_set_spin_limit(self.h, int(limit)))
+
+    def poison_lookback(self, on: bool):
+        N.check(self.lib.pfe_test_poison_lookback(self.h, 1 if on else 0))
+
+    def enable_timing(self, slots: int):
+        """Record CUDA events around the fused step kernel of each eager step."""
+        N.check(self.lib.pfe_enable_timing(self.h, int(slots)))
+        self._timing_slots = int(slots)
+
+    def read_timing(self):
+        """(fused step kernel ms, whole step ms) per step since the last read."""
+        n = max(1, getattr(self, "_timing_slots", 0))
+        a = (C.c_float * n)()
+        b = (C.c_float * n)()
+        c = C.c_int(0)
+        N.check(self.lib.pfe_read_timing(self.h, a, b, n, C.byref(c)))
+        return np.array(a[: c.value]), np.array(b[: c.value])

@@ -1,0 +1,299 @@
+/*
+ * gnss_pf_b200.h -- C ABI of the B200 (sm_100a) GNSS particle-filter step.
+ *
+ * Two groups of entry points live in libgnsspf_b200.so:
+ *
+ *  1. The stateless host-array functions `pf_*`.  Each one replaces the
+ *     function of the same name that the reference binds through pybind11
+ *     (include/gnss_gpu/particle_filter.h:15-64 of rsasaki0109/gnss_gpu,
+ *     bound in python/gnss_gpu/_particle_filter_bindings.cpp:10-145).  They take
+ *     caller-owned FP64 host arrays in the reference's SoA layout (px, py, pz,
+ *     pcb) and keep the reference's argument order and meaning.  They differ in
+ *     two visible ways: they return a status code instead of throwing, and the
+ *     random streams come from this library's Philox4x32-10 keyed by
+ *     (seed, particle, step) instead of cuRAND's, so draws are not bit-equal to
+ *     the reference's (only equal in distribution).
+ *
+ *  2. The device-resident engine `pfe_*`: FP32 ENU offsets about an FP64
+ *     anchor, one or many independent filters advanced by fused kernels,
+ *     ESS-conditional resampling decided on the device, CUDA-graph capture.
+ *     The Python `ParticleFilter` drop-in (gnss_gpu_b200/particle_filter.py)
+ *     runs on this group.
+ *
+ * Every function returns a pf_status_t; the message of the last failure on the
+ * calling thread is available from pf_last_error().  No function aborts or
+ * throws across the ABI.
+ */
+#ifndef GNSS_PF_B200_H
+#define GNSS_PF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PF_ABI_VERSION 1
+
+typedef enum {
+  PF_OK = 0,
+  PF_EINVAL = 1,    /* bad size, NaN/Inf input, sigma <= 0, bad enum      */
+  PF_ENOTINIT = 2,  /* engine filter used before pfe_initialize            */
+  PF_ECUDA = 3,     /* CUDA runtime error (message in pf_last_error)       */
+  PF_ETIMEOUT = 4,  /* a bounded device spin-wait gave up                  */
+  PF_ECAP = 5,      /* n_sat above the configured capacity                 */
+  PF_ENOMEM = 6     /* workspace too small / host allocation failed        */
+} pf_status_t;
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* pf_last_error(void);
+int pf_abi_version(void);
+
+/* ------------------------------------------------------------------------
+ * 1. Stateless host-array API (drop-in for the reference's _gnss_gpu_pf).
+ * All arrays are host memory, FP64, length n_particles unless stated.
+ * Calls are synchronous: on return the outputs are in host memory.
+ * ---------------------------------------------------------------------- */
+
+/* Replaces gnss_gpu::pf_initialize (include/gnss_gpu/particle_filter.h:15-19;
+ * kernel src/particle_filter/predict.cu:7-21). */
+int pf_initialize(double* px, double* py, double* pz, double* pcb,
+                  double init_x, double init_y, double init_z, double init_cb,
+                  double spread_pos, double spread_cb,
+                  int n_particles, unsigned long long seed);
+
+/* Replaces gnss_gpu::pf_predict (particle_filter.h:21-26; predict.cu:23-38).
+ * vx, vy, vz point to one element each (the velocity broadcast to every
+ * particle, predict.cu:33-37). */
+int pf_predict(double* px, double* py, double* pz, double* pcb,
+               const double* vx, const double* vy, const double* vz,
+               double dt, double sigma_pos, double sigma_cb,
+               int n_particles, unsigned long long seed, int step);
+
+/* Replaces gnss_gpu::pf_weight (particle_filter.h:28-35; weight.cu:13-57).
+ * Overwrites log_weights (weight.cu:56).  sat_ecef is [n_sat*3]. */
+int pf_weight(const double* px, const double* py, const double* pz,
+              const double* pcb, const double* sat_ecef,
+              const double* pseudoranges, const double* weights_sat,
+              double* log_weights, int n_particles, int n_sat,
+              double sigma_pr);
+
+/* Replaces gnss_gpu::pf_compute_ess (particle_filter.h:37-38;
+ * weight.cu:61-160).  The reference returns the ESS; here it is written to
+ * *ess_out. */
+int pf_compute_ess(const double* log_weights, int n_particles,
+                   double* ess_out);
+
+/* Replaces gnss_gpu::pf_resample_systematic (particle_filter.h:40-44;
+ * resampling.cu:60-168).  Keeps the reference's offset
+ * u0 = (seed % 1e6) / (1e6 * N) (resampling.cu:152) and its lower-bound
+ * predicate cdf[i] < (u0 + k) / N (resampling.cu:69-77), evaluated exactly
+ * on an integer CDF of quantised weights. */
+int pf_resample_systematic(double* px, double* py, double* pz, double* pcb,
+                           const double* log_weights, int n_particles,
+                           unsigned long long seed);
+
+/* Replaces gnss_gpu::pf_resample_megopolis (particle_filter.h:46-51;
+ * resampling.cu:175-272).  Keeps the reference's chain: per iteration a
+ * per-particle offset j = (k + 1 + floor(U (N-1))) mod N, acceptance against
+ * the slot's own log-weight, double-buffered copy. */
+int pf_resample_megopolis(double* px, double* py, double* pz, double* pcb,
+                          const double* log_weights, int n_particles,
+                          int n_iterations, unsigned long long seed);
+
+/* Replaces gnss_gpu::pf_estimate (particle_filter.h:53-58;
+ * weight.cu:163-220,264-328).  result is [4] = (x, y, z, cb). */
+int pf_estimate(const double* px, const double* py, const double* pz,
+                const double* pcb, const double* log_weights, double* result,
+                int n_particles);
+
+/* Replaces gnss_gpu::pf_get_particles (particle_filter.h:60-64;
+ * weight.cu:331-368).  output is [n_particles*4] interleaved. */
+int pf_get_particles(const double* px, const double* py, const double* pz,
+                     const double* pcb, double* output, int n_particles);
+
+/* ------------------------------------------------------------------------
+ * 2. Device-resident engine.
+ * No reference counterpart as a C ABI; it is the B200 implementation behind
+ * python/gnss_gpu/particle_filter.py:10-222 (ParticleFilter) and the batched
+ * many-filter step.
+ * ---------------------------------------------------------------------- */
+
+#define PF_MAX_CLK 4        /* clock states per filter (one per constellation) */
+#define PF_MAX_SATS 64      /* satellites per filter per epoch                 */
+#define PF_TILE 1024        /* particles per work tile                          */
+
+typedef enum { PF_RESAMPLE_SYSTEMATIC = 0, PF_RESAMPLE_MEGOPOLIS = 1 } pf_resampler_t;
+typedef enum { PF_WEIGHT_GAUSSIAN = 0, PF_WEIGHT_HUBER = 1 } pf_weight_mode_t;
+typedef enum { PF_LW_OVERWRITE = 0, PF_LW_ACCUMULATE = 1 } pf_lw_mode_t;
+typedef enum {
+  PF_SYS_OFFSET_RANDOM = 0,    /* Philox draw per filter and epoch            */
+  PF_SYS_OFFSET_REFERENCE = 1  /* (seed % 1e6) / (1e6 N), resampling.cu:152  */
+} pf_sys_offset_t;
+
+/* Engine flags. */
+#define PF_FLAG_COVARIANCE 1u  /* fused 3x3 position covariance in the step   */
+#define PF_FLAG_RECENTER 2u    /* re-anchor each filter at its weighted mean  */
+
+typedef struct {
+  int n_filters;
+  int n_clk;             /* 1..PF_MAX_CLK; state dimension D = 3 + n_clk     */
+  int resampler;         /* pf_resampler_t                                    */
+  int megopolis_iters;   /* iterations of the Megopolis chain                 */
+  int weight_mode;       /* pf_weight_mode_t                                  */
+  int lw_mode;           /* pf_lw_mode_t                                      */
+  int sys_offset;        /* pf_sys_offset_t                                   */
+  int max_sats;          /* capacity per filter per epoch, <= PF_MAX_SATS    */
+  int obs_slots;         /* resident epoch-input blocks (ring)                */
+  unsigned flags;        /* PF_FLAG_*                                         */
+  double ess_threshold;  /* resample when ESS < threshold * N                 */
+  double huber_k;        /* Huber threshold in sigmas (PF_WEIGHT_HUBER)       */
+} pf_engine_config_t;
+
+typedef struct {
+  int n_particles;
+  int pad_;
+  unsigned long long seed;
+  double sigma_pos[3];   /* predict noise per local axis (E, N, U), m         */
+  double sigma_clk;      /* predict noise of every clock state, m             */
+  double sigma_pr;       /* pseudorange sigma of the likelihood, m            */
+} pf_filter_params_t;
+
+/* Per-filter, per-epoch input record. */
+#define PF_EP_PREDICT 1        /* apply displacement + noise               */
+#define PF_EP_WEIGHT 2         /* evaluate the likelihood (else keep lw)   */
+#define PF_EP_FORCE_RESAMPLE 4 /* resample regardless of ESS               */
+#define PF_EP_NO_RESAMPLE 8    /* never resample this epoch                */
+typedef struct {
+  double disp[3];        /* displacement in the filter's local E/N/U frame, m */
+  int n_sat;
+  int sat_offset;        /* index of the first pf_sat_t of this filter        */
+  int flags;             /* PF_EP_*                                           */
+  int pad_;
+} pf_filter_epoch_t;
+
+typedef struct {
+  double x, y, z;        /* satellite ECEF, m                                 */
+  double pr;             /* pseudorange, m                                    */
+  double w;              /* per-satellite weight (1/sigma^2 scale), >= 0      */
+  int clk;               /* clock state index, 0..n_clk-1                     */
+  int pad_;
+} pf_sat_t;
+
+typedef struct {
+  double est_ecef[3];    /* fused weighted mean (pre-resample), ECEF          */
+  double est_clk[PF_MAX_CLK];
+  double cov_enu[6];     /* xx, xy, xz, yy, yz, zz of the local frame         */
+  double ess;
+  double sum_w;          /* sum of exp(lw - max_lw)                           */
+  float max_lw;
+  int resampled;         /* resampling ran in the last epoch                  */
+  unsigned epoch;        /* completed steps of this filter                    */
+  int initialized;
+} pf_filter_result_t;
+
+typedef struct pf_engine pf_engine_t;
+
+/* Bytes of device workspace pfe_create needs for this configuration. */
+int pfe_workspace_bytes(const pf_engine_config_t* cfg,
+                        const pf_filter_params_t* filters, size_t* bytes);
+
+/* Create an engine on the current CUDA device.  dev_workspace is caller-owned
+ * device memory of at least pfe_workspace_bytes (e.g. a torch uint8 tensor);
+ * it must outlive the engine.  stream is a cudaStream_t (NULL = legacy). */
+int pfe_create(const pf_engine_config_t* cfg,
+               const pf_filter_params_t* filters, void* dev_workspace,
+               size_t workspace_bytes, void* stream, pf_engine_t** out);
+int pfe_destroy(pf_engine_t* eng);
+int pfe_set_stream(pf_engine_t* eng, void* stream);
+int pfe_set_filter_params(pf_engine_t* eng, int filter,
+                          const pf_filter_params_t* params);
+
+/* Scatter N(0, spread) offsets about anchor_ecef / clk0 (n_clk values). */
+int pfe_initialize(pf_engine_t* eng, int filter, const double anchor_ecef[3],
+                   const double* clk0, double spread_pos, double spread_clk);
+
+/* ECEF -> local frame rotation of a filter (row-major 3x3, rows E, N, U). */
+int pfe_get_frame(pf_engine_t* eng, int filter, double rot[9],
+                  double anchor_ecef[3]);
+
+/* Copy one epoch's inputs (n_filters records + sats) from host memory into
+ * resident ring slot `slot` (async on the engine stream; the host buffers
+ * are staged, so they may be reused on return). */
+int pfe_upload_obs(pf_engine_t* eng, int slot, const pf_filter_epoch_t* fe,
+                   const pf_sat_t* sats, int n_sats_total);
+/* Bytes of one resident input slot. */
+int pfe_obs_slot_bytes(pf_engine_t* eng, size_t* bytes);
+
+/* One epoch for every filter: fused predict+weight+estimate, then the
+ * configured resampler where the device decided to resample.  The input
+ * block is ring slot (epoch % obs_slots). */
+int pfe_step(pf_engine_t* eng);
+/* The same kernels launched once per filter (comparison path). */
+int pfe_step_per_filter(pf_engine_t* eng);
+
+/* Capture one epoch (pfe_step, or pfe_step_per_filter if per_filter != 0)
+ * into a CUDA graph; pfe_graph_launch replays it n_epochs times. */
+int pfe_graph_capture(pf_engine_t* eng, int per_filter);
+int pfe_graph_launch(pf_engine_t* eng, int n_epochs);
+
+/* Copy per-filter results to host (synchronises the engine stream). */
+int pfe_read_results(pf_engine_t* eng, pf_filter_result_t* out);
+/* Bytes pfe_read_results copies from the device. */
+int pfe_result_bytes(pf_engine_t* eng, size_t* bytes);
+
+/* Weighted mean over the current particle set with the current log-weights
+ * (zero after a resample), as the reference's pf_estimate.  out is
+ * [3 + n_clk] in ECEF / m.  Synchronous. */
+int pfe_estimate(pf_engine_t* eng, int filter, double* out);
+/* ESS of the current log-weights (N after a resample).  Synchronous. */
+int pfe_get_ess(pf_engine_t* eng, int filter, double* out);
+/* Export particles as FP64 ECEF rows [N][3 + n_clk] into host memory. */
+int pfe_get_particles(pf_engine_t* eng, int filter, double* out_host);
+/* Local-frame FP32 state [D][N] and FP32 log-weights of a filter.
+ * raw == 0: the current particle set (gathered through the last resample's
+ * ancestors) and the current log-weights (zeros after a resample).
+ * raw != 0: the state buffer and log-weight array exactly as the last step
+ * wrote them (before the resample gather). */
+int pfe_get_state_f32(pf_engine_t* eng, int filter, float* out_host_DxN,
+                      float* out_lw_host, int raw);
+/* Committed anchor (ECEF), clock anchors [PF_MAX_CLK] and the pending
+ * re-centring shift [8] that the next step subtracts. */
+int pfe_get_anchor(pf_engine_t* eng, int filter, double anchor_ecef[3],
+                   double clk_anchor[PF_MAX_CLK], float shift[8]);
+/* Replace a filter's state: offsets [D][N] (FP32, local frame), lw (may be
+ * NULL = zeros).  Used for checkpoint/restore and tests. */
+int pfe_set_state_f32(pf_engine_t* eng, int filter, const float* state_DxN,
+                      const float* lw_or_null);
+/* Ancestor indices written by the last resample (host copy, N ints). */
+int pfe_get_ancestors(pf_engine_t* eng, int filter, int* out_host);
+/* Systematic offset (u32 fraction of a slot) and quantised weight total
+ * used by the last systematic resample. */
+int pfe_get_resample_info(pf_engine_t* eng, int filter, uint32_t* u32,
+                          uint64_t* wq_total, float* max_lw);
+/* Device error word (0 = fine); non-zero after a bounded spin gave up. */
+int pfe_error_word(pf_engine_t* eng, unsigned* word);
+/* Test hook: spin limit of the decoupled look-back (0 = default). */
+int pfe_set_spin_limit(pf_engine_t* eng, unsigned long long limit);
+/* Test hook: on != 0 makes the look-back wait for a tag that is never
+ * published, so its bounded spin runs out and sets the error word (no hang);
+ * on == 0 restores normal operation and clears the error word. */
+int pfe_test_poison_lookback(pf_engine_t* eng, int on);
+/* Kernels launched by the last pfe_step / pfe_step_per_filter. */
+int pfe_last_launch_count(pf_engine_t* eng, int* count);
+
+/* Device timing of eager steps: with slots > 0, each pfe_step records CUDA
+ * events on the engine stream before the fused step kernel, after it, and
+ * after the last resampling kernel, into a ring of `slots` entries
+ * (slots == 0 switches timing off).  pfe_read_timing synchronises and
+ * returns, for the steps since the last read (at most `slots`), the fused
+ * step kernel's duration and the whole step's duration in milliseconds. */
+int pfe_enable_timing(pf_engine_t* eng, int slots);
+int pfe_read_timing(pf_engine_t* eng, float* step_kernel_ms, float* whole_step_ms,
+                    int max_entries, int* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GNSS_PF_B200_H */

@@ -1,0 +1,239 @@
+"""ctypes wrapper of the FP64 CPU oracle (oracle/pf_oracle.c).
+
+Test infrastructure only: imported by tests/, by __graft_entry__.smoke() as the
+checker, and by bench.py's CPU-baseline leg.  The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+SRC = HERE / "pf_oracle.c"
+LIB = HERE / "liboracle.so"
+
+_lib = None
+
+F64 = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+F32 = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+I32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+U64 = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+U32 = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+
+TAG_SYS_U = 0x03000000
+
+
+def build(force: bool = False) -> Path:
+    if force or not LIB.exists() or LIB.stat().st_mtime < SRC.stat().st_mtime:
+        tmp = LIB.with_suffix(".so.tmp")
+        subprocess.run(["gcc", "-O2", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared",
+                        "-std=gnu11", str(SRC), "-o", str(tmp), "-lm"], check=True)
+        os.replace(tmp, LIB)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(str(LIB))
+        u32, i32, f32, f64 = C.c_uint32, C.c_int, C.c_float, C.c_double
+        P = C.c_void_p
+        L.orc_philox10.argtypes = [U32, u32, u32, U32]
+        L.orc_quant_exponent.argtypes = [i32]
+        L.orc_quant_exponent.restype = i32
+        L.orc_quantize.argtypes = [f32, f32, i32]
+        L.orc_quantize.restype = C.c_uint64
+        L.orc_quantize_all.argtypes = [F32, i32, f32, U64]
+        L.orc_systematic.argtypes = [F32, i32, f32, u32, I32, C.POINTER(C.c_uint64)]
+        L.orc_systematic.restype = i32
+        L.orc_megopolis.argtypes = [F32, i32, i32, u32, u32, u32, u32, I32]
+        L.orc_init.argtypes = [i32, i32, f32, f32, u32, u32, u32, F64]
+        L.orc_predict.argtypes = [i32, i32, F64, P, F64, F64, F32, i32, u32, u32, u32, u32, F64]
+        L.orc_weight.argtypes = [i32, i32, F64, F64, F64, F64, i32, F64, I32, f64, i32, f64, P, F64]
+        L.orc_stats.argtypes = [i32, i32, F64, F64, F64, F64, F64, F64]
+        L.orc_epoch.argtypes = [i32, i32, F64, F64, F64, F32, I32, F64, F64, F64, F64, F32, u32, u32,
+                                u32, i32, F64, I32, f64, f64, F64]
+        L.orc_epoch.restype = i32
+        L.orc_pf_initialize.argtypes = [F64, F64, F64, F64, f64, f64, f64, f64, f64, f64, i32, C.c_ulonglong]
+        L.orc_pf_predict.argtypes = [F64, F64, F64, F64, f64, f64, f64, f64, f64, f64, i32, C.c_ulonglong, i32]
+        L.orc_pf_weight.argtypes = [F64, F64, F64, F64, F64, F64, F64, F64, i32, i32, f64]
+        L.orc_pf_ess.argtypes = [F64, i32]
+        L.orc_pf_ess.restype = f64
+        L.orc_pf_estimate.argtypes = [F64, F64, F64, F64, F64, F64, i32]
+        L.orc_pf_systematic_ancestors.argtypes = [F64, i32, C.c_ulonglong, I32]
+        L.orc_pf_systematic_ancestors.restype = i32
+        L.orc_pf_megopolis_ref_ancestors.argtypes = [F64, i32, i32, C.c_ulonglong, I32]
+        L.orc_num_threads.restype = i32
+        L.orc_set_threads.argtypes = [i32]
+        _lib = L
+    return _lib
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+# ------------------------------------------------------------------ RNG
+def philox10(ctr, key):
+    out = np.zeros(4, np.uint32)
+    lib().orc_philox10(np.asarray(ctr, np.uint32), int(key[0]), int(key[1]), out)
+    return out
+
+
+def seed_key(seed: int):
+    seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    return seed & 0xFFFFFFFF, seed >> 32
+
+
+# ------------------------------------------------------------ quantiser
+def quant_exponent(n: int) -> int:
+    return int(lib().orc_quant_exponent(int(n)))
+
+
+def quantize(lw32, max_lw) -> np.ndarray:
+    lw32 = _f32(lw32)
+    q = np.zeros(len(lw32), np.uint64)
+    lib().orc_quantize_all(lw32, len(lw32), float(np.float32(max_lw)), q)
+    return q
+
+
+def systematic(lw32, max_lw, u32):
+    """Ancestor of every slot and the integer weight total."""
+    lw32 = _f32(lw32)
+    anc = np.zeros(len(lw32), np.int32)
+    w = C.c_uint64(0)
+    r = lib().orc_systematic(lw32, len(lw32), float(np.float32(max_lw)), int(u32), anc, C.byref(w))
+    if r != 0:
+        raise ValueError("all weights quantised to zero")
+    return anc, int(w.value)
+
+
+def megopolis(lw32, iters, seed, epoch, filter_id=0):
+    lw32 = _f32(lw32)
+    anc = np.zeros(len(lw32), np.int32)
+    k0, k1 = seed_key(seed)
+    lib().orc_megopolis(lw32, len(lw32), int(iters), k0, k1, int(epoch), int(filter_id), anc)
+    return anc
+
+
+# ----------------------------------------------------- engine semantics
+def init_state(n, D, spread_pos, spread_clk, seed, filter_id=0):
+    x = np.zeros(D * n, np.float64)
+    k0, k1 = seed_key(seed)
+    lib().orc_init(n, D, float(np.float32(spread_pos)), float(np.float32(spread_clk)), k0, k1,
+                   int(filter_id), x)
+    return x.reshape(D, n)
+
+
+def predict(x_prev, anc, disp, shift, sigma, do_predict, seed, epoch, filter_id=0):
+    x_prev = _f64(x_prev)
+    D, n = x_prev.shape
+    out = np.zeros((D, n), np.float64)
+    sh = np.zeros(8)
+    sh[:len(shift)] = shift
+    sg = np.zeros(8, np.float32)
+    sg[:len(sigma)] = sigma
+    anc_p = None if anc is None else np.ascontiguousarray(anc, np.int32)
+    k0, k1 = seed_key(seed)
+    lib().orc_predict(n, D, x_prev, None if anc_p is None else anc_p.ctypes.data, _f64(disp), sh, sg,
+                      int(bool(do_predict)), k0, k1, int(epoch), int(filter_id), out)
+    return out
+
+
+def weight(x, anchor, clk_anchor, rot, sats, clk, sigma_pr, mode=0, huber_k=1.5, lw_base=None):
+    """sats: (S, 5) rows x, y, z, pr, w."""
+    x = _f64(x)
+    D, n = x.shape
+    sats = _f64(sats).reshape(-1, 5)
+    ca = np.zeros(4)
+    ca[:len(clk_anchor)] = clk_anchor
+    out = np.zeros(n, np.float64)
+    base = None if lw_base is None else _f64(lw_base)
+    lib().orc_weight(n, D, x, _f64(anchor), ca, _f64(rot).ravel(), len(sats), sats.ravel(),
+                     np.ascontiguousarray(clk, np.int32), float(sigma_pr), int(mode), float(huber_k),
+                     None if base is None else base.ctypes.data, out)
+    return out
+
+
+def stats(x, lw, anchor, clk_anchor, rot):
+    x = _f64(x)
+    D, n = x.shape
+    ca = np.zeros(4)
+    ca[:len(clk_anchor)] = clk_anchor
+    out = np.zeros(24)
+    lib().orc_stats(n, D, x, _f64(lw), _f64(anchor), ca, _f64(rot).ravel(), out)
+    return {
+        "max_lw": out[0], "sum_w": out[1], "sum_w2": out[2], "ess": out[3],
+        "mean": out[4:4 + D].copy(), "est_ecef": out[11:14].copy(),
+        "est_clk": out[14:14 + D - 3].copy(), "cov": out[18:24].copy(),
+    }
+
+
+def sys_offset_random(seed, epoch, filter_id=0):
+    return int(philox10([0, epoch, TAG_SYS_U, filter_id], seed_key(seed))[0])
+
+
+# ------------------------------------------- reference host-array semantics
+def pf_initialize(init, init_cb, spread_pos, spread_cb, n, seed):
+    px, py, pz, pcb = (np.zeros(n) for _ in range(4))
+    lib().orc_pf_initialize(px, py, pz, pcb, float(init[0]), float(init[1]), float(init[2]),
+                            float(init_cb), float(spread_pos), float(spread_cb), int(n), int(seed))
+    return px, py, pz, pcb
+
+
+def pf_predict(px, py, pz, pcb, v, dt, sp, scb, seed, step):
+    px, py, pz, pcb = (_f64(a).copy() for a in (px, py, pz, pcb))
+    lib().orc_pf_predict(px, py, pz, pcb, float(v[0]), float(v[1]), float(v[2]), float(dt), float(sp),
+                         float(scb), len(px), int(seed), int(step))
+    return px, py, pz, pcb
+
+
+def pf_weight(px, py, pz, pcb, sat, pr, ws, sigma_pr):
+    lw = np.zeros(len(px))
+    sat = _f64(sat).ravel()
+    lib().orc_pf_weight(_f64(px), _f64(py), _f64(pz), _f64(pcb), sat, _f64(pr), _f64(ws), lw, len(px),
+                        len(_f64(pr)), float(sigma_pr))
+    return lw
+
+
+def pf_ess(lw):
+    lw = _f64(lw)
+    return float(lib().orc_pf_ess(lw, len(lw)))
+
+
+def pf_estimate(px, py, pz, pcb, lw):
+    out = np.zeros(4)
+    lib().orc_pf_estimate(_f64(px), _f64(py), _f64(pz), _f64(pcb), _f64(lw), out, len(px))
+    return out
+
+
+def pf_systematic_ancestors(lw, seed):
+    lw = _f64(lw)
+    anc = np.zeros(len(lw), np.int32)
+    if lib().orc_pf_systematic_ancestors(lw, len(lw), int(seed), anc) != 0:
+        raise ValueError("all weights quantised to zero")
+    return anc
+
+
+def pf_megopolis_ref_ancestors(lw, iters, seed):
+    lw = _f64(lw)
+    anc = np.zeros(len(lw), np.int32)
+    lib().orc_pf_megopolis_ref_ancestors(lw, len(lw), int(iters), int(seed), anc)
+    return anc
+
+
+def num_threads() -> int:
+    return int(lib().orc_num_threads())
+
+
+def set_threads(n: int):
+    lib().orc_set_threads(int(n))

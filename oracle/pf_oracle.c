@@ -1,0 +1,494 @@
+/*
+ * pf_oracle.c -- FP64 CPU restatement of the particle-filter step of
+ * rsasaki0109/gnss_gpu, used ONLY as test infrastructure: by tests/, by
+ * __graft_entry__.smoke() as the checker, and by bench.py's CPU-baseline leg.
+ * Nothing in the product links or calls it.
+ *
+ * Sources restated (paths inside the reference project):
+ *   predict.cu:7-21        init_kernel        -> orc_init
+ *   predict.cu:23-38       predict_kernel     -> orc_predict, orc_pf_predict
+ *   weight.cu:13-57        weight_kernel      -> orc_weight_*, orc_pf_weight
+ *   pf_device.cu:19-26     Huber cost         -> orc_weight_* (mode 1)
+ *   weight.cu:61-160       ESS                -> orc_stats, orc_pf_ess
+ *   weight.cu:163-328      weighted mean      -> orc_stats, orc_pf_estimate
+ *   resampling.cu:60-83,152 systematic search -> orc_systematic
+ *   resampling.cu:175-272  reference Megopolis -> orc_pf_megopolis_ref
+ *   Chesser et al. arXiv:2109.13504, canonical Megopolis -> orc_megopolis
+ *   particle_filter.py:129-175 update order   -> orc_epoch
+ * Random numbers: Philox4x32-10 from Salmon et al., SC'11, with this
+ * project's counter layout (particle, epoch, tag, filter), so the oracle and
+ * the CUDA path draw identical 32-bit words.  Normals: Box-Muller in FP64.
+ *
+ * Compile with -ffp-contract=off: orc_quantize must round exactly like the
+ * device's __fmul_rn/__fsub_rn/__fmaf_rn sequence.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define TAG_INIT 0x01000000u
+#define TAG_PREDICT 0x02000000u
+#define TAG_SYS_U 0x03000000u
+#define TAG_MEGO_OFF 0x04000000u
+#define TAG_MEGO_U 0x05000000u
+#define TAG_COMPAT_INIT 0x11000000u
+#define TAG_COMPAT_PREDICT 0x12000000u
+#define TAG_COMPAT_MEGO 0x13000000u
+
+/* ------------------------------------------------------------ Philox */
+void orc_philox10(const uint32_t in[4], uint32_t k0, uint32_t k1, uint32_t out[4]) {
+  uint32_t c0 = in[0], c1 = in[1], c2 = in[2], c3 = in[3];
+  for (int r = 0; r < 10; ++r) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+    uint32_t n1 = (uint32_t)p1;
+    uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+    uint32_t n3 = (uint32_t)p0;
+    c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+static void bm(uint32_t a, uint32_t b, double* n0, double* n1) {
+  const double two_m32 = 2.3283064365386963e-10;
+  double u1 = ((double)a + 0.5) * two_m32;
+  double u2 = (double)b * two_m32 - 0.5;
+  double r = sqrt(-2.0 * log(u1));
+  double th = 6.283185307179586476925286766559 * u2;
+  *n0 = r * cos(th);
+  *n1 = r * sin(th);
+}
+
+/* Eight normals of one particle: words of (p, epoch, tag|0) then (tag|1). */
+static void normals8(uint32_t p, uint32_t epoch, uint32_t tag, uint32_t fid, uint32_t k0,
+                     uint32_t k1, int need, double nz[8]) {
+  uint32_t c[4] = {p, epoch, tag, fid}, w[4];
+  orc_philox10(c, k0, k1, w);
+  bm(w[0], w[1], &nz[0], &nz[1]);
+  bm(w[2], w[3], &nz[2], &nz[3]);
+  if (need > 4) {
+    c[2] = tag | 1u;
+    orc_philox10(c, k0, k1, w);
+    bm(w[0], w[1], &nz[4], &nz[5]);
+    bm(w[2], w[3], &nz[6], &nz[7]);
+  } else {
+    nz[4] = nz[5] = nz[6] = nz[7] = 0.0;
+  }
+}
+
+/* ------------------------------------------------ deterministic quantiser */
+static float dsub(float a, float b) { volatile float r = a - b; return r; }
+static float dmul(float a, float b) { volatile float r = a * b; return r; }
+
+int orc_quant_exponent(int n) {
+  int lg = 0;
+  while ((1ll << lg) < (long long)n) ++lg;
+  int k = 62 - lg;
+  return k < 40 ? k : 40;
+}
+
+uint64_t orc_quantize(float lw, float max_lw, int K) {
+  float d = dsub(lw, max_lw);
+  float x = dmul(d, 1.44269504088896341f);
+  if (!(x > -40.0f)) return 0;
+  float n = floorf(x);
+  float f = dsub(x, n);
+  float p = 1.0178086009239699e-07f;
+  p = fmaf(p, f, 1.3215486790144307e-06f);
+  p = fmaf(p, f, 1.5252733804059840e-05f);
+  p = fmaf(p, f, 1.5403530393381606e-04f);
+  p = fmaf(p, f, 1.3333558146428443e-03f);
+  p = fmaf(p, f, 9.6181291076284772e-03f);
+  p = fmaf(p, f, 5.5504108664821580e-02f);
+  p = fmaf(p, f, 2.4022650695910071e-01f);
+  p = fmaf(p, f, 6.9314718055994531e-01f);
+  p = fmaf(p, f, 1.0f);
+  uint32_t P = (uint32_t)dmul(p, 8388608.0f);
+  int sh = K - 23 + (int)n;
+  return sh >= 0 ? ((uint64_t)P << sh) : ((uint64_t)P >> (-sh));
+}
+
+void orc_quantize_all(const float* lw, int n, float max_lw, uint64_t* q) {
+  const int K = orc_quant_exponent(n);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) q[i] = orc_quantize(lw[i], max_lw, K);
+}
+
+/* ------------------------------------------------------------ systematic
+ * resampling.cu:69-77: for slot k the lower-bound search over [0, N-1]
+ * for the first i with !(cdf[i] < (u + k)/N).  With an integer CDF C and
+ * total W the comparison is exact: C_i*N*2^32 < (k*2^32 + u32)*W.
+ * Returns 0 on success, -1 if every weight quantised to zero. */
+int orc_systematic(const float* lw, int n, float max_lw, uint32_t u32, int* anc, uint64_t* wq_out) {
+  uint64_t* C = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)n);
+  if (!C) return -2;
+  orc_quantize_all(lw, n, max_lw, C);
+  uint64_t acc = 0;
+  for (int i = 0; i < n; ++i) {
+    acc += C[i];
+    C[i] = acc;
+  }
+  const uint64_t W = acc;
+  if (wq_out) *wq_out = W;
+  if (W == 0) {
+    free(C);
+    return -1;
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < n; ++k) {
+    const unsigned __int128 rhs = (unsigned __int128)((((uint64_t)k) << 32) | u32) * W;
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      int mid = (lo + hi) / 2;
+      unsigned __int128 lhs = ((unsigned __int128)C[mid] * (uint64_t)n) << 32;
+      if (lhs < rhs) lo = mid + 1;
+      else hi = mid;
+    }
+    anc[k] = lo;
+  }
+  free(C);
+  return 0;
+}
+
+/* ------------------------------------------------------ canonical Megopolis
+ * Chesser et al. (arXiv:2109.13504): for each slot k the chain starts at
+ * ancestor k; iteration b proposes j = (k + o_{b,g}) mod N with an offset
+ * shared by the 32-slot segment g = k / 32 and accepts with probability
+ * min(1, w_j / w_ancestor). */
+void orc_megopolis(const float* lw, int n, int iters, uint32_t k0, uint32_t k1, uint32_t epoch,
+                   uint32_t fid, int* anc) {
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < n; ++k) {
+    const uint32_t g = (uint32_t)(k / 32);
+    int a = k;
+    double la = (double)lw[k];
+    uint32_t ow[4], uw[4];
+    for (int b = 0; b < iters; ++b) {
+      if ((b & 3) == 0) {
+        uint32_t co[4] = {g, epoch, TAG_MEGO_OFF | (uint32_t)(b >> 2), fid};
+        orc_philox10(co, k0, k1, ow);
+        uint32_t cu[4] = {(uint32_t)k, epoch, TAG_MEGO_U | (uint32_t)(b >> 2), fid};
+        orc_philox10(cu, k0, k1, uw);
+      }
+      const uint32_t o = (uint32_t)(((uint64_t)ow[b & 3] * (uint64_t)(uint32_t)n) >> 32);
+      int cand = k + (int)o;
+      if (cand >= n) cand -= n;
+      const double lc = (double)lw[cand];
+      const double u = ((double)uw[b & 3] + 0.5) * 2.3283064365386963e-10;
+      if (log(u) < lc - la) {
+        a = cand;
+        la = lc;
+      }
+    }
+    anc[k] = a;
+  }
+}
+
+/* ------------------------------------------------------ engine-semantics step
+ * State: D = 3 + nclk components (local E, N, U offsets about an ECEF anchor
+ * with rotation rot (rows E, N, U), then clock offsets about clk_anchor).
+ */
+void orc_local_to_ecef(const double rot[9], const double anchor[3], double e, double nn, double u,
+                       double out[3]) {
+  out[0] = anchor[0] + rot[0] * e + rot[3] * nn + rot[6] * u;
+  out[1] = anchor[1] + rot[1] * e + rot[4] * nn + rot[7] * u;
+  out[2] = anchor[2] + rot[2] * e + rot[5] * nn + rot[8] * u;
+}
+
+/* predict.cu:7-21 -- N(0, spread) about the anchor. */
+void orc_init(int n, int D, float spread_pos, float spread_clk, uint32_t k0, uint32_t k1,
+              uint32_t fid, double* x) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    double nz[8];
+    normals8((uint32_t)i, 0u, TAG_INIT, fid, k0, k1, D, nz);
+    for (int d = 0; d < D; ++d) x[(size_t)d * n + i] = (d < 3 ? (double)spread_pos : (double)spread_clk) * nz[d];
+  }
+}
+
+/* predict.cu:23-38 -- x += v dt + N(0, sigma), with the re-centring shift
+ * subtracted; src may be gathered through anc (the previous resample). */
+void orc_predict(int n, int D, const double* x_prev, const int* anc, const double* disp,
+                 const double* shift, const float* sigma, int do_predict, uint32_t k0, uint32_t k1,
+                 uint32_t epoch, uint32_t fid, double* x_out) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    const int a = anc ? anc[i] : i;
+    double nz[8];
+    if (do_predict) normals8((uint32_t)i, epoch, TAG_PREDICT, fid, k0, k1, D, nz);
+    for (int d = 0; d < D; ++d) {
+      double v = x_prev[(size_t)d * n + a] - shift[d];
+      if (do_predict) v += (d < 3 ? disp[d] : 0.0) + (double)sigma[d] * nz[d];
+      x_out[(size_t)d * n + i] = v;
+    }
+  }
+}
+
+/* weight.cu:13-57 (mode 0, Gaussian) and pf_device.cu:19-26 (mode 1, Huber):
+ * the residual pr - (|sat - p| + cb) in FP64 with p = anchor + R^T d.
+ * sats: [n_sat][5] = x, y, z, pr, w; clk[s] picks the clock state. */
+void orc_weight(int n, int D, const double* x, const double anchor[3], const double* clk_anchor,
+                const double rot[9], int n_sat, const double* sats, const int* clk, double sigma_pr,
+                int mode, double huber_k, const double* lw_base, double* lw_out) {
+  const double inv_s2 = 1.0 / (sigma_pr * sigma_pr);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    double p[3];
+    orc_local_to_ecef(rot, anchor, x[i], x[(size_t)n + i], x[(size_t)2 * n + i], p);
+    double acc = lw_base ? lw_base[i] : 0.0;
+    for (int s = 0; s < n_sat; ++s) {
+      const double* sv = sats + 5 * s;
+      const double dx = p[0] - sv[0], dy = p[1] - sv[1], dz = p[2] - sv[2];
+      const double r = sqrt(dx * dx + dy * dy + dz * dz);
+      const int c = clk[s];
+      const double cb = clk_anchor[c] + x[(size_t)(3 + c) * n + i];
+      const double res = sv[3] - (r + cb);
+      if (mode == 0) {
+        acc += -0.5 * sv[4] * res * res * inv_s2;
+      } else {
+        const double z = fabs(res) / sigma_pr;
+        const double rho = (z < huber_k) ? 0.5 * z * z : huber_k * z - 0.5 * huber_k * huber_k;
+        acc += -sv[4] * rho;
+      }
+    }
+    lw_out[i] = acc;
+  }
+  (void)D;
+}
+
+/* weight.cu:61-160,163-328 -- max-shifted sums.  out:
+ * [0] max lw, [1] W, [2] W2, [3] ESS, [4..4+D) weighted mean offsets,
+ * [11..14) ECEF estimate, [14..18) clock estimates, [18..24) 3x3 covariance
+ * (xx, xy, xz, yy, yz, zz) of the local frame. */
+void orc_stats(int n, int D, const double* x, const double* lw, const double anchor[3],
+               const double* clk_anchor, const double rot[9], double* out) {
+  double m = -INFINITY;
+  for (int i = 0; i < n; ++i)
+    if (lw[i] > m) m = lw[i];
+  double W = 0, W2 = 0, sx[7] = {0}, sxx[6] = {0};
+#pragma omp parallel
+  {
+    double w_ = 0, w2_ = 0, sx_[7] = {0}, sxx_[6] = {0};
+#pragma omp for schedule(static) nowait
+    for (int i = 0; i < n; ++i) {
+      const double w = exp(lw[i] - m);
+      w_ += w;
+      w2_ += w * w;
+      for (int d = 0; d < D; ++d) sx_[d] += w * x[(size_t)d * n + i];
+      const double e = x[i], nn = x[(size_t)n + i], u = x[(size_t)2 * n + i];
+      sxx_[0] += w * e * e; sxx_[1] += w * e * nn; sxx_[2] += w * e * u;
+      sxx_[3] += w * nn * nn; sxx_[4] += w * nn * u; sxx_[5] += w * u * u;
+    }
+#pragma omp critical
+    {
+      W += w_;
+      W2 += w2_;
+      for (int d = 0; d < 7; ++d) sx[d] += sx_[d];
+      for (int k = 0; k < 6; ++k) sxx[k] += sxx_[k];
+    }
+  }
+  memset(out, 0, sizeof(double) * 24);
+  out[0] = m;
+  out[1] = W;
+  out[2] = W2;
+  out[3] = W * W / W2;
+  double mu[7] = {0};
+  for (int d = 0; d < D; ++d) mu[d] = sx[d] / W;
+  for (int d = 0; d < D; ++d) out[4 + d] = mu[d];
+  orc_local_to_ecef(rot, anchor, mu[0], mu[1], mu[2], out + 11);
+  for (int c = 0; c < D - 3; ++c) out[14 + c] = clk_anchor[c] + mu[3 + c];
+  out[18] = sxx[0] / W - mu[0] * mu[0];
+  out[19] = sxx[1] / W - mu[0] * mu[1];
+  out[20] = sxx[2] / W - mu[0] * mu[2];
+  out[21] = sxx[3] / W - mu[1] * mu[1];
+  out[22] = sxx[4] / W - mu[1] * mu[2];
+  out[23] = sxx[5] / W - mu[2] * mu[2];
+}
+
+/* ------------------------------------------------------- full CPU epoch
+ * particle_filter.py:102-175 order on an FP64 state (the CPU baseline):
+ * predict, weight (overwrite), ESS, systematic resample (gather) when
+ * ESS < thr * N, weighted-mean estimate.  Returns 1 if it resampled. */
+int orc_epoch(int n, int D, double* x, double* x_tmp, double* lw, float* lw32, int* anc,
+              const double anchor[3], const double* clk_anchor, const double rot[9],
+              const double disp[3], const float* sigma, uint32_t k0, uint32_t k1, uint32_t epoch,
+              int n_sat, const double* sats, const int* clk, double sigma_pr, double ess_thr,
+              double* stats_out) {
+  static const double zero_shift[8] = {0};
+  orc_predict(n, D, x, NULL, disp, zero_shift, sigma, 1, k0, k1, epoch, 0u, x_tmp);
+  orc_weight(n, D, x_tmp, anchor, clk_anchor, rot, n_sat, sats, clk, sigma_pr, 0, 0.0, NULL, lw);
+  orc_stats(n, D, x_tmp, lw, anchor, clk_anchor, rot, stats_out);
+  int rs = stats_out[3] < ess_thr * (double)n;
+  if (rs) {
+    const double m = stats_out[0];
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) lw32[i] = (float)(lw[i] - m);
+    uint32_t c[4] = {0u, epoch, TAG_SYS_U, 0u}, w[4];
+    orc_philox10(c, k0, k1, w);
+    orc_systematic(lw32, n, 0.0f, w[0], anc, NULL);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i)
+      for (int d = 0; d < D; ++d) x[(size_t)d * n + i] = x_tmp[(size_t)d * n + anc[i]];
+  } else {
+    memcpy(x, x_tmp, sizeof(double) * (size_t)D * n);
+  }
+  return rs;
+}
+
+/* --------------------------------------- reference host-array semantics */
+void orc_pf_initialize(double* px, double* py, double* pz, double* pcb, double ix, double iy,
+                       double iz, double icb, double sp, double scb, int n, unsigned long long seed) {
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    uint32_t c[4] = {(uint32_t)i, 0u, TAG_COMPAT_INIT, 0u}, w[4];
+    orc_philox10(c, k0, k1, w);
+    double a0, a1, b0, b1;
+    bm(w[0], w[1], &a0, &a1);
+    bm(w[2], w[3], &b0, &b1);
+    px[i] = ix + a0 * sp;
+    py[i] = iy + a1 * sp;
+    pz[i] = iz + b0 * sp;
+    pcb[i] = icb + b1 * scb;
+  }
+}
+
+void orc_pf_predict(double* px, double* py, double* pz, double* pcb, double vx, double vy,
+                    double vz, double dt, double sp, double scb, int n, unsigned long long seed,
+                    int step) {
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    uint32_t c[4] = {(uint32_t)i, (uint32_t)step, TAG_COMPAT_PREDICT, 0u}, w[4];
+    orc_philox10(c, k0, k1, w);
+    double a0, a1, b0, b1;
+    bm(w[0], w[1], &a0, &a1);
+    bm(w[2], w[3], &b0, &b1);
+    px[i] += vx * dt + a0 * sp;
+    py[i] += vy * dt + a1 * sp;
+    pz[i] += vz * dt + b0 * sp;
+    pcb[i] += b1 * scb;
+  }
+}
+
+void orc_pf_weight(const double* px, const double* py, const double* pz, const double* pcb,
+                   const double* sat, const double* pr, const double* ws, double* lw, int n,
+                   int n_sat, double sigma_pr) {
+  const double inv_s2 = 1.0 / (sigma_pr * sigma_pr);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    double acc = 0.0;
+    for (int s = 0; s < n_sat; ++s) {
+      const double dx = px[i] - sat[3 * s], dy = py[i] - sat[3 * s + 1], dz = pz[i] - sat[3 * s + 2];
+      const double r = sqrt(dx * dx + dy * dy + dz * dz);
+      const double res = pr[s] - (r + pcb[i]);
+      acc += -0.5 * ws[s] * res * res * inv_s2;
+    }
+    lw[i] = acc;
+  }
+}
+
+double orc_pf_ess(const double* lw, int n) {
+  double m = -INFINITY;
+  for (int i = 0; i < n; ++i)
+    if (lw[i] > m) m = lw[i];
+  double s = 0, s2 = 0;
+  for (int i = 0; i < n; ++i) {
+    double w = exp(lw[i] - m);
+    s += w;
+    s2 += w * w;
+  }
+  return s * s / s2;
+}
+
+void orc_pf_estimate(const double* px, const double* py, const double* pz, const double* pcb,
+                     const double* lw, double* out, int n) {
+  double m = -INFINITY;
+  for (int i = 0; i < n; ++i)
+    if (lw[i] > m) m = lw[i];
+  double s = 0, a = 0, b = 0, c = 0, d = 0;
+  for (int i = 0; i < n; ++i) {
+    double w = exp(lw[i] - m);
+    s += w;
+    a += w * px[i];
+    b += w * py[i];
+    c += w * pz[i];
+    d += w * pcb[i];
+  }
+  out[0] = a / s;
+  out[1] = b / s;
+  out[2] = c / s;
+  out[3] = d / s;
+}
+
+/* resampling.cu:152 offset and :60-83 search, ancestors only. */
+int orc_pf_systematic_ancestors(const double* lw, int n, unsigned long long seed, int* anc) {
+  double m = -INFINITY;
+  for (int i = 0; i < n; ++i)
+    if (lw[i] > m) m = lw[i];
+  float* l32 = (float*)malloc(sizeof(float) * (size_t)n);
+  if (!l32) return -2;
+  for (int i = 0; i < n; ++i) l32[i] = (float)(lw[i] - m);
+  double u0 = (double)(seed % 1000000ull) / (1000000.0 * (double)n);
+  double v = floor(u0 * 4294967296.0);
+  uint32_t u32 = (uint32_t)(v < 0 ? 0 : (v > 4294967295.0 ? 4294967295.0 : v));
+  int r = orc_systematic(l32, n, 0.0f, u32, anc, NULL);
+  free(l32);
+  return r;
+}
+
+/* resampling.cu:175-272 chain on ancestor indices (the reference's
+ * acceptance against the slot's own weight), same Philox words as the
+ * CUDA stateless path. */
+static double u53(uint32_t a, uint32_t b) {
+  return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+void orc_pf_megopolis_ref_ancestors(const double* lw, int n, int iters, unsigned long long seed,
+                                    int* anc) {
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  int* a = (int*)malloc(sizeof(int) * (size_t)n);
+  int* b = (int*)malloc(sizeof(int) * (size_t)n);
+  for (int k = 0; k < n; ++k) a[k] = k;
+  for (int it = 0; it < iters; ++it) {
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < n; ++k) {
+      uint32_t c[4] = {(uint32_t)k, (uint32_t)it, TAG_COMPAT_MEGO, 0u}, w[4];
+      orc_philox10(c, k0, k1, w);
+      const double U1 = u53(w[0], w[1]), U2 = u53(w[2], w[3]);
+      const long long off = (long long)(U1 * (double)(n - 1)) + 1;
+      const int j = (int)(((long long)k + off) % n);
+      const double alpha = fmin(1.0, exp(lw[j] - lw[k]));
+      b[k] = (U2 < alpha) ? a[j] : a[k];
+    }
+    int* t = a;
+    a = b;
+    b = t;
+  }
+  memcpy(anc, a, sizeof(int) * (size_t)n);
+  free(a);
+  free(b);
+}
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}

@@ -1,0 +1,187 @@
+"""CPU tests: the FP64 oracle pinned against the reference's own code and
+fixtures, plus properties of the exact systematic predicate."""
+import numpy as np
+import pytest
+
+from conftest import TOKYO_SATS, TOKYO_PR, TOKYO_TRUE_POS, TOKYO_TRUE_CB
+from oracle import oracle as O
+
+GOLD = np.load(__import__("pathlib").Path(__file__).parent / "golden" / "simple_pf_cpu.npz")
+
+
+# --------------------------------------------------------------- Philox
+# Known-answer vectors of Philox4x32-10 published with the Random123 library
+# of Salmon et al. (SC'11).
+PHILOX_KAT = [
+    ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+    ((0xFFFFFFFF,) * 4, (0xFFFFFFFF, 0xFFFFFFFF), (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+    ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+     (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+]
+
+
+@pytest.mark.parametrize("ctr,key,want", PHILOX_KAT)
+def test_philox_known_answers(ctr, key, want):
+    assert tuple(int(v) for v in O.philox10(ctr, key)) == want
+
+
+def test_philox_matches_curand_fixture_if_present():
+    """Words of cuRAND's Philox4_32_10 (the reference's generator,
+    predict.cu:14-20) recorded on a GPU by tests/golden/make_curand_fixture.py."""
+    import json
+    from pathlib import Path
+    p = Path(__file__).parent / "golden" / "curand_philox.json"
+    if not p.exists():
+        pytest.skip("cuRAND fixture not generated yet")
+    d = json.loads(p.read_text())
+    for rec in d["records"]:
+        seed, subseq = rec["seed"], rec["subsequence"]
+        key = (seed & 0xFFFFFFFF, seed >> 32)
+        ctr = (0, 0, subseq & 0xFFFFFFFF, subseq >> 32)
+        words = []
+        c = list(ctr)
+        for _ in range(len(rec["words"]) // 4):
+            words.extend(int(v) for v in O.philox10(c, key))
+            c[0] = (c[0] + 1) & 0xFFFFFFFF
+        assert words == rec["words"], f"seed {seed} subsequence {subseq}"
+
+
+# ------------------------------------------------------------ weights
+def test_weight_matches_reference_simple_pf_cpu():
+    """Shifted log-likelihoods equal the reference CPU filter's
+    (experiments/evaluate.py:735-749) to FP64 round-off."""
+    for c in range(3):
+        parts = GOLD[f"c{c}_particles"]
+        ws = GOLD[f"c{c}_wsat"]
+        lw = O.pf_weight(parts[:, 0], parts[:, 1], parts[:, 2], parts[:, 3], TOKYO_SATS, TOKYO_PR, ws, 5.0)
+        got = lw - lw.max()
+        want = GOLD[f"c{c}_shifted_loglik"]
+        np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-7 * max(1.0, np.abs(want).max()) * 1e-3)
+
+
+def test_ess_and_estimate_match_reference_simple_pf_cpu():
+    for c in range(3):
+        parts = GOLD[f"c{c}_particles"]
+        lw = GOLD[f"c{c}_lw_rand"]
+        assert O.pf_ess(lw) == pytest.approx(float(GOLD[f"c{c}_ess"]), rel=1e-12)
+        est = O.pf_estimate(parts[:, 0], parts[:, 1], parts[:, 2], parts[:, 3], lw)
+        np.testing.assert_allclose(est, GOLD[f"c{c}_estimate"], rtol=1e-13, atol=1e-7)
+
+
+def test_gaussian_and_huber_known_answers():
+    """A 100 m outlier at sigma 5: Gaussian -200, Huber (k = 1.5) -28.875
+    (reference tests/test_cuda_streams.py:668-693)."""
+    sats = TOKYO_SATS[:5]
+    rng = np.linalg.norm(sats - TOKYO_TRUE_POS, axis=1)
+    pr = rng + TOKYO_TRUE_CB
+    pr[0] += 100.0
+    rot = np.eye(3)
+    x = np.zeros((4, 1))
+    rows = np.column_stack([sats, pr, np.ones(5)])
+    clk = np.zeros(5, np.int32)
+    g = O.weight(x, TOKYO_TRUE_POS, [TOKYO_TRUE_CB], rot, rows, clk, 5.0, mode=0)
+    h = O.weight(x, TOKYO_TRUE_POS, [TOKYO_TRUE_CB], rot, rows, clk, 5.0, mode=1, huber_k=1.5)
+    assert g[0] == pytest.approx(-200.0, abs=1e-6)
+    assert h[0] == pytest.approx(-28.875, abs=1e-6)
+
+
+def test_reference_scenario_near_beats_far():
+    """tests/test_particle_filter.py:136-168 of the reference, on the oracle."""
+    r = np.random.default_rng(42)
+    n = 1000
+    half = n // 2
+    px = np.r_[TOKYO_TRUE_POS[0] + r.normal(0, 1, half), TOKYO_TRUE_POS[0] + 1000 + r.normal(0, 1, half)]
+    py = np.r_[TOKYO_TRUE_POS[1] + r.normal(0, 1, half), TOKYO_TRUE_POS[1] + 1000 + r.normal(0, 1, half)]
+    pz = TOKYO_TRUE_POS[2] + r.normal(0, 1, n)
+    pcb = TOKYO_TRUE_CB + r.normal(0, 10, n)
+    lw = O.pf_weight(px, py, pz, pcb, TOKYO_SATS, TOKYO_PR, np.ones(8), 5.0)
+    assert lw[:half].mean() > lw[half:].mean()
+
+
+# -------------------------------------------------------- systematic
+def _slow_systematic(lw32, max_lw, u32):
+    """Pure-Python restatement of resampling.cu:60-83 on exact integers."""
+    q = [int(v) for v in O.quantize(lw32, max_lw)]
+    n = len(q)
+    C = np.cumsum(np.array(q, dtype=object))
+    W = int(C[-1])
+    anc = []
+    for k in range(n):
+        T = (k << 32) | u32
+        lo, hi = 0, n - 1
+        while lo < hi:
+            mid = (lo + hi) // 2
+            if (int(C[mid]) * n << 32) < T * W:
+                lo = mid + 1
+            else:
+                hi = mid
+        anc.append(lo)
+    return np.array(anc)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 7, 64, 257, 1000])
+def test_systematic_matches_slow_restatement(n):
+    r = np.random.default_rng(n)
+    lw = r.normal(0, 3, n).astype(np.float32)
+    u = int(r.integers(0, 2 ** 32))
+    anc, _ = O.systematic(lw, lw.max(), u)
+    np.testing.assert_array_equal(anc, _slow_systematic(lw, lw.max(), u))
+
+
+def test_systematic_agrees_with_float64_cdf_search():
+    """Away from exact ties the integer predicate reproduces the
+    reference's FP64 search (resampling.cu:143-158)."""
+    r = np.random.default_rng(7)
+    n = 5000
+    lw = r.normal(0, 2, n)
+    anc = O.pf_systematic_ancestors(lw, 12345)
+    w = np.exp(lw - lw.max())
+    cdf = np.cumsum(w / w.sum())
+    u0 = (12345 % 1000000) / (1000000.0 * n)
+    target = (u0 + np.arange(n)) / n
+    ref = np.minimum(np.searchsorted(cdf, target, side="left"), n - 1)
+    assert np.mean(anc == ref) > 0.999
+
+
+def test_systematic_offspring_counts_are_floor_or_ceil():
+    """Systematic resampling gives every particle floor(N w) or ceil(N w)
+    offspring (up to quantisation of w)."""
+    r = np.random.default_rng(3)
+    n = 4096
+    lw = r.normal(0, 1.5, n).astype(np.float32)
+    anc, W = O.systematic(lw, lw.max(), int(r.integers(0, 2 ** 32)))
+    q = O.quantize(lw, lw.max()).astype(np.float64)
+    expect = n * q / q.sum()
+    cnt = np.bincount(anc, minlength=n)
+    assert np.all(cnt >= np.floor(expect) - 1) and np.all(cnt <= np.ceil(expect) + 1)
+    assert np.all(np.diff(anc) >= 0)
+
+
+def test_quantiser_properties():
+    n = 1 << 20
+    K = O.quant_exponent(n)
+    assert K == 40
+    q = O.quantize(np.array([0.0, -0.5, -1.0, -27.0, -28.0, -100.0, np.nan], np.float32), 0.0)
+    assert q[0] == 1 << K
+    assert q[0] > q[1] > q[2] > q[3] > 0
+    assert q[5] == 0 and q[6] == 0
+    assert abs(q[2] / q[0] - np.exp(-1.0)) < 2e-6
+
+
+# ----------------------------------------------------------- megopolis
+def test_megopolis_prefers_heavy_particles():
+    n = 2000
+    lw = np.full(n, -10.0, np.float32)
+    lw[: n // 4] = 0.0
+    anc = O.megopolis(lw, 32, seed=5, epoch=0)
+    frac = np.mean(anc < n // 4)
+    # weight mass of the first quarter: 500 / (500 + 1500 e^-10) ~ 1
+    assert frac > 0.99
+
+
+def test_reference_megopolis_chain_prefers_heavy_particles():
+    n = 2000
+    lw = np.full(n, -10.0)
+    lw[: n // 4] = 0.0
+    anc = O.pf_megopolis_ref_ancestors(lw, 20, 12345)
+    assert np.mean(anc < n // 4) > 0.9
