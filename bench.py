@@ -247,6 +247,7 @@ def run_b200(args, world, rank, local, pg):
     barrier(pg)
     clk = clocks.stop()
     k_ms, step_ms = eng.read_timing()
+    per_kernel = eng.read_timing_kernels()
     assert len(step_ms) == K, (len(step_ms), K)
     total_s = float(np.sum(step_ms)) / 1e3
     total_s = reduce_max(pg, total_s)
@@ -307,6 +308,8 @@ def run_b200(args, world, rank, local, pg):
                           "achieved_gbs": value / world * b_alg / 1e9,
                           "frac_of_measured_peak": value / world * b_alg / 1e9 / peak,
                           "frac_of_nominal_8tbs": value / world * b_alg / 1e9 / 8000.0},
+        "kernel_ms_mean": dict(zip(["k_step", "k_scan" if resampler == "systematic" else "k_mego",
+                                    "k_offs", "k_merge"], [float(v) for v in per_kernel.mean(axis=0)])),
         "resampled_fraction": float(np.mean(resampled)),
         "p50_2d_error_m": float(np.median(errs)),
         "clocks": clk,

@@ -82,7 +82,7 @@ EXPORTED = [
     "pfe_estimate", "pfe_get_ess", "pfe_get_particles", "pfe_get_state_f32", "pfe_set_state_f32",
     "pfe_get_ancestors", "pfe_get_resample_info", "pfe_error_word", "pfe_set_spin_limit",
     "pfe_last_launch_count", "pfe_get_anchor", "pfe_test_poison_lookback", "pfe_enable_timing",
-    "pfe_read_timing", "pfe_result_bytes",
+    "pfe_read_timing", "pfe_result_bytes", "pfe_read_timing_kernels",
 ]
 
 _lib = None
@@ -145,6 +145,7 @@ def load():
     L.pfe_result_bytes.argtypes = [p, C.POINTER(C.c_size_t)]
     L.pfe_enable_timing.argtypes = [p, i]
     L.pfe_read_timing.argtypes = [p, C.POINTER(C.c_float), C.POINTER(C.c_float), i, C.POINTER(C.c_int)]
+    L.pfe_read_timing_kernels.argtypes = [p, C.POINTER(C.c_float), i, C.POINTER(C.c_int)]
     for name in EXPORTED:
         fn = getattr(L, name)
         if name not in ("pf_last_error",) and fn.restype is not C.c_char_p:

@@ -72,14 +72,32 @@ enum : uint32_t {
 };
 
 #ifdef __CUDACC__
-// Two standard normals from two 32-bit words (Box-Muller).  u1 lies in
-// (0, 1]; the angle is 2*pi*(b * 2^-32 - 1/2), inside [-pi, pi) where the
-// fast sine/cosine are accurate to about 2^-21.
+// Two standard normals from two 32-bit words (Box-Muller) with
+// u1 = (a + 1/2) 2^-32 in (0, 1) and angle 2*pi*(b 2^-32 - 1/2) in
+// [-pi, pi), where the fast sine/cosine are accurate to about 2^-21.
+// log(u1) keeps ~1e-7 relative accuracy over the whole range: below 0.75
+// the fast logarithm; from 0.75 up, u1 = 1 - v with v = (~a + 1/2) 2^-32
+// formed exactly and log(1 - v) = -2 atanh(s), s = v / (2 - v) <= 1/7,
+// from the odd series s + s^3/3 + ... + s^9/9.
+__device__ __forceinline__ float bm_log_u1(uint32_t a) {
+  const float two_m32 = 2.3283064365386963e-10f;
+  const float half_ulp = 1.1641532182693481e-10f;
+  const float u1 = fmaf((float)a, two_m32, half_ulp);
+  const float v = fmaf((float)(~a), two_m32, half_ulp);
+  const float s = __fdividef(v, 2.0f - v);
+  const float s2 = s * s;
+  float p = fmaf(s2, 1.0f / 9.0f, 1.0f / 7.0f);
+  p = fmaf(s2, p, 0.2f);
+  p = fmaf(s2, p, 1.0f / 3.0f);
+  p = fmaf(s2, p, 1.0f);
+  const float near_one = -2.0f * s * p;
+  return (a >= 0xC0000000u) ? near_one : __logf(u1);
+}
+
 __device__ __forceinline__ float2 box_muller_f32(uint32_t a, uint32_t b) {
   const float two_m32 = 2.3283064365386963e-10f;  // 2^-32
-  float u1 = fmaf((float)a, two_m32, 1.1641532182693481e-10f);  // (a+1/2) 2^-32
   float u2 = fmaf((float)b, two_m32, -0.5f);
-  float r = sqrtf(fmaxf(-2.0f * __logf(u1), 0.0f));
+  float r = sqrtf(fmaxf(-2.0f * bm_log_u1(a), 0.0f));
   float s, c;
   __sincosf(6.283185307179586f * u2, &s, &c);
   return make_float2(r * c, r * s);
@@ -97,29 +115,30 @@ __device__ __forceinline__ double2 box_muller_f64(uint32_t a, uint32_t b) {
 #endif
 
 // ------------------------------------------------ deterministic quantiser
-// Single-precision operations with round-to-nearest that neither the host
-// compiler nor nvcc may contract or reorder.
-PF_HD float det_sub(float a, float b) {
+// Double-precision operations with round-to-nearest that neither the host
+// compiler nor nvcc may contract or reorder, so host and device produce the
+// same bits.
+PF_HD double det_mul(double a, double b) {
 #ifdef __CUDA_ARCH__
-  return __fsub_rn(a, b);
+  return __dmul_rn(a, b);
 #else
-  volatile float r = a - b;
+  volatile double r = a * b;
   return r;
 #endif
 }
-PF_HD float det_mul(float a, float b) {
+PF_HD double det_sub(double a, double b) {
 #ifdef __CUDA_ARCH__
-  return __fmul_rn(a, b);
+  return __dsub_rn(a, b);
 #else
-  volatile float r = a * b;
+  volatile double r = a - b;
   return r;
 #endif
 }
-PF_HD float det_fma(float a, float b, float c) {
+PF_HD double det_fma(double a, double b, double c) {
 #ifdef __CUDA_ARCH__
-  return __fmaf_rn(a, b, c);
+  return __fma_rn(a, b, c);
 #else
-  return fmaf(a, b, c);
+  return fma(a, b, c);
 #endif
 }
 
@@ -132,28 +151,34 @@ PF_HD int quant_exponent(int n) {
   return k < 40 ? k : 40;
 }
 
-// q = floor(2^K * 2^x) with x = (lw - max) * log2(e), 2^frac(x) from its
-// Taylor series (coefficients (ln 2)^j / j!), Horner form with fma.
-// Weights below 2^-40 of the largest quantise to zero.
-PF_HD uint64_t quantize_weight(float lw, float max_lw, int K) {
-  float d = det_sub(lw, max_lw);
-  float x = det_mul(d, 1.44269504088896341f);
-  if (!(x > -40.0f)) return 0ull;  // also catches NaN
-  float n = floorf(x);
-  float f = det_sub(x, n);         // exact: f in [0, 1)
-  float p = 1.0178086009239699e-07f;
-  p = det_fma(p, f, 1.3215486790144307e-06f);
-  p = det_fma(p, f, 1.5252733804059840e-05f);
-  p = det_fma(p, f, 1.5403530393381606e-04f);
-  p = det_fma(p, f, 1.3333558146428443e-03f);
-  p = det_fma(p, f, 9.6181291076284772e-03f);
-  p = det_fma(p, f, 5.5504108664821580e-02f);
-  p = det_fma(p, f, 2.4022650695910071e-01f);
-  p = det_fma(p, f, 6.9314718055994531e-01f);
-  p = det_fma(p, f, 1.0f);
-  uint32_t P = (uint32_t)det_mul(p, 8388608.0f);  // p * 2^23, p in [1, 2]
-  int sh = K - 23 + (int)n;
-  return sh >= 0 ? ((uint64_t)P << sh) : ((uint64_t)P >> (-sh));
+// q = floor(2^K * exp(d)) for a shifted log-weight d = lw - max <= 0.
+// x = d * log2(e), n = floor(x), f = x - n (exact), t = f * ln 2, and
+// e^t = 2^f from the Taylor series of the exponential (coefficients 1/j!,
+// degree 13, truncation error < 1e-13 for t in [0, ln 2)) in Horner form
+// with fma; 2^n scales exactly.  Weights below 2^-40 of the largest
+// quantise to zero.
+PF_HD uint64_t quantize_shifted(double d, int K) {
+  const double x = det_mul(d, 1.4426950408889634074);
+  if (!(x > -40.0)) return 0ull;  // also catches NaN
+  const double n = floor(x);
+  const double f = det_sub(x, n);  // exact: f in [0, 1)
+  const double t = det_mul(f, 0.69314718055994530942);
+  double q = 1.6059043836821615e-10;  // 1/13!
+  q = det_fma(q, t, 2.0876756987868099e-09);  // 1/12!
+  q = det_fma(q, t, 2.5052108385441720e-08);  // 1/11!
+  q = det_fma(q, t, 2.7557319223985893e-07);  // 1/10!
+  q = det_fma(q, t, 2.7557319223985888e-06);  // 1/9!
+  q = det_fma(q, t, 2.4801587301587302e-05);  // 1/8!
+  q = det_fma(q, t, 1.9841269841269841e-04);  // 1/7!
+  q = det_fma(q, t, 1.3888888888888889e-03);  // 1/6!
+  q = det_fma(q, t, 8.3333333333333333e-03);  // 1/5!
+  q = det_fma(q, t, 4.1666666666666667e-02);  // 1/4!
+  q = det_fma(q, t, 1.6666666666666667e-01);  // 1/3!
+  q = det_fma(q, t, 0.5);
+  q = det_fma(q, t, 1.0);
+  q = det_fma(q, t, 1.0);  // e^t = 2^f in [1, 2]
+  const double v = ldexp(q, K + (int)n);  // exact scaling, <= 2^(K+1)
+  return (uint64_t)v;                     // truncation
 }
 
 // ------------------------------------------------ 128-bit exact compare

@@ -21,8 +21,8 @@
 
 namespace pfb {
 size_t systematic_scratch_bytes(int n);
-int systematic_ancestors(const float* d_lw32, int n, uint32_t u, int* d_anc, void* d_scratch,
-                         cudaStream_t st);
+int systematic_ancestors(const double* d_lw64, const double* d_max, int n, uint32_t u, int* d_anc,
+                         void* d_scratch, cudaStream_t st);
 }  // namespace pfb
 
 using namespace pfb;
@@ -233,12 +233,6 @@ __global__ void c_stats(const double* lw, const double* px, const double* py, co
     out[7] = gm;
     *ticket = 0u;
   }
-}
-
-__global__ void c_shift_f32(const double* lw, const double* stats, float* lw32, int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  lw32[i] = (float)(lw[i] - stats[7]);
 }
 
 __global__ void c_gather4(const double* ix, const double* iy, const double* iz, const double* icb,
@@ -483,7 +477,7 @@ int pf_resample_systematic(double* px, double* py, double* pz, double* pcb, cons
   const int n = n_particles;
   const size_t nb = (size_t)n * 8;
   const int g = grid_of(n);
-  const size_t need = 9 * align_up(nb, 256) + align_up((size_t)n * 4, 256) * 2 +
+  const size_t need = 9 * align_up(nb, 256) + align_up((size_t)n * 4, 256) +
                       align_up((size_t)g * 64, 256) + 512 + pfb::systematic_scratch_bytes(n) + 256;
   Workspace* w;
   if ((s = workspace(need, &w)) != PF_OK) return s;
@@ -491,7 +485,6 @@ int pf_resample_systematic(double* px, double* py, double* pz, double* pcb, cons
   double *ix = c.take<double>(n), *iy = c.take<double>(n), *iz = c.take<double>(n), *icb = c.take<double>(n);
   double *ox = c.take<double>(n), *oy = c.take<double>(n), *oz = c.take<double>(n), *ocb = c.take<double>(n);
   double* dlw = c.take<double>(n);
-  float* lw32 = c.take<float>(align_up(n, 4));
   int* anc = c.take<int>(n);
   double* rows = c.take<double>((size_t)g * 8);
   double* out = c.take<double>(8);
@@ -504,9 +497,8 @@ int pf_resample_systematic(double* px, double* py, double* pz, double* pcb, cons
   CK(cudaMemcpyAsync(dlw, log_weights, nb, cudaMemcpyHostToDevice, w->stream));
   CK(cudaMemsetAsync(ticket, 0, 16, w->stream));
   c_stats<<<g, kB, 0, w->stream>>>(dlw, nullptr, nullptr, nullptr, nullptr, n, rows, ticket, out);
-  c_shift_f32<<<g, kB, 0, w->stream>>>(dlw, out, lw32, n);
   CK(cudaGetLastError());
-  if ((s = pfb::systematic_ancestors(lw32, n, sys_u_reference(seed, n), anc, scratch, w->stream)) != PF_OK)
+  if ((s = pfb::systematic_ancestors(dlw, out + 7, n, sys_u_reference(seed, n), anc, scratch, w->stream)) != PF_OK)
     return s;
   c_gather4<<<g, kB, 0, w->stream>>>(ix, iy, iz, icb, ox, oy, oz, ocb, anc, n);
   CK(cudaMemcpyAsync(px, ox, nb, cudaMemcpyDeviceToHost, w->stream));

@@ -42,13 +42,18 @@ struct pf_engine {
   int last_launches = 0;
   std::vector<int> initialized;
   // timing ring (pfe_enable_timing)
-  std::vector<cudaEvent_t> tev;  // 3 per slot
+  std::vector<cudaEvent_t> tev;  // kTimingEvents per slot
+  std::vector<float> t_kernel_ms; // per-kernel durations of the last read
   int t_slots = 0;
   int t_next = 0;
   int t_pending = 0;
 };
 
 namespace {
+
+// events per timed step: before k_step, after k_step, after each of the
+// three resampling kernels
+constexpr int kTimingEvents = 5;
 
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -237,21 +242,27 @@ int launch_step(pf_engine* eng, int t0, int count) {
   }
 }
 
-int launch_resample(pf_engine* eng, int t0, int count, int* n_launch) {
+// ev (optional): events recorded after each resampling kernel (3 entries).
+int launch_resample(pf_engine* eng, int t0, int count, int* n_launch, cudaEvent_t* ev = nullptr) {
   if (eng->cfg.resampler == PF_RESAMPLE_SYSTEMATIC) {
     k_scan<<<grid_for(eng, Q_SCAN, count), kThreads, 0, eng->stream>>>(eng->dev, t0, count);
+    if (ev) cudaEventRecord(ev[0], eng->stream);
     k_offs<<<grid_for(eng, Q_OFFS, count), kThreads, 0, eng->stream>>>(eng->dev, t0, count);
+    if (ev) cudaEventRecord(ev[1], eng->stream);
     k_merge<<<grid_for(eng, Q_MERGE, count), kThreads, 0, eng->stream>>>(eng->dev, t0, count);
+    if (ev) cudaEventRecord(ev[2], eng->stream);
     *n_launch += 3;
   } else {
     k_mego<<<grid_for(eng, Q_MEGO, count), kThreads, 0, eng->stream>>>(eng->dev, t0, count);
+    if (ev) {
+      cudaEventRecord(ev[0], eng->stream);
+      cudaEventRecord(ev[1], eng->stream);
+      cudaEventRecord(ev[2], eng->stream);
+    }
     *n_launch += 1;
   }
   return check_cuda(cudaGetLastError(), "resample launch");
 }
-
-template <template <int> class Kn>
-struct DSwitch;
 
 int sync_and_check(pf_engine* eng) {
   CK(cudaStreamSynchronize(eng->stream));
@@ -590,7 +601,7 @@ int pfe_step(pf_engine_t* eng) {
   int n = 1;
   cudaEvent_t* ev = nullptr;
   if (eng->t_slots > 0) {
-    ev = &eng->tev[3 * (size_t)eng->t_next];
+    ev = &eng->tev[kTimingEvents * (size_t)eng->t_next];
     eng->t_next = (eng->t_next + 1) % eng->t_slots;
     eng->t_pending = std::min(eng->t_pending + 1, eng->t_slots);
     CK(cudaEventRecord(ev[0], eng->stream));
@@ -598,10 +609,18 @@ int pfe_step(pf_engine_t* eng) {
   int s = launch_step(eng, 0, eng->T);
   if (s != PF_OK) return s;
   if (ev) CK(cudaEventRecord(ev[1], eng->stream));
-  s = launch_resample(eng, 0, eng->T, &n);
+  s = launch_resample(eng, 0, eng->T, &n, ev ? ev + 2 : nullptr);
   if (s != PF_OK) return s;
-  if (ev) CK(cudaEventRecord(ev[2], eng->stream));
   eng->last_launches = n;
+  return PF_OK;
+}
+
+int pfe_read_timing_kernels(pf_engine_t* eng, float* out, int max_entries, int* count) {
+  clear_err();
+  if (!eng || !out || !count) return set_err(PF_EINVAL, "null argument");
+  const int n = std::min((int)(eng->t_kernel_ms.size() / (kTimingEvents - 1)), max_entries);
+  memcpy(out, eng->t_kernel_ms.data(), sizeof(float) * (size_t)n * (kTimingEvents - 1));
+  *count = n;
   return PF_OK;
 }
 
@@ -617,7 +636,7 @@ int pfe_enable_timing(pf_engine_t* eng, int slots) {
   eng->t_next = 0;
   eng->t_pending = 0;
   if (slots == 0) return PF_OK;
-  eng->tev.resize(3 * (size_t)slots, nullptr);
+  eng->tev.resize(kTimingEvents * (size_t)slots, nullptr);
   for (auto& e : eng->tev) CK(cudaEventCreate(&e));
   eng->t_slots = slots;
   return PF_OK;
@@ -631,14 +650,20 @@ int pfe_read_timing(pf_engine_t* eng, float* step_kernel_ms, float* whole_step_m
   if (eng->t_slots == 0) return set_err(PF_EINVAL, "timing is not enabled");
   CK(cudaStreamSynchronize(eng->stream));
   const int n = std::min(eng->t_pending, max_entries);
+  eng->t_kernel_ms.assign((size_t)n * (kTimingEvents - 1), 0.f);
   const int first = (eng->t_next - eng->t_pending + eng->t_slots) % eng->t_slots;
   for (int i = 0; i < n; ++i) {
-    const cudaEvent_t* ev = &eng->tev[3 * (size_t)((first + i) % eng->t_slots)];
+    const cudaEvent_t* ev = &eng->tev[kTimingEvents * (size_t)((first + i) % eng->t_slots)];
     float a = 0.f, b = 0.f;
     CK(cudaEventElapsedTime(&a, ev[0], ev[1]));
-    CK(cudaEventElapsedTime(&b, ev[0], ev[2]));
+    CK(cudaEventElapsedTime(&b, ev[0], ev[kTimingEvents - 1]));
     if (step_kernel_ms) step_kernel_ms[i] = a;
     if (whole_step_ms) whole_step_ms[i] = b;
+    for (int k = 0; k < kTimingEvents - 1; ++k) {
+      float m = 0.f;
+      CK(cudaEventElapsedTime(&m, ev[k], ev[k + 1]));
+      eng->t_kernel_ms[(size_t)i * (kTimingEvents - 1) + k] = m;
+    }
   }
   *count = n;
   eng->t_pending = 0;
@@ -919,46 +944,63 @@ int pfe_test_poison_lookback(pf_engine_t* eng, int on) {
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
-// Internal hook for the stateless API: systematic ancestors of one weight
-// vector, with the engine's look-back scan and merge-path kernels.  lw32 holds
-// log-weights already shifted by their maximum (so the maximum is 0).
+// Internal hook for the stateless API: systematic ancestors of one FP64
+// log-weight vector (maximum at *d_max on the device), with the engine's
+// look-back scan and merge-path kernels.
 namespace pfb {
 
-size_t systematic_scratch_bytes(int n) {
-  const int T = (n + PF_TILE - 1) / PF_TILE;
-  size_t o = 0;
-  auto take = [&](size_t b) { o = align_up(o + b, 256); };
-  take(sizeof(FilterDesc));
-  take(sizeof(FilterCtrl));
-  take((size_t)T * 4);                 // tile table
-  take((size_t)align_up(n, 4) * 4);    // offs
-  take((size_t)T * 4);                 // mp_part
-  take((size_t)T * 8 * 3);             // agg, inc, excl
-  take((size_t)T * 4);                 // flags
-  take(sizeof(unsigned) * 2 * Q_COUNT + 16);
-  return o;
-}
+struct SysScratch {
+  FilterDesc* desc;
+  FilterCtrl* ctrl;
+  int* tf;
+  uint32_t* offs;
+  uint32_t* mp;
+  unsigned long long *agg, *inc, *excl;
+  unsigned* flag;
+  unsigned* queue;
+  size_t bytes;
+};
 
-int systematic_ancestors(const float* d_lw32, int n, uint32_t u, int* d_anc, void* d_scratch,
-                         cudaStream_t st) {
+// One layout for both the size query and the carve.
+static SysScratch carve_sys_scratch(unsigned char* w, int n) {
   const int T = (n + PF_TILE - 1) / PF_TILE;
-  unsigned char* w = (unsigned char*)d_scratch;
   size_t o = 0;
   auto take = [&](size_t b) {
     unsigned char* p = w + o;
     o = align_up(o + b, 256);
     return p;
   };
-  FilterDesc* desc = (FilterDesc*)take(sizeof(FilterDesc));
-  FilterCtrl* ctrl = (FilterCtrl*)take(sizeof(FilterCtrl));
-  int* tf = (int*)take((size_t)T * 4);
-  uint32_t* offs = (uint32_t*)take((size_t)align_up(n, 4) * 4);
-  uint32_t* mp = (uint32_t*)take((size_t)T * 4);
-  unsigned long long* agg = (unsigned long long*)take((size_t)T * 8);
-  unsigned long long* inc = (unsigned long long*)take((size_t)T * 8);
-  unsigned long long* excl = (unsigned long long*)take((size_t)T * 8);
-  unsigned* flag = (unsigned*)take((size_t)T * 4);
-  unsigned* queue = (unsigned*)take(sizeof(unsigned) * 2 * Q_COUNT + 16);
+  SysScratch s;
+  s.desc = (FilterDesc*)take(sizeof(FilterDesc));
+  s.ctrl = (FilterCtrl*)take(sizeof(FilterCtrl));
+  s.tf = (int*)take((size_t)T * 4);
+  s.offs = (uint32_t*)take(align_up((size_t)n, 4) * 4);
+  s.mp = (uint32_t*)take((size_t)T * 4);
+  s.agg = (unsigned long long*)take((size_t)T * 8);
+  s.inc = (unsigned long long*)take((size_t)T * 8);
+  s.excl = (unsigned long long*)take((size_t)T * 8);
+  s.flag = (unsigned*)take((size_t)T * 4);
+  s.queue = (unsigned*)take(sizeof(unsigned) * 2 * Q_COUNT + 16);
+  s.bytes = o;
+  return s;
+}
+
+size_t systematic_scratch_bytes(int n) { return carve_sys_scratch(nullptr, n).bytes; }
+
+int systematic_ancestors(const double* d_lw64, const double* d_max, int n, uint32_t u, int* d_anc,
+                         void* d_scratch, cudaStream_t st) {
+  const int T = (n + PF_TILE - 1) / PF_TILE;
+  SysScratch sc = carve_sys_scratch((unsigned char*)d_scratch, n);
+  FilterDesc* desc = sc.desc;
+  FilterCtrl* ctrl = sc.ctrl;
+  int* tf = sc.tf;
+  uint32_t* offs = sc.offs;
+  uint32_t* mp = sc.mp;
+  unsigned long long* agg = sc.agg;
+  unsigned long long* inc = sc.inc;
+  unsigned long long* excl = sc.excl;
+  unsigned* flag = sc.flag;
+  unsigned* queue = sc.queue;
   unsigned* err = queue + 2 * Q_COUNT;
 
   FilterDesc hd;
@@ -986,7 +1028,9 @@ int systematic_ancestors(const float* d_lw32, int n, uint32_t u, int* d_anc, voi
   e.desc = desc;
   e.ctrl = ctrl;
   e.tile_filter = tf;
-  e.lw = const_cast<float*>(d_lw32);
+  e.lw = nullptr;
+  e.lw64 = d_lw64;
+  e.lw64_max = d_max;
   e.anc = d_anc;
   e.offs = offs;
   e.mp_part = mp;

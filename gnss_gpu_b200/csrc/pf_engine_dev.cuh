@@ -94,6 +94,8 @@ struct EngineDev {
   unsigned flags;
   float ess_threshold;
   int lookback_poison;    // test hook: wait for a tag nobody publishes
+  const double* lw64;     // stateless API: FP64 log-weights (else null)
+  const double* lw64_max; // device pointer to their maximum
 };
 
 }  // namespace pfb

@@ -264,6 +264,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(EngineDev e, int t0, int c
   constexpr int D = 3 + NCLK;
   __shared__ float4 s_sat[2 * PF_MAX_SATS];
   __shared__ int s_grp[PF_MAX_CLK + 1];
+  __shared__ unsigned char s_clk[PF_MAX_SATS];
   __shared__ float s_red[kThreads / 32][kPartStride];
   __shared__ float s_maxtmp[kThreads / 32];
   __shared__ double s_dred[(kThreads / 32) * 16];
@@ -298,14 +299,21 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(EngineDev e, int t0, int c
     // ---- per-filter satellite geometry in FP64, stored as FP32 in smem,
     //      grouped by clock state.
     if (f != cached) {
+      // clock index of every satellite, staged once (one coalesced read)
+      int my_c = 0;
+      const pf_sat_t* sp = sats + fe->sat_offset + threadIdx.x;
+      if (do_weight && threadIdx.x < n_sat) {
+        my_c = sp->clk;
+        my_c = my_c < 0 ? 0 : (my_c >= NCLK ? NCLK - 1 : my_c);
+        s_clk[threadIdx.x] = (unsigned char)my_c;
+      }
+      __syncthreads();
       if (do_weight && threadIdx.x < n_sat) {
         const double* rot = fd->rot;
         const double sh0 = fc->shift[0], sh1 = fc->shift[1], sh2 = fc->shift[2];
         double A[3];
         local_to_ecef(rot, fc->anchor, sh0, sh1, sh2, A);
-        const pf_sat_t* sp = sats + fe->sat_offset + threadIdx.x;
-        int c = sp->clk;
-        c = c < 0 ? 0 : (c >= NCLK ? NCLK - 1 : c);
+        const int c = my_c;
         const double clkA = fc->clk_anchor[c] + (double)fc->shift[3 + c];
         double vx = sp->x - A[0], vy = sp->y - A[1], vz = sp->z - A[2];
         double r0 = sqrt(vx * vx + vy * vy + vz * vz);
@@ -319,10 +327,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(EngineDev e, int t0, int c
         float wq = WMODE == PF_WEIGHT_GAUSSIAN ? (float)((double)fd->wscale * sp->w) : (float)sp->w;
         float4 a4 = make_float4((float)eE, (float)eN, (float)eU, -0.5f * g);
         float4 b4 = make_float4(0.5f * g * g, 0.5f * g, y, wq);
+        // stable order by clock state
         int rank = 0;
         for (int s2 = 0; s2 < n_sat; ++s2) {
-          int c2 = sats[fe->sat_offset + s2].clk;
-          c2 = c2 < 0 ? 0 : (c2 >= NCLK ? NCLK - 1 : c2);
+          const int c2 = s_clk[s2];
           rank += (c2 < c) || (c2 == c && s2 < (int)threadIdx.x);
         }
         s_sat[2 * rank] = a4;
@@ -330,13 +338,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(EngineDev e, int t0, int c
       }
       if (threadIdx.x <= NCLK) {
         int cnt = 0;
-        if (do_weight) {
-          for (int s2 = 0; s2 < n_sat; ++s2) {
-            int c2 = sats[fe->sat_offset + s2].clk;
-            c2 = c2 < 0 ? 0 : (c2 >= NCLK ? NCLK - 1 : c2);
-            cnt += c2 < (int)threadIdx.x;
-          }
-        }
+        if (do_weight)
+          for (int s2 = 0; s2 < n_sat; ++s2) cnt += s_clk[s2] < (int)threadIdx.x;
         s_grp[threadIdx.x] = cnt;
       }
       cached = f;
@@ -541,11 +544,32 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(EngineDev e, int t0, int c
   queue_exit(q);
 }
 
+// Quantised weights of particles [p0, p0+4): from the FP32 log-weights of
+// the engine, or from FP64 log-weights when the stateless API set lw64.
+// The shift lw - max is exact in FP64 for FP32 inputs.
+__device__ __forceinline__ void load_q4(const EngineDev& e, long long base, int p0, int n, float M,
+                                        int K, unsigned long long (&q)[4]) {
+  q[0] = q[1] = q[2] = q[3] = 0ull;
+  if (p0 >= n) return;
+  if (e.lw64) {
+    const double m64 = __ldcg(e.lw64_max);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (p0 + k < n) q[k] = quantize_shifted(__ldcg(e.lw64 + base + p0 + k) - m64, K);
+  } else {
+    const float4 v = __ldcg(reinterpret_cast<const float4*>(e.lw + base + p0));
+    const float l[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (p0 + k < n) q[k] = quantize_shifted((double)l[k] - (double)M, K);
+  }
+}
+
 // -------------------------------------------------------------------------
 // k_scan: quantised weights, tile sums, decoupled look-back over tiles.
 __global__ void __launch_bounds__(kThreads) k_scan(EngineDev e, int t0, int count) {
   __shared__ unsigned long long s_u64[kThreads / 32];
-  __shared__ int s_slot;
+  __shared__ int s_slot, s_first;
   unsigned* q = e.queue + 2 * Q_SCAN;
   for (;;) {
     const int tq = dequeue(q, &s_slot);
@@ -561,82 +585,79 @@ __global__ void __launch_bounds__(kThreads) k_scan(EngineDev e, int t0, int coun
     const int tb = fd->tile_begin, j = t - tb;
     const int p0 = j * kTile + (int)threadIdx.x * 4;
     const long long base = fd->p_off;
-    unsigned long long qs = 0;
-    if (p0 < n) {
-      float4 v = __ldcg(reinterpret_cast<const float4*>(e.lw + base + p0));
-      float l[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        if (p0 + k < n) qs += quantize_weight(l[k], M, K);
-    }
+    unsigned long long qv[4];
+    load_q4(e, base, p0, n, M, K, qv);
+    const unsigned long long qs = qv[0] + qv[1] + qv[2] + qv[3];
     unsigned long long tot;
     block_excl_scan_u64(qs, s_u64, &tot);
-    if (threadIdx.x < 32) {
-      const int lane = threadIdx.x;
-      unsigned long long excl = 0;
-      if (j == 0) {
-        if (lane == 0) {
-          e.lb_inc[t] = tot;
-          __threadfence();
-          atomicExch(e.lb_flag + t, tag | 2u);
-        }
-      } else {
-        if (lane == 0) {
-          e.lb_agg[t] = tot;
-          __threadfence();
-          atomicExch(e.lb_flag + t, tag | 1u);
-        }
-        const unsigned want = e.lookback_poison ? ((tag + 4u) >> 2) : (tag >> 2);
-        int pred = t - 1;
-        bool done = false;
-        while (!done) {
-          const int idx = pred - lane;
-          const bool inr = idx >= tb;
-          unsigned fl = 0;
-          unsigned long long spins = 0;
-          bool ok = !inr;
-          bool timed_out = false;
-          while (true) {
-            if (!ok) {
-              fl = *(volatile unsigned*)(e.lb_flag + idx);
-              ok = ((fl >> 2) == want) && ((fl & 3u) != 0u);
-            }
-            if (__all_sync(0xffffffffu, ok)) break;
-            if (++spins > e.spin_limit) {
-              timed_out = true;
-              break;
-            }
-            if (spins > 64) __nanosleep(64);
+    unsigned long long excl = 0;
+    if (j == 0) {
+      if (threadIdx.x == 0) {
+        e.lb_inc[t] = tot;
+        __threadfence();
+        atomicExch(e.lb_flag + t, tag | 2u);
+      }
+    } else {
+      if (threadIdx.x == 0) {
+        e.lb_agg[t] = tot;
+        __threadfence();
+        atomicExch(e.lb_flag + t, tag | 1u);
+      }
+      // Look back over a window of kThreads predecessors per round: thread
+      // i inspects tile pred - i.  The sum stops at the closest predecessor
+      // that published an inclusive prefix.  Spins are bounded; when the
+      // limit is reached the error word is set and the scan moves on.
+      const unsigned want = e.lookback_poison ? ((tag + 4u) >> 2) : (tag >> 2);
+      int pred = t - 1;
+      for (;;) {
+        const int idx = pred - (int)threadIdx.x;
+        const bool inr = idx >= tb;
+        unsigned fl = 0;
+        bool ok = !inr;
+        unsigned long long spins = 0;
+        bool timed_out = false;
+        for (;;) {
+          if (!ok) {
+            fl = *(volatile unsigned*)(e.lb_flag + idx);
+            ok = ((fl >> 2) == want) && ((fl & 3u) != 0u);
           }
-          if (__any_sync(0xffffffffu, timed_out)) {
-            if (lane == 0) atomicOr(e.err, ERR_LOOKBACK_TIMEOUT);
+          if (__syncthreads_and(ok)) break;
+          if (++spins > e.spin_limit) {  // uniform across the CTA
+            timed_out = true;
             break;
           }
-          __threadfence();
-          unsigned long long val = 0;
-          const bool is_inc = inr && ((fl & 3u) == 2u);
-          if (inr) val = is_inc ? *(volatile unsigned long long*)(e.lb_inc + idx)
-                                : *(volatile unsigned long long*)(e.lb_agg + idx);
-          const unsigned inc_mask = __ballot_sync(0xffffffffu, is_inc);
-          if (inc_mask) {
-            const int first = __ffs(inc_mask) - 1;  // closest predecessor with a prefix
-            if (lane > first) val = 0;
-            done = true;
-          }
-          excl += warp_sum_u64(val);
-          pred -= 32;
-          if (pred < tb) done = true;
+          if (spins > 32) __nanosleep(64);
         }
-        if (lane == 0) {
-          e.lb_inc[t] = excl + tot;
-          __threadfence();
-          atomicExch(e.lb_flag + t, tag | 2u);
+        if (timed_out) {
+          if (threadIdx.x == 0) atomicOr(e.err, ERR_LOOKBACK_TIMEOUT);
+          break;
         }
+        __threadfence();
+        const bool is_inc = inr && ((fl & 3u) == 2u);
+        if (threadIdx.x == 0) s_first = kThreads;
+        __syncthreads();
+        if (is_inc) atomicMin(&s_first, (int)threadIdx.x);
+        __syncthreads();
+        const int first = s_first;  // closest predecessor with a prefix
+        unsigned long long val = 0;
+        if (inr && (int)threadIdx.x <= first)
+          val = is_inc ? *(volatile unsigned long long*)(e.lb_inc + idx)
+                       : *(volatile unsigned long long*)(e.lb_agg + idx);
+        unsigned long long round_sum;
+        block_excl_scan_u64(val, s_u64, &round_sum);
+        excl += round_sum;
+        pred -= kThreads;
+        if (first < kThreads || pred < tb) break;
       }
-      if (lane == 0) {
-        e.tile_excl[t] = excl;
-        if (j == fd->n_tiles - 1) fc->wq_total = excl + tot;
+      if (threadIdx.x == 0) {
+        e.lb_inc[t] = excl + tot;
+        __threadfence();
+        atomicExch(e.lb_flag + t, tag | 2u);
       }
+    }
+    if (threadIdx.x == 0) {
+      e.tile_excl[t] = excl;
+      if (j == fd->n_tiles - 1) fc->wq_total = excl + tot;
     }
   }
   queue_exit(q);
@@ -664,14 +685,8 @@ __global__ void __launch_bounds__(kThreads) k_offs(EngineDev e, int t0, int coun
     const int tb = fd->tile_begin, j = t - tb;
     const int p0 = j * kTile + (int)threadIdx.x * 4;
     const long long base = fd->p_off;
-    unsigned long long qv[4] = {0, 0, 0, 0};
-    if (p0 < n) {
-      float4 v = __ldcg(reinterpret_cast<const float4*>(e.lw + base + p0));
-      float l[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        if (p0 + k < n) qv[k] = quantize_weight(l[k], M, K);
-    }
+    unsigned long long qv[4];
+    load_q4(e, base, p0, n, M, K, qv);
     unsigned long long tot;
     const unsigned long long texcl = block_excl_scan_u64(qv[0] + qv[1] + qv[2] + qv[3], s_u64, &tot);
     if (p0 < n) {

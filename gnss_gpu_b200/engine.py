@@ -276,3 +276,12 @@ class Engine:
         c = C.c_int(0)
         N.check(self.lib.pfe_read_timing(self.h, a, b, n, C.byref(c)))
         return np.array(a[: c.value]), np.array(b[: c.value])
+
+    def read_timing_kernels(self):
+        """Per-kernel ms of the steps returned by the last read_timing():
+        (steps, 4) = fused step kernel, scan, offspring ends, merge path."""
+        n = max(1, getattr(self, "_timing_slots", 0))
+        a = (C.c_float * (4 * n))()
+        c = C.c_int(0)
+        N.check(self.lib.pfe_read_timing_kernels(self.h, a, n, C.byref(c)))
+        return np.array(a[: 4 * c.value]).reshape(-1, 4)

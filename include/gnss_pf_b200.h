@@ -292,6 +292,12 @@ int pfe_last_launch_count(pf_engine_t* eng, int* count);
 int pfe_enable_timing(pf_engine_t* eng, int slots);
 int pfe_read_timing(pf_engine_t* eng, float* step_kernel_ms, float* whole_step_ms,
                     int max_entries, int* count);
+/* Per-kernel durations (ms) of the steps returned by the last
+ * pfe_read_timing: 4 per step -- fused step kernel, then the three
+ * resampling kernels (look-back scan, offspring ends, merge path; for
+ * Megopolis the chain kernel then two zeros). */
+int pfe_read_timing_kernels(pf_engine_t* eng, float* out_4_per_step,
+                            int max_entries, int* count);
 
 #ifdef __cplusplus
 }

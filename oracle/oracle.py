@@ -46,9 +46,12 @@ def lib():
         L.orc_philox10.argtypes = [U32, u32, u32, U32]
         L.orc_quant_exponent.argtypes = [i32]
         L.orc_quant_exponent.restype = i32
-        L.orc_quantize.argtypes = [f32, f32, i32]
+        L.orc_quantize.argtypes = [f64, i32]
         L.orc_quantize.restype = C.c_uint64
         L.orc_quantize_all.argtypes = [F32, i32, f32, U64]
+        L.orc_quantize_all64.argtypes = [F64, i32, f64, U64]
+        L.orc_systematic64.argtypes = [F64, i32, f64, u32, I32, C.POINTER(C.c_uint64)]
+        L.orc_systematic64.restype = i32
         L.orc_systematic.argtypes = [F32, i32, f32, u32, I32, C.POINTER(C.c_uint64)]
         L.orc_systematic.restype = i32
         L.orc_megopolis.argtypes = [F32, i32, i32, u32, u32, u32, u32, I32]

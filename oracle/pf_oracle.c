@@ -83,9 +83,14 @@ static void normals8(uint32_t p, uint32_t epoch, uint32_t tag, uint32_t fid, uin
   }
 }
 
-/* ------------------------------------------------ deterministic quantiser */
-static float dsub(float a, float b) { volatile float r = a - b; return r; }
-static float dmul(float a, float b) { volatile float r = a * b; return r; }
+/* ------------------------------------------------ deterministic quantiser
+ * q = floor(2^K exp(d)) for d = lw - max <= 0, with exactly the operation
+ * sequence of the device (every step an IEEE-rounded double operation):
+ * x = d log2(e), n = floor(x), f = x - n, t = f ln 2, e^t by its Taylor
+ * series (1/j!, degree 13) in Horner form with fma, times 2^(K+n),
+ * truncated.  Weights below 2^-40 of the largest quantise to zero. */
+static double dmul(double a, double b) { volatile double r = a * b; return r; }
+static double dsub(double a, double b) { volatile double r = a - b; return r; }
 
 int orc_quant_exponent(int n) {
   int lg = 0;
@@ -94,31 +99,40 @@ int orc_quant_exponent(int n) {
   return k < 40 ? k : 40;
 }
 
-uint64_t orc_quantize(float lw, float max_lw, int K) {
-  float d = dsub(lw, max_lw);
-  float x = dmul(d, 1.44269504088896341f);
-  if (!(x > -40.0f)) return 0;
-  float n = floorf(x);
-  float f = dsub(x, n);
-  float p = 1.0178086009239699e-07f;
-  p = fmaf(p, f, 1.3215486790144307e-06f);
-  p = fmaf(p, f, 1.5252733804059840e-05f);
-  p = fmaf(p, f, 1.5403530393381606e-04f);
-  p = fmaf(p, f, 1.3333558146428443e-03f);
-  p = fmaf(p, f, 9.6181291076284772e-03f);
-  p = fmaf(p, f, 5.5504108664821580e-02f);
-  p = fmaf(p, f, 2.4022650695910071e-01f);
-  p = fmaf(p, f, 6.9314718055994531e-01f);
-  p = fmaf(p, f, 1.0f);
-  uint32_t P = (uint32_t)dmul(p, 8388608.0f);
-  int sh = K - 23 + (int)n;
-  return sh >= 0 ? ((uint64_t)P << sh) : ((uint64_t)P >> (-sh));
+uint64_t orc_quantize(double d, int K) {
+  const double x = dmul(d, 1.4426950408889634074);
+  if (!(x > -40.0)) return 0;
+  const double n = floor(x);
+  const double f = dsub(x, n);
+  const double t = dmul(f, 0.69314718055994530942);
+  double q = 1.6059043836821615e-10;
+  q = fma(q, t, 2.0876756987868099e-09);
+  q = fma(q, t, 2.5052108385441720e-08);
+  q = fma(q, t, 2.7557319223985893e-07);
+  q = fma(q, t, 2.7557319223985888e-06);
+  q = fma(q, t, 2.4801587301587302e-05);
+  q = fma(q, t, 1.9841269841269841e-04);
+  q = fma(q, t, 1.3888888888888889e-03);
+  q = fma(q, t, 8.3333333333333333e-03);
+  q = fma(q, t, 4.1666666666666667e-02);
+  q = fma(q, t, 1.6666666666666667e-01);
+  q = fma(q, t, 0.5);
+  q = fma(q, t, 1.0);
+  q = fma(q, t, 1.0);
+  return (uint64_t)ldexp(q, K + (int)n);
 }
 
+/* FP32 log-weights of the engine: the shift lw - max is exact in FP64. */
 void orc_quantize_all(const float* lw, int n, float max_lw, uint64_t* q) {
   const int K = orc_quant_exponent(n);
 #pragma omp parallel for schedule(static)
-  for (int i = 0; i < n; ++i) q[i] = orc_quantize(lw[i], max_lw, K);
+  for (int i = 0; i < n; ++i) q[i] = orc_quantize((double)lw[i] - (double)max_lw, K);
+}
+
+void orc_quantize_all64(const double* lw, int n, double max_lw, uint64_t* q) {
+  const int K = orc_quant_exponent(n);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) q[i] = orc_quantize(lw[i] - max_lw, K);
 }
 
 /* ------------------------------------------------------------ systematic
@@ -126,10 +140,7 @@ void orc_quantize_all(const float* lw, int n, float max_lw, uint64_t* q) {
  * for the first i with !(cdf[i] < (u + k)/N).  With an integer CDF C and
  * total W the comparison is exact: C_i*N*2^32 < (k*2^32 + u32)*W.
  * Returns 0 on success, -1 if every weight quantised to zero. */
-int orc_systematic(const float* lw, int n, float max_lw, uint32_t u32, int* anc, uint64_t* wq_out) {
-  uint64_t* C = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)n);
-  if (!C) return -2;
-  orc_quantize_all(lw, n, max_lw, C);
+static int systematic_from_q(uint64_t* C, int n, uint32_t u32, int* anc, uint64_t* wq_out) {
   uint64_t acc = 0;
   for (int i = 0; i < n; ++i) {
     acc += C[i];
@@ -137,10 +148,7 @@ int orc_systematic(const float* lw, int n, float max_lw, uint32_t u32, int* anc,
   }
   const uint64_t W = acc;
   if (wq_out) *wq_out = W;
-  if (W == 0) {
-    free(C);
-    return -1;
-  }
+  if (W == 0) return -1;
 #pragma omp parallel for schedule(static)
   for (int k = 0; k < n; ++k) {
     const unsigned __int128 rhs = (unsigned __int128)((((uint64_t)k) << 32) | u32) * W;
@@ -153,8 +161,25 @@ int orc_systematic(const float* lw, int n, float max_lw, uint32_t u32, int* anc,
     }
     anc[k] = lo;
   }
-  free(C);
   return 0;
+}
+
+int orc_systematic(const float* lw, int n, float max_lw, uint32_t u32, int* anc, uint64_t* wq_out) {
+  uint64_t* C = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)n);
+  if (!C) return -2;
+  orc_quantize_all(lw, n, max_lw, C);
+  int r = systematic_from_q(C, n, u32, anc, wq_out);
+  free(C);
+  return r;
+}
+
+int orc_systematic64(const double* lw, int n, double max_lw, uint32_t u32, int* anc, uint64_t* wq_out) {
+  uint64_t* C = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)n);
+  if (!C) return -2;
+  orc_quantize_all64(lw, n, max_lw, C);
+  int r = systematic_from_q(C, n, u32, anc, wq_out);
+  free(C);
+  return r;
 }
 
 /* ------------------------------------------------------ canonical Megopolis
@@ -327,12 +352,10 @@ int orc_epoch(int n, int D, double* x, double* x_tmp, double* lw, float* lw32, i
   orc_stats(n, D, x_tmp, lw, anchor, clk_anchor, rot, stats_out);
   int rs = stats_out[3] < ess_thr * (double)n;
   if (rs) {
-    const double m = stats_out[0];
-#pragma omp parallel for schedule(static)
-    for (int i = 0; i < n; ++i) lw32[i] = (float)(lw[i] - m);
     uint32_t c[4] = {0u, epoch, TAG_SYS_U, 0u}, w[4];
     orc_philox10(c, k0, k1, w);
-    orc_systematic(lw32, n, 0.0f, w[0], anc, NULL);
+    orc_systematic64(lw, n, stats_out[0], w[0], anc, NULL);
+    (void)lw32;
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i)
       for (int d = 0; d < D; ++d) x[(size_t)d * n + i] = x_tmp[(size_t)d * n + anc[i]];
@@ -433,15 +456,10 @@ int orc_pf_systematic_ancestors(const double* lw, int n, unsigned long long seed
   double m = -INFINITY;
   for (int i = 0; i < n; ++i)
     if (lw[i] > m) m = lw[i];
-  float* l32 = (float*)malloc(sizeof(float) * (size_t)n);
-  if (!l32) return -2;
-  for (int i = 0; i < n; ++i) l32[i] = (float)(lw[i] - m);
   double u0 = (double)(seed % 1000000ull) / (1000000.0 * (double)n);
   double v = floor(u0 * 4294967296.0);
   uint32_t u32 = (uint32_t)(v < 0 ? 0 : (v > 4294967295.0 ? 4294967295.0 : v));
-  int r = orc_systematic(l32, n, 0.0f, u32, anc, NULL);
-  free(l32);
-  return r;
+  return orc_systematic64(lw, n, m, u32, anc, NULL);
 }
 
 /* resampling.cu:175-272 chain on ancestor indices (the reference's
