@@ -73,8 +73,8 @@ enum : uint32_t {
 
 #ifdef __CUDACC__
 // Two standard normals from two 32-bit words (Box-Muller) with
-// u1 = (a + 1/2) 2^-32 in (0, 1) and angle 2*pi*(b 2^-32 - 1/2) in
-// [-pi, pi), where the fast sine/cosine are accurate to about 2^-21.
+// u1 = (a + 1/2) 2^-32 in (0, 1) and angle 2*pi*u2 in [-pi, pi), where the
+// fast sine/cosine are accurate to about 2^-21.
 // log(u1) keeps ~1e-7 relative accuracy over the whole range: below 0.75
 // the fast logarithm; from 0.75 up, u1 = 1 - v with v = (~a + 1/2) 2^-32
 // formed exactly and log(1 - v) = -2 atanh(s), s = v / (2 - v) <= 1/7,
@@ -94,9 +94,10 @@ __device__ __forceinline__ float bm_log_u1(uint32_t a) {
   return (a >= 0xC0000000u) ? near_one : __logf(u1);
 }
 
+// The angle uses the top 24 bits of b: u2 = (b >> 8) 2^-24 - 1/2 is exact in
+// FP32.
 __device__ __forceinline__ float2 box_muller_f32(uint32_t a, uint32_t b) {
-  const float two_m32 = 2.3283064365386963e-10f;  // 2^-32
-  float u2 = fmaf((float)b, two_m32, -0.5f);
+  float u2 = fmaf((float)(b >> 8), 5.9604644775390625e-08f, -0.5f);
   float r = sqrtf(fmaxf(-2.0f * bm_log_u1(a), 0.0f));
   float s, c;
   __sincosf(6.283185307179586f * u2, &s, &c);

@@ -20,7 +20,7 @@
  * the CUDA path draw identical 32-bit words.  Normals: Box-Muller in FP64.
  *
  * Compile with -ffp-contract=off: orc_quantize must round exactly like the
- * device's __fmul_rn/__fsub_rn/__fmaf_rn sequence.
+ * device's sequence of IEEE double multiply, subtract and fma.
  */
 #include <math.h>
 #include <stdint.h>
@@ -56,10 +56,24 @@ void orc_philox10(const uint32_t in[4], uint32_t k0, uint32_t k1, uint32_t out[4
   out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
 
+/* Box-Muller of the stateless (FP64) path: u1 = (a + 1/2) 2^-32,
+ * u2 = b 2^-32 - 1/2. */
 static void bm(uint32_t a, uint32_t b, double* n0, double* n1) {
   const double two_m32 = 2.3283064365386963e-10;
   double u1 = ((double)a + 0.5) * two_m32;
   double u2 = (double)b * two_m32 - 0.5;
+  double r = sqrt(-2.0 * log(u1));
+  double th = 6.283185307179586476925286766559 * u2;
+  *n0 = r * cos(th);
+  *n1 = r * sin(th);
+}
+
+/* Box-Muller of the engine (FP32 on the device): same u1, angle from the
+ * top 24 bits of b, u2 = (b >> 8) 2^-24 - 1/2. */
+static void bm24(uint32_t a, uint32_t b, double* n0, double* n1) {
+  const double two_m32 = 2.3283064365386963e-10;
+  double u1 = ((double)a + 0.5) * two_m32;
+  double u2 = (double)(b >> 8) * 5.9604644775390625e-08 - 0.5;
   double r = sqrt(-2.0 * log(u1));
   double th = 6.283185307179586476925286766559 * u2;
   *n0 = r * cos(th);
@@ -71,13 +85,13 @@ static void normals8(uint32_t p, uint32_t epoch, uint32_t tag, uint32_t fid, uin
                      uint32_t k1, int need, double nz[8]) {
   uint32_t c[4] = {p, epoch, tag, fid}, w[4];
   orc_philox10(c, k0, k1, w);
-  bm(w[0], w[1], &nz[0], &nz[1]);
-  bm(w[2], w[3], &nz[2], &nz[3]);
+  bm24(w[0], w[1], &nz[0], &nz[1]);
+  bm24(w[2], w[3], &nz[2], &nz[3]);
   if (need > 4) {
     c[2] = tag | 1u;
     orc_philox10(c, k0, k1, w);
-    bm(w[0], w[1], &nz[4], &nz[5]);
-    bm(w[2], w[3], &nz[6], &nz[7]);
+    bm24(w[0], w[1], &nz[4], &nz[5]);
+    bm24(w[2], w[3], &nz[6], &nz[7]);
   } else {
     nz[4] = nz[5] = nz[6] = nz[7] = 0.0;
   }

@@ -62,7 +62,10 @@ def check_step(eng: Engine, k: int, before_state, before_shift, rec, weight_mode
     x_pred = O.predict(before_state.astype(np.float64), None, np.asarray(rec.get("disp", (0, 0, 0))),
                        before_shift.astype(np.float64), sigma, fl & N.PF_EP_PREDICT, spec.seed, epoch, k)
     dx = np.abs(x_raw.astype(np.float64) - x_pred)
-    state_ok = np.all(dx <= STATE_RTOL * np.maximum(1.0, np.abs(x_pred)) + 2e-6)
+    # FP32 storage of the offsets plus FP32 Box-Muller noise (~1e-6 of sigma
+    # per normal, scaled with the draw's magnitude)
+    noise = 2e-6 * sigma.astype(np.float64)[:, None] * 6.0 if fl & N.PF_EP_PREDICT else 0.0
+    state_ok = np.all(dx <= STATE_RTOL * np.maximum(1.0, np.abs(x_pred)) + 2e-6 + noise)
     out = {"state_err": float(dx.max()) if dx.size else 0.0, "state_ok": bool(state_ok)}
     if fl & N.PF_EP_WEIGHT:
         rows = sat_rows(rec["sats"], rec["pr"], rec.get("w"))
