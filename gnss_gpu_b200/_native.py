@@ -17,6 +17,7 @@ PF_OK, PF_EINVAL, PF_ENOTINIT, PF_ECUDA, PF_ETIMEOUT, PF_ECAP, PF_ENOMEM = range
 PF_MAX_CLK = 4
 PF_MAX_SATS = 64
 PF_TILE = 1024
+PF_NOALLOC_MAX_PARTICLES = 1 << 22
 
 PF_RESAMPLE_SYSTEMATIC, PF_RESAMPLE_MEGOPOLIS = 0, 1
 PF_WEIGHT_GAUSSIAN, PF_WEIGHT_HUBER = 0, 1
@@ -75,7 +76,7 @@ assert SAT_DTYPE.itemsize == C.sizeof(Sat) == 48
 EXPORTED = [
     "pf_last_error", "pf_abi_version",
     "pf_initialize", "pf_predict", "pf_weight", "pf_compute_ess", "pf_resample_systematic",
-    "pf_resample_megopolis", "pf_estimate", "pf_get_particles",
+    "pf_resample_megopolis", "pf_estimate", "pf_get_particles", "pf_compute_ess_noalloc",
     "pfe_workspace_bytes", "pfe_create", "pfe_destroy", "pfe_set_stream", "pfe_set_filter_params",
     "pfe_initialize", "pfe_get_frame", "pfe_upload_obs", "pfe_obs_slot_bytes", "pfe_step",
     "pfe_step_per_filter", "pfe_graph_capture", "pfe_graph_launch", "pfe_read_results",
@@ -114,6 +115,7 @@ def load():
     L.pf_resample_megopolis.argtypes = [dp, dp, dp, dp, dp, i, i, u]
     L.pf_estimate.argtypes = [dp, dp, dp, dp, dp, dp, i]
     L.pf_get_particles.argtypes = [dp, dp, dp, dp, dp, i]
+    L.pf_compute_ess_noalloc.argtypes = [p, i, p, p]
     L.pfe_workspace_bytes.argtypes = [C.POINTER(EngineConfig), C.POINTER(FilterParams), C.POINTER(C.c_size_t)]
     L.pfe_create.argtypes = [C.POINTER(EngineConfig), C.POINTER(FilterParams), p, C.c_size_t, p,
                              C.POINTER(p)]

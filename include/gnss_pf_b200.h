@@ -85,6 +85,23 @@ int pf_weight(const double* px, const double* py, const double* pz,
 int pf_compute_ess(const double* log_weights, int n_particles,
                    double* ess_out);
 
+/* No counterpart in the reference.  ESS of log-weights already in device
+ * memory, for callers that cannot allocate device memory (during CUDA graph
+ * capture, in real-time loops that must not allocate after start-up, or when
+ * another allocator owns the device memory).  d_log_weights and d_ess_out
+ * are caller-owned device pointers; the work is queued on `stream` (a
+ * cudaStream_t, NULL = legacy) and *d_ess_out is valid once that stream
+ * reaches this point.  The function allocates nothing: its scratch is one
+ * fixed device array in the library, held by every GPU that loads the
+ * library until the process exits.  Limits: n_particles <=
+ * PF_NOALLOC_MAX_PARTICLES (larger -> PF_ECAP); all calls share that array,
+ * so calls that overlap on the GPU race and must be serialised; the first
+ * call on a device looks up the array's address and should come before any
+ * stream capture. */
+#define PF_NOALLOC_MAX_PARTICLES (1 << 22)
+int pf_compute_ess_noalloc(const double* d_log_weights, int n_particles,
+                           double* d_ess_out, void* stream);
+
 /* Replaces gnss_gpu::pf_resample_systematic (particle_filter.h:40-44;
  * resampling.cu:60-168).  Keeps the reference's offset
  * u0 = (seed % 1e6) / (1e6 * N) (resampling.cu:152) and its lower-bound
