@@ -11,7 +11,7 @@ from pathlib import Path
 
 import numpy as np
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libgnsspf_b200.so"
+LIB_PATH = Path(os.environ.get("PF_B200_LIB") or Path(__file__).resolve().parent / "lib" / "libgnsspf_b200.so")
 
 PF_OK, PF_EINVAL, PF_ENOTINIT, PF_ECUDA, PF_ETIMEOUT, PF_ECAP, PF_ENOMEM = range(7)
 PF_MAX_CLK = 4
@@ -23,7 +23,7 @@ PF_RESAMPLE_SYSTEMATIC, PF_RESAMPLE_MEGOPOLIS = 0, 1
 PF_WEIGHT_GAUSSIAN, PF_WEIGHT_HUBER = 0, 1
 PF_LW_OVERWRITE, PF_LW_ACCUMULATE = 0, 1
 PF_SYS_OFFSET_RANDOM, PF_SYS_OFFSET_REFERENCE = 0, 1
-PF_FLAG_COVARIANCE, PF_FLAG_RECENTER = 1, 2
+PF_FLAG_COVARIANCE, PF_FLAG_RECENTER, PF_FLAG_KERNEL_CHAIN = 1, 2, 4
 PF_EP_PREDICT, PF_EP_WEIGHT, PF_EP_FORCE_RESAMPLE, PF_EP_NO_RESAMPLE = 1, 2, 4, 8
 
 
@@ -145,7 +145,7 @@ def load():
     L.pfe_last_launch_count.argtypes = [p, C.POINTER(C.c_int)]
     L.pfe_test_poison_lookback.argtypes = [p, i]
     L.pfe_result_bytes.argtypes = [p, C.POINTER(C.c_size_t)]
-    L.pfe_enable_timing.argtypes = [p, i]
+    L.pfe_enable_timing.argtypes = [p, i, i]
     L.pfe_read_timing.argtypes = [p, C.POINTER(C.c_float), C.POINTER(C.c_float), i, C.POINTER(C.c_int)]
     L.pfe_read_timing_kernels.argtypes = [p, C.POINTER(C.c_float), i, C.POINTER(C.c_int)]
     for name in EXPORTED:

@@ -6,7 +6,7 @@
 //   resampling.cu:183-205).
 // * Box-Muller normals.
 // * Deterministic weight quantisation: exp(lw - max) evaluated with IEEE
-//   single-precision operations that round identically on host and device,
+//   double-precision operations that round identically on host and device,
 //   then scaled to a 64-bit integer.  The systematic resampler's CDF is an
 //   exact integer prefix sum of these values, so the ancestor indices are a
 //   function of (log-weights, offset) alone, independent of scan order.
@@ -75,23 +75,17 @@ enum : uint32_t {
 // Two standard normals from two 32-bit words (Box-Muller) with
 // u1 = (a + 1/2) 2^-32 in (0, 1) and angle 2*pi*u2 in [-pi, pi), where the
 // fast sine/cosine are accurate to about 2^-21.
-// log(u1) keeps ~1e-7 relative accuracy over the whole range: below 0.75
-// the fast logarithm; from 0.75 up, u1 = 1 - v with v = (~a + 1/2) 2^-32
-// formed exactly and log(1 - v) = -2 atanh(s), s = v / (2 - v) <= 1/7,
-// from the odd series s + s^3/3 + ... + s^9/9.
+// log(u1) keeps r = sqrt(-2 log u1) accurate to ~4e-6 absolute or better:
+// the fast logarithm (absolute error ~2^-21) wherever |log u1| >= 2^-8;
+// above 1 - 2^-8, u1 = 1 - v with v = (~a + 1/2) 2^-32 formed exactly and
+// log(1 - v) = -v (1 + v/2 + v^2/3) (next term v^4/4 < 6e-11).
 __device__ __forceinline__ float bm_log_u1(uint32_t a) {
   const float two_m32 = 2.3283064365386963e-10f;
   const float half_ulp = 1.1641532182693481e-10f;
   const float u1 = fmaf((float)a, two_m32, half_ulp);
   const float v = fmaf((float)(~a), two_m32, half_ulp);
-  const float s = __fdividef(v, 2.0f - v);
-  const float s2 = s * s;
-  float p = fmaf(s2, 1.0f / 9.0f, 1.0f / 7.0f);
-  p = fmaf(s2, p, 0.2f);
-  p = fmaf(s2, p, 1.0f / 3.0f);
-  p = fmaf(s2, p, 1.0f);
-  const float near_one = -2.0f * s * p;
-  return (a >= 0xC0000000u) ? near_one : __logf(u1);
+  const float near_one = -v * fmaf(v, fmaf(v, 1.0f / 3.0f, 0.5f), 1.0f);
+  return (a >= 0xFF000000u) ? near_one : __logf(u1);
 }
 
 // The angle uses the top 24 bits of b: u2 = (b >> 8) 2^-24 - 1/2 is exact in
@@ -213,6 +207,18 @@ PF_HD bool slot_at_or_below(uint64_t k, uint32_t u, uint64_t W, uint64_t C,
 PF_HD uint32_t offspring_end(uint64_t C, uint64_t W, uint32_t N, uint32_t u) {
   double est = (double)C / (double)W * (double)N - (double)u * 2.3283064365386963e-10;
   long long k = (long long)floor(est);
+  if (k < -1) k = -1;
+  if (k > (long long)N - 1) k = (long long)N - 1;
+  while (k >= 0 && !slot_at_or_below((uint64_t)k, u, W, C, N)) --k;
+  while (k + 1 < (long long)N && slot_at_or_below((uint64_t)(k + 1), u, W, C, N)) ++k;
+  return (uint32_t)(k + 1);
+}
+
+// offspring_end with the FP64 estimate C * (N / W) - u 2^-32 from a
+// precomputed scale; the exact 128-bit checks make the result identical.
+PF_HD uint32_t offspring_end_scaled(uint64_t C, uint64_t W, uint32_t N, uint32_t u, double scale,
+                                    double uf) {
+  long long k = (long long)floor((double)C * scale - uf);
   if (k < -1) k = -1;
   if (k > (long long)N - 1) k = (long long)N - 1;
   while (k >= 0 && !slot_at_or_below((uint64_t)k, u, W, C, N)) --k;

@@ -3,13 +3,14 @@
 #include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
 #include <string>
 #include <vector>
 
-#include "pf_engine_kernels.cuh"
+#include "pf_epoch_kernel.cuh"
 #include "pf_status.h"
 
 using namespace pfb;
@@ -38,6 +39,9 @@ struct pf_engine {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   int resident[Q_COUNT];
+  int epoch_resident = 0;     // co-resident CTAs of the cooperative epoch kernel
+  size_t epoch_smem = 0;      // its dynamic shared memory (two stage buffers)
+  unsigned* bar = nullptr;    // grid barrier words (count, generation, any-resample)
   int sm_count = 0;
   int last_launches = 0;
   std::vector<int> initialized;
@@ -45,6 +49,7 @@ struct pf_engine {
   std::vector<cudaEvent_t> tev;  // kTimingEvents per slot
   std::vector<float> t_kernel_ms; // per-kernel durations of the last read
   int t_slots = 0;
+  int t_detailed = 0;  // events after every resampling kernel too
   int t_next = 0;
   int t_pending = 0;
 };
@@ -137,7 +142,7 @@ Layout make_layout(const pf_engine_config_t* cfg, const pf_filter_params_t* fp) 
   L.off_desc = take(sizeof(FilterDesc) * cfg->n_filters);
   L.off_ctrl = take(sizeof(FilterCtrl) * cfg->n_filters);
   L.off_tf = take((size_t)T * 4);
-  L.off_queue = take(sizeof(unsigned) * 2 * Q_COUNT);
+  L.off_queue = take(sizeof(unsigned) * (2 * Q_COUNT + 8));
   L.off_err = take(sizeof(unsigned) * 4);
   L.obs_slot_bytes = align_up(sizeof(pf_filter_epoch_t) * cfg->n_filters +
                                   sizeof(pf_sat_t) * (size_t)cfg->n_filters * cfg->max_sats,
@@ -223,14 +228,42 @@ inline int grid_for(const pf_engine* eng, int slot, int count) {
   return std::max(1, std::min(count, eng->resident[slot]));
 }
 
+// Kernel launch with programmatic dependent launch: the kernel may start
+// while the previous kernel of the stream drains; it waits
+// (griddepcontrol.wait) before reading that kernel's results.  PF_B200_NO_PDL=1
+// in the environment turns it off (plain stream order).
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* v = getenv("PF_B200_NO_PDL");
+    return !(v && v[0] == '1');
+  }();
+  return on;
+}
+
+template <typename... KArgs, typename... Args>
+int launch_k(void (*kernel)(KArgs...), int grid, cudaStream_t st, const char* what, Args... args) {
+  cudaLaunchConfig_t lc;
+  memset(&lc, 0, sizeof(lc));
+  lc.gridDim = dim3((unsigned)grid);
+  lc.blockDim = dim3(kThreads);
+  lc.dynamicSmemBytes = 0;
+  lc.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = attr;
+  lc.numAttrs = pdl_enabled() ? 1 : 0;
+  cudaError_t e = cudaLaunchKernelEx(&lc, kernel, args...);
+  if (e != cudaSuccess) return set_err(PF_ECUDA, "%s launch: %s", what, cudaGetErrorString(e));
+  return PF_OK;
+}
+
 template <int NCLK>
 int launch_step_t(pf_engine* eng, int t0, int count) {
   const int g = grid_for(eng, Q_STEP, count);
   if (eng->cfg.weight_mode == PF_WEIGHT_GAUSSIAN)
-    k_step<NCLK, PF_WEIGHT_GAUSSIAN><<<g, kThreads, 0, eng->stream>>>(eng->dev, t0, count);
-  else
-    k_step<NCLK, PF_WEIGHT_HUBER><<<g, kThreads, 0, eng->stream>>>(eng->dev, t0, count);
-  return check_cuda(cudaGetLastError(), "k_step launch");
+    return launch_k(k_step<NCLK, PF_WEIGHT_GAUSSIAN>, g, eng->stream, "k_step", eng->dev, t0, count);
+  return launch_k(k_step<NCLK, PF_WEIGHT_HUBER>, g, eng->stream, "k_step", eng->dev, t0, count);
 }
 
 int launch_step(pf_engine* eng, int t0, int count) {
@@ -244,16 +277,21 @@ int launch_step(pf_engine* eng, int t0, int count) {
 
 // ev (optional): events recorded after each resampling kernel (3 entries).
 int launch_resample(pf_engine* eng, int t0, int count, int* n_launch, cudaEvent_t* ev = nullptr) {
+  int s;
   if (eng->cfg.resampler == PF_RESAMPLE_SYSTEMATIC) {
-    k_scan<<<grid_for(eng, Q_SCAN, count), kThreads, 0, eng->stream>>>(eng->dev, t0, count);
+    if ((s = launch_k(k_scan, grid_for(eng, Q_SCAN, count), eng->stream, "k_scan", eng->dev, t0, count)) != PF_OK)
+      return s;
     if (ev) cudaEventRecord(ev[0], eng->stream);
-    k_offs<<<grid_for(eng, Q_OFFS, count), kThreads, 0, eng->stream>>>(eng->dev, t0, count);
+    if ((s = launch_k(k_offs, grid_for(eng, Q_OFFS, count), eng->stream, "k_offs", eng->dev, t0, count)) != PF_OK)
+      return s;
     if (ev) cudaEventRecord(ev[1], eng->stream);
-    k_merge<<<grid_for(eng, Q_MERGE, count), kThreads, 0, eng->stream>>>(eng->dev, t0, count);
+    if ((s = launch_k(k_merge, grid_for(eng, Q_MERGE, count), eng->stream, "k_merge", eng->dev, t0, count)) != PF_OK)
+      return s;
     if (ev) cudaEventRecord(ev[2], eng->stream);
     *n_launch += 3;
   } else {
-    k_mego<<<grid_for(eng, Q_MEGO, count), kThreads, 0, eng->stream>>>(eng->dev, t0, count);
+    if ((s = launch_k(k_mego, grid_for(eng, Q_MEGO, count), eng->stream, "k_mego", eng->dev, t0, count)) != PF_OK)
+      return s;
     if (ev) {
       cudaEventRecord(ev[0], eng->stream);
       cudaEventRecord(ev[1], eng->stream);
@@ -264,11 +302,69 @@ int launch_resample(pf_engine* eng, int t0, int count, int* n_launch, cudaEvent_
   return check_cuda(cudaGetLastError(), "resample launch");
 }
 
+// ---- cooperative epoch kernel: instantiation table, occupancy, launch
+typedef void (*EpochKernel)(EngineDev, int, int, unsigned*);
+
+template <int NCLK, int WMODE>
+EpochKernel epoch_kernel_r(int resampler) {
+  return resampler == PF_RESAMPLE_SYSTEMATIC ? (EpochKernel)k_epoch<NCLK, WMODE, PF_RESAMPLE_SYSTEMATIC>
+                                             : (EpochKernel)k_epoch<NCLK, WMODE, PF_RESAMPLE_MEGOPOLIS>;
+}
+template <int NCLK>
+EpochKernel epoch_kernel_w(int wmode, int resampler) {
+  return wmode == PF_WEIGHT_GAUSSIAN ? epoch_kernel_r<NCLK, PF_WEIGHT_GAUSSIAN>(resampler)
+                                     : epoch_kernel_r<NCLK, PF_WEIGHT_HUBER>(resampler);
+}
+EpochKernel epoch_kernel(const pf_engine* eng) {
+  const int w = eng->cfg.weight_mode, r = eng->cfg.resampler;
+  switch (eng->cfg.n_clk) {
+    case 1: return epoch_kernel_w<1>(w, r);
+    case 2: return epoch_kernel_w<2>(w, r);
+    case 3: return epoch_kernel_w<3>(w, r);
+    default: return epoch_kernel_w<4>(w, r);
+  }
+}
+
+int prepare_epoch_kernel(pf_engine* eng) {
+  EpochKernel k = epoch_kernel(eng);
+  eng->epoch_smem = (size_t)2 * eng->D * kTile * sizeof(float);
+  CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eng->epoch_smem));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, eng->epoch_smem));
+  if (per_sm < 1) return set_err(PF_ECUDA, "epoch kernel does not fit on an SM");
+  eng->epoch_resident = per_sm * eng->sm_count;
+  return PF_OK;
+}
+
+// One cooperative launch over work items [t0, t0 + count): every CTA is
+// resident at once, which the grid barriers require (the driver refuses the
+// launch otherwise).
+int launch_epoch(pf_engine* eng, int t0, int count) {
+  const int grid = std::max(1, std::min(count, eng->epoch_resident));
+  cudaLaunchConfig_t lc;
+  memset(&lc, 0, sizeof(lc));
+  lc.gridDim = dim3((unsigned)grid);
+  lc.blockDim = dim3(kThreads);
+  lc.dynamicSmemBytes = eng->epoch_smem;
+  lc.stream = eng->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&lc, epoch_kernel(eng), eng->dev, t0, count, eng->bar);
+  if (e != cudaSuccess) return set_err(PF_ECUDA, "k_epoch cooperative launch: %s", cudaGetErrorString(e));
+  return PF_OK;
+}
+
+bool use_chain(const pf_engine* eng) { return (eng->cfg.flags & PF_FLAG_KERNEL_CHAIN) != 0; }
+
 int sync_and_check(pf_engine* eng) {
   CK(cudaStreamSynchronize(eng->stream));
   unsigned w = 0;
   CK(cudaMemcpy(&w, eng->dev.err, sizeof(unsigned), cudaMemcpyDeviceToHost));
   if (w & ERR_LOOKBACK_TIMEOUT) return set_err(PF_ETIMEOUT, "device look-back spin limit reached (error word 0x%x)", w);
+  if (w & ERR_BARRIER_TIMEOUT) return set_err(PF_ETIMEOUT, "device grid-barrier spin limit reached (error word 0x%x)", w);
   if (w & ERR_SAT_CAP) return set_err(PF_ECAP, "n_sat above max_sats (error word 0x%x)", w);
   if (w & ERR_BAD_WEIGHTS) return set_err(PF_EINVAL, "all log-weights non-finite (error word 0x%x)", w);
   return PF_OK;
@@ -372,6 +468,7 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
   e.ctrl = eng->ctrl_dev;
   e.tile_filter = (const int*)(w + L.off_tf);
   e.queue = (unsigned*)(w + L.off_queue);
+  eng->bar = e.queue + 2 * Q_COUNT;
   e.err = (unsigned*)(w + L.off_err);
   e.obs = w + L.off_obs;
   e.obs_slot_bytes = L.obs_slot_bytes;
@@ -407,6 +504,7 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
   if ((st = occupancy(k_offs, eng->sm_count, &eng->resident[Q_OFFS])) != PF_OK) return fail(st);
   if ((st = occupancy(k_merge, eng->sm_count, &eng->resident[Q_MERGE])) != PF_OK) return fail(st);
   if ((st = occupancy(k_mego, eng->sm_count, &eng->resident[Q_MEGO])) != PF_OK) return fail(st);
+  if ((st = prepare_epoch_kernel(eng)) != PF_OK) return fail(st);
   if ((st = occupancy(k_init<7>, eng->sm_count, &eng->resident[Q_INIT])) != PF_OK) return fail(st);
   if ((st = occupancy(k_estimate<7>, eng->sm_count, &eng->resident[Q_EST])) != PF_OK) return fail(st);
   if ((st = occupancy(k_export<7>, eng->sm_count, &eng->resident[Q_EXPORT])) != PF_OK) return fail(st);
@@ -429,7 +527,7 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
     c.rs_seq = 1;
   }
   if (check_cuda(cudaMemsetAsync(w + L.off_flag, 0, (size_t)L.T * 4, eng->stream), "memset flags") != PF_OK ||
-      check_cuda(cudaMemsetAsync(w + L.off_queue, 0, sizeof(unsigned) * 2 * Q_COUNT, eng->stream), "memset queue") != PF_OK ||
+      check_cuda(cudaMemsetAsync(w + L.off_queue, 0, sizeof(unsigned) * (2 * Q_COUNT + 8), eng->stream), "memset queue") != PF_OK ||
       check_cuda(cudaMemsetAsync(w + L.off_err, 0, sizeof(unsigned) * 4, eng->stream), "memset err") != PF_OK ||
       check_cuda(cudaMemsetAsync(w + L.off_obs, 0, L.obs_slot_bytes * cfg->obs_slots, eng->stream), "memset obs") != PF_OK ||
       check_cuda(cudaMemsetAsync(w + L.off_state0, 0, (size_t)L.D * L.P * 4, eng->stream), "memset state") != PF_OK ||
@@ -606,11 +704,20 @@ int pfe_step(pf_engine_t* eng) {
     eng->t_pending = std::min(eng->t_pending + 1, eng->t_slots);
     CK(cudaEventRecord(ev[0], eng->stream));
   }
+  if (!use_chain(eng)) {
+    int s = launch_epoch(eng, 0, eng->T);
+    if (s != PF_OK) return s;
+    if (ev)
+      for (int k = 1; k < kTimingEvents; ++k) CK(cudaEventRecord(ev[k], eng->stream));
+    eng->last_launches = 1;
+    return PF_OK;
+  }
   int s = launch_step(eng, 0, eng->T);
   if (s != PF_OK) return s;
   if (ev) CK(cudaEventRecord(ev[1], eng->stream));
-  s = launch_resample(eng, 0, eng->T, &n, ev ? ev + 2 : nullptr);
+  s = launch_resample(eng, 0, eng->T, &n, (ev && eng->t_detailed) ? ev + 2 : nullptr);
   if (s != PF_OK) return s;
+  if (ev && !eng->t_detailed) CK(cudaEventRecord(ev[kTimingEvents - 1], eng->stream));
   eng->last_launches = n;
   return PF_OK;
 }
@@ -624,9 +731,10 @@ int pfe_read_timing_kernels(pf_engine_t* eng, float* out, int max_entries, int* 
   return PF_OK;
 }
 
-int pfe_enable_timing(pf_engine_t* eng, int slots) {
+int pfe_enable_timing(pf_engine_t* eng, int slots, int detailed) {
   clear_err();
   if (!eng) return set_err(PF_EINVAL, "null engine");
+  eng->t_detailed = detailed ? 1 : 0;
   if (slots < 0) return set_err(PF_EINVAL, "slots must be >= 0");
   if (eng->gexec || eng->graph) return set_err(PF_EINVAL, "timing applies to eager steps, not captured graphs");
   CK(cudaStreamSynchronize(eng->stream));
@@ -661,9 +769,10 @@ int pfe_read_timing(pf_engine_t* eng, float* step_kernel_ms, float* whole_step_m
     if (whole_step_ms) whole_step_ms[i] = b;
     for (int k = 0; k < kTimingEvents - 1; ++k) {
       float m = 0.f;
-      CK(cudaEventElapsedTime(&m, ev[k], ev[k + 1]));
+      if (eng->t_detailed || k == 0) CK(cudaEventElapsedTime(&m, ev[k], ev[k + 1]));
       eng->t_kernel_ms[(size_t)i * (kTimingEvents - 1) + k] = m;
     }
+    if (!eng->t_detailed) eng->t_kernel_ms[(size_t)i * (kTimingEvents - 1) + 1] = b - a;
   }
   *count = n;
   eng->t_pending = 0;
@@ -677,6 +786,12 @@ int pfe_step_per_filter(pf_engine_t* eng) {
   for (int f = 0; f < eng->cfg.n_filters; ++f) {
     if (!eng->initialized[f]) return set_err(PF_ENOTINIT, "filter %d not initialized", f);
     const FilterDesc& d = eng->hdesc[f];
+    if (!use_chain(eng)) {
+      int s = launch_epoch(eng, d.tile_begin, d.n_tiles);
+      if (s != PF_OK) return s;
+      ++n;
+      continue;
+    }
     int s = launch_step(eng, d.tile_begin, d.n_tiles);
     if (s != PF_OK) return s;
     ++n;
@@ -937,6 +1052,8 @@ int pfe_test_poison_lookback(pf_engine_t* eng, int on) {
   if (!on) {
     CK(cudaStreamSynchronize(eng->stream));
     CK(cudaMemset(eng->dev.err, 0, sizeof(unsigned)));
+    // timed-out barriers leave their arrival count behind: start clean
+    CK(cudaMemset(eng->bar, 0, sizeof(unsigned) * 8));
   }
   return PF_OK;
 }

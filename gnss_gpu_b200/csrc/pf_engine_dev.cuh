@@ -21,7 +21,7 @@ enum QueueSlot : int {
 };
 
 // Error word bits.
-enum : unsigned { ERR_LOOKBACK_TIMEOUT = 1u, ERR_BAD_WEIGHTS = 2u, ERR_SAT_CAP = 4u };
+enum : unsigned { ERR_LOOKBACK_TIMEOUT = 1u, ERR_BAD_WEIGHTS = 2u, ERR_SAT_CAP = 4u, ERR_BARRIER_TIMEOUT = 8u };
 
 struct FilterDesc {
   int n;

@@ -25,6 +25,14 @@ namespace pfb {
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ float2 bc(float a) { return make_float2(a, a); }
 
+// Programmatic dependent launch (sm_90+): a kernel lets the next kernel of
+// the stream start launching as soon as all of its CTAs are running, and
+// waits for the previous kernel's completion (and memory flush) before it
+// reads anything that kernel wrote.  Both are no-ops without a programmatic
+// dependency.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ int dequeue(unsigned* q, int* s_slot) {
   if (threadIdx.x == 0) *s_slot = (int)atomicAdd(q, 1u);
   __syncthreads();
@@ -181,14 +189,16 @@ __device__ __forceinline__ MergedStats merge_tiles(const float* part, int tb, in
   for (int i = 0; i < NV; ++i) acc[i] = 0.0;
   if (M > -INFINITY) {
     for (int i = threadIdx.x; i < nt; i += kThreads) {
-      const float* row = part + (size_t)(tb + i) * kPartStride;
-      float pm = __ldcg(row);
-      if (!(pm > -INFINITY)) continue;
-      double sc = exp((double)pm - (double)M);
-      acc[0] += sc * (double)__ldcg(row + 1);
-      acc[1] += sc * sc * (double)__ldcg(row + 2);
+      const float4* row4 = reinterpret_cast<const float4*>(part + (size_t)(tb + i) * kPartStride);
+      const float4 a0 = __ldcg(row4), a1 = __ldcg(row4 + 1), a2 = __ldcg(row4 + 2), a3 = __ldcg(row4 + 3);
+      const float r[16] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w,
+                           a2.x, a2.y, a2.z, a2.w, a3.x, a3.y, a3.z, a3.w};
+      if (!(r[0] > -INFINITY)) continue;
+      const double sc = exp((double)r[0] - (double)M);
+      acc[0] += sc * (double)r[1];
+      acc[1] += sc * sc * (double)r[2];
 #pragma unroll
-      for (int v = 2; v < NV; ++v) acc[v] += sc * (double)__ldcg(row + 1 + v);
+      for (int v = 2; v < NV; ++v) acc[v] += sc * (double)r[1 + v];
     }
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -257,24 +267,160 @@ __device__ __forceinline__ void load_particles(const EngineDev& e, const float* 
   }
 }
 
+// Sums 16 per-lane values over a warp with 16 shuffles (a transpose-style
+// butterfly: every step halves the values a lane holds).  Afterwards v[0]
+// of lane l holds the warp total of value index
+//   ((l >> 4) & 1) * 8 + ((l >> 3) & 1) * 4 + ((l >> 2) & 1) * 2 + ((l >> 1) & 1),
+// which is returned; lanes l and l ^ 1 hold the same total.
+__device__ __forceinline__ int warp_transpose_sum16(float (&v)[16]) {
+  const int lane = threadIdx.x & 31;
+  {
+    const bool up = (lane & 16) != 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const float send = up ? v[i] : v[i + 8];
+      const float keep = up ? v[i + 8] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+  }
+  {
+    const bool up = (lane & 8) != 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float send = up ? v[i] : v[i + 4];
+      const float keep = up ? v[i + 4] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+  }
+  {
+    const bool up = (lane & 4) != 0;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const float send = up ? v[i] : v[i + 2];
+      const float keep = up ? v[i + 2] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+  }
+  {
+    const bool up = (lane & 2) != 0;
+    const float send = up ? v[0] : v[1];
+    const float keep = up ? v[1] : v[0];
+    v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+  }
+  v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+  return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+}
+
+// The last tile of a filter: merged statistics -> estimate, covariance,
+// ESS, the device-side resample decision (particle_filter.py:159-161), the
+// next re-centring shift, the systematic offset, and the epoch/parity step.
+// Executed by one thread.
+template <int D>
+__device__ __forceinline__ void finalize_filter(const EngineDev& e, const FilterDesc* fd, FilterCtrl* fc,
+                                                const MergedStats& ms, unsigned epoch, int parity,
+                                                bool lw_zero, int eflags, bool do_weight) {
+  constexpr int NCLK = D - 3;
+  const int n = fd->n;
+  const double W = ms.w;
+  const double ess = (ms.w2 > 0.0) ? (W * W) / ms.w2 : 0.0;
+  double mu[kMaxD];
+#pragma unroll
+  for (int d = 0; d < kMaxD; ++d) mu[d] = (W > 0.0 && d < D) ? ms.sx[d] / W : 0.0;
+  double A[3];
+  local_to_ecef(fd->rot, fc->anchor, fc->shift[0], fc->shift[1], fc->shift[2], A);
+  double est[3];
+  local_to_ecef(fd->rot, A, mu[0], mu[1], mu[2], est);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    fc->anchor[i] = A[i];
+    fc->est_ecef[i] = est[i];
+  }
+#pragma unroll
+  for (int c = 0; c < PF_MAX_CLK; ++c) {
+    if (c < NCLK) {
+      const double ca = fc->clk_anchor[c] + (double)fc->shift[3 + c];
+      fc->clk_anchor[c] = ca;
+      fc->est_clk[c] = ca + mu[3 + c];
+    } else {
+      fc->est_clk[c] = 0.0;
+    }
+  }
+  if ((e.flags & PF_FLAG_COVARIANCE) && W > 0.0) {
+    fc->cov[0] = ms.sxx[0] / W - mu[0] * mu[0];
+    fc->cov[1] = ms.sxx[1] / W - mu[0] * mu[1];
+    fc->cov[2] = ms.sxx[2] / W - mu[0] * mu[2];
+    fc->cov[3] = ms.sxx[3] / W - mu[1] * mu[1];
+    fc->cov[4] = ms.sxx[4] / W - mu[1] * mu[2];
+    fc->cov[5] = ms.sxx[5] / W - mu[2] * mu[2];
+  }
+  fc->ess = ess;
+  fc->sum_w = W;
+  fc->max_lw = ms.max_lw;
+  const bool recenter = (e.flags & PF_FLAG_RECENTER) != 0 && W > 0.0;
+#pragma unroll
+  for (int d = 0; d < 8; ++d) fc->shift[d] = (recenter && d < D) ? (float)mu[d] : 0.f;
+  bool rs = do_weight && !(eflags & PF_EP_NO_RESAMPLE) &&
+            ((eflags & PF_EP_FORCE_RESAMPLE) || ess < (double)e.ess_threshold * (double)n);
+  if (!(W > 0.0) || !(ms.max_lw > -INFINITY)) {
+    if (do_weight) atomicOr(e.err, ERR_BAD_WEIGHTS);
+    rs = false;
+  }
+  fc->resample_flag = rs ? 1 : 0;
+  fc->lw_zero = rs ? 1 : (do_weight ? 0 : (lw_zero ? 1 : 0));
+  if (rs) {
+    fc->rs_seq = fc->rs_seq + 1u;
+    uint32_t u = fd->sys_ref_u;
+    if (e.sys_offset == PF_SYS_OFFSET_RANDOM) {
+      const U4 r = philox10(U4{0u, epoch, TAG_SYS_U, (uint32_t)fd->filter_id}, fd->key0, fd->key1);
+      u = r.x;
+    }
+    fc->sys_u = u;
+  }
+  fc->parity = parity ^ 1;
+  fc->epoch = epoch + 1u;
+  fc->ticket = 0u;
+  __threadfence();
+}
+
 // -------------------------------------------------------------------------
 // k_step: fused predict + weight + statistics (+ per-filter finalize).
+//
+// Per tile (1024 particles, 4 per thread as one float4 per component):
+//   load (gathered through the last resample's ancestors if any) ->
+//   predict with Philox/Box-Muller noise -> store -> likelihood over the
+//   filter's satellites -> store log-weights -> per-warp statistics with a
+//   transpose-style butterfly reduction -> one barrier -> warp 0 merges the
+//   eight warp rows into the tile row, takes the filter's ticket and the
+//   next tile -> one barrier.  The last tile of a filter merges all tile
+//   rows in FP64 and writes the filter's control block.
+//
+// Satellite constants sit in shared memory as pre-broadcast pairs, so the
+// packed f32x2 operations read them without register moves.
+#ifndef PF_KSTEP_MINB
+#define PF_KSTEP_MINB 2  // resident CTAs per SM the fused step is compiled for
+#endif
 template <int NCLK, int WMODE>
-__global__ void __launch_bounds__(kThreads, 2) k_step(EngineDev e, int t0, int count) {
+__global__ void __launch_bounds__(kThreads, PF_KSTEP_MINB) k_step(EngineDev e, int t0, int count) {
   constexpr int D = 3 + NCLK;
-  __shared__ float4 s_sat[2 * PF_MAX_SATS];
+  constexpr int NV = 2 + D + 6;  // s, s2, sx[D], xx, xy, xz, yy, yz, zz
+  constexpr int kWarps = kThreads / 32;
+  __shared__ float2 s_sat[8 * PF_MAX_SATS];  // per satellite: e_E, e_N, e_U, -g/2, g^2/2, g/2, y, wq
   __shared__ int s_grp[PF_MAX_CLK + 1];
   __shared__ unsigned char s_clk[PF_MAX_SATS];
-  __shared__ float s_red[kThreads / 32][kPartStride];
-  __shared__ float s_maxtmp[kThreads / 32];
-  __shared__ double s_dred[(kThreads / 32) * 16];
-  __shared__ int s_slot, s_last;
+  __shared__ float s_wrow[kWarps][17];       // per-warp max + NV sums
+  __shared__ float s_maxtmp[kWarps];
+  __shared__ double s_dred[kWarps * 16];
+  __shared__ int s_next, s_last;
 
   unsigned* q = e.queue + 2 * Q_STEP;
+  pdl_trigger();
+  pdl_wait();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_next = (int)atomicAdd(q, 1u);
+  __syncthreads();
+  int tq = s_next;
   int cached = -1;
-  for (;;) {
-    const int tq = dequeue(q, &s_slot);
-    if (tq >= count) break;
+  while (tq < count) {
     const int t = t0 + tq;
     const int f = __ldg(e.tile_filter + t);
     const FilterDesc* fd = e.desc + f;
@@ -296,10 +442,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(EngineDev e, int t0, int c
     const bool do_predict = (eflags & PF_EP_PREDICT) != 0;
     const bool do_weight = (eflags & PF_EP_WEIGHT) != 0;
 
-    // ---- per-filter satellite geometry in FP64, stored as FP32 in smem,
-    //      grouped by clock state.
+    // ---- per-filter satellite geometry in FP64, stored as FP32 pairs in
+    //      smem, grouped by clock state (stable order).
     if (f != cached) {
-      // clock index of every satellite, staged once (one coalesced read)
       int my_c = 0;
       const pf_sat_t* sp = sats + fe->sat_offset + threadIdx.x;
       if (do_weight && threadIdx.x < n_sat) {
@@ -310,31 +455,34 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(EngineDev e, int t0, int c
       __syncthreads();
       if (do_weight && threadIdx.x < n_sat) {
         const double* rot = fd->rot;
-        const double sh0 = fc->shift[0], sh1 = fc->shift[1], sh2 = fc->shift[2];
         double A[3];
-        local_to_ecef(rot, fc->anchor, sh0, sh1, sh2, A);
+        local_to_ecef(rot, fc->anchor, fc->shift[0], fc->shift[1], fc->shift[2], A);
         const int c = my_c;
         const double clkA = fc->clk_anchor[c] + (double)fc->shift[3 + c];
         double vx = sp->x - A[0], vy = sp->y - A[1], vz = sp->z - A[2];
-        double r0 = sqrt(vx * vx + vy * vy + vz * vz);
-        double inv = 1.0 / r0;
+        const double r0 = sqrt(vx * vx + vy * vy + vz * vz);
+        const double inv = 1.0 / r0;
         vx *= inv; vy *= inv; vz *= inv;
-        double eE = rot[0] * vx + rot[1] * vy + rot[2] * vz;
-        double eN = rot[3] * vx + rot[4] * vy + rot[5] * vz;
-        double eU = rot[6] * vx + rot[7] * vy + rot[8] * vz;
-        float g = (float)inv;
-        float y = (float)(sp->pr - r0 - clkA);
-        float wq = WMODE == PF_WEIGHT_GAUSSIAN ? (float)((double)fd->wscale * sp->w) : (float)sp->w;
-        float4 a4 = make_float4((float)eE, (float)eN, (float)eU, -0.5f * g);
-        float4 b4 = make_float4(0.5f * g * g, 0.5f * g, y, wq);
-        // stable order by clock state
+        const float eE = (float)(rot[0] * vx + rot[1] * vy + rot[2] * vz);
+        const float eN = (float)(rot[3] * vx + rot[4] * vy + rot[5] * vz);
+        const float eU = (float)(rot[6] * vx + rot[7] * vy + rot[8] * vz);
+        const float g = (float)inv;
+        const float y = (float)(sp->pr - r0 - clkA);
+        const float wq = WMODE == PF_WEIGHT_GAUSSIAN ? (float)((double)fd->wscale * sp->w) : (float)sp->w;
         int rank = 0;
         for (int s2 = 0; s2 < n_sat; ++s2) {
           const int c2 = s_clk[s2];
           rank += (c2 < c) || (c2 == c && s2 < (int)threadIdx.x);
         }
-        s_sat[2 * rank] = a4;
-        s_sat[2 * rank + 1] = b4;
+        float2* o = s_sat + 8 * rank;
+        o[0] = bc(eE);
+        o[1] = bc(eN);
+        o[2] = bc(eU);
+        o[3] = bc(-0.5f * g);
+        o[4] = bc(0.5f * g * g);
+        o[5] = bc(0.5f * g);
+        o[6] = bc(y);
+        o[7] = bc(wq);
       }
       if (threadIdx.x <= NCLK) {
         int cnt = 0;
@@ -355,13 +503,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(EngineDev e, int t0, int c
     float* dst = parity ? e.state0 : e.state1;
 
     float x[D][4];
-    float lwv[4];
+    float lwv[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
 #pragma unroll
     for (int d = 0; d < D; ++d)
 #pragma unroll
       for (int k = 0; k < 4; ++k) x[d][k] = 0.f;
     if (active) {
       load_particles<D>(e, src, base, p0, n, gather, x);
+      float lw0[4] = {0.f, 0.f, 0.f, 0.f};
+      const bool need_prev = !lw_zero && (!do_weight || e.lw_mode == PF_LW_ACCUMULATE);
+      if (need_prev) {
+        float4 v = __ldcs(reinterpret_cast<const float4*>(e.lw + base + p0));
+        lw0[0] = v.x; lw0[1] = v.y; lw0[2] = v.z; lw0[3] = v.w;
+      }
       // predict: x += disp - shift + sigma * N(0,1)
       float ds[D];
 #pragma unroll
@@ -371,14 +525,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(EngineDev e, int t0, int c
         ds[1] += (float)fe->disp[1];
         ds[2] += (float)fe->disp[2];
         const uint32_t fid = (uint32_t)fd->filter_id;
+        const uint32_t k0 = fd->key0, k1 = fd->key1;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           float nz[8];
-          U4 r = philox10(U4{(uint32_t)(p0 + k), epoch, TAG_PREDICT, fid}, fd->key0, fd->key1);
+          U4 r = philox10(U4{(uint32_t)(p0 + k), epoch, TAG_PREDICT, fid}, k0, k1);
           float2 a = box_muller_f32(r.x, r.y), b = box_muller_f32(r.z, r.w);
           nz[0] = a.x; nz[1] = a.y; nz[2] = b.x; nz[3] = b.y;
           if (D > 4) {
-            U4 r2 = philox10(U4{(uint32_t)(p0 + k), epoch, TAG_PREDICT | 1u, fid}, fd->key0, fd->key1);
+            U4 r2 = philox10(U4{(uint32_t)(p0 + k), epoch, TAG_PREDICT | 1u, fid}, k0, k1);
             float2 c = box_muller_f32(r2.x, r2.y), dd = box_muller_f32(r2.z, r2.w);
             nz[4] = c.x; nz[5] = c.y; nz[6] = dd.x; nz[7] = dd.y;
           } else {
@@ -398,14 +553,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(EngineDev e, int t0, int c
         __stcs(reinterpret_cast<float4*>(dst + (size_t)d * e.p_total + base + p0),
                make_float4(x[d][0], x[d][1], x[d][2], x[d][3]));
 
-      // previous log-weights (accumulate mode, or statistics of a
-      // predict-only step)
-      float lw0[4] = {0.f, 0.f, 0.f, 0.f};
-      const bool need_prev = !lw_zero && (!do_weight || e.lw_mode == PF_LW_ACCUMULATE);
-      if (need_prev) {
-        float4 v = __ldcs(reinterpret_cast<const float4*>(e.lw + base + p0));
-        lw0[0] = v.x; lw0[1] = v.y; lw0[2] = v.z; lw0[3] = v.w;
-      }
       if (do_weight) {
         float2 lwp[2] = {f2(lw0[0], lw0[1]), f2(lw0[2], lw0[3])};
         float2 dx[2], dy[2], dz[2], bb[2];
@@ -420,31 +567,34 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(EngineDev e, int t0, int c
         }
 #pragma unroll
         for (int c = 0; c < NCLK; ++c) {
-          float2 ncb[2] = {f2(-x[3 + c][0], -x[3 + c][1]), f2(-x[3 + c][2], -x[3 + c][3])};
+          const float2 ncb[2] = {f2(-x[3 + c][0], -x[3 + c][1]), f2(-x[3 + c][2], -x[3 + c][3])};
           const int s_end = s_grp[c + 1];
+#pragma unroll 2
           for (int s = s_grp[c]; s < s_end; ++s) {
-            const float4 A = s_sat[2 * s];
-            const float4 B = s_sat[2 * s + 1];
+            const float4* sv = reinterpret_cast<const float4*>(s_sat + 8 * s);
+            const float4 q0 = sv[0], q1 = sv[1], q2 = sv[2], q3 = sv[3];
+            const float2 eE = f2(q0.x, q0.y), eN = f2(q0.z, q0.w), eU = f2(q1.x, q1.y), ng2 = f2(q1.z, q1.w);
+            const float2 c2 = f2(q2.x, q2.y), nc1 = f2(q2.z, q2.w), yy = f2(q3.x, q3.y), wq = f2(q3.z, q3.w);
 #pragma unroll
             for (int p = 0; p < 2; ++p) {
-              float2 ed = __fmul2_rn(bc(A.x), dx[p]);
-              ed = __ffma2_rn(bc(A.y), dy[p], ed);
-              ed = __ffma2_rn(bc(A.z), dz[p], ed);           // e . d
-              float2 nh = __ffma2_rn(bb[p], bc(A.w), ed);     // -h = e.d - |d|^2 g/2
-              float2 ninner = __ffma2_rn(nh, bc(B.x), bc(B.y));
-              float2 hh = __fmul2_rn(nh, nh);
-              float2 ndl = __ffma2_rn(hh, ninner, nh);        // -(|s-d| - r0)
-              float2 r = __fadd2_rn(__fadd2_rn(bc(B.z), ncb[p]), ndl);
+              float2 ed = __fmul2_rn(eE, dx[p]);
+              ed = __ffma2_rn(eN, dy[p], ed);
+              ed = __ffma2_rn(eU, dz[p], ed);                 // e . d
+              const float2 nh = __ffma2_rn(bb[p], ng2, ed);   // -h = e.d - |d|^2 g/2
+              const float2 ninner = __ffma2_rn(nh, c2, nc1);
+              const float2 hh = __fmul2_rn(nh, nh);
+              const float2 ndl = __ffma2_rn(hh, ninner, nh);  // -(|s-d| - r0)
+              const float2 r = __fadd2_rn(__fadd2_rn(yy, ncb[p]), ndl);
               if (WMODE == PF_WEIGHT_GAUSSIAN) {
-                float2 rw = __fmul2_rn(r, bc(B.w));
+                const float2 rw = __fmul2_rn(r, wq);
                 lwp[p] = __ffma2_rn(rw, r, lwp[p]);
               } else {
                 const float ks = fd->huber_k;
-                float z0 = fabsf(r.x) * fd->inv_sigma_pr, z1 = fabsf(r.y) * fd->inv_sigma_pr;
-                float rho0 = z0 < ks ? 0.5f * z0 * z0 : fmaf(ks, z0, -0.5f * ks * ks);
-                float rho1 = z1 < ks ? 0.5f * z1 * z1 : fmaf(ks, z1, -0.5f * ks * ks);
-                lwp[p].x = fmaf(-B.w, rho0, lwp[p].x);
-                lwp[p].y = fmaf(-B.w, rho1, lwp[p].y);
+                const float z0 = fabsf(r.x) * fd->inv_sigma_pr, z1 = fabsf(r.y) * fd->inv_sigma_pr;
+                const float rho0 = z0 < ks ? 0.5f * z0 * z0 : fmaf(ks, z0, -0.5f * ks * ks);
+                const float rho1 = z1 < ks ? 0.5f * z1 * z1 : fmaf(ks, z1, -0.5f * ks * ks);
+                lwp[p].x = fmaf(-wq.x, rho0, lwp[p].x);
+                lwp[p].y = fmaf(-wq.x, rho1, lwp[p].y);
               }
             }
           }
@@ -458,92 +608,81 @@ __global__ void __launch_bounds__(kThreads, 2) k_step(EngineDev e, int t0, int c
 #pragma unroll
       for (int k = 0; k < 4; ++k)
         if (p0 + k >= n) lwv[k] = -INFINITY;
-    } else {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) lwv[k] = -INFINITY;
     }
 
-    float* row = e.part + (size_t)t * kPartStride;
-    tile_stats<D>(x, lwv, (e.flags & PF_FLAG_COVARIANCE) != 0, row, s_maxtmp, s_red);
-
-    if (threadIdx.x == 0) {
-      __threadfence();
-      unsigned old = atomicAdd(&fc->ticket, 1u);
-      s_last = (old == (unsigned)fd->n_tiles - 1u);
+    // ---- per-warp statistics (own max), butterfly-transposed sums
+    {
+      float wm = fmaxf(fmaxf(lwv[0], lwv[1]), fmaxf(lwv[2], lwv[3]));
+      wm = warp_max(wm);
+      float v[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) v[i] = 0.f;
+      if (wm > -INFINITY) {
+        const bool cov = (e.flags & PF_FLAG_COVARIANCE) != 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const float w = exp2f((lwv[k] - wm) * 1.4426950408889634f);
+          v[0] += w;
+          v[1] = fmaf(w, w, v[1]);
+#pragma unroll
+          for (int d = 0; d < D; ++d) v[2 + d] = fmaf(w, x[d][k], v[2 + d]);
+          if (cov) {
+            const float wx = w * x[0][k], wy = w * x[1][k], wz = w * x[2][k];
+            v[2 + D + 0] = fmaf(wx, x[0][k], v[2 + D + 0]);
+            v[2 + D + 1] = fmaf(wx, x[1][k], v[2 + D + 1]);
+            v[2 + D + 2] = fmaf(wx, x[2][k], v[2 + D + 2]);
+            v[2 + D + 3] = fmaf(wy, x[1][k], v[2 + D + 3]);
+            v[2 + D + 4] = fmaf(wy, x[2][k], v[2 + D + 4]);
+            v[2 + D + 5] = fmaf(wz, x[2][k], v[2 + D + 5]);
+          }
+        }
+      }
+      const int idx = warp_transpose_sum16(v);  // lane holds the warp total of value idx
+      if ((lane & 1) == 0 && idx < NV) s_wrow[warp][1 + idx] = v[0];
+      if (lane == 0) s_wrow[warp][0] = wm;
     }
     __syncthreads();
+    if (warp == 0) {
+      // merge the warp rows: lane i < NV sums value i with max-shift scales
+      float tm = lane < kWarps ? s_wrow[lane][0] : -INFINITY;
+      tm = warp_max(tm);
+      float acc = 0.f;
+      if (lane < NV && tm > -INFINITY) {
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+          const float mw = s_wrow[w][0];
+          if (mw > -INFINITY) {
+            float sc = exp2f((mw - tm) * 1.4426950408889634f);
+            if (lane == 1) sc *= sc;
+            acc = fmaf(sc, s_wrow[w][1 + lane], acc);
+          }
+        }
+      }
+      float* row = e.part + (size_t)t * kPartStride;
+      if (lane < NV) row[1 + lane] = acc;
+      if (lane == 0) row[0] = tm;
+      __syncwarp();
+      if (lane == 0) {
+        __threadfence();
+        const unsigned old = atomicAdd(&fc->ticket, 1u);
+        s_last = (old == (unsigned)fd->n_tiles - 1u);
+        s_next = (int)atomicAdd(q, 1u);
+      }
+    }
+    __syncthreads();
+    const int next = s_next;
     if (s_last) {
       __threadfence();
       MergedStats ms = merge_tiles<D>(e.part, fd->tile_begin, fd->n_tiles, s_maxtmp, s_dred);
-      if (threadIdx.x == 0) {
-        const double W = ms.w;
-        const double ess = (ms.w2 > 0.0) ? (W * W) / ms.w2 : 0.0;
-        double mu[kMaxD];
-#pragma unroll
-        for (int d = 0; d < kMaxD; ++d) mu[d] = (W > 0.0 && d < D) ? ms.sx[d] / W : 0.0;
-        double A[3];
-        local_to_ecef(fd->rot, fc->anchor, fc->shift[0], fc->shift[1], fc->shift[2], A);
-        double est[3];
-        local_to_ecef(fd->rot, A, mu[0], mu[1], mu[2], est);
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          fc->anchor[i] = A[i];
-          fc->est_ecef[i] = est[i];
-        }
-#pragma unroll
-        for (int c = 0; c < PF_MAX_CLK; ++c) {
-          if (c < NCLK) {
-            double ca = fc->clk_anchor[c] + (double)fc->shift[3 + c];
-            fc->clk_anchor[c] = ca;
-            fc->est_clk[c] = ca + mu[3 + c];
-          } else {
-            fc->est_clk[c] = 0.0;
-          }
-        }
-        if (e.flags & PF_FLAG_COVARIANCE) {
-          if (W > 0.0) {
-            fc->cov[0] = ms.sxx[0] / W - mu[0] * mu[0];
-            fc->cov[1] = ms.sxx[1] / W - mu[0] * mu[1];
-            fc->cov[2] = ms.sxx[2] / W - mu[0] * mu[2];
-            fc->cov[3] = ms.sxx[3] / W - mu[1] * mu[1];
-            fc->cov[4] = ms.sxx[4] / W - mu[1] * mu[2];
-            fc->cov[5] = ms.sxx[5] / W - mu[2] * mu[2];
-          }
-        }
-        fc->ess = ess;
-        fc->sum_w = W;
-        fc->max_lw = ms.max_lw;
-        const bool recenter = (e.flags & PF_FLAG_RECENTER) != 0 && W > 0.0;
-#pragma unroll
-        for (int d = 0; d < 8; ++d) fc->shift[d] = (recenter && d < D) ? (float)mu[d] : 0.f;
-        bool rs = do_weight && !(eflags & PF_EP_NO_RESAMPLE) &&
-                  ((eflags & PF_EP_FORCE_RESAMPLE) || ess < (double)e.ess_threshold * (double)n);
-        if (!(W > 0.0) || !(ms.max_lw > -INFINITY)) {
-          if (do_weight) atomicOr(e.err, ERR_BAD_WEIGHTS);
-          rs = false;
-        }
-        fc->resample_flag = rs ? 1 : 0;
-        fc->lw_zero = rs ? 1 : (do_weight ? 0 : (lw_zero ? 1 : 0));
-        if (rs) {
-          fc->rs_seq = fc->rs_seq + 1u;
-          uint32_t u = fd->sys_ref_u;
-          if (e.sys_offset == PF_SYS_OFFSET_RANDOM) {
-            U4 r = philox10(U4{0u, epoch, TAG_SYS_U, (uint32_t)fd->filter_id}, fd->key0, fd->key1);
-            u = r.x;
-          }
-          fc->sys_u = u;
-        }
-        fc->parity = parity ^ 1;
-        fc->epoch = epoch + 1u;
-        fc->ticket = 0u;
-        __threadfence();
-      }
+      if (threadIdx.x == 0) finalize_filter<D>(e, fd, fc, ms, epoch, parity, lw_zero, eflags, do_weight);
       __syncthreads();
     }
+    tq = next;
   }
   queue_exit(q);
 }
 
+// -------------------------------------------------------------------------
 // Quantised weights of particles [p0, p0+4): from the FP32 log-weights of
 // the engine, or from FP64 log-weights when the stateless API set lw64.
 // The shift lw - max is exact in FP64 for FP32 inputs.
@@ -571,6 +710,8 @@ __global__ void __launch_bounds__(kThreads) k_scan(EngineDev e, int t0, int coun
   __shared__ unsigned long long s_u64[kThreads / 32];
   __shared__ int s_slot, s_first;
   unsigned* q = e.queue + 2 * Q_SCAN;
+  pdl_trigger();
+  pdl_wait();
   for (;;) {
     const int tq = dequeue(q, &s_slot);
     if (tq >= count) break;
@@ -670,6 +811,8 @@ __global__ void __launch_bounds__(kThreads) k_offs(EngineDev e, int t0, int coun
   __shared__ unsigned long long s_u64[kThreads / 32];
   __shared__ int s_slot;
   unsigned* q = e.queue + 2 * Q_OFFS;
+  pdl_trigger();
+  pdl_wait();
   for (;;) {
     const int tq = dequeue(q, &s_slot);
     if (tq >= count) break;
@@ -695,12 +838,13 @@ __global__ void __launch_bounds__(kThreads) k_offs(EngineDev e, int t0, int coun
         continue;
       }
       unsigned long long C = __ldcg(e.tile_excl + t) + texcl;
-      uint32_t Fprev = (p0 == 0) ? 0u : offspring_end(C, W, (uint32_t)n, u);
+      const double scale = (double)n / (double)W, uf = (double)u * 2.3283064365386963e-10;
+      uint32_t Fprev = (p0 == 0) ? 0u : offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf);
       uint32_t Fk[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         C += qv[k];
-        Fk[k] = (p0 + k < n) ? offspring_end(C, W, (uint32_t)n, u) : (uint32_t)n;
+        Fk[k] = (p0 + k < n) ? offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf) : (uint32_t)n;
       }
       *reinterpret_cast<uint4*>(e.offs + base + p0) = make_uint4(Fk[0], Fk[1], Fk[2], Fk[3]);
 #pragma unroll
@@ -719,13 +863,56 @@ __global__ void __launch_bounds__(kThreads) k_offs(EngineDev e, int t0, int coun
 }
 
 // -------------------------------------------------------------------------
-// k_merge: walk the merge path of (offspring ends F, slots) over a window of
-// 2*kTile diagonals; slot k gets ancestor i when F(i-1) <= k < F(i).
-__global__ void __launch_bounds__(kThreads) k_merge(EngineDev e, int t0, int count) {
+// Merge path of one diagonal tile (t - tile_begin = c): walk the merge of
+// (offspring ends F, slots) over diagonals [c*2*kTile, (c+1)*2*kTile); slot
+// k gets ancestor i when F(i-1) <= k < F(i).  s_F: 2*kTile+1 words of smem.
+__device__ __forceinline__ void merge_tile(const EngineDev& e, const FilterDesc* fd, int t, uint32_t* s_F) {
   constexpr int kSteps = kMergeDiag / kThreads;  // 8
+  const int n = fd->n;
+  const int tb = fd->tile_begin, c = t - tb;
+  const long long base = fd->p_off;
+  const long long d0 = (long long)c * kMergeDiag;
+  const long long dend = min(d0 + kMergeDiag, 2ll * n);
+  const int i0 = (int)__ldcg(e.mp_part + t);
+  if (i0 < 0 || i0 >= n) {  // cannot happen with valid weights; never index with it
+    if (threadIdx.x == 0) atomicOr(e.err, ERR_BAD_WEIGHTS);
+    return;
+  }
+  const int win = min(kMergeDiag + 1, n - i0);
+  __syncthreads();  // the window buffer is free
+  for (int w = threadIdx.x; w < win; w += kThreads) s_F[w] = __ldcg(e.offs + base + i0 + w);
+  __syncthreads();
+  const long long d = d0 + (long long)threadIdx.x * kSteps;
+  if (d < dend) {
+    int lo = 0, hi = (int)min((long long)(win - 1), d - d0);
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if ((long long)(i0 + mid) + (long long)s_F[mid] >= d) hi = mid;
+      else lo = mid + 1;
+    }
+    int i = i0 + lo;
+    long long k = d - i;
+    const int steps = (int)min((long long)kSteps, dend - d);
+    for (int s = 0; s < steps; ++s) {
+      const int wi = i - i0;
+      if (wi >= win) break;
+      if (k < (long long)s_F[wi]) {
+        if (k >= 0 && k < n) e.anc[base + k] = i;
+        ++k;
+      } else {
+        ++i;
+      }
+    }
+  }
+}
+
+// k_merge: merge_tile over the launch's tiles.
+__global__ void __launch_bounds__(kThreads) k_merge(EngineDev e, int t0, int count) {
   __shared__ uint32_t s_F[kMergeDiag + 1];
   __shared__ int s_slot;
   unsigned* q = e.queue + 2 * Q_MERGE;
+  pdl_trigger();
+  pdl_wait();
   for (;;) {
     const int tq = dequeue(q, &s_slot);
     if (tq >= count) break;
@@ -734,56 +921,69 @@ __global__ void __launch_bounds__(kThreads) k_merge(EngineDev e, int t0, int cou
     const FilterDesc* fd = e.desc + f;
     const FilterCtrl* fc = e.ctrl + f;
     if (!fc->resample_flag) continue;
-    const int n = fd->n;
-    const int tb = fd->tile_begin, c = t - tb;
-    const long long base = fd->p_off;
-    const long long d0 = (long long)c * kMergeDiag;
-    const long long dend = min(d0 + kMergeDiag, 2ll * n);
-    const int i0 = (int)__ldcg(e.mp_part + t);
-    if (i0 < 0 || i0 >= n) {  // cannot happen with valid weights; never index with it
-      if (threadIdx.x == 0) atomicOr(e.err, ERR_BAD_WEIGHTS);
-      continue;
-    }
-    const int win = min(kMergeDiag + 1, n - i0);
-    for (int w = threadIdx.x; w < win; w += kThreads) s_F[w] = __ldcg(e.offs + base + i0 + w);
-    __syncthreads();
-    const long long d = d0 + (long long)threadIdx.x * kSteps;
-    if (d < dend) {
-      int lo = 0, hi = (int)min((long long)(win - 1), d - d0);
-      while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if ((long long)(i0 + mid) + (long long)s_F[mid] >= d) hi = mid;
-        else lo = mid + 1;
-      }
-      int i = i0 + lo;
-      long long k = d - i;
-      const int steps = (int)min((long long)kSteps, dend - d);
-      for (int s = 0; s < steps; ++s) {
-        const int wi = i - i0;
-        if (wi >= win) break;
-        if (k < (long long)s_F[wi]) {
-          if (k >= 0 && k < n) e.anc[base + k] = i;
-          ++k;
-        } else {
-          ++i;
-        }
-      }
-    }
-    __syncthreads();
+    merge_tile(e, fd, t, s_F);
   }
   queue_exit(q);
 }
 
 // -------------------------------------------------------------------------
-// k_mego: Megopolis (Chesser et al., arXiv:2109.13504) with the ancestor and
-// its log-weight in registers.  Iteration b proposes j = (k + o_{b,g}) mod N
-// with one random offset per (iteration, 32-slot segment g), so a warp reads
-// 32 consecutive candidate weights, and accepts with probability
-// min(1, w_j / w_ancestor).
+// Megopolis (Chesser et al., arXiv:2109.13504) for the slots of one tile,
+// the ancestor and its log-weight in registers.  Iteration b proposes
+// j = (k + o_{b,g}) mod N with one random offset per (iteration, 32-slot
+// segment g), so a warp reads 32 consecutive candidate weights, and accepts
+// with probability min(1, w_j / w_ancestor).  `epoch` is the step that
+// decided to resample.  Log-weights are read through L2 (another CTA of the
+// same launch may have written them).
+__device__ __forceinline__ void mego_tile(const EngineDev& e, const FilterDesc* fd, unsigned epoch, int t) {
+  const int lane = threadIdx.x & 31;
+  const int n = fd->n;
+  const int j = t - fd->tile_begin;
+  const long long base = fd->p_off;
+  const uint32_t fid = (uint32_t)fd->filter_id;
+  const int B = e.mego_iters;
+  const float* lw = e.lw + base;
+#pragma unroll 1
+  for (int r = 0; r < 4; ++r) {
+    const int seg0 = j * kTile + r * kThreads + ((int)threadIdx.x & ~31);  // warp's first slot
+    if (seg0 >= n) continue;  // whole warp past the filter's end
+    const int k_real = seg0 + lane;
+    const bool valid = k_real < n;
+    const int k = valid ? k_real : seg0;  // lanes past the end shadow a valid slot
+    const uint32_t g = (uint32_t)(seg0 / 32);
+    // lane l draws the offsets of iterations 4l .. 4l+3 of this segment
+    const U4 ol = philox10(U4{g, epoch, TAG_MEGO_OFF | (uint32_t)lane, fid}, fd->key0, fd->key1);
+    int a = k;
+    float la = __ldcg(lw + k);
+#pragma unroll 1
+    for (int b0 = 0; b0 < B; b0 += 4) {
+      const U4 ur = philox10(U4{(uint32_t)k, epoch, TAG_MEGO_U | (uint32_t)(b0 >> 2), fid}, fd->key0, fd->key1);
+      const uint32_t uw[4] = {ur.x, ur.y, ur.z, ur.w};
+#pragma unroll
+      for (int bb = 0; bb < 4; ++bb) {
+        if (b0 + bb >= B) break;
+        const int src_lane = (b0 + bb) >> 2;
+        const uint32_t ow = (bb == 0) ? ol.x : (bb == 1) ? ol.y : (bb == 2) ? ol.z : ol.w;
+        const uint32_t o = __umulhi(__shfl_sync(0xffffffffu, ow, src_lane), (uint32_t)n);
+        int cand = k + (int)o;
+        if (cand >= n) cand -= n;
+        const float lc = __ldcg(lw + cand);
+        const float lu = __logf(fmaf((float)uw[bb], 2.3283064365386963e-10f, 1.1641532182693481e-10f));
+        if (lc - la > lu) {
+          a = cand;
+          la = lc;
+        }
+      }
+    }
+    if (valid) e.anc[base + k] = a;
+  }
+}
+
+// k_mego: mego_tile over the launch's tiles.
 __global__ void __launch_bounds__(kThreads) k_mego(EngineDev e, int t0, int count) {
   __shared__ int s_slot;
   unsigned* q = e.queue + 2 * Q_MEGO;
-  const int lane = threadIdx.x & 31;
+  pdl_trigger();
+  pdl_wait();
   for (;;) {
     const int tq = dequeue(q, &s_slot);
     if (tq >= count) break;
@@ -792,47 +992,7 @@ __global__ void __launch_bounds__(kThreads) k_mego(EngineDev e, int t0, int coun
     const FilterDesc* fd = e.desc + f;
     const FilterCtrl* fc = e.ctrl + f;
     if (!fc->resample_flag) continue;
-    const int n = fd->n;
-    const int j = t - fd->tile_begin;
-    const long long base = fd->p_off;
-    const unsigned epoch = fc->epoch - 1u;  // the step that decided to resample
-    const uint32_t fid = (uint32_t)fd->filter_id;
-    const int B = e.mego_iters;
-    const float* lw = e.lw + base;
-#pragma unroll 1
-    for (int r = 0; r < 4; ++r) {
-      const int seg0 = j * kTile + r * kThreads + ((int)threadIdx.x & ~31);  // warp's first slot
-      if (seg0 >= n) continue;  // whole warp past the filter's end
-      const int k_real = seg0 + lane;
-      const bool valid = k_real < n;
-      const int k = valid ? k_real : seg0;  // lanes past the end shadow a valid slot
-      const uint32_t g = (uint32_t)(seg0 / 32);
-      // lane l draws the offsets of iterations 4l .. 4l+3 of this segment
-      U4 ol = philox10(U4{g, epoch, TAG_MEGO_OFF | (uint32_t)lane, fid}, fd->key0, fd->key1);
-      int a = k;
-      float la = __ldg(lw + k);
-#pragma unroll 1
-      for (int b0 = 0; b0 < B; b0 += 4) {
-        U4 ur = philox10(U4{(uint32_t)k, epoch, TAG_MEGO_U | (uint32_t)(b0 >> 2), fid}, fd->key0, fd->key1);
-        const uint32_t uw[4] = {ur.x, ur.y, ur.z, ur.w};
-#pragma unroll
-        for (int bb = 0; bb < 4; ++bb) {
-          if (b0 + bb >= B) break;
-          const int src_lane = (b0 + bb) >> 2;
-          const uint32_t ow = (bb == 0) ? ol.x : (bb == 1) ? ol.y : (bb == 2) ? ol.z : ol.w;
-          const uint32_t o = __umulhi(__shfl_sync(0xffffffffu, ow, src_lane), (uint32_t)n);
-          int cand = k + (int)o;
-          if (cand >= n) cand -= n;
-          const float lc = __ldg(lw + cand);
-          const float lu = __logf(fmaf((float)uw[bb], 2.3283064365386963e-10f, 1.1641532182693481e-10f));
-          if (lc - la > lu) {
-            a = cand;
-            la = lc;
-          }
-        }
-      }
-      if (valid) e.anc[base + k] = a;
-    }
+    mego_tile(e, fd, fc->epoch - 1u, t);
   }
   queue_exit(q);
 }
@@ -844,6 +1004,8 @@ __global__ void __launch_bounds__(kThreads) k_init(EngineDev e, int t0, int coun
                                                     float spread_pos, float spread_clk) {
   __shared__ int s_slot;
   unsigned* q = e.queue + 2 * Q_INIT;
+  pdl_trigger();
+  pdl_wait();
   for (;;) {
     const int tq = dequeue(q, &s_slot);
     if (tq >= count) break;
@@ -892,6 +1054,8 @@ __global__ void __launch_bounds__(kThreads) k_estimate(EngineDev e, int t0, int 
   __shared__ double s_dred[(kThreads / 32) * 16];
   __shared__ int s_slot, s_last;
   unsigned* q = e.queue + 2 * Q_EST;
+  pdl_trigger();
+  pdl_wait();
   for (;;) {
     const int tq = dequeue(q, &s_slot);
     if (tq >= count) break;
@@ -959,6 +1123,8 @@ template <int D>
 __global__ void __launch_bounds__(kThreads) k_export(EngineDev e, int t0, int count, double* out) {
   __shared__ int s_slot;
   unsigned* q = e.queue + 2 * Q_EXPORT;
+  pdl_trigger();
+  pdl_wait();
   for (;;) {
     const int tq = dequeue(q, &s_slot);
     if (tq >= count) break;

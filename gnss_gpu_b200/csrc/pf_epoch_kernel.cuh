@@ -1,0 +1,514 @@
+// pf_epoch_kernel.cuh -- one cooperative persistent kernel per epoch.
+//
+// All CTAs are co-resident (cooperative launch); each owns a contiguous
+// chunk of (filter, tile) work items and the phases of the epoch are
+// separated by grid barriers with bounded spins:
+//
+//   1  predict + likelihood + tile statistics.  The next tile's particles
+//      are copied into shared memory with cp.async while the current tile is
+//      computed (each thread copies and later reads only its own particles,
+//      so the stage needs no CTA barrier; contiguous rows use 16-byte copies,
+//      a gather through the last resample's ancestors 4-byte copies).
+//   -- barrier
+//   2  per-filter merge of the tile rows (filter f by CTA f mod G): ESS,
+//      weighted mean / covariance, device-side resample decision.
+//   -- barrier (phases 3-5 only if some filter resamples)
+//   3  systematic: quantised weights and tile sums.   Megopolis: the chain.
+//   -- barrier
+//   4  exclusive tile prefixes, in-tile scan, offspring ends F(i) and the
+//      merge-path partition points.
+//   -- barrier
+//   5  merge path: ancestor of every slot.
+//
+// Compared with one kernel per phase this removes four launch/drain gaps and
+// every per-tile queue atomic; the log-weights reread in phases 3 and 4 come
+// from L2 (the epoch just wrote them).
+#pragma once
+#include "pf_engine_kernels.cuh"
+
+namespace pfb {
+
+// Sense-counting grid barrier for co-resident CTAs.  bar[0] counts
+// arrivals, bar[1] is the generation; `gen` is this CTA's copy of the
+// generation.  The wait is bounded: on timeout the error word is set and
+// the CTA goes on (results are then invalid, and the host reports
+// PF_ETIMEOUT).
+__device__ __forceinline__ void grid_barrier(const EngineDev& e, unsigned* bar, unsigned& gen) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned target = gen + 1u;
+    // test hook: wait for a generation nobody publishes (bounded spin)
+    const unsigned want = e.lookback_poison ? target + 1u : target;
+    __threadfence();
+    const unsigned arrived = atomicAdd(&bar[0], 1u);
+    const bool last = arrived == gridDim.x - 1u;
+    if (last) {  // the last CTA to arrive resets the count and releases
+      bar[0] = 0u;
+      __threadfence();
+      atomicExch(&bar[1], target);
+    }
+    if (!last || want != target) {
+      unsigned long long spins = 0;
+      while (*(volatile unsigned*)&bar[1] != want) {
+        if (++spins > e.spin_limit) {
+          atomicOr(e.err, ERR_BARRIER_TIMEOUT);
+          break;
+        }
+        if (spins > 16) __nanosleep(100);
+      }
+    }
+    gen = target;
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Reads through L2 of control-block fields that another CTA wrote before a
+// grid barrier (L1 is not coherent across SMs).
+__device__ __forceinline__ int ld_cg_int(const int* p) { return __ldcg(p); }
+__device__ __forceinline__ unsigned ld_cg_u(const unsigned* p) { return __ldcg(p); }
+__device__ __forceinline__ float ld_cg_f(const float* p) { return __ldcg(p); }
+
+// Per-CTA chunk of the work items [t0, t0 + count).
+__device__ __forceinline__ void cta_chunk(int t0, int count, int& b, int& e) {
+  const int per = count / (int)gridDim.x, rem = count % (int)gridDim.x;
+  const int c = blockIdx.x;
+  b = t0 + c * per + min(c, rem);
+  e = b + per + (c < rem ? 1 : 0);
+}
+
+// Issue the cp.async copies of one thread's 4 particles of tile t into its
+// stage slots (stage layout [D][kThreads][4] floats).
+template <int D>
+__device__ __forceinline__ void stage_tile(const EngineDev& e, float* stage, int t) {
+  const int f = __ldg(e.tile_filter + t);
+  const FilterDesc* fd = e.desc + f;
+  const FilterCtrl* fc = e.ctrl + f;
+  const int n = fd->n;
+  const int p0 = (t - fd->tile_begin) * kTile + (int)threadIdx.x * 4;
+  if (p0 >= n) return;
+  const long long base = fd->p_off;
+  const float* src = fc->parity ? e.state1 : e.state0;
+  float* mine = stage + (size_t)threadIdx.x * 4;
+  if (fc->resample_flag) {
+    const int4 a = __ldcg(reinterpret_cast<const int4*>(e.anc + base + p0));
+    int ai[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (p0 + k >= n || (unsigned)ai[k] >= (unsigned)n) ai[k] = p0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const float* s = src + (size_t)d * e.p_total + base;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) cp_async4(mine + (size_t)d * kTile + k, s + ai[k]);
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < D; ++d) cp_async16(mine + (size_t)d * kTile, src + (size_t)d * e.p_total + base + p0);
+  }
+}
+
+// Phases 3-5 of the systematic resampler (see the header comment).
+__device__ __forceinline__ void epoch_systematic(const EngineDev& e, unsigned* bar, unsigned& gen, int cb, int ce,
+                                                 unsigned long long* s_u64, uint32_t* s_F) {
+  for (int t = cb; t < ce; ++t) {
+    const int f = __ldg(e.tile_filter + t);
+    const FilterDesc* fd = e.desc + f;
+    const FilterCtrl* fc = e.ctrl + f;
+    if (!ld_cg_int(&fc->resample_flag)) continue;
+    const int p0 = (t - fd->tile_begin) * kTile + (int)threadIdx.x * 4;
+    unsigned long long qv[4];
+    load_q4(e, fd->p_off, p0, fd->n, ld_cg_f(&fc->max_lw), fd->K, qv);
+    unsigned long long tot;
+    block_excl_scan_u64(qv[0] + qv[1] + qv[2] + qv[3], s_u64, &tot);
+    if (threadIdx.x == 0) e.lb_agg[t] = tot;
+  }
+  grid_barrier(e, bar, gen);
+
+  // ---------------------------------------------------------------- phase 4
+  {
+    int run_f = -1;
+    unsigned long long run_excl = 0, W = 0;
+    for (int t = cb; t < ce; ++t) {
+      const int f = __ldg(e.tile_filter + t);
+      const FilterDesc* fd = e.desc + f;
+      FilterCtrl* fc = e.ctrl + f;
+      if (!ld_cg_int(&fc->resample_flag)) continue;
+      const int tb = fd->tile_begin, nt = fd->n_tiles;
+      if (f != run_f) {
+        // exclusive prefix of this tile and the filter total from the tile sums
+        unsigned long long pre = 0, all = 0;
+        for (int i = threadIdx.x; i < nt; i += kThreads) {
+          const unsigned long long v = __ldcg(e.lb_agg + tb + i);
+          all += v;
+          if (tb + i < t) pre += v;
+        }
+        unsigned long long tp, ta;
+        block_excl_scan_u64(pre, s_u64, &tp);
+        block_excl_scan_u64(all, s_u64, &ta);
+        run_excl = tp;
+        W = ta;
+        run_f = f;
+      }
+      if (threadIdx.x == 0 && t == tb + nt - 1) fc->wq_total = W;  // owner of the filter's last tile
+      const int n = fd->n;
+      const int p0 = (t - tb) * kTile + (int)threadIdx.x * 4;
+      const long long base = fd->p_off;
+      unsigned long long qv[4];
+      load_q4(e, base, p0, n, ld_cg_f(&fc->max_lw), fd->K, qv);
+      unsigned long long tile_tot;
+      const unsigned long long texcl = block_excl_scan_u64(qv[0] + qv[1] + qv[2] + qv[3], s_u64, &tile_tot);
+      if (p0 < n && W > 0ull) {
+        const uint32_t u = ld_cg_u(&fc->sys_u);
+        const double scale = (double)n / (double)W, uf = (double)u * 2.3283064365386963e-10;
+        unsigned long long C = run_excl + texcl;
+        uint32_t Fprev = (p0 == 0) ? 0u : offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf);
+        uint32_t Fk[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          C += qv[k];
+          Fk[k] = (p0 + k < n) ? offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf) : (uint32_t)n;
+        }
+        *reinterpret_cast<uint4*>(e.offs + base + p0) = make_uint4(Fk[0], Fk[1], Fk[2], Fk[3]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const long long i = p0 + k;
+          if (i >= n) break;
+          const long long hprev = i - 1 + (long long)Fprev;
+          const long long h = i + (long long)Fk[k];
+          long long c = (hprev < 0) ? 0 : hprev / kMergeDiag + 1;
+          for (; c * kMergeDiag <= h; ++c) e.mp_part[tb + c] = (uint32_t)i;
+          Fprev = Fk[k];
+        }
+      } else if (W == 0ull && threadIdx.x == 0) {
+        atomicOr(e.err, ERR_BAD_WEIGHTS);
+      }
+      run_excl += tile_tot;
+    }
+  }
+  grid_barrier(e, bar, gen);
+
+  // ---------------------------------------------------------------- phase 5
+  for (int t = cb; t < ce; ++t) {
+    const int f = __ldg(e.tile_filter + t);
+    const FilterDesc* fd = e.desc + f;
+    const FilterCtrl* fc = e.ctrl + f;
+    if (!ld_cg_int(&fc->resample_flag)) continue;
+    merge_tile(e, fd, t, s_F);
+  }
+}
+
+
+template <int NCLK, int WMODE, int RESAMPLER>
+__global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int count, unsigned* bar) {
+  constexpr int D = 3 + NCLK;
+  constexpr int NV = 2 + D + 6;
+  constexpr int kWarps = kThreads / 32;
+  extern __shared__ __align__(16) float s_stage[];  // [2][D][kTile]
+  __shared__ float2 s_sat[8 * PF_MAX_SATS];
+  __shared__ int s_grp[PF_MAX_CLK + 1];
+  __shared__ unsigned char s_clk[PF_MAX_SATS];
+  __shared__ float s_wrow[2][kWarps][17];
+  __shared__ float s_maxtmp[kWarps];
+  __shared__ double s_dred[kWarps * 16];
+  __shared__ unsigned long long s_u64[kWarps];
+  __shared__ int s_any;
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned gen = 0;
+  if (threadIdx.x == 0) {
+    gen = *(volatile unsigned*)&bar[1];
+    if (blockIdx.x == 0) bar[2] = 0u;  // any-filter-resamples flag of this epoch
+  }
+  int cb, ce;
+  cta_chunk(t0, count, cb, ce);
+
+  // ---------------------------------------------------------------- phase 1
+  if (cb < ce) stage_tile<D>(e, s_stage, cb);
+  cp_async_commit();
+  int cached = -1;
+  int it = 0;
+  for (int t = cb; t < ce; ++t, ++it) {
+    float* stage = s_stage + (size_t)(it & 1) * D * kTile;
+    if (t + 1 < ce) stage_tile<D>(e, s_stage + (size_t)((it + 1) & 1) * D * kTile, t + 1);
+    cp_async_commit();
+    cp_async_wait_1();  // this thread's copies of tile t have landed
+
+    const int f = __ldg(e.tile_filter + t);
+    const FilterDesc* fd = e.desc + f;
+    FilterCtrl* fc = e.ctrl + f;
+    const unsigned epoch = fc->epoch;
+    const bool lw_zero = fc->lw_zero != 0;
+    const unsigned char* ob = e.obs + (size_t)(epoch % (unsigned)e.obs_slots) * e.obs_slot_bytes;
+    const pf_filter_epoch_t* fe = reinterpret_cast<const pf_filter_epoch_t*>(ob) + f;
+    const pf_sat_t* sats = reinterpret_cast<const pf_sat_t*>(ob + sizeof(pf_filter_epoch_t) * e.n_filters);
+    const int eflags = fe->flags;
+    int n_sat = fe->n_sat;
+    if (n_sat > e.max_sats) {
+      if (threadIdx.x == 0) atomicOr(e.err, ERR_SAT_CAP);
+      n_sat = e.max_sats;
+    }
+    if (n_sat < 0) n_sat = 0;
+    const bool do_predict = (eflags & PF_EP_PREDICT) != 0;
+    const bool do_weight = (eflags & PF_EP_WEIGHT) != 0;
+
+    if (f != cached) {  // satellite geometry of this filter (FP64 -> FP32 pairs)
+      __syncthreads();   // nobody still reads the previous filter's table
+      int my_c = 0;
+      const pf_sat_t* sp = sats + fe->sat_offset + threadIdx.x;
+      if (do_weight && threadIdx.x < n_sat) {
+        my_c = sp->clk;
+        my_c = my_c < 0 ? 0 : (my_c >= NCLK ? NCLK - 1 : my_c);
+        s_clk[threadIdx.x] = (unsigned char)my_c;
+      }
+      __syncthreads();
+      if (do_weight && threadIdx.x < n_sat) {
+        const double* rot = fd->rot;
+        double A[3];
+        local_to_ecef(rot, fc->anchor, fc->shift[0], fc->shift[1], fc->shift[2], A);
+        const int c = my_c;
+        const double clkA = fc->clk_anchor[c] + (double)fc->shift[3 + c];
+        double vx = sp->x - A[0], vy = sp->y - A[1], vz = sp->z - A[2];
+        const double r0 = sqrt(vx * vx + vy * vy + vz * vz);
+        const double inv = 1.0 / r0;
+        vx *= inv; vy *= inv; vz *= inv;
+        const float eE = (float)(rot[0] * vx + rot[1] * vy + rot[2] * vz);
+        const float eN = (float)(rot[3] * vx + rot[4] * vy + rot[5] * vz);
+        const float eU = (float)(rot[6] * vx + rot[7] * vy + rot[8] * vz);
+        const float g = (float)inv;
+        const float y = (float)(sp->pr - r0 - clkA);
+        const float wq = WMODE == PF_WEIGHT_GAUSSIAN ? (float)((double)fd->wscale * sp->w) : (float)sp->w;
+        int rank = 0;
+        for (int s2 = 0; s2 < n_sat; ++s2) {
+          const int c2 = s_clk[s2];
+          rank += (c2 < c) || (c2 == c && s2 < (int)threadIdx.x);
+        }
+        float2* o = s_sat + 8 * rank;
+        o[0] = bc(eE); o[1] = bc(eN); o[2] = bc(eU); o[3] = bc(-0.5f * g);
+        o[4] = bc(0.5f * g * g); o[5] = bc(0.5f * g); o[6] = bc(y); o[7] = bc(wq);
+      }
+      if (threadIdx.x <= NCLK) {
+        int cnt = 0;
+        if (do_weight)
+          for (int s2 = 0; s2 < n_sat; ++s2) cnt += s_clk[s2] < (int)threadIdx.x;
+        s_grp[threadIdx.x] = cnt;
+      }
+      cached = f;
+      __syncthreads();
+    }
+
+    const int n = fd->n;
+    const int p0 = (t - fd->tile_begin) * kTile + (int)threadIdx.x * 4;
+    const bool active = p0 < n;
+    const long long base = fd->p_off;
+    float* dst = fc->parity ? e.state0 : e.state1;
+    float x[D][4];
+    float lwv[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const float4 v = active ? *reinterpret_cast<const float4*>(stage + (size_t)d * kTile + threadIdx.x * 4)
+                              : make_float4(0.f, 0.f, 0.f, 0.f);
+      x[d][0] = v.x; x[d][1] = v.y; x[d][2] = v.z; x[d][3] = v.w;
+    }
+    if (active) {
+      float lw0[4] = {0.f, 0.f, 0.f, 0.f};
+      const bool need_prev = !lw_zero && (!do_weight || e.lw_mode == PF_LW_ACCUMULATE);
+      if (need_prev) {
+        const float4 v = __ldcs(reinterpret_cast<const float4*>(e.lw + base + p0));
+        lw0[0] = v.x; lw0[1] = v.y; lw0[2] = v.z; lw0[3] = v.w;
+      }
+      float ds[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) ds[d] = -fc->shift[d];
+      if (do_predict) {
+        ds[0] += (float)fe->disp[0];
+        ds[1] += (float)fe->disp[1];
+        ds[2] += (float)fe->disp[2];
+        const uint32_t fid = (uint32_t)fd->filter_id;
+        const uint32_t k0 = fd->key0, k1 = fd->key1;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          float nz[8];
+          const U4 r = philox10(U4{(uint32_t)(p0 + k), epoch, TAG_PREDICT, fid}, k0, k1);
+          const float2 a = box_muller_f32(r.x, r.y), b = box_muller_f32(r.z, r.w);
+          nz[0] = a.x; nz[1] = a.y; nz[2] = b.x; nz[3] = b.y;
+          if (D > 4) {
+            const U4 r2 = philox10(U4{(uint32_t)(p0 + k), epoch, TAG_PREDICT | 1u, fid}, k0, k1);
+            const float2 c = box_muller_f32(r2.x, r2.y), dd = box_muller_f32(r2.z, r2.w);
+            nz[4] = c.x; nz[5] = c.y; nz[6] = dd.x; nz[7] = dd.y;
+          } else {
+            nz[4] = nz[5] = nz[6] = nz[7] = 0.f;
+          }
+#pragma unroll
+          for (int d = 0; d < D; ++d) x[d][k] = fmaf(fd->sigma[d], nz[d], x[d][k] + ds[d]);
+        }
+      } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+#pragma unroll
+          for (int k = 0; k < 4; ++k) x[d][k] += ds[d];
+      }
+#pragma unroll
+      for (int d = 0; d < D; ++d)
+        __stcs(reinterpret_cast<float4*>(dst + (size_t)d * e.p_total + base + p0),
+               make_float4(x[d][0], x[d][1], x[d][2], x[d][3]));
+
+      if (do_weight) {
+        float2 lwp[2] = {f2(lw0[0], lw0[1]), f2(lw0[2], lw0[3])};
+        float2 dx[2], dy[2], dz[2], bb[2];
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+          dx[p] = f2(x[0][2 * p], x[0][2 * p + 1]);
+          dy[p] = f2(x[1][2 * p], x[1][2 * p + 1]);
+          dz[p] = f2(x[2][2 * p], x[2][2 * p + 1]);
+          bb[p] = __fmul2_rn(dx[p], dx[p]);
+          bb[p] = __ffma2_rn(dy[p], dy[p], bb[p]);
+          bb[p] = __ffma2_rn(dz[p], dz[p], bb[p]);
+        }
+#pragma unroll
+        for (int c = 0; c < NCLK; ++c) {
+          const float2 ncb[2] = {f2(-x[3 + c][0], -x[3 + c][1]), f2(-x[3 + c][2], -x[3 + c][3])};
+          const int s_end = s_grp[c + 1];
+#pragma unroll 2
+          for (int s = s_grp[c]; s < s_end; ++s) {
+            const float4* sv = reinterpret_cast<const float4*>(s_sat + 8 * s);
+            const float4 q0 = sv[0], q1 = sv[1], q2 = sv[2], q3 = sv[3];
+            const float2 eE = f2(q0.x, q0.y), eN = f2(q0.z, q0.w), eU = f2(q1.x, q1.y), ng2 = f2(q1.z, q1.w);
+            const float2 c2 = f2(q2.x, q2.y), nc1 = f2(q2.z, q2.w), yy = f2(q3.x, q3.y), wq = f2(q3.z, q3.w);
+#pragma unroll
+            for (int p = 0; p < 2; ++p) {
+              float2 ed = __fmul2_rn(eE, dx[p]);
+              ed = __ffma2_rn(eN, dy[p], ed);
+              ed = __ffma2_rn(eU, dz[p], ed);
+              const float2 nh = __ffma2_rn(bb[p], ng2, ed);
+              const float2 ninner = __ffma2_rn(nh, c2, nc1);
+              const float2 hh = __fmul2_rn(nh, nh);
+              const float2 ndl = __ffma2_rn(hh, ninner, nh);
+              const float2 r = __fadd2_rn(__fadd2_rn(yy, ncb[p]), ndl);
+              if (WMODE == PF_WEIGHT_GAUSSIAN) {
+                const float2 rw = __fmul2_rn(r, wq);
+                lwp[p] = __ffma2_rn(rw, r, lwp[p]);
+              } else {
+                const float ks = fd->huber_k;
+                const float z0 = fabsf(r.x) * fd->inv_sigma_pr, z1 = fabsf(r.y) * fd->inv_sigma_pr;
+                const float rho0 = z0 < ks ? 0.5f * z0 * z0 : fmaf(ks, z0, -0.5f * ks * ks);
+                const float rho1 = z1 < ks ? 0.5f * z1 * z1 : fmaf(ks, z1, -0.5f * ks * ks);
+                lwp[p].x = fmaf(-wq.x, rho0, lwp[p].x);
+                lwp[p].y = fmaf(-wq.x, rho1, lwp[p].y);
+              }
+            }
+          }
+        }
+        lwv[0] = lwp[0].x; lwv[1] = lwp[0].y; lwv[2] = lwp[1].x; lwv[3] = lwp[1].y;
+        __stcs(reinterpret_cast<float4*>(e.lw + base + p0), make_float4(lwv[0], lwv[1], lwv[2], lwv[3]));
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) lwv[k] = lw0[k];
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (p0 + k >= n) lwv[k] = -INFINITY;
+    }
+
+    // per-warp statistics, then warp 0 merges the warp rows into the tile row
+    {
+      float wm = fmaxf(fmaxf(lwv[0], lwv[1]), fmaxf(lwv[2], lwv[3]));
+      wm = warp_max(wm);
+      float v[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) v[i] = 0.f;
+      if (wm > -INFINITY) {
+        const bool cov = (e.flags & PF_FLAG_COVARIANCE) != 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const float w = exp2f((lwv[k] - wm) * 1.4426950408889634f);
+          v[0] += w;
+          v[1] = fmaf(w, w, v[1]);
+#pragma unroll
+          for (int d = 0; d < D; ++d) v[2 + d] = fmaf(w, x[d][k], v[2 + d]);
+          if (cov) {
+            const float wx = w * x[0][k], wy = w * x[1][k], wz = w * x[2][k];
+            v[2 + D + 0] = fmaf(wx, x[0][k], v[2 + D + 0]);
+            v[2 + D + 1] = fmaf(wx, x[1][k], v[2 + D + 1]);
+            v[2 + D + 2] = fmaf(wx, x[2][k], v[2 + D + 2]);
+            v[2 + D + 3] = fmaf(wy, x[1][k], v[2 + D + 3]);
+            v[2 + D + 4] = fmaf(wy, x[2][k], v[2 + D + 4]);
+            v[2 + D + 5] = fmaf(wz, x[2][k], v[2 + D + 5]);
+          }
+        }
+      }
+      const int idx = warp_transpose_sum16(v);
+      float (*wr)[17] = s_wrow[it & 1];
+      if ((lane & 1) == 0 && idx < NV) wr[warp][1 + idx] = v[0];
+      if (lane == 0) wr[warp][0] = wm;
+      __syncthreads();
+      if (warp == 0) {
+        float tm = lane < kWarps ? wr[lane][0] : -INFINITY;
+        tm = warp_max(tm);
+        float acc = 0.f;
+        if (lane < NV && tm > -INFINITY) {
+#pragma unroll
+          for (int w = 0; w < kWarps; ++w) {
+            const float mw = wr[w][0];
+            if (mw > -INFINITY) {
+              float sc = exp2f((mw - tm) * 1.4426950408889634f);
+              if (lane == 1) sc *= sc;
+              acc = fmaf(sc, wr[w][1 + lane], acc);
+            }
+          }
+        }
+        float* row = e.part + (size_t)t * kPartStride;
+        if (lane < NV) row[1 + lane] = acc;
+        if (lane == 0) row[0] = tm;
+      }
+    }
+  }
+  grid_barrier(e, bar, gen);
+
+  // ---------------------------------------------------------------- phase 2
+  for (int f = blockIdx.x; f < e.n_filters; f += gridDim.x) {
+    const FilterDesc* fd = e.desc + f;
+    if (fd->n_tiles == 0 || fd->tile_begin + fd->n_tiles <= t0 || fd->tile_begin >= t0 + count) continue;
+    FilterCtrl* fc = e.ctrl + f;
+    const unsigned epoch = fc->epoch;
+    const unsigned char* ob = e.obs + (size_t)(epoch % (unsigned)e.obs_slots) * e.obs_slot_bytes;
+    const pf_filter_epoch_t* fe = reinterpret_cast<const pf_filter_epoch_t*>(ob) + f;
+    const int eflags = fe->flags;
+    MergedStats ms = merge_tiles<D>(e.part, fd->tile_begin, fd->n_tiles, s_maxtmp, s_dred);
+    if (threadIdx.x == 0) {
+      finalize_filter<D>(e, fd, fc, ms, epoch, fc->parity, fc->lw_zero != 0, eflags, (eflags & PF_EP_WEIGHT) != 0);
+      if (fc->resample_flag) atomicOr(&bar[2], 1u);
+    }
+    __syncthreads();
+  }
+  grid_barrier(e, bar, gen);
+  if (threadIdx.x == 0) s_any = (int)ld_cg_u(&bar[2]);
+  __syncthreads();
+  if (!s_any) return;  // uniform: no filter resamples this epoch
+
+  // ---------------------------------------------------------------- phase 3
+  if constexpr (RESAMPLER == PF_RESAMPLE_MEGOPOLIS) {
+    for (int t = cb; t < ce; ++t) {
+      const int f = __ldg(e.tile_filter + t);
+      const FilterDesc* fd = e.desc + f;
+      const FilterCtrl* fc = e.ctrl + f;
+      if (!ld_cg_int(&fc->resample_flag)) continue;
+      mego_tile(e, fd, ld_cg_u(&fc->epoch) - 1u, t);
+    }
+  } else {
+    epoch_systematic(e, bar, gen, cb, ce, s_u64, reinterpret_cast<uint32_t*>(s_stage));
+  }
+}
+
+}  // namespace pfb

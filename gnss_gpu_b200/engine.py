@@ -37,6 +37,7 @@ class EngineOptions:
     covariance: bool = True
     recenter: bool = True
     ess_threshold: float = 0.5
+    kernel_chain: bool = False             # one kernel per phase (comparison path)
 
 
 def _torch():
@@ -67,7 +68,8 @@ class Engine:
         cfg.sys_offset = {"random": N.PF_SYS_OFFSET_RANDOM, "reference": N.PF_SYS_OFFSET_REFERENCE}[o.sys_offset]
         cfg.max_sats = int(o.max_sats)
         cfg.obs_slots = int(o.obs_slots)
-        cfg.flags = (N.PF_FLAG_COVARIANCE if o.covariance else 0) | (N.PF_FLAG_RECENTER if o.recenter else 0)
+        cfg.flags = ((N.PF_FLAG_COVARIANCE if o.covariance else 0) | (N.PF_FLAG_RECENTER if o.recenter else 0)
+                     | (N.PF_FLAG_KERNEL_CHAIN if o.kernel_chain else 0))
         cfg.ess_threshold = float(o.ess_threshold)
         cfg.huber_k = float(o.huber_k)
         self.cfg = cfg
@@ -263,9 +265,10 @@ class Engine:
     def poison_lookback(self, on: bool):
         N.check(self.lib.pfe_test_poison_lookback(self.h, 1 if on else 0))
 
-    def enable_timing(self, slots: int):
-        """Record CUDA events around the fused step kernel of each eager step."""
-        N.check(self.lib.pfe_enable_timing(self.h, int(slots)))
+    def enable_timing(self, slots: int, detailed: bool = False):
+        """Record CUDA events around the fused step kernel of each eager step
+        (detailed: also after every resampling kernel, which serialises them)."""
+        N.check(self.lib.pfe_enable_timing(self.h, int(slots), 1 if detailed else 0))
         self._timing_slots = int(slots)
 
     def read_timing(self):

@@ -152,6 +152,8 @@ typedef enum {
 /* Engine flags. */
 #define PF_FLAG_COVARIANCE 1u  /* fused 3x3 position covariance in the step   */
 #define PF_FLAG_RECENTER 2u    /* re-anchor each filter at its weighted mean  */
+#define PF_FLAG_KERNEL_CHAIN 4u /* one kernel per phase instead of the single
+                                   cooperative epoch kernel (comparison path) */
 
 typedef struct {
   int n_filters;
@@ -293,9 +295,11 @@ int pfe_get_resample_info(pf_engine_t* eng, int filter, uint32_t* u32,
 int pfe_error_word(pf_engine_t* eng, unsigned* word);
 /* Test hook: spin limit of the decoupled look-back (0 = default). */
 int pfe_set_spin_limit(pf_engine_t* eng, unsigned long long limit);
-/* Test hook: on != 0 makes the look-back wait for a tag that is never
- * published, so its bounded spin runs out and sets the error word (no hang);
- * on == 0 restores normal operation and clears the error word. */
+/* Test hook: on != 0 makes the device waits (the look-back of the kernel
+ * chain, the grid barriers of the epoch kernel) wait for a value that is
+ * never published, so their bounded spins run out and set the error word
+ * (no hang); on == 0 restores normal operation and clears the error word
+ * and the barrier state. */
 int pfe_test_poison_lookback(pf_engine_t* eng, int on);
 /* Kernels launched by the last pfe_step / pfe_step_per_filter. */
 int pfe_last_launch_count(pf_engine_t* eng, int* count);
@@ -303,16 +307,20 @@ int pfe_last_launch_count(pf_engine_t* eng, int* count);
 /* Device timing of eager steps: with slots > 0, each pfe_step records CUDA
  * events on the engine stream before the fused step kernel, after it, and
  * after the last resampling kernel, into a ring of `slots` entries
- * (slots == 0 switches timing off).  pfe_read_timing synchronises and
- * returns, for the steps since the last read (at most `slots`), the fused
- * step kernel's duration and the whole step's duration in milliseconds. */
-int pfe_enable_timing(pf_engine_t* eng, int slots);
+ * (slots == 0 switches timing off).  detailed != 0 also records an event
+ * after every resampling kernel; that serialises the kernels (no
+ * programmatic overlap), so use it for breakdowns, not for throughput.
+ * pfe_read_timing synchronises and returns, for the steps since the last
+ * read (at most `slots`), the fused step kernel's duration and the whole
+ * step's duration in milliseconds. */
+int pfe_enable_timing(pf_engine_t* eng, int slots, int detailed);
 int pfe_read_timing(pf_engine_t* eng, float* step_kernel_ms, float* whole_step_ms,
                     int max_entries, int* count);
 /* Per-kernel durations (ms) of the steps returned by the last
  * pfe_read_timing: 4 per step -- fused step kernel, then the three
  * resampling kernels (look-back scan, offspring ends, merge path; for
- * Megopolis the chain kernel then two zeros). */
+ * Megopolis the chain kernel then two zeros).  Without detailed timing the
+ * second entry holds all resampling kernels together and the rest are 0. */
 int pfe_read_timing_kernels(pf_engine_t* eng, float* out_4_per_step,
                             int max_entries, int* count);
 

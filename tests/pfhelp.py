@@ -29,13 +29,13 @@ def lw_close(got, want, rtol=LW_RTOL):
 
 def make_engine(ns, n_clk=1, resampler="systematic", iters=32, seeds=None, sigma_pos=(1.0, 1.0, 0.5),
                 sigma_clk=0.5, sigma_pr=3.0, ess=0.5, sys_offset="random", weight_mode="gaussian",
-                lw_mode="overwrite", recenter=True, max_sats=64, obs_slots=1):
+                lw_mode="overwrite", recenter=True, max_sats=64, obs_slots=1, chain=False):
     seeds = seeds if seeds is not None else [1000 + k for k in range(len(ns))]
     specs = [FilterSpec(n_particles=int(n), seed=int(seeds[k]), sigma_pos=sigma_pos, sigma_clk=sigma_clk,
                         sigma_pr=sigma_pr) for k, n in enumerate(ns)]
     opts = EngineOptions(n_clk=n_clk, resampler=resampler, megopolis_iters=iters, ess_threshold=ess,
                          sys_offset=sys_offset, weight_mode=weight_mode, lw_mode=lw_mode, recenter=recenter,
-                         max_sats=max_sats, obs_slots=obs_slots)
+                         max_sats=max_sats, obs_slots=obs_slots, kernel_chain=chain)
     return Engine(specs, opts)
 
 

@@ -218,18 +218,20 @@ def test_degenerate_weights_single_survivor():
     assert np.all(x == st[:, 54_321][:, None])
 
 
-def test_lookback_timeout_sets_error_without_hang():
-    """The look-back's bounded spin gives up, flags the error word and the
-    context stays usable (no trap, no hang)."""
+@pytest.mark.parametrize("chain", [False, True])
+def test_device_wait_timeout_sets_error_without_hang(chain):
+    """A bounded device wait (grid barrier of the epoch kernel, look-back of
+    the kernel chain) gives up, flags the error word, and the context stays
+    usable (no trap, no hang)."""
     tr = S.config0()
-    eng = H.make_engine([16 * 1024])
+    eng = H.make_engine([16 * 1024], chain=chain)
     eng.initialize(0, tr.anchor, tr.truth_clk[0], 10.0, 30.0)
     eng.set_spin_limit(2000)
     eng.poison_lookback(True)
     fe, sv = eng.pack_epoch([_epoch_rec(tr, 0, N.PF_EP_PREDICT | N.PF_EP_WEIGHT | N.PF_EP_FORCE_RESAMPLE)])
     eng.upload(0, fe, sv)
     eng.step()
-    assert eng.error_word() & 1
+    assert eng.error_word() & (1 | 8)
     with pytest.raises(N.PFError) as ei:
         eng.results()
     assert ei.value.status == N.PF_ETIMEOUT
