@@ -214,16 +214,33 @@ PF_HD uint32_t offspring_end(uint64_t C, uint64_t W, uint32_t N, uint32_t u) {
   return (uint32_t)(k + 1);
 }
 
-// offspring_end with the FP64 estimate C * (N / W) - u 2^-32 from a
-// precomputed scale; the exact 128-bit checks make the result identical.
-PF_HD uint32_t offspring_end_scaled(uint64_t C, uint64_t W, uint32_t N, uint32_t u, double scale,
-                                    double uf) {
-  long long k = (long long)floor((double)C * scale - uf);
-  if (k < -1) k = -1;
-  if (k > (long long)N - 1) k = (long long)N - 1;
+// Exact F from an estimate k of the last slot at or below C (moved to the
+// right value by the 128-bit predicate).  Out of line: it runs only for
+// estimates close to a slot boundary.
+static __host__ __device__ __noinline__ uint32_t offspring_end_settle(long long k, uint64_t C, uint64_t W, uint32_t N,
+                                                              uint32_t u) {
   while (k >= 0 && !slot_at_or_below((uint64_t)k, u, W, C, N)) --k;
   while (k + 1 < (long long)N && slot_at_or_below((uint64_t)(k + 1), u, W, C, N)) ++k;
   return (uint32_t)(k + 1);
+}
+
+// offspring_end with the FP64 estimate x = C * (N / W) - u 2^-32 from a
+// precomputed scale.  F = clamp(floor(x_exact), -1, N-1) + 1 where x_exact
+// is the real-valued x.  For C <= W and N <= 2^30 the estimate is off by
+// less than 2^-20 (four roundings of relative size 2^-53 on |x| < 2^31), so
+// when x lies more than 2^-16 from an integer its floor is exact and the
+// 128-bit checks are skipped; otherwise they decide.  The result is the
+// exact F either way.
+PF_HD uint32_t offspring_end_scaled(uint64_t C, uint64_t W, uint32_t N, uint32_t u, double scale,
+                                    double uf) {
+  const double x = (double)C * scale - uf;
+  const double fl = floor(x);
+  long long k = (long long)fl;
+  if (k < -1) k = -1;
+  if (k > (long long)N - 1) k = (long long)N - 1;
+  const double fr = x - fl;
+  if (fr > 0x1p-16 && fr < 1.0 - 0x1p-16) return (uint32_t)(k + 1);
+  return offspring_end_settle(k, C, W, N, u);
 }
 
 }  // namespace pfb

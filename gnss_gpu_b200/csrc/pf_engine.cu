@@ -40,7 +40,7 @@ struct pf_engine {
   cudaGraphExec_t gexec = nullptr;
   int resident[Q_COUNT];
   int epoch_resident = 0;     // co-resident CTAs of the cooperative epoch kernel
-  size_t epoch_smem = 0;      // its dynamic shared memory (two stage buffers)
+  size_t epoch_smem = 0;      // its dynamic shared memory (merge-path windows)
   unsigned* bar = nullptr;    // grid barrier words (count, generation, any-resample)
   int sm_count = 0;
   int last_launches = 0;
@@ -64,7 +64,7 @@ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
   size_t off_state0, off_state1, off_lw, off_anc, off_offs, off_mp, off_part, off_agg, off_inc,
-      off_flag, off_excl, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
+      off_flag, off_excl, off_wq, off_wsum, off_mpw, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
       total;
   size_t obs_slot_bytes;
   long long P;
@@ -139,6 +139,9 @@ Layout make_layout(const pf_engine_config_t* cfg, const pf_filter_params_t* fp) 
   L.off_inc = take((size_t)T * 8);
   L.off_flag = take((size_t)T * 4);
   L.off_excl = take((size_t)T * 8);
+  L.off_wq = take((size_t)P * 8);
+  L.off_wsum = take((size_t)T * kSubTiles * 8);
+  L.off_mpw = take((size_t)T * kSubTiles * 4);
   L.off_desc = take(sizeof(FilterDesc) * cfg->n_filters);
   L.off_ctrl = take(sizeof(FilterCtrl) * cfg->n_filters);
   L.off_tf = take((size_t)T * 4);
@@ -327,7 +330,8 @@ EpochKernel epoch_kernel(const pf_engine* eng) {
 
 int prepare_epoch_kernel(pf_engine* eng) {
   EpochKernel k = epoch_kernel(eng);
-  eng->epoch_smem = (size_t)2 * eng->D * kTile * sizeof(float);
+  // merge-path windows of the systematic phases
+  eng->epoch_smem = (size_t)kSubTiles * kWindowWords * sizeof(uint32_t);
   CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eng->epoch_smem));
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, eng->epoch_smem));
@@ -462,6 +466,9 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
   e.lb_inc = (unsigned long long*)(w + L.off_inc);
   e.lb_flag = (unsigned*)(w + L.off_flag);
   e.tile_excl = (unsigned long long*)(w + L.off_excl);
+  e.wq = (unsigned long long*)(w + L.off_wq);
+  e.wsum = (unsigned long long*)(w + L.off_wsum);
+  e.mp_warp = (uint32_t*)(w + L.off_mpw);
   eng->desc_dev = (FilterDesc*)(w + L.off_desc);
   eng->ctrl_dev = (FilterCtrl*)(w + L.off_ctrl);
   e.desc = eng->desc_dev;

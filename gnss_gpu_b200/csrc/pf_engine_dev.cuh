@@ -12,6 +12,10 @@ constexpr int kTile = kThreads * kPerThread;
 static_assert(kTile == PF_TILE, "tile size mismatch");
 constexpr int kMergeDiag = 2 * kTile;  // merge-path diagonals per tile
 constexpr int kPartStride = 16;        // floats per tile partial
+constexpr int kWarpTile = 32 * kPerThread;      // particles per warp segment (epoch kernel)
+constexpr int kSubTiles = kTile / kWarpTile;    // warp segments per tile
+constexpr int kWarpDiag = 2 * kWarpTile;        // merge-path diagonals per warp block
+constexpr int kWindowWords = kWarpDiag + 4;     // offspring-end window per warp block
 constexpr int kMaxD = 3 + PF_MAX_CLK;
 
 // Work-queue slots (two words each: next tile, exit ticket).
@@ -78,6 +82,9 @@ struct EngineDev {
   unsigned long long* lb_inc;
   unsigned* lb_flag;
   unsigned long long* tile_excl;
+  unsigned long long* wq;    // epoch kernel: quantised weight per particle
+  unsigned long long* wsum;  // epoch kernel: quantised weight sum per warp segment
+  uint32_t* mp_warp;         // epoch kernel: merge-path start per warp block
   unsigned* queue;
   unsigned* err;
   const unsigned char* obs;

@@ -74,6 +74,51 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
   return v;
 }
 
+// Sums 16 per-lane values over a warp with 16 shuffles (a transpose-style
+// butterfly: every step halves the values a lane holds).  Afterwards v[0]
+// of lane l holds the warp total of value index
+//   ((l >> 4) & 1) * 8 + ((l >> 3) & 1) * 4 + ((l >> 2) & 1) * 2 + ((l >> 1) & 1),
+// which is returned; lanes l and l ^ 1 hold the same total.
+template <typename T>
+__device__ __forceinline__ int warp_transpose_sum16(T (&v)[16]) {
+  const int lane = threadIdx.x & 31;
+  {
+    const bool up = (lane & 16) != 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const T send = up ? v[i] : v[i + 8];
+      const T keep = up ? v[i + 8] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+  }
+  {
+    const bool up = (lane & 8) != 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const T send = up ? v[i] : v[i + 4];
+      const T keep = up ? v[i + 4] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+  }
+  {
+    const bool up = (lane & 4) != 0;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const T send = up ? v[i] : v[i + 2];
+      const T keep = up ? v[i + 2] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+  }
+  {
+    const bool up = (lane & 2) != 0;
+    const T send = up ? v[0] : v[1];
+    const T keep = up ? v[1] : v[0];
+    v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+  }
+  v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+  return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+}
+
 // Inclusive warp scan of 64-bit integers.
 __device__ __forceinline__ unsigned long long warp_incl_scan_u64(unsigned long long v) {
   const int lane = threadIdx.x & 31;
@@ -177,16 +222,21 @@ struct MergedStats {
 
 // Merge the tile rows [tb, tb + nt) of one filter (executed by a whole CTA,
 // result valid in thread 0).  Rows written by other CTAs are read through L2.
+// Each thread folds rows i, i + kThreads, ... in FP64 (rescaled to the
+// filter maximum), a transpose butterfly sums the 16 accumulators over the
+// warp, and NV threads add the warp totals; the order is fixed, so the
+// result does not depend on how the tiles were scheduled.
 template <int D>
 __device__ __forceinline__ MergedStats merge_tiles(const float* part, int tb, int nt,
                                                    float* s_maxtmp, double* s_dred) {
   constexpr int NV = 2 + D + 6;
+  static_assert(NV <= 16, "row layout");
   float m = -INFINITY;
   for (int i = threadIdx.x; i < nt; i += kThreads) m = fmaxf(m, __ldcg(part + (size_t)(tb + i) * kPartStride));
   const float M = block_max(m, s_maxtmp);
-  double acc[NV];
+  double acc[16];
 #pragma unroll
-  for (int i = 0; i < NV; ++i) acc[i] = 0.0;
+  for (int i = 0; i < 16; ++i) acc[i] = 0.0;
   if (M > -INFINITY) {
     for (int i = threadIdx.x; i < nt; i += kThreads) {
       const float4* row4 = reinterpret_cast<const float4*>(part + (size_t)(tb + i) * kPartStride);
@@ -202,30 +252,26 @@ __device__ __forceinline__ MergedStats merge_tiles(const float* part, int tb, in
     }
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int i = 0; i < NV; ++i) acc[i] = warp_sum_d(acc[i]);
+  const int idx = warp_transpose_sum16(acc);
+  __syncthreads();  // s_dred is free
+  if ((lane & 1) == 0) s_dred[warp * 16 + idx] = acc[0];
   __syncthreads();
-  if (lane == 0) {
+  if (threadIdx.x < NV) {
+    double t = 0.0;
 #pragma unroll
-    for (int i = 0; i < NV; ++i) s_dred[warp * 16 + i] = acc[i];
+    for (int w = 0; w < kThreads / 32; ++w) t += s_dred[w * 16 + threadIdx.x];
+    s_dred[threadIdx.x] = t;  // column threadIdx.x is read by this thread only
   }
   __syncthreads();
   MergedStats r;
   r.max_lw = M;
   if (threadIdx.x == 0) {
-    double t[NV];
+    r.w = s_dred[0];
+    r.w2 = s_dred[1];
 #pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      double s = 0.0;
-      for (int w = 0; w < kThreads / 32; ++w) s += s_dred[w * 16 + i];
-      t[i] = s;
-    }
-    r.w = t[0];
-    r.w2 = t[1];
+    for (int d = 0; d < kMaxD; ++d) r.sx[d] = d < D ? s_dred[2 + d] : 0.0;
 #pragma unroll
-    for (int d = 0; d < kMaxD; ++d) r.sx[d] = d < D ? t[2 + d] : 0.0;
-#pragma unroll
-    for (int i = 0; i < 6; ++i) r.sxx[i] = t[2 + D + i];
+    for (int i = 0; i < 6; ++i) r.sxx[i] = s_dred[2 + D + i];
   }
   return r;
 }
@@ -267,49 +313,6 @@ __device__ __forceinline__ void load_particles(const EngineDev& e, const float* 
   }
 }
 
-// Sums 16 per-lane values over a warp with 16 shuffles (a transpose-style
-// butterfly: every step halves the values a lane holds).  Afterwards v[0]
-// of lane l holds the warp total of value index
-//   ((l >> 4) & 1) * 8 + ((l >> 3) & 1) * 4 + ((l >> 2) & 1) * 2 + ((l >> 1) & 1),
-// which is returned; lanes l and l ^ 1 hold the same total.
-__device__ __forceinline__ int warp_transpose_sum16(float (&v)[16]) {
-  const int lane = threadIdx.x & 31;
-  {
-    const bool up = (lane & 16) != 0;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const float send = up ? v[i] : v[i + 8];
-      const float keep = up ? v[i + 8] : v[i];
-      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-    }
-  }
-  {
-    const bool up = (lane & 8) != 0;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const float send = up ? v[i] : v[i + 4];
-      const float keep = up ? v[i + 4] : v[i];
-      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-    }
-  }
-  {
-    const bool up = (lane & 4) != 0;
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const float send = up ? v[i] : v[i + 2];
-      const float keep = up ? v[i + 2] : v[i];
-      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-    }
-  }
-  {
-    const bool up = (lane & 2) != 0;
-    const float send = up ? v[0] : v[1];
-    const float keep = up ? v[1] : v[0];
-    v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
-  }
-  v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
-  return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
-}
 
 // The last tile of a filter: merged statistics -> estimate, covariance,
 // ESS, the device-side resample decision (particle_filter.py:159-161), the
@@ -832,30 +835,43 @@ __global__ void __launch_bounds__(kThreads) k_offs(EngineDev e, int t0, int coun
     load_q4(e, base, p0, n, M, K, qv);
     unsigned long long tot;
     const unsigned long long texcl = block_excl_scan_u64(qv[0] + qv[1] + qv[2] + qv[3], s_u64, &tot);
+    if (W == 0ull) {  // uniform over the CTA (one filter per tile)
+      if (threadIdx.x == 0) atomicOr(e.err, ERR_BAD_WEIGHTS);
+      continue;
+    }
+    uint32_t Fprev = 0u, Fk[4] = {0u, 0u, 0u, 0u};
     if (p0 < n) {
-      if (W == 0ull) {
-        if (threadIdx.x == 0) atomicOr(e.err, ERR_BAD_WEIGHTS);
-        continue;
-      }
       unsigned long long C = __ldcg(e.tile_excl + t) + texcl;
       const double scale = (double)n / (double)W, uf = (double)u * 2.3283064365386963e-10;
-      uint32_t Fprev = (p0 == 0) ? 0u : offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf);
-      uint32_t Fk[4];
+      Fprev = (p0 == 0) ? 0u : offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         C += qv[k];
         Fk[k] = (p0 + k < n) ? offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf) : (uint32_t)n;
       }
       *reinterpret_cast<uint4*>(e.offs + base + p0) = make_uint4(Fk[0], Fk[1], Fk[2], Fk[3]);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
+    }
+    // merge-path tile starts: tile c begins in particle i when
+    // i - 1 + F(i-1) < c * kMergeDiag <= i + F(i); each lane's run of starts
+    // is written by the whole warp (heavy particles start many tiles)
+    const int lane = threadIdx.x & 31;
+#pragma unroll 1
+    for (int k = 0; k < 4; ++k) {
+      long long c_lo = 0, c_hi = 0;
+      if (p0 + k < n) {
         const long long i = p0 + k;
-        if (i >= n) break;
-        const long long hprev = i - 1 + (long long)Fprev;
+        const long long hprev = i - 1 + (long long)(k == 0 ? Fprev : Fk[k - 1]);
         const long long h = i + (long long)Fk[k];
-        long long c = (hprev < 0) ? 0 : hprev / kMergeDiag + 1;
-        for (; c * kMergeDiag <= h; ++c) e.mp_part[tb + c] = (uint32_t)i;
-        Fprev = Fk[k];
+        c_lo = (hprev < 0) ? 0 : hprev / kMergeDiag + 1;
+        c_hi = h / kMergeDiag + 1;
+      }
+      unsigned runs = __ballot_sync(0xffffffffu, c_hi > c_lo);
+      while (runs) {
+        const int src = __ffs(runs) - 1;
+        runs &= runs - 1u;
+        const long long lo = __shfl_sync(0xffffffffu, c_lo, src), hi = __shfl_sync(0xffffffffu, c_hi, src);
+        const uint32_t iv = (uint32_t)(p0 - lane * 4 + src * 4 + k);
+        for (long long c = lo + lane; c < hi; c += 32) e.mp_part[tb + c] = iv;
       }
     }
   }

@@ -4,25 +4,28 @@
 // chunk of (filter, tile) work items and the phases of the epoch are
 // separated by grid barriers with bounded spins:
 //
-//   1  predict + likelihood + tile statistics.  The next tile's particles
-//      are copied into shared memory with cp.async while the current tile is
-//      computed (each thread copies and later reads only its own particles,
-//      so the stage needs no CTA barrier; contiguous rows use 16-byte copies,
-//      a gather through the last resample's ancestors 4-byte copies).
+//   1  predict + likelihood + tile statistics (particles loaded straight
+//      into registers, gathered through the last resample's ancestors;
+//      measured faster than staging them through shared memory with
+//      cp.async).
 //   -- barrier
 //   2  per-filter merge of the tile rows (filter f by CTA f mod G): ESS,
 //      weighted mean / covariance, device-side resample decision.
 //   -- barrier (phases 3-5 only if some filter resamples)
-//   3  systematic: quantised weights and tile sums.   Megopolis: the chain.
+//   3  systematic: quantised weights, one sum per 128-particle warp segment
+//      and (integer atomics) one per tile.   Megopolis: the chain.
 //   -- barrier
-//   4  exclusive tile prefixes, in-tile scan, offspring ends F(i) and the
-//      merge-path partition points.
+//   4  exclusive prefix of every particle (filter prefix of the tile from
+//      the tile sums, segment prefix from the warp sums, warp scan),
+//      offspring ends F(i), merge-path start of every 256-diagonal block.
 //   -- barrier
-//   5  merge path: ancestor of every slot.
+//   5  merge path, one warp per 256-diagonal block: ancestor of every slot.
 //
 // Compared with one kernel per phase this removes four launch/drain gaps and
-// every per-tile queue atomic; the log-weights reread in phases 3 and 4 come
-// from L2 (the epoch just wrote them).
+// every per-tile queue atomic; the log-weights and quantised weights reread
+// in phases 3 and 4 come from L2 (the epoch just wrote them).  Phases 3-5
+// need no CTA barrier per tile: warps work on independent segments and
+// blocks.
 #pragma once
 #include "pf_engine_kernels.cuh"
 
@@ -63,17 +66,6 @@ __device__ __forceinline__ void grid_barrier(const EngineDev& e, unsigned* bar, 
   __syncthreads();
 }
 
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-
 // Reads through L2 of control-block fields that another CTA wrote before a
 // grid barrier (L1 is not coherent across SMs).
 __device__ __forceinline__ int ld_cg_int(const int* p) { return __ldcg(p); }
@@ -88,141 +80,243 @@ __device__ __forceinline__ void cta_chunk(int t0, int count, int& b, int& e) {
   e = b + per + (c < rem ? 1 : 0);
 }
 
-// Issue the cp.async copies of one thread's 4 particles of tile t into its
-// stage slots (stage layout [D][kThreads][4] floats).
-template <int D>
-__device__ __forceinline__ void stage_tile(const EngineDev& e, float* stage, int t) {
-  const int f = __ldg(e.tile_filter + t);
-  const FilterDesc* fd = e.desc + f;
-  const FilterCtrl* fc = e.ctrl + f;
-  const int n = fd->n;
-  const int p0 = (t - fd->tile_begin) * kTile + (int)threadIdx.x * 4;
-  if (p0 >= n) return;
-  const long long base = fd->p_off;
-  const float* src = fc->parity ? e.state1 : e.state0;
-  float* mine = stage + (size_t)threadIdx.x * 4;
-  if (fc->resample_flag) {
-    const int4 a = __ldcg(reinterpret_cast<const int4*>(e.anc + base + p0));
-    int ai[4] = {a.x, a.y, a.z, a.w};
+// Block-wide sums of two 64-bit values (s_tmp: 2 * kWarps words).
+__device__ __forceinline__ void block_sum2_u64(unsigned long long a, unsigned long long b,
+                                               unsigned long long* s_tmp, unsigned long long& ra,
+                                               unsigned long long& rb) {
+  constexpr int kWarps = kThreads / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  a = warp_sum_u64(a);
+  b = warp_sum_u64(b);
+  __syncthreads();
+  if (lane == 0) {
+    s_tmp[warp] = a;
+    s_tmp[kWarps + warp] = b;
+  }
+  __syncthreads();
+  ra = 0ull;
+  rb = 0ull;
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (p0 + k >= n || (unsigned)ai[k] >= (unsigned)n) ai[k] = p0;
-#pragma unroll
-    for (int d = 0; d < D; ++d) {
-      const float* s = src + (size_t)d * e.p_total + base;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) cp_async4(mine + (size_t)d * kTile + k, s + ai[k]);
-    }
-  } else {
-#pragma unroll
-    for (int d = 0; d < D; ++d) cp_async16(mine + (size_t)d * kTile, src + (size_t)d * e.p_total + base + p0);
+  for (int w = 0; w < kWarps; ++w) {
+    ra += s_tmp[w];
+    rb += s_tmp[kWarps + w];
   }
 }
 
-// Phases 3-5 of the systematic resampler (see the header comment).
+// Quantised weights of particles [p0, p0 + 4) (zero past the filter end).
+__device__ __forceinline__ void quantize4(float4 v, int p0, int n, float M, int K, unsigned long long (&q)[4]) {
+  const float l[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) q[k] = (p0 + k < n) ? quantize_shifted((double)l[k] - (double)M, K) : 0ull;
+}
+
+// Phases 3-5 of the systematic resampler.  The chunk is walked filter
+// segment by filter segment (the tiles of one filter inside the chunk).
+// Every warp works on its own 128-particle segment (phases 3, 4) or
+// 256-diagonal merge-path block (phase 5) without CTA barriers; only the
+// per-filter prefix of phase 4 is a CTA reduction.  The loops are kept
+// compact (not unrolled over tiles): this code runs a few times per CTA and
+// epoch, so instruction fetch, not arithmetic, sets its speed.  Integer sums
+// are exact, so the result does not depend on the order of the atomics or
+// on the chunking.
 __device__ __forceinline__ void epoch_systematic(const EngineDev& e, unsigned* bar, unsigned& gen, int cb, int ce,
-                                                 unsigned long long* s_u64, uint32_t* s_F) {
-  for (int t = cb; t < ce; ++t) {
+                                                 unsigned long long* s_u64, uint32_t* s_win) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // ---------------------------------------------------------------- phase 3
+  for (int t = cb; t < ce;) {
     const int f = __ldg(e.tile_filter + t);
     const FilterDesc* fd = e.desc + f;
     const FilterCtrl* fc = e.ctrl + f;
-    if (!ld_cg_int(&fc->resample_flag)) continue;
-    const int p0 = (t - fd->tile_begin) * kTile + (int)threadIdx.x * 4;
-    unsigned long long qv[4];
-    load_q4(e, fd->p_off, p0, fd->n, ld_cg_f(&fc->max_lw), fd->K, qv);
-    unsigned long long tot;
-    block_excl_scan_u64(qv[0] + qv[1] + qv[2] + qv[3], s_u64, &tot);
-    if (threadIdx.x == 0) e.lb_agg[t] = tot;
+    const int tb = fd->tile_begin, se = min(ce, tb + fd->n_tiles);
+    if (ld_cg_int(&fc->resample_flag)) {
+      const int n = fd->n, K = fd->K;
+      const long long base = fd->p_off;
+      const float M = ld_cg_f(&fc->max_lw);
+      int p0 = (t - tb) * kTile + warp * kWarpTile + lane * 4;
+      float4 v = (p0 < n) ? __ldcg(reinterpret_cast<const float4*>(e.lw + base + p0)) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 1
+      for (int g = t; g < se; ++g, p0 += kTile) {
+        const int pn = p0 + kTile;  // prefetch the next tile's log-weights
+        const float4 vn = (g + 1 < se && pn < n) ? __ldcg(reinterpret_cast<const float4*>(e.lw + base + pn))
+                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (p0 - lane * 4 < n) {  // warp-uniform: the segment holds particles
+          unsigned long long q[4];
+          quantize4(v, p0, n, M, K, q);
+          if (p0 < n) {  // the filter's slots are padded to a multiple of 4
+            ulonglong2* dst = reinterpret_cast<ulonglong2*>(e.wq + base + p0);
+            dst[0] = make_ulonglong2(q[0], q[1]);
+            dst[1] = make_ulonglong2(q[2], q[3]);
+          }
+          const unsigned long long sw = warp_sum_u64(q[0] + q[1] + q[2] + q[3]);
+          if (lane == 0) {
+            e.wsum[(size_t)g * kSubTiles + warp] = sw;
+            atomicAdd(e.lb_agg + g, sw);  // tile sum (zeroed in phase 1)
+          }
+        }
+        v = vn;
+      }
+    }
+    t = se;
   }
   grid_barrier(e, bar, gen);
 
   // ---------------------------------------------------------------- phase 4
-  {
-    int run_f = -1;
-    unsigned long long run_excl = 0, W = 0;
-    for (int t = cb; t < ce; ++t) {
-      const int f = __ldg(e.tile_filter + t);
-      const FilterDesc* fd = e.desc + f;
-      FilterCtrl* fc = e.ctrl + f;
-      if (!ld_cg_int(&fc->resample_flag)) continue;
-      const int tb = fd->tile_begin, nt = fd->n_tiles;
-      if (f != run_f) {
-        // exclusive prefix of this tile and the filter total from the tile sums
+  for (int t = cb; t < ce;) {
+    const int f = __ldg(e.tile_filter + t);
+    const FilterDesc* fd = e.desc + f;
+    FilterCtrl* fc = e.ctrl + f;
+    const int tb = fd->tile_begin, nt = fd->n_tiles, se = min(ce, tb + nt);
+    if (ld_cg_int(&fc->resample_flag)) {  // CTA-uniform
+      // prefix of tile t inside its filter and the filter total, from the tile sums
+      unsigned long long P = 0, W = 0;
+      {
         unsigned long long pre = 0, all = 0;
         for (int i = threadIdx.x; i < nt; i += kThreads) {
           const unsigned long long v = __ldcg(e.lb_agg + tb + i);
           all += v;
           if (tb + i < t) pre += v;
         }
-        unsigned long long tp, ta;
-        block_excl_scan_u64(pre, s_u64, &tp);
-        block_excl_scan_u64(all, s_u64, &ta);
-        run_excl = tp;
-        W = ta;
-        run_f = f;
+        block_sum2_u64(pre, all, s_u64, P, W);
       }
-      if (threadIdx.x == 0 && t == tb + nt - 1) fc->wq_total = W;  // owner of the filter's last tile
-      const int n = fd->n;
-      const int p0 = (t - tb) * kTile + (int)threadIdx.x * 4;
-      const long long base = fd->p_off;
-      unsigned long long qv[4];
-      load_q4(e, base, p0, n, ld_cg_f(&fc->max_lw), fd->K, qv);
-      unsigned long long tile_tot;
-      const unsigned long long texcl = block_excl_scan_u64(qv[0] + qv[1] + qv[2] + qv[3], s_u64, &tile_tot);
-      if (p0 < n && W > 0ull) {
+      if (threadIdx.x == 0) {
+        if (se == tb + nt) fc->wq_total = W;  // the chunk holding the filter's last tile
+        if (W == 0ull) atomicOr(e.err, ERR_BAD_WEIGHTS);
+      }
+      if (W > 0ull) {
+        const int n = fd->n;
+        const long long base = fd->p_off;
         const uint32_t u = ld_cg_u(&fc->sys_u);
         const double scale = (double)n / (double)W, uf = (double)u * 2.3283064365386963e-10;
-        unsigned long long C = run_excl + texcl;
-        uint32_t Fprev = (p0 == 0) ? 0u : offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf);
-        uint32_t Fk[4];
+#pragma unroll 1
+        for (int g = t; g < se; ++g) {
+          const int pw = (g - tb) * kTile + warp * kWarpTile;
+          const int p0 = pw + lane * 4;
+          const unsigned long long ts = __ldcg(e.lb_agg + g);
+          if (pw < n) {  // warp-uniform
+            const unsigned long long ws = (lane < warp) ? __ldcg(e.wsum + (size_t)g * kSubTiles + lane) : 0ull;
+            ulonglong2 qa = make_ulonglong2(0ull, 0ull), qb = qa;
+            if (p0 < n) {
+              const ulonglong2* src = reinterpret_cast<const ulonglong2*>(e.wq + base + p0);
+              qa = __ldcg(src);
+              qb = __ldcg(src + 1);
+            }
+            const unsigned long long seg_pre = warp_sum_u64(ws);  // earlier segments of the tile
+            const unsigned long long q[4] = {qa.x, qa.y, qb.x, qb.y};
+            const unsigned long long mine = q[0] + q[1] + q[2] + q[3];
+            unsigned long long C = P + seg_pre + warp_incl_scan_u64(mine) - mine;
+            uint32_t Fprev = 0u, Fk[4] = {0u, 0u, 0u, 0u};
+            if (p0 < n) {
+              Fprev = (p0 == 0) ? 0u : offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          C += qv[k];
-          Fk[k] = (p0 + k < n) ? offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf) : (uint32_t)n;
+              for (int k = 0; k < 4; ++k) {
+                C += q[k];
+                Fk[k] = (p0 + k < n) ? offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf) : (uint32_t)n;
+              }
+              *reinterpret_cast<uint4*>(e.offs + base + p0) = make_uint4(Fk[0], Fk[1], Fk[2], Fk[3]);
+            }
+            // merge-path block starts: block c begins in particle i when
+            // i - 1 + F(i-1) < c * kWarpDiag <= i + F(i).  A heavy particle
+            // starts many blocks, and heavy particles sit next to each other
+            // after a resample, so the warp writes each lane's run of block
+            // starts together.
+#pragma unroll 1
+            for (int k = 0; k < 4; ++k) {
+              long long c_lo = 0, c_hi = 0;  // blocks [c_lo, c_hi) start in particle p0 + k
+              if (p0 + k < n) {
+                const long long i = p0 + k;
+                const long long hprev = i - 1 + (long long)(k == 0 ? Fprev : Fk[k - 1]);
+                const long long h = i + (long long)Fk[k];
+                c_lo = (hprev < 0) ? 0 : hprev / kWarpDiag + 1;
+                c_hi = h / kWarpDiag + 1;
+              }
+              unsigned runs = __ballot_sync(0xffffffffu, c_hi > c_lo);
+              while (runs) {
+                const int src = __ffs(runs) - 1;
+                runs &= runs - 1u;
+                const long long lo = __shfl_sync(0xffffffffu, c_lo, src), hi = __shfl_sync(0xffffffffu, c_hi, src);
+                const uint32_t iv = (uint32_t)(pw + src * 4 + k);
+                for (long long c = lo + lane; c < hi; c += 32) e.mp_warp[(size_t)tb * kSubTiles + c] = iv;
+              }
+            }
+          }
+          P += ts;
         }
-        *reinterpret_cast<uint4*>(e.offs + base + p0) = make_uint4(Fk[0], Fk[1], Fk[2], Fk[3]);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const long long i = p0 + k;
-          if (i >= n) break;
-          const long long hprev = i - 1 + (long long)Fprev;
-          const long long h = i + (long long)Fk[k];
-          long long c = (hprev < 0) ? 0 : hprev / kMergeDiag + 1;
-          for (; c * kMergeDiag <= h; ++c) e.mp_part[tb + c] = (uint32_t)i;
-          Fprev = Fk[k];
-        }
-      } else if (W == 0ull && threadIdx.x == 0) {
-        atomicOr(e.err, ERR_BAD_WEIGHTS);
       }
-      run_excl += tile_tot;
     }
+    t = se;
   }
   grid_barrier(e, bar, gen);
 
   // ---------------------------------------------------------------- phase 5
-  for (int t = cb; t < ce; ++t) {
+  // Warp block c of a filter covers merge diagonals [c*256, c*256 + 256):
+  // lane l walks 8 of them from diagonal c*256 + 8l, reading the offspring
+  // ends of particles [i0, i0 + 257) staged in the warp's window.
+  uint32_t* s_F = s_win + warp * kWindowWords;
+  for (int t = cb; t < ce;) {
     const int f = __ldg(e.tile_filter + t);
     const FilterDesc* fd = e.desc + f;
     const FilterCtrl* fc = e.ctrl + f;
-    if (!ld_cg_int(&fc->resample_flag)) continue;
-    merge_tile(e, fd, t, s_F);
+    const int tb = fd->tile_begin, se = min(ce, tb + fd->n_tiles);
+    if (ld_cg_int(&fc->resample_flag)) {
+      const int n = fd->n;
+      const long long base = fd->p_off, n2 = 2ll * n;
+#pragma unroll 1
+      for (int g = t; g < se; ++g) {
+        const int c = (g - tb) * kSubTiles + warp;  // block index inside the filter
+        const long long d0 = (long long)c * kWarpDiag;
+        if (d0 >= n2) continue;  // warp-uniform
+        const int i0 = (int)__ldcg(e.mp_warp + (size_t)tb * kSubTiles + c);
+        if (i0 < 0 || i0 >= n) {  // cannot happen with valid weights; never index with it
+          if (lane == 0) atomicOr(e.err, ERR_BAD_WEIGHTS);
+          continue;
+        }
+        const int win = min(kWarpDiag + 1, n - i0);
+        __syncwarp();  // the window is free
+        for (int w = lane; w < win; w += 32) s_F[w] = __ldcg(e.offs + base + i0 + w);
+        __syncwarp();
+        const long long d = d0 + (long long)lane * (kWarpDiag / 32);
+        const long long dend = min(d0 + (long long)kWarpDiag, n2);
+        if (d < dend) {
+          int lo = 0, hi = (int)min((long long)(win - 1), d - d0);
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((long long)(i0 + mid) + (long long)s_F[mid] >= d) hi = mid;
+            else lo = mid + 1;
+          }
+          int i = i0 + lo;
+          long long k = d - i;
+          const int steps = (int)min((long long)(kWarpDiag / 32), dend - d);
+#pragma unroll 1
+          for (int s = 0; s < steps; ++s) {
+            const int wi = i - i0;
+            if (wi >= win) break;
+            if (k < (long long)s_F[wi]) {
+              if (k >= 0 && k < n) e.anc[base + k] = i;
+              ++k;
+            } else {
+              ++i;
+            }
+          }
+        }
+      }
+    }
+    t = se;
   }
 }
-
 
 template <int NCLK, int WMODE, int RESAMPLER>
 __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int count, unsigned* bar) {
   constexpr int D = 3 + NCLK;
   constexpr int NV = 2 + D + 6;
   constexpr int kWarps = kThreads / 32;
-  extern __shared__ __align__(16) float s_stage[];  // [2][D][kTile]
+  extern __shared__ __align__(16) uint32_t s_win[];  // merge-path windows [kWarps][kWindowWords]
   __shared__ float2 s_sat[8 * PF_MAX_SATS];
   __shared__ int s_grp[PF_MAX_CLK + 1];
   __shared__ unsigned char s_clk[PF_MAX_SATS];
   __shared__ float s_wrow[2][kWarps][17];
   __shared__ float s_maxtmp[kWarps];
   __shared__ double s_dred[kWarps * 16];
-  __shared__ unsigned long long s_u64[kWarps];
+  __shared__ unsigned long long s_u64[2 * kWarps];
   __shared__ int s_any;
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -233,17 +327,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
   }
   int cb, ce;
   cta_chunk(t0, count, cb, ce);
+  for (int t = cb + (int)threadIdx.x; t < ce; t += kThreads) e.lb_agg[t] = 0ull;  // tile sums of phase 3
 
   // ---------------------------------------------------------------- phase 1
-  if (cb < ce) stage_tile<D>(e, s_stage, cb);
-  cp_async_commit();
   int cached = -1;
   int it = 0;
   for (int t = cb; t < ce; ++t, ++it) {
-    float* stage = s_stage + (size_t)(it & 1) * D * kTile;
-    if (t + 1 < ce) stage_tile<D>(e, s_stage + (size_t)((it + 1) & 1) * D * kTile, t + 1);
-    cp_async_commit();
-    cp_async_wait_1();  // this thread's copies of tile t have landed
 
     const int f = __ldg(e.tile_filter + t);
     const FilterDesc* fd = e.desc + f;
@@ -315,11 +404,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
     float* dst = fc->parity ? e.state0 : e.state1;
     float x[D][4];
     float lwv[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    if (active) {
+      load_particles<D>(e, fc->parity ? e.state1 : e.state0, base, p0, n, fc->resample_flag != 0, x);
+    } else {
 #pragma unroll
-    for (int d = 0; d < D; ++d) {
-      const float4 v = active ? *reinterpret_cast<const float4*>(stage + (size_t)d * kTile + threadIdx.x * 4)
-                              : make_float4(0.f, 0.f, 0.f, 0.f);
-      x[d][0] = v.x; x[d][1] = v.y; x[d][2] = v.z; x[d][3] = v.w;
+      for (int d = 0; d < D; ++d)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) x[d][k] = 0.f;
     }
     if (active) {
       float lw0[4] = {0.f, 0.f, 0.f, 0.f};
@@ -507,7 +598,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
       mego_tile(e, fd, ld_cg_u(&fc->epoch) - 1u, t);
     }
   } else {
-    epoch_systematic(e, bar, gen, cb, ce, s_u64, reinterpret_cast<uint32_t*>(s_stage));
+    epoch_systematic(e, bar, gen, cb, ce, s_u64, s_win);
   }
 }
 

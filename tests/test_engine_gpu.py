@@ -176,6 +176,37 @@ def test_batched_parity_each_filter():
                 assert o["anc_equal"], (k, o)
 
 
+@pytest.mark.parametrize("resampler", ["systematic", "megopolis"])
+def test_epoch_kernel_equals_kernel_chain(resampler):
+    """The cooperative one-kernel epoch and the one-kernel-per-phase chain
+    compute the same tile rows, merge them in the same order and resample
+    with the same integer arithmetic: every output is bit-identical."""
+    ns = [70_000, 1500, 4097]
+    trs = [S.single_filter(n_epochs=4, sats_per_const=8 + 3 * k, seed=20 + k, nlos_frac=0.25) for k in range(3)]
+
+    def run(chain):
+        eng = H.make_engine(ns, resampler=resampler, chain=chain, seeds=[31, 32, 33])
+        for k, tr in enumerate(trs):
+            eng.initialize(k, tr.anchor, tr.truth_clk[0], 20.0, 30.0)
+        outs = []
+        for t in range(4):
+            fl = N.PF_EP_PREDICT | N.PF_EP_WEIGHT | (N.PF_EP_FORCE_RESAMPLE if t % 2 else 0)
+            fe, sv = eng.pack_epoch([_epoch_rec(tr, t, fl) for tr in trs])
+            eng.upload(0, fe, sv)
+            eng.step()
+            outs.append([(eng.state_f32(k, raw=True), eng.ancestors(k), eng.results()[k]) for k in range(3)])
+        return outs
+
+    a, b = run(False), run(True)
+    for sa, sb in zip(a, b):
+        for (xa, anca, ra), (xb, ancb, rb) in zip(sa, sb):
+            assert np.array_equal(xa[0], xb[0]) and np.array_equal(xa[1], xb[1])
+            assert ra["resampled"] == rb["resampled"]
+            if ra["resampled"]:
+                assert np.array_equal(anca, ancb)
+            assert np.array_equal(ra["est_ecef"], rb["est_ecef"]) and ra["ess"] == rb["ess"]
+
+
 def test_determinism_same_seed_bit_identical():
     tr = S.config0()
 
