@@ -64,7 +64,7 @@ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
   size_t off_state0, off_state1, off_lw, off_anc, off_offs, off_mp, off_part, off_agg, off_inc,
-      off_flag, off_excl, off_wq, off_wsum, off_mpw, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
+      off_flag, off_excl, off_wq, off_wsum, off_mpw, off_fmax, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
       total;
   size_t obs_slot_bytes;
   long long P;
@@ -142,10 +142,11 @@ Layout make_layout(const pf_engine_config_t* cfg, const pf_filter_params_t* fp) 
   L.off_wq = take((size_t)P * 8);
   L.off_wsum = take((size_t)T * kSubTiles * 8);
   L.off_mpw = take((size_t)T * kSubTiles * 4);
+  L.off_fmax = take((size_t)cfg->n_filters * 4);
   L.off_desc = take(sizeof(FilterDesc) * cfg->n_filters);
   L.off_ctrl = take(sizeof(FilterCtrl) * cfg->n_filters);
   L.off_tf = take((size_t)T * 4);
-  L.off_queue = take(sizeof(unsigned) * (2 * Q_COUNT + 8));
+  L.off_queue = take(sizeof(unsigned) * (2 * Q_COUNT + kBarFlags + kMaxEpochGrid));
   L.off_err = take(sizeof(unsigned) * 4);
   L.obs_slot_bytes = align_up(sizeof(pf_filter_epoch_t) * cfg->n_filters +
                                   sizeof(pf_sat_t) * (size_t)cfg->n_filters * cfg->max_sats,
@@ -344,7 +345,7 @@ int prepare_epoch_kernel(pf_engine* eng) {
 // resident at once, which the grid barriers require (the driver refuses the
 // launch otherwise).
 int launch_epoch(pf_engine* eng, int t0, int count) {
-  const int grid = std::max(1, std::min(count, eng->epoch_resident));
+  const int grid = std::max(1, std::min(std::min(count, eng->epoch_resident), kMaxEpochGrid));
   cudaLaunchConfig_t lc;
   memset(&lc, 0, sizeof(lc));
   lc.gridDim = dim3((unsigned)grid);
@@ -469,6 +470,7 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
   e.wq = (unsigned long long*)(w + L.off_wq);
   e.wsum = (unsigned long long*)(w + L.off_wsum);
   e.mp_warp = (uint32_t*)(w + L.off_mpw);
+  e.fmax = (unsigned*)(w + L.off_fmax);
   eng->desc_dev = (FilterDesc*)(w + L.off_desc);
   eng->ctrl_dev = (FilterCtrl*)(w + L.off_ctrl);
   e.desc = eng->desc_dev;
@@ -534,8 +536,10 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
     c.rs_seq = 1;
   }
   if (check_cuda(cudaMemsetAsync(w + L.off_flag, 0, (size_t)L.T * 4, eng->stream), "memset flags") != PF_OK ||
-      check_cuda(cudaMemsetAsync(w + L.off_queue, 0, sizeof(unsigned) * (2 * Q_COUNT + 8), eng->stream), "memset queue") != PF_OK ||
+      check_cuda(cudaMemsetAsync(w + L.off_queue, 0, sizeof(unsigned) * (2 * Q_COUNT + kBarFlags + kMaxEpochGrid),
+                                 eng->stream), "memset queue") != PF_OK ||
       check_cuda(cudaMemsetAsync(w + L.off_err, 0, sizeof(unsigned) * 4, eng->stream), "memset err") != PF_OK ||
+      check_cuda(cudaMemsetAsync(w + L.off_fmax, 0, (size_t)cfg->n_filters * 4, eng->stream), "memset fmax") != PF_OK ||
       check_cuda(cudaMemsetAsync(w + L.off_obs, 0, L.obs_slot_bytes * cfg->obs_slots, eng->stream), "memset obs") != PF_OK ||
       check_cuda(cudaMemsetAsync(w + L.off_state0, 0, (size_t)L.D * L.P * 4, eng->stream), "memset state") != PF_OK ||
       check_cuda(cudaMemsetAsync(w + L.off_lw, 0, (size_t)L.P * 4, eng->stream), "memset lw") != PF_OK)
@@ -1059,8 +1063,8 @@ int pfe_test_poison_lookback(pf_engine_t* eng, int on) {
   if (!on) {
     CK(cudaStreamSynchronize(eng->stream));
     CK(cudaMemset(eng->dev.err, 0, sizeof(unsigned)));
-    // timed-out barriers leave their arrival count behind: start clean
-    CK(cudaMemset(eng->bar, 0, sizeof(unsigned) * 8));
+    // timed-out barriers leave their generation and arrival flags behind: start clean
+    CK(cudaMemset(eng->bar, 0, sizeof(unsigned) * (kBarFlags + kMaxEpochGrid)));
   }
   return PF_OK;
 }

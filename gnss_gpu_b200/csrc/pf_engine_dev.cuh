@@ -16,6 +16,8 @@ constexpr int kWarpTile = 32 * kPerThread;      // particles per warp segment (e
 constexpr int kSubTiles = kTile / kWarpTile;    // warp segments per tile
 constexpr int kWarpDiag = 2 * kWarpTile;        // merge-path diagonals per warp block
 constexpr int kWindowWords = kWarpDiag + 4;     // offspring-end window per warp block
+constexpr int kBarFlags = 8;                    // epoch kernel: first arrival-flag word of the barrier block
+constexpr int kMaxEpochGrid = 2048;             // epoch kernel: most CTAs of one launch
 constexpr int kMaxD = 3 + PF_MAX_CLK;
 
 // Work-queue slots (two words each: next tile, exit ticket).
@@ -85,6 +87,7 @@ struct EngineDev {
   unsigned long long* wq;    // epoch kernel: quantised weight per particle
   unsigned long long* wsum;  // epoch kernel: quantised weight sum per warp segment
   uint32_t* mp_warp;         // epoch kernel: merge-path start per warp block
+  unsigned* fmax;            // epoch kernel: per filter, order-preserving code of the max log-weight
   unsigned* queue;
   unsigned* err;
   const unsigned char* obs;

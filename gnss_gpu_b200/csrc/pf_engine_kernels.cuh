@@ -25,6 +25,56 @@ namespace pfb {
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ float2 bc(float a) { return make_float2(a, a); }
 
+// ---- satellite table of the likelihood (shared memory, one entry per
+// satellite, every constant stored twice so the packed f32x2 operations
+// read it without register moves): e_E, e_N, e_U (unit line of sight in the
+// local frame), g/2 with g = 1/r0, y = pr - r0 - clock anchor, weight.
+constexpr int kSatStride = 6;  // float2 per satellite entry (three float4)
+
+__device__ __forceinline__ void write_sat_entry(float2* o, float eE, float eN, float eU, float g, float y, float wq) {
+  o[0] = bc(eE);
+  o[1] = bc(eN);
+  o[2] = bc(eU);
+  o[3] = bc(0.5f * g);
+  o[4] = bc(y);
+  o[5] = bc(wq);
+}
+
+// Log-weight update of two particles for one satellite.  With d the
+// particle offset from the anchor, ed = e.d and the receiver clock cb, the
+// range residual to second order in |d|/r0 is
+//   r = (y - cb + ed) + (g/2) (ed^2 - |d|^2)
+// (the next term, of order |d|^3 g^2, is below 1e-8 m for |d| < 1 km).
+// ye = y - cb + ed is formed first and ed recovered as ye - (y - cb): both
+// are of the size of the residual, so no large range is ever subtracted.
+// nbb = -|d|^2 and ncb = -cb of the pair.
+template <int WMODE>
+__device__ __forceinline__ void sat_pair_update(const float2* entry, float2 dx, float2 dy, float2 dz, float2 nbb,
+                                                float2 ncb, float2& lw, const FilterDesc* fd) {
+  const float4* sv = reinterpret_cast<const float4*>(entry);
+  const float4 q0 = sv[0], q1 = sv[1], q2 = sv[2];
+  const float2 eE = f2(q0.x, q0.y), eN = f2(q0.z, q0.w), eU = f2(q1.x, q1.y), g2 = f2(q1.z, q1.w);
+  const float2 yy = f2(q2.x, q2.y), wq = f2(q2.z, q2.w);
+  const float2 yc = __fadd2_rn(yy, ncb);
+  float2 ye = __ffma2_rn(eE, dx, yc);
+  ye = __ffma2_rn(eN, dy, ye);
+  ye = __ffma2_rn(eU, dz, ye);
+  const float2 ed = __ffma2_rn(yc, bc(-1.0f), ye);
+  const float2 sq = __ffma2_rn(ed, ed, nbb);
+  const float2 r = __ffma2_rn(sq, g2, ye);
+  if (WMODE == PF_WEIGHT_GAUSSIAN) {
+    const float2 rw = __fmul2_rn(r, wq);
+    lw = __ffma2_rn(rw, r, lw);
+  } else {
+    const float ks = fd->huber_k;
+    const float z0 = fabsf(r.x) * fd->inv_sigma_pr, z1 = fabsf(r.y) * fd->inv_sigma_pr;
+    const float rho0 = z0 < ks ? 0.5f * z0 * z0 : fmaf(ks, z0, -0.5f * ks * ks);
+    const float rho1 = z1 < ks ? 0.5f * z1 * z1 : fmaf(ks, z1, -0.5f * ks * ks);
+    lw.x = fmaf(-wq.x, rho0, lw.x);
+    lw.y = fmaf(-wq.x, rho1, lw.y);
+  }
+}
+
 // Programmatic dependent launch (sm_90+): a kernel lets the next kernel of
 // the stream start launching as soon as all of its CTAs are running, and
 // waits for the previous kernel's completion (and memory flush) before it
@@ -220,20 +270,28 @@ struct MergedStats {
   double sxx[6];
 };
 
-// Merge the tile rows [tb, tb + nt) of one filter (executed by a whole CTA,
-// result valid in thread 0).  Rows written by other CTAs are read through L2.
-// Each thread folds rows i, i + kThreads, ... in FP64 (rescaled to the
-// filter maximum), a transpose butterfly sums the 16 accumulators over the
-// warp, and NV threads add the warp totals; the order is fixed, so the
-// result does not depend on how the tiles were scheduled.
+// Order-preserving code of a float (larger float, larger code; 0 is below
+// every code, so a zeroed word means "no finite value seen").
+__device__ __forceinline__ unsigned ord_code(float f) {
+  const unsigned b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float ord_decode(unsigned c) {
+  if (c == 0u) return -INFINITY;
+  return __uint_as_float((c & 0x80000000u) ? (c & 0x7FFFFFFFu) : ~c);
+}
+
+// Merge the tile rows [tb, tb + nt) of one filter whose maximum tile
+// log-weight M is known (executed by a whole CTA, result valid in thread
+// 0).  Rows written by other CTAs are read through L2.  Each thread folds
+// rows i, i + kThreads, ... in FP64 (rescaled to M), a transpose butterfly
+// sums the 16 accumulators over the warp, and NV threads add the warp
+// totals; the order is fixed, so the result does not depend on how the
+// tiles were scheduled.
 template <int D>
-__device__ __forceinline__ MergedStats merge_tiles(const float* part, int tb, int nt,
-                                                   float* s_maxtmp, double* s_dred) {
+__device__ __forceinline__ MergedStats merge_tiles_at(const float* part, int tb, int nt, float M, double* s_dred) {
   constexpr int NV = 2 + D + 6;
   static_assert(NV <= 16, "row layout");
-  float m = -INFINITY;
-  for (int i = threadIdx.x; i < nt; i += kThreads) m = fmaxf(m, __ldcg(part + (size_t)(tb + i) * kPartStride));
-  const float M = block_max(m, s_maxtmp);
   double acc[16];
 #pragma unroll
   for (int i = 0; i < 16; ++i) acc[i] = 0.0;
@@ -274,6 +332,20 @@ __device__ __forceinline__ MergedStats merge_tiles(const float* part, int tb, in
     for (int i = 0; i < 6; ++i) r.sxx[i] = s_dred[2 + D + i];
   }
   return r;
+}
+
+// Maximum tile log-weight of the rows [tb, tb + nt) (whole CTA).
+__device__ __forceinline__ float rows_max(const float* part, int tb, int nt, float* s_maxtmp) {
+  float m = -INFINITY;
+  for (int i = threadIdx.x; i < nt; i += kThreads) m = fmaxf(m, __ldcg(part + (size_t)(tb + i) * kPartStride));
+  return block_max(m, s_maxtmp);
+}
+
+// As merge_tiles_at, with the maximum taken over the rows first.
+template <int D>
+__device__ __forceinline__ MergedStats merge_tiles(const float* part, int tb, int nt,
+                                                   float* s_maxtmp, double* s_dred) {
+  return merge_tiles_at<D>(part, tb, nt, rows_max(part, tb, nt, s_maxtmp), s_dred);
 }
 
 // Local offsets -> ECEF: anchor + R^T v.
@@ -407,7 +479,7 @@ __global__ void __launch_bounds__(kThreads, PF_KSTEP_MINB) k_step(EngineDev e, i
   constexpr int D = 3 + NCLK;
   constexpr int NV = 2 + D + 6;  // s, s2, sx[D], xx, xy, xz, yy, yz, zz
   constexpr int kWarps = kThreads / 32;
-  __shared__ float2 s_sat[8 * PF_MAX_SATS];  // per satellite: e_E, e_N, e_U, -g/2, g^2/2, g/2, y, wq
+  __shared__ __align__(16) float2 s_sat[kSatStride * PF_MAX_SATS];
   __shared__ int s_grp[PF_MAX_CLK + 1];
   __shared__ unsigned char s_clk[PF_MAX_SATS];
   __shared__ float s_wrow[kWarps][17];       // per-warp max + NV sums
@@ -477,15 +549,7 @@ __global__ void __launch_bounds__(kThreads, PF_KSTEP_MINB) k_step(EngineDev e, i
           const int c2 = s_clk[s2];
           rank += (c2 < c) || (c2 == c && s2 < (int)threadIdx.x);
         }
-        float2* o = s_sat + 8 * rank;
-        o[0] = bc(eE);
-        o[1] = bc(eN);
-        o[2] = bc(eU);
-        o[3] = bc(-0.5f * g);
-        o[4] = bc(0.5f * g * g);
-        o[5] = bc(0.5f * g);
-        o[6] = bc(y);
-        o[7] = bc(wq);
+        write_sat_entry(s_sat + kSatStride * rank, eE, eN, eU, g, y, wq);
       }
       if (threadIdx.x <= NCLK) {
         int cnt = 0;
@@ -558,15 +622,16 @@ __global__ void __launch_bounds__(kThreads, PF_KSTEP_MINB) k_step(EngineDev e, i
 
       if (do_weight) {
         float2 lwp[2] = {f2(lw0[0], lw0[1]), f2(lw0[2], lw0[3])};
-        float2 dx[2], dy[2], dz[2], bb[2];
+        float2 dx[2], dy[2], dz[2], nbb[2];
 #pragma unroll
         for (int p = 0; p < 2; ++p) {
           dx[p] = f2(x[0][2 * p], x[0][2 * p + 1]);
           dy[p] = f2(x[1][2 * p], x[1][2 * p + 1]);
           dz[p] = f2(x[2][2 * p], x[2][2 * p + 1]);
-          bb[p] = __fmul2_rn(dx[p], dx[p]);
-          bb[p] = __ffma2_rn(dy[p], dy[p], bb[p]);
-          bb[p] = __ffma2_rn(dz[p], dz[p], bb[p]);
+          float2 bb = __fmul2_rn(dx[p], dx[p]);
+          bb = __ffma2_rn(dy[p], dy[p], bb);
+          bb = __ffma2_rn(dz[p], dz[p], bb);
+          nbb[p] = f2(-bb.x, -bb.y);
         }
 #pragma unroll
         for (int c = 0; c < NCLK; ++c) {
@@ -574,32 +639,9 @@ __global__ void __launch_bounds__(kThreads, PF_KSTEP_MINB) k_step(EngineDev e, i
           const int s_end = s_grp[c + 1];
 #pragma unroll 2
           for (int s = s_grp[c]; s < s_end; ++s) {
-            const float4* sv = reinterpret_cast<const float4*>(s_sat + 8 * s);
-            const float4 q0 = sv[0], q1 = sv[1], q2 = sv[2], q3 = sv[3];
-            const float2 eE = f2(q0.x, q0.y), eN = f2(q0.z, q0.w), eU = f2(q1.x, q1.y), ng2 = f2(q1.z, q1.w);
-            const float2 c2 = f2(q2.x, q2.y), nc1 = f2(q2.z, q2.w), yy = f2(q3.x, q3.y), wq = f2(q3.z, q3.w);
 #pragma unroll
-            for (int p = 0; p < 2; ++p) {
-              float2 ed = __fmul2_rn(eE, dx[p]);
-              ed = __ffma2_rn(eN, dy[p], ed);
-              ed = __ffma2_rn(eU, dz[p], ed);                 // e . d
-              const float2 nh = __ffma2_rn(bb[p], ng2, ed);   // -h = e.d - |d|^2 g/2
-              const float2 ninner = __ffma2_rn(nh, c2, nc1);
-              const float2 hh = __fmul2_rn(nh, nh);
-              const float2 ndl = __ffma2_rn(hh, ninner, nh);  // -(|s-d| - r0)
-              const float2 r = __fadd2_rn(__fadd2_rn(yy, ncb[p]), ndl);
-              if (WMODE == PF_WEIGHT_GAUSSIAN) {
-                const float2 rw = __fmul2_rn(r, wq);
-                lwp[p] = __ffma2_rn(rw, r, lwp[p]);
-              } else {
-                const float ks = fd->huber_k;
-                const float z0 = fabsf(r.x) * fd->inv_sigma_pr, z1 = fabsf(r.y) * fd->inv_sigma_pr;
-                const float rho0 = z0 < ks ? 0.5f * z0 * z0 : fmaf(ks, z0, -0.5f * ks * ks);
-                const float rho1 = z1 < ks ? 0.5f * z1 * z1 : fmaf(ks, z1, -0.5f * ks * ks);
-                lwp[p].x = fmaf(-wq.x, rho0, lwp[p].x);
-                lwp[p].y = fmaf(-wq.x, rho1, lwp[p].y);
-              }
-            }
+            for (int p = 0; p < 2; ++p)
+              sat_pair_update<WMODE>(s_sat + kSatStride * s, dx[p], dy[p], dz[p], nbb[p], ncb[p], lwp[p], fd);
           }
         }
         lwv[0] = lwp[0].x; lwv[1] = lwp[0].y; lwv[2] = lwp[1].x; lwv[3] = lwp[1].y;

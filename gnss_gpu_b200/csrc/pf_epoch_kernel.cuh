@@ -9,19 +9,21 @@
 //      measured faster than staging them through shared memory with
 //      cp.async).
 //   -- barrier
-//   2  per-filter merge of the tile rows (filter f by CTA f mod G): ESS,
+//   2  per-filter merge of the tile rows (filter f_first + j by CTA j mod G;
+//      one pass, the filter maximum having been collected in phase 1): ESS,
 //      weighted mean / covariance, device-side resample decision.
-//   -- barrier (phases 3-5 only if some filter resamples)
-//   3  systematic: quantised weights, one sum per 128-particle warp segment
-//      and (integer atomics) one per tile.   Megopolis: the chain.
-//   -- barrier
+//      At the same time, systematic only, on the CTAs that own no filter:
+//   3  quantised weights, one sum per 128-particle warp segment and
+//      (integer atomics) one per tile, for every filter that may resample.
+//   -- barrier (what follows only if some filter resamples)
+//   3' Megopolis: the chain per slot.   Systematic:
 //   4  exclusive prefix of every particle (filter prefix of the tile from
 //      the tile sums, segment prefix from the warp sums, warp scan),
 //      offspring ends F(i), merge-path start of every 256-diagonal block.
 //   -- barrier
 //   5  merge path, one warp per 256-diagonal block: ancestor of every slot.
 //
-// Compared with one kernel per phase this removes four launch/drain gaps and
+// Compared with one kernel per phase this removes the launch/drain gaps and
 // every per-tile queue atomic; the log-weights and quantised weights reread
 // in phases 3 and 4 come from L2 (the epoch just wrote them).  Phases 3-5
 // need no CTA barrier per tile: warps work on independent segments and
@@ -31,39 +33,66 @@
 
 namespace pfb {
 
-// Sense-counting grid barrier for co-resident CTAs.  bar[0] counts
-// arrivals, bar[1] is the generation; `gen` is this CTA's copy of the
-// generation.  The wait is bounded: on timeout the error word is set and
-// the CTA goes on (results are then invalid, and the host reports
-// PF_ETIMEOUT).
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid barrier for co-resident CTAs.  bar[1] is the generation and
+// bar[kBarFlags + c] CTA c's arrival flag; `gen` is this CTA's copy of the
+// generation.  Every CTA publishes its arrival with a release store of the
+// next generation into its own flag (no contended atomic), the threads of
+// CTA 0 watch all flags, and CTA 0 then releases the grid with one store
+// of the generation word that every CTA watches.  Waits are bounded: on
+// timeout the error word is set and the CTA goes on (results are then
+// invalid, and the host reports PF_ETIMEOUT).
 __device__ __forceinline__ void grid_barrier(const EngineDev& e, unsigned* bar, unsigned& gen) {
+  const unsigned target = gen + 1u;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned target = gen + 1u;
-    // test hook: wait for a generation nobody publishes (bounded spin)
-    const unsigned want = e.lookback_poison ? target + 1u : target;
-    __threadfence();
-    const unsigned arrived = atomicAdd(&bar[0], 1u);
-    const bool last = arrived == gridDim.x - 1u;
-    if (last) {  // the last CTA to arrive resets the count and releases
-      bar[0] = 0u;
-      __threadfence();
-      atomicExch(&bar[1], target);
-    }
-    if (!last || want != target) {
+  if (threadIdx.x == 0) st_release(bar + kBarFlags + blockIdx.x, target);
+  if (blockIdx.x == 0) {
+    for (int c = threadIdx.x; c < (int)gridDim.x; c += kThreads) {
       unsigned long long spins = 0;
-      while (*(volatile unsigned*)&bar[1] != want) {
+      while (ld_acquire(bar + kBarFlags + c) != target) {
         if (++spins > e.spin_limit) {
           atomicOr(e.err, ERR_BARRIER_TIMEOUT);
           break;
         }
-        if (spins > 16) __nanosleep(100);
+        if (spins > 64) __nanosleep(32);
       }
     }
-    gen = target;
-    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) st_release(bar + 1, target);
   }
+  if (threadIdx.x == 0) {
+    // test hook: wait for a generation nobody publishes (bounded spin)
+    const unsigned want = e.lookback_poison ? target + 1u : target;
+    unsigned long long spins = 0;
+    while (ld_acquire(bar + 1) != want) {
+      if (++spins > e.spin_limit) {
+        atomicOr(e.err, ERR_BARRIER_TIMEOUT);
+        break;
+      }
+      if (spins > 64) __nanosleep(32);
+    }
+  }
+  gen = target;
   __syncthreads();
+}
+
+// Named CTA barriers over all kThreads threads: arrive without waiting,
+// or wait for the barrier to complete.
+template <int ID>
+__device__ __forceinline__ void named_arrive() {
+  asm volatile("bar.arrive %0, %1;" ::"n"(ID), "n"(kThreads) : "memory");
+}
+template <int ID>
+__device__ __forceinline__ void named_sync() {
+  asm volatile("bar.sync %0, %1;" ::"n"(ID), "n"(kThreads) : "memory");
 }
 
 // Reads through L2 of control-block fields that another CTA wrote before a
@@ -72,12 +101,14 @@ __device__ __forceinline__ int ld_cg_int(const int* p) { return __ldcg(p); }
 __device__ __forceinline__ unsigned ld_cg_u(const unsigned* p) { return __ldcg(p); }
 __device__ __forceinline__ float ld_cg_f(const float* p) { return __ldcg(p); }
 
-// Per-CTA chunk of the work items [t0, t0 + count).
+// Chunk of worker w out of nw over the work items [t0, t0 + count).
+__device__ __forceinline__ void chunk_of(int t0, int count, int w, int nw, int& b, int& e) {
+  const int per = count / nw, rem = count % nw;
+  b = t0 + w * per + min(w, rem);
+  e = b + per + (w < rem ? 1 : 0);
+}
 __device__ __forceinline__ void cta_chunk(int t0, int count, int& b, int& e) {
-  const int per = count / (int)gridDim.x, rem = count % (int)gridDim.x;
-  const int c = blockIdx.x;
-  b = t0 + c * per + min(c, rem);
-  e = b + per + (c < rem ? 1 : 0);
+  chunk_of(t0, count, (int)blockIdx.x, (int)gridDim.x, b, e);
 }
 
 // Block-wide sums of two 64-bit values (s_tmp: 2 * kWarps words).
@@ -110,28 +141,33 @@ __device__ __forceinline__ void quantize4(float4 v, int p0, int n, float M, int 
   for (int k = 0; k < 4; ++k) q[k] = (p0 + k < n) ? quantize_shifted((double)l[k] - (double)M, K) : 0ull;
 }
 
-// Phases 3-5 of the systematic resampler.  The chunk is walked filter
-// segment by filter segment (the tiles of one filter inside the chunk).
-// Every warp works on its own 128-particle segment (phases 3, 4) or
-// 256-diagonal merge-path block (phase 5) without CTA barriers; only the
-// per-filter prefix of phase 4 is a CTA reduction.  The loops are kept
-// compact (not unrolled over tiles): this code runs a few times per CTA and
-// epoch, so instruction fetch, not arithmetic, sets its speed.  Integer sums
-// are exact, so the result does not depend on the order of the atomics or
-// on the chunking.
-__device__ __forceinline__ void epoch_systematic(const EngineDev& e, unsigned* bar, unsigned& gen, int cb, int ce,
-                                                 unsigned long long* s_u64, uint32_t* s_win) {
+// The systematic resampler's phases walk a chunk of tiles filter segment by
+// filter segment (the tiles of one filter inside the chunk).  Every warp
+// works on its own 128-particle segment (phases 3, 4) or 256-diagonal
+// merge-path block (phase 5) without CTA barriers; only the per-filter
+// prefix of phase 4 is a CTA reduction.  The loops are kept compact (not
+// unrolled over tiles): this code runs a few times per CTA and epoch, so
+// instruction fetch, not arithmetic, sets its speed.  Integer sums are
+// exact, so the result does not depend on the order of the atomics or on
+// the chunking.
+
+// Phase 3, run while the filters' owners merge statistics and decide: the
+// quantised weights, one sum per warp segment and (integer atomics) one per
+// tile, for every filter that may resample this epoch (weights updated,
+// resampling not suppressed: its max-code word is set).  Whether it does
+// resample is known only after the next barrier; when it does not, this
+// work is unused.
+__device__ __forceinline__ void epoch_sys_quantise(const EngineDev& e, int cb, int ce) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // ---------------------------------------------------------------- phase 3
   for (int t = cb; t < ce;) {
     const int f = __ldg(e.tile_filter + t);
     const FilterDesc* fd = e.desc + f;
-    const FilterCtrl* fc = e.ctrl + f;
     const int tb = fd->tile_begin, se = min(ce, tb + fd->n_tiles);
-    if (ld_cg_int(&fc->resample_flag)) {
+    const unsigned mcode = __ldcg(e.fmax + f);
+    if (mcode != 0u) {
       const int n = fd->n, K = fd->K;
       const long long base = fd->p_off;
-      const float M = ld_cg_f(&fc->max_lw);
+      const float M = ord_decode(mcode);
       int p0 = (t - tb) * kTile + warp * kWarpTile + lane * 4;
       float4 v = (p0 < n) ? __ldcg(reinterpret_cast<const float4*>(e.lw + base + p0)) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll 1
@@ -158,8 +194,12 @@ __device__ __forceinline__ void epoch_systematic(const EngineDev& e, unsigned* b
     }
     t = se;
   }
-  grid_barrier(e, bar, gen);
+}
 
+// Phases 4 and 5 for the filters that resample.
+__device__ __forceinline__ void epoch_sys_assign(const EngineDev& e, unsigned* bar, unsigned& gen, int cb, int ce,
+                                                 unsigned long long* s_u64, uint32_t* s_win) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // ---------------------------------------------------------------- phase 4
   for (int t = cb; t < ce;) {
     const int f = __ldg(e.tile_filter + t);
@@ -310,7 +350,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
   constexpr int NV = 2 + D + 6;
   constexpr int kWarps = kThreads / 32;
   extern __shared__ __align__(16) uint32_t s_win[];  // merge-path windows [kWarps][kWindowWords]
-  __shared__ float2 s_sat[8 * PF_MAX_SATS];
+  __shared__ __align__(16) float2 s_sat[kSatStride * PF_MAX_SATS];
   __shared__ int s_grp[PF_MAX_CLK + 1];
   __shared__ unsigned char s_clk[PF_MAX_SATS];
   __shared__ float s_wrow[2][kWarps][17];
@@ -320,11 +360,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
   __shared__ int s_any;
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  unsigned gen = 0;
-  if (threadIdx.x == 0) {
-    gen = *(volatile unsigned*)&bar[1];
-    if (blockIdx.x == 0) bar[2] = 0u;  // any-filter-resamples flag of this epoch
-  }
+  // generation of the last barrier (every thread reads it before its CTA
+  // first arrives, so no CTA can have moved it on yet)
+  unsigned gen = ld_acquire(bar + 1);
+  if (threadIdx.x == 0 && blockIdx.x == 0) bar[2] = 0u;  // any-filter-resamples flag of this epoch
   int cb, ce;
   cta_chunk(t0, count, cb, ce);
   for (int t = cb + (int)threadIdx.x; t < ce; t += kThreads) e.lb_agg[t] = 0ull;  // tile sums of phase 3
@@ -383,9 +422,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
           const int c2 = s_clk[s2];
           rank += (c2 < c) || (c2 == c && s2 < (int)threadIdx.x);
         }
-        float2* o = s_sat + 8 * rank;
-        o[0] = bc(eE); o[1] = bc(eN); o[2] = bc(eU); o[3] = bc(-0.5f * g);
-        o[4] = bc(0.5f * g * g); o[5] = bc(0.5f * g); o[6] = bc(y); o[7] = bc(wq);
+        write_sat_entry(s_sat + kSatStride * rank, eE, eN, eU, g, y, wq);
       }
       if (threadIdx.x <= NCLK) {
         int cnt = 0;
@@ -457,15 +494,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
 
       if (do_weight) {
         float2 lwp[2] = {f2(lw0[0], lw0[1]), f2(lw0[2], lw0[3])};
-        float2 dx[2], dy[2], dz[2], bb[2];
+        float2 dx[2], dy[2], dz[2], nbb[2];
 #pragma unroll
         for (int p = 0; p < 2; ++p) {
           dx[p] = f2(x[0][2 * p], x[0][2 * p + 1]);
           dy[p] = f2(x[1][2 * p], x[1][2 * p + 1]);
           dz[p] = f2(x[2][2 * p], x[2][2 * p + 1]);
-          bb[p] = __fmul2_rn(dx[p], dx[p]);
-          bb[p] = __ffma2_rn(dy[p], dy[p], bb[p]);
-          bb[p] = __ffma2_rn(dz[p], dz[p], bb[p]);
+          float2 bb = __fmul2_rn(dx[p], dx[p]);
+          bb = __ffma2_rn(dy[p], dy[p], bb);
+          bb = __ffma2_rn(dz[p], dz[p], bb);
+          nbb[p] = f2(-bb.x, -bb.y);
         }
 #pragma unroll
         for (int c = 0; c < NCLK; ++c) {
@@ -473,32 +511,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
           const int s_end = s_grp[c + 1];
 #pragma unroll 2
           for (int s = s_grp[c]; s < s_end; ++s) {
-            const float4* sv = reinterpret_cast<const float4*>(s_sat + 8 * s);
-            const float4 q0 = sv[0], q1 = sv[1], q2 = sv[2], q3 = sv[3];
-            const float2 eE = f2(q0.x, q0.y), eN = f2(q0.z, q0.w), eU = f2(q1.x, q1.y), ng2 = f2(q1.z, q1.w);
-            const float2 c2 = f2(q2.x, q2.y), nc1 = f2(q2.z, q2.w), yy = f2(q3.x, q3.y), wq = f2(q3.z, q3.w);
 #pragma unroll
-            for (int p = 0; p < 2; ++p) {
-              float2 ed = __fmul2_rn(eE, dx[p]);
-              ed = __ffma2_rn(eN, dy[p], ed);
-              ed = __ffma2_rn(eU, dz[p], ed);
-              const float2 nh = __ffma2_rn(bb[p], ng2, ed);
-              const float2 ninner = __ffma2_rn(nh, c2, nc1);
-              const float2 hh = __fmul2_rn(nh, nh);
-              const float2 ndl = __ffma2_rn(hh, ninner, nh);
-              const float2 r = __fadd2_rn(__fadd2_rn(yy, ncb[p]), ndl);
-              if (WMODE == PF_WEIGHT_GAUSSIAN) {
-                const float2 rw = __fmul2_rn(r, wq);
-                lwp[p] = __ffma2_rn(rw, r, lwp[p]);
-              } else {
-                const float ks = fd->huber_k;
-                const float z0 = fabsf(r.x) * fd->inv_sigma_pr, z1 = fabsf(r.y) * fd->inv_sigma_pr;
-                const float rho0 = z0 < ks ? 0.5f * z0 * z0 : fmaf(ks, z0, -0.5f * ks * ks);
-                const float rho1 = z1 < ks ? 0.5f * z1 * z1 : fmaf(ks, z1, -0.5f * ks * ks);
-                lwp[p].x = fmaf(-wq.x, rho0, lwp[p].x);
-                lwp[p].y = fmaf(-wq.x, rho1, lwp[p].y);
-              }
-            }
+            for (int p = 0; p < 2; ++p)
+              sat_pair_update<WMODE>(s_sat + kSatStride * s, dx[p], dy[p], dz[p], nbb[p], ncb[p], lwp[p], fd);
           }
         }
         lwv[0] = lwp[0].x; lwv[1] = lwp[0].y; lwv[2] = lwp[1].x; lwv[3] = lwp[1].y;
@@ -540,10 +555,23 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
         }
       }
       const int idx = warp_transpose_sum16(v);
-      float (*wr)[17] = s_wrow[it & 1];
+      // Warp rows go to buffer it & 1; warp 0 merges them while the other
+      // warps move on (named barriers: FULL[b] = 1 + b, EMPTY[b] = 3 + b).
+      const int b = it & 1;
+      float (*wr)[17] = s_wrow[b];
+      if (warp != 0 && it >= 2) {  // warp 0 has merged tile it - 2 from this buffer
+        if (b) named_sync<4>();
+        else named_sync<3>();
+      }
       if ((lane & 1) == 0 && idx < NV) wr[warp][1 + idx] = v[0];
       if (lane == 0) wr[warp][0] = wm;
-      __syncthreads();
+      if (warp != 0) {
+        if (b) named_arrive<2>();
+        else named_arrive<1>();
+      } else {
+        if (b) named_sync<2>();
+        else named_sync<1>();
+      }
       if (warp == 0) {
         float tm = lane < kWarps ? wr[lane][0] : -INFINITY;
         tm = warp_max(tm);
@@ -561,34 +589,57 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
         }
         float* row = e.part + (size_t)t * kPartStride;
         if (lane < NV) row[1 + lane] = acc;
-        if (lane == 0) row[0] = tm;
+        if (lane == 0) {
+          row[0] = tm;
+          // filter maximum for the one-pass merge and the quantiser, kept
+          // only when the filter may resample this epoch
+          if (tm > -INFINITY && do_weight && !(eflags & PF_EP_NO_RESAMPLE)) atomicMax(e.fmax + f, ord_code(tm));
+        }
+        if (it + 2 < ce - cb) {  // buffer b is free again
+          if (b) named_arrive<4>();
+          else named_arrive<3>();
+        }
       }
     }
   }
   grid_barrier(e, bar, gen);
 
   // ---------------------------------------------------------------- phase 2
-  for (int f = blockIdx.x; f < e.n_filters; f += gridDim.x) {
+  // Filter f_first + j is merged and decided by CTA j mod G.  With fewer
+  // filters than CTAs the other CTAs start phase 3 meanwhile.
+  const int f_first = __ldg(e.tile_filter + t0), nf = __ldg(e.tile_filter + t0 + count - 1) - f_first + 1;
+  for (int j = blockIdx.x; j < nf; j += gridDim.x) {
+    const int f = f_first + j;
     const FilterDesc* fd = e.desc + f;
-    if (fd->n_tiles == 0 || fd->tile_begin + fd->n_tiles <= t0 || fd->tile_begin >= t0 + count) continue;
     FilterCtrl* fc = e.ctrl + f;
     const unsigned epoch = fc->epoch;
     const unsigned char* ob = e.obs + (size_t)(epoch % (unsigned)e.obs_slots) * e.obs_slot_bytes;
     const pf_filter_epoch_t* fe = reinterpret_cast<const pf_filter_epoch_t*>(ob) + f;
     const int eflags = fe->flags;
-    MergedStats ms = merge_tiles<D>(e.part, fd->tile_begin, fd->n_tiles, s_maxtmp, s_dred);
+    const unsigned mcode = __ldcg(e.fmax + f);
+    const float M = mcode ? ord_decode(mcode) : rows_max(e.part, fd->tile_begin, fd->n_tiles, s_maxtmp);
+    MergedStats ms = merge_tiles_at<D>(e.part, fd->tile_begin, fd->n_tiles, M, s_dred);
     if (threadIdx.x == 0) {
       finalize_filter<D>(e, fd, fc, ms, epoch, fc->parity, fc->lw_zero != 0, eflags, (eflags & PF_EP_WEIGHT) != 0);
       if (fc->resample_flag) atomicOr(&bar[2], 1u);
     }
     __syncthreads();
   }
+  if constexpr (RESAMPLER == PF_RESAMPLE_SYSTEMATIC) {
+    const int h0 = nf < (int)gridDim.x ? nf : 0;  // first CTA of phase 3
+    if ((int)blockIdx.x >= h0) {
+      int b3, e3;
+      chunk_of(t0, count, (int)blockIdx.x - h0, (int)gridDim.x - h0, b3, e3);
+      epoch_sys_quantise(e, b3, e3);
+    }
+  }
   grid_barrier(e, bar, gen);
+  for (int j = blockIdx.x; j < nf; j += gridDim.x)  // every reader of the max codes is past the barrier
+    if (threadIdx.x == 0) e.fmax[f_first + j] = 0u;
   if (threadIdx.x == 0) s_any = (int)ld_cg_u(&bar[2]);
   __syncthreads();
   if (!s_any) return;  // uniform: no filter resamples this epoch
 
-  // ---------------------------------------------------------------- phase 3
   if constexpr (RESAMPLER == PF_RESAMPLE_MEGOPOLIS) {
     for (int t = cb; t < ce; ++t) {
       const int f = __ldg(e.tile_filter + t);
@@ -598,7 +649,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
       mego_tile(e, fd, ld_cg_u(&fc->epoch) - 1u, t);
     }
   } else {
-    epoch_systematic(e, bar, gen, cb, ce, s_u64, s_win);
+    epoch_sys_assign(e, bar, gen, cb, ce, s_u64, s_win);
   }
 }
 
