@@ -718,8 +718,9 @@ int pfe_step(pf_engine_t* eng) {
   if (!use_chain(eng)) {
     int s = launch_epoch(eng, 0, eng->T);
     if (s != PF_OK) return s;
-    if (ev)
-      for (int k = 1; k < kTimingEvents; ++k) CK(cudaEventRecord(ev[k], eng->stream));
+    // one event after the single kernel: every extra event record on the
+    // stream adds microseconds to the measured step
+    if (ev) CK(cudaEventRecord(ev[1], eng->stream));
     eng->last_launches = 1;
     return PF_OK;
   }
@@ -775,15 +776,16 @@ int pfe_read_timing(pf_engine_t* eng, float* step_kernel_ms, float* whole_step_m
     const cudaEvent_t* ev = &eng->tev[kTimingEvents * (size_t)((first + i) % eng->t_slots)];
     float a = 0.f, b = 0.f;
     CK(cudaEventElapsedTime(&a, ev[0], ev[1]));
-    CK(cudaEventElapsedTime(&b, ev[0], ev[kTimingEvents - 1]));
+    if (use_chain(eng)) CK(cudaEventElapsedTime(&b, ev[0], ev[kTimingEvents - 1]));
+    else b = a;  // the epoch kernel is the whole step
     if (step_kernel_ms) step_kernel_ms[i] = a;
     if (whole_step_ms) whole_step_ms[i] = b;
     for (int k = 0; k < kTimingEvents - 1; ++k) {
       float m = 0.f;
-      if (eng->t_detailed || k == 0) CK(cudaEventElapsedTime(&m, ev[k], ev[k + 1]));
+      if ((eng->t_detailed && use_chain(eng)) || k == 0) CK(cudaEventElapsedTime(&m, ev[k], ev[k + 1]));
       eng->t_kernel_ms[(size_t)i * (kTimingEvents - 1) + k] = m;
     }
-    if (!eng->t_detailed) eng->t_kernel_ms[(size_t)i * (kTimingEvents - 1) + 1] = b - a;
+    if (!eng->t_detailed && use_chain(eng)) eng->t_kernel_ms[(size_t)i * (kTimingEvents - 1) + 1] = b - a;
   }
   *count = n;
   eng->t_pending = 0;

@@ -42,14 +42,22 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   return v;
 }
 
-// Grid barrier for co-resident CTAs.  bar[1] is the generation and
-// bar[kBarFlags + c] CTA c's arrival flag; `gen` is this CTA's copy of the
-// generation.  Every CTA publishes its arrival with a release store of the
-// next generation into its own flag (no contended atomic), the threads of
-// CTA 0 watch all flags, and CTA 0 then releases the grid with one store
-// of the generation word that every CTA watches.  Waits are bounded: on
-// timeout the error word is set and the CTA goes on (results are then
-// invalid, and the host reports PF_ETIMEOUT).
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// Grid barrier for co-resident CTAs.  bar[1] is the generation (the count
+// of barriers passed over all launches) and bar[kBarFlags + c] CTA c's
+// arrival flag; `gen` is this CTA's copy of the generation.  Every CTA
+// publishes its arrival with a release store of the next generation into
+// its own flag (no contended atomic), the threads of CTA 0 watch all flags,
+// and CTA 0 then releases the grid with one store of the generation word
+// that every CTA watches.  Polls are relaxed loads followed by one fence.
+// Waits are bounded: on timeout the error word is set and the CTA goes on
+// (results are then invalid, and the host reports PF_ETIMEOUT).
 __device__ __forceinline__ void grid_barrier(const EngineDev& e, unsigned* bar, unsigned& gen) {
   const unsigned target = gen + 1u;
   __syncthreads();
@@ -57,7 +65,7 @@ __device__ __forceinline__ void grid_barrier(const EngineDev& e, unsigned* bar, 
   if (blockIdx.x == 0) {
     for (int c = threadIdx.x; c < (int)gridDim.x; c += kThreads) {
       unsigned long long spins = 0;
-      while (ld_acquire(bar + kBarFlags + c) != target) {
+      while (ld_relaxed(bar + kBarFlags + c) != target) {
         if (++spins > e.spin_limit) {
           atomicOr(e.err, ERR_BARRIER_TIMEOUT);
           break;
@@ -65,6 +73,7 @@ __device__ __forceinline__ void grid_barrier(const EngineDev& e, unsigned* bar, 
         if (spins > 64) __nanosleep(32);
       }
     }
+    fence_acq_rel();
     __syncthreads();
     if (threadIdx.x == 0) st_release(bar + 1, target);
   }
@@ -72,13 +81,14 @@ __device__ __forceinline__ void grid_barrier(const EngineDev& e, unsigned* bar, 
     // test hook: wait for a generation nobody publishes (bounded spin)
     const unsigned want = e.lookback_poison ? target + 1u : target;
     unsigned long long spins = 0;
-    while (ld_acquire(bar + 1) != want) {
+    while (ld_relaxed(bar + 1) != want) {
       if (++spins > e.spin_limit) {
         atomicOr(e.err, ERR_BARRIER_TIMEOUT);
         break;
       }
       if (spins > 64) __nanosleep(32);
     }
+    fence_acq_rel();
   }
   gen = target;
   __syncthreads();
