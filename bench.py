@@ -329,13 +329,107 @@ def run_b200(args, world, rank, local, pg):
     if e2e:
         out["e2e"] = e2e
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        n_cpu = 200_000
-        v, cores, dt = cpu_baseline_cfg1(n_cpu, 3, 7)
+        # bounded sample of the same workload: one epoch to size it, then
+        # about 10 s of CPU work on the full particle count
+        _, _, dt1 = cpu_baseline_cfg1(n, 1, 7)
+        epochs = int(max(2, min(200, 10.0 / max(dt1, 1e-3))))
+        v, cores, dt = cpu_baseline_cfg1(n, epochs, 7)
         out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                               "sample": f"oracle FP64 C port (OpenMP), {n_cpu} particles x 32 satellites, "
-                                         f"3 epochs, {dt:.1f} s"}
+                               "sample": f"oracle FP64 C port (OpenMP), {n} particles x 32 satellites, "
+                                         f"{epochs} epochs, {dt:.1f} s"}
     eng.close()
     return out
+
+
+# ------------------------------------------------------ cfg2: batched
+def run_cfg2(args, world, rank, local, pg):
+    """256 independent filters (particle counts log-uniform 1K-100K,
+    6-40 satellites per filter and epoch, D = 4), all advanced by one
+    cooperative launch per epoch replayed from a CUDA graph, against the
+    same engine stepping the filters one launch each."""
+    import torch
+    from gnss_gpu_b200 import _native as N
+    from gnss_gpu_b200.engine import Engine, EngineOptions, FilterSpec
+    from gnss_gpu_b200 import scenario as S
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    W, K = args.warmup, args.steps
+    E = W + K + 2
+    n_part, trajs = S.batched(n_filters=256, n_epochs=E, seed=2 + rank)
+    flags = N.PF_EP_PREDICT | N.PF_EP_WEIGHT
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def make():
+        specs = [FilterSpec(n_particles=int(nf), seed=100 + k, sigma_pos=(1.0, 1.0, 0.5), sigma_clk=0.5,
+                            sigma_pr=3.0) for k, nf in enumerate(n_part)]
+        eng = Engine(specs, EngineOptions(n_clk=1, resampler="systematic", ess_threshold=0.5, max_sats=40,
+                                          obs_slots=E, covariance=True, recenter=True), device=local)
+        for k, tr in enumerate(trajs):
+            eng.initialize(k, tr.truth_ecef[0], tr.truth_clk[0], 10.0, 30.0)
+        for t in range(E):
+            recs = [{"disp": tr.disp_enu[t], "sats": tr.sats[t], "pr": tr.pr[t], "flags": flags} for tr in trajs]
+            fe, sv = eng.pack_epoch(recs)
+            eng.upload(t, fe, sv)
+        return eng
+
+    def timed(eng, fn, launches):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        with torch.cuda.stream(eng.stream):
+            for i in range(W):
+                flush.fill_(i & 0xFF)
+                fn()
+            for i in range(K):
+                flush.fill_(i & 0xFF)
+                ev[i][0].record(eng.stream)
+                fn()
+                ev[i][1].record(eng.stream)
+        eng.synchronize()
+        barrier(pg)
+        return reduce_max(pg, sum(a.elapsed_time(b) for a, b in ev) / 1e3)
+
+    total_n = int(np.sum(n_part))
+    clocks = ClockSampler(local)
+    clocks.start()
+    eng = make()
+    eng.capture(False)
+    t_graph = timed(eng, lambda: eng.replay(1), 1)
+    eng.close()
+    eng = make()
+    t_pf = timed(eng, eng.step_per_filter, len(n_part))
+    pf_launches = eng.last_launch_count()
+    eng.close()
+    eng = make()
+    eng.capture(True)
+    t_pfg = timed(eng, lambda: eng.replay(1), len(n_part))
+    eng.close()
+    clk = clocks.stop()
+    value = total_n * K * world / t_graph
+    v_pf = total_n * K * world / t_pf
+    peak, peak_kind = peaks()
+    D = 4
+    b_alg = 2 * D * 4 + 4 + 4 + 4  # state r+w, log-weight, ancestor read + write (resampling each epoch at most)
+    achieved = value / world * b_alg / 1e9
+    return {
+        "metric": "PF particle-steps/s (256 batched uneven filters, 1 launch per epoch from a CUDA graph)",
+        "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": t_graph / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 state / f64 anchor+scan-free int64 CDF", "data": "synthetic",
+        "config": {"workload": f"cfg2-batched: 256 filters, particles log-uniform 1K-100K (total {total_n}), "
+                               "6-40 satellites per filter and epoch, D=4, ESS<N/2 systematic resampling",
+                   "particles": total_n, "filters": 256, "parallelism": f"replicas x{world}",
+                   "l2": "flushed between steps (512 MiB device write outside the event intervals)"},
+        "gpu_launches": K,
+        "per_filter_launches": {"value": v_pf, "unit": UNIT, "ms_per_step": t_pf / K * 1e3,
+                                "launches_per_step": pf_launches},
+        "per_filter_launches_graph": {"value": total_n * K * world / t_pfg, "unit": UNIT,
+                                      "ms_per_step": t_pfg / K * 1e3},
+        "batched_over_per_filter": value / v_pf,
+        "roofline": {"bound": "hbm", "kernel": "k_epoch (cooperative, all filters)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",
+                     "algorithmic_bytes_per_launch": b_alg * total_n, "traffic": committed_traffic("k_epoch:cfg2-batched")},
+        "clocks": clk,
+    }
 
 
 # ------------------------------------------------------- reference arm
@@ -371,6 +465,8 @@ def main():
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
         out = run_reference(args, world, rank)
+    elif args.workload == "cfg2-batched":
+        out = run_cfg2(args, world, rank, local, pg)
     else:
         out = run_b200(args, world, rank, local, pg)
     if rank == 0 and out is not None:

@@ -12,7 +12,9 @@
 //   2  per-filter merge of the tile rows (filter f_first + j by CTA j mod G;
 //      one pass, the filter maximum having been collected in phase 1): ESS,
 //      weighted mean / covariance, device-side resample decision.
-//      At the same time, systematic only, on the CTAs that own no filter:
+//      At the same time, systematic only, on the CTAs that own no filter
+//      (when filters are fewer than a quarter of the CTAs; otherwise every
+//      CTA after its merges):
 //   3  quantised weights, one sum per 128-particle warp segment and
 //      (integer atomics) one per tile, for every filter that may resample.
 //   -- barrier (what follows only if some filter resamples)
@@ -636,7 +638,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
     __syncthreads();
   }
   if constexpr (RESAMPLER == PF_RESAMPLE_SYSTEMATIC) {
-    const int h0 = nf < (int)gridDim.x ? nf : 0;  // first CTA of phase 3
+    // With few filters their owners sit phase 3 out (it overlaps their
+    // merges); with many, every CTA takes a share after its merges.
+    const int h0 = 4 * nf <= (int)gridDim.x ? nf : 0;  // first CTA of phase 3
     if ((int)blockIdx.x >= h0) {
       int b3, e3;
       chunk_of(t0, count, (int)blockIdx.x - h0, (int)gridDim.x - h0, b3, e3);
