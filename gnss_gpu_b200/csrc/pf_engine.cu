@@ -40,7 +40,7 @@ struct pf_engine {
   cudaGraphExec_t gexec = nullptr;
   int resident[Q_COUNT];
   int epoch_resident = 0;     // co-resident CTAs of the cooperative epoch kernel
-  size_t epoch_smem = 0;      // its dynamic shared memory (merge-path windows)
+  size_t epoch_smem = 0;      // its dynamic shared memory
   unsigned* bar = nullptr;    // grid barrier words (count, generation, any-resample)
   int sm_count = 0;
   int last_launches = 0;
@@ -64,9 +64,10 @@ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
   size_t off_state0, off_state1, off_lw, off_anc, off_offs, off_mp, off_part, off_agg, off_inc,
-      off_flag, off_excl, off_wq, off_wsum, off_mpw, off_fmax, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
+      off_flag, off_excl, off_wq, off_wsum, off_chunks, off_fmax, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
       total;
   size_t obs_slot_bytes;
+  size_t max_chunks;
   long long P;
   int T, D, max_n;
 };
@@ -141,7 +142,10 @@ Layout make_layout(const pf_engine_config_t* cfg, const pf_filter_params_t* fp) 
   L.off_excl = take((size_t)T * 8);
   L.off_wq = take((size_t)P * 8);
   L.off_wsum = take((size_t)T * kSubTiles * 8);
-  L.off_mpw = take((size_t)T * kSubTiles * 4);
+  // a run longer than kLightRun slots needs ceil(len / kRunChunk) chunks:
+  // at most P / (kLightRun + 1) runs and P / kRunChunk + T extra chunks
+  L.max_chunks = (size_t)(P / kLightRun) + (size_t)T + 64;
+  L.off_chunks = take(L.max_chunks * sizeof(uint4));
   L.off_fmax = take((size_t)cfg->n_filters * 4);
   L.off_desc = take(sizeof(FilterDesc) * cfg->n_filters);
   L.off_ctrl = take(sizeof(FilterCtrl) * cfg->n_filters);
@@ -331,8 +335,7 @@ EpochKernel epoch_kernel(const pf_engine* eng) {
 
 int prepare_epoch_kernel(pf_engine* eng) {
   EpochKernel k = epoch_kernel(eng);
-  // merge-path windows of the systematic phases
-  eng->epoch_smem = (size_t)kSubTiles * kWindowWords * sizeof(uint32_t);
+  eng->epoch_smem = 0;  // no dynamic shared memory
   CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eng->epoch_smem));
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, eng->epoch_smem));
@@ -372,6 +375,7 @@ int sync_and_check(pf_engine* eng) {
   if (w & ERR_BARRIER_TIMEOUT) return set_err(PF_ETIMEOUT, "device grid-barrier spin limit reached (error word 0x%x)", w);
   if (w & ERR_SAT_CAP) return set_err(PF_ECAP, "n_sat above max_sats (error word 0x%x)", w);
   if (w & ERR_BAD_WEIGHTS) return set_err(PF_EINVAL, "all log-weights non-finite (error word 0x%x)", w);
+  if (w & ERR_INTERNAL_CAP) return set_err(PF_ECUDA, "internal capacity exceeded (error word 0x%x)", w);
   return PF_OK;
 }
 
@@ -469,7 +473,8 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
   e.tile_excl = (unsigned long long*)(w + L.off_excl);
   e.wq = (unsigned long long*)(w + L.off_wq);
   e.wsum = (unsigned long long*)(w + L.off_wsum);
-  e.mp_warp = (uint32_t*)(w + L.off_mpw);
+  e.chunks = (uint4*)(w + L.off_chunks);
+  e.max_chunks = (unsigned)L.max_chunks;
   e.fmax = (unsigned*)(w + L.off_fmax);
   eng->desc_dev = (FilterDesc*)(w + L.off_desc);
   eng->ctrl_dev = (FilterCtrl*)(w + L.off_ctrl);

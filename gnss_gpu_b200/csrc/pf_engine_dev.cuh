@@ -14,8 +14,9 @@ constexpr int kMergeDiag = 2 * kTile;  // merge-path diagonals per tile
 constexpr int kPartStride = 16;        // floats per tile partial
 constexpr int kWarpTile = 32 * kPerThread;      // particles per warp segment (epoch kernel)
 constexpr int kSubTiles = kTile / kWarpTile;    // warp segments per tile
-constexpr int kWarpDiag = 2 * kWarpTile;        // merge-path diagonals per warp block
-constexpr int kWindowWords = kWarpDiag + 4;     // offspring-end window per warp block
+constexpr int kLightRun = 32;                   // epoch kernel: longest offspring run written in phase 4
+constexpr int kRunChunk = 1024;                 // epoch kernel: slots per queued chunk of a longer run
+constexpr int kBarChunks = 3;                   // epoch kernel: queued-chunk counter in the barrier block
 constexpr int kBarFlags = 8;                    // epoch kernel: first arrival-flag word of the barrier block
 constexpr int kMaxEpochGrid = 2048;             // epoch kernel: most CTAs of one launch
 constexpr int kMaxD = 3 + PF_MAX_CLK;
@@ -27,7 +28,9 @@ enum QueueSlot : int {
 };
 
 // Error word bits.
-enum : unsigned { ERR_LOOKBACK_TIMEOUT = 1u, ERR_BAD_WEIGHTS = 2u, ERR_SAT_CAP = 4u, ERR_BARRIER_TIMEOUT = 8u };
+enum : unsigned {
+  ERR_LOOKBACK_TIMEOUT = 1u, ERR_BAD_WEIGHTS = 2u, ERR_SAT_CAP = 4u, ERR_BARRIER_TIMEOUT = 8u, ERR_INTERNAL_CAP = 16u
+};
 
 struct FilterDesc {
   int n;
@@ -86,7 +89,8 @@ struct EngineDev {
   unsigned long long* tile_excl;
   unsigned long long* wq;    // epoch kernel: quantised weight per particle
   unsigned long long* wsum;  // epoch kernel: quantised weight sum per warp segment
-  uint32_t* mp_warp;         // epoch kernel: merge-path start per warp block
+  uint4* chunks;             // epoch kernel: queued offspring-run chunks (first slot lo/hi, length, ancestor)
+  unsigned max_chunks;
   unsigned* fmax;            // epoch kernel: per filter, order-preserving code of the max log-weight
   unsigned* queue;
   unsigned* err;

@@ -21,9 +21,10 @@
 //   3' Megopolis: the chain per slot.   Systematic:
 //   4  exclusive prefix of every particle (filter prefix of the tile from
 //      the tile sums, segment prefix from the warp sums, warp scan),
-//      offspring ends F(i), merge-path start of every 256-diagonal block.
+//      offspring ends F(i); slots [F(i-1), F(i)) get ancestor i, written
+//      here when the run is short, queued in chunks of 1024 slots when long.
 //   -- barrier
-//   5  merge path, one warp per 256-diagonal block: ancestor of every slot.
+//   5  the queued chunks, taken by all warps of the grid in turn.
 //
 // Compared with one kernel per phase this removes the launch/drain gaps and
 // every per-tile queue atomic; the log-weights and quantised weights reread
@@ -155,8 +156,8 @@ __device__ __forceinline__ void quantize4(float4 v, int p0, int n, float M, int 
 
 // The systematic resampler's phases walk a chunk of tiles filter segment by
 // filter segment (the tiles of one filter inside the chunk).  Every warp
-// works on its own 128-particle segment (phases 3, 4) or 256-diagonal
-// merge-path block (phase 5) without CTA barriers; only the per-filter
+// works on its own 128-particle segment (phases 3, 4) or on queued chunks of
+// long offspring runs (phase 5) without CTA barriers; only the per-filter
 // prefix of phase 4 is a CTA reduction.  The loops are kept compact (not
 // unrolled over tiles): this code runs a few times per CTA and epoch, so
 // instruction fetch, not arithmetic, sets its speed.  Integer sums are
@@ -210,7 +211,7 @@ __device__ __forceinline__ void epoch_sys_quantise(const EngineDev& e, int cb, i
 
 // Phases 4 and 5 for the filters that resample.
 __device__ __forceinline__ void epoch_sys_assign(const EngineDev& e, unsigned* bar, unsigned& gen, int cb, int ce,
-                                                 unsigned long long* s_u64, uint32_t* s_win) {
+                                                 unsigned long long* s_u64) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // ---------------------------------------------------------------- phase 4
   for (int t = cb; t < ce;) {
@@ -264,30 +265,37 @@ __device__ __forceinline__ void epoch_sys_assign(const EngineDev& e, unsigned* b
                 C += q[k];
                 Fk[k] = (p0 + k < n) ? offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf) : (uint32_t)n;
               }
-              *reinterpret_cast<uint4*>(e.offs + base + p0) = make_uint4(Fk[0], Fk[1], Fk[2], Fk[3]);
             }
-            // merge-path block starts: block c begins in particle i when
-            // i - 1 + F(i-1) < c * kWarpDiag <= i + F(i).  A heavy particle
-            // starts many blocks, and heavy particles sit next to each other
-            // after a resample, so the warp writes each lane's run of block
-            // starts together.
+            // Slots [F(i-1), F(i)) take ancestor i.  Runs of up to kLightRun
+            // slots are written here by their lane; longer runs (heavy
+            // particles, which sit next to each other after a resample) are
+            // cut into chunks of kRunChunk slots and queued for phase 5,
+            // where every warp of the grid takes chunks.
 #pragma unroll 1
             for (int k = 0; k < 4; ++k) {
-              long long c_lo = 0, c_hi = 0;  // blocks [c_lo, c_hi) start in particle p0 + k
-              if (p0 + k < n) {
-                const long long i = p0 + k;
-                const long long hprev = i - 1 + (long long)(k == 0 ? Fprev : Fk[k - 1]);
-                const long long h = i + (long long)Fk[k];
-                c_lo = (hprev < 0) ? 0 : hprev / kWarpDiag + 1;
-                c_hi = h / kWarpDiag + 1;
-              }
-              unsigned runs = __ballot_sync(0xffffffffu, c_hi > c_lo);
-              while (runs) {
-                const int src = __ffs(runs) - 1;
-                runs &= runs - 1u;
-                const long long lo = __shfl_sync(0xffffffffu, c_lo, src), hi = __shfl_sync(0xffffffffu, c_hi, src);
-                const uint32_t iv = (uint32_t)(pw + src * 4 + k);
-                for (long long c = lo + lane; c < hi; c += 32) e.mp_warp[(size_t)tb * kSubTiles + c] = iv;
+              const uint32_t lo = (k == 0) ? Fprev : Fk[k - 1], hi = Fk[k];
+              const int i = p0 + k;
+              const bool run = i < n && hi > lo;
+              if (run && hi - lo <= (uint32_t)kLightRun)
+                for (uint32_t j = lo; j < hi; ++j) e.anc[base + j] = i;
+              // long runs: the lane reserves its chunks, the warp writes them
+              const bool heavy = run && hi - lo > (uint32_t)kLightRun;
+              const uint32_t nch = heavy ? (hi - lo + kRunChunk - 1) / kRunChunk : 0u;
+              const unsigned at = heavy ? atomicAdd(bar + kBarChunks, nch) : 0u;
+              if (heavy && at + nch > e.max_chunks) atomicOr(e.err, ERR_INTERNAL_CAP);  // cannot happen: bounded by the layout
+              unsigned todo = __ballot_sync(0xffffffffu, heavy);
+              while (todo) {
+                const int src = __ffs(todo) - 1;
+                todo &= todo - 1u;
+                const uint32_t slo = __shfl_sync(0xffffffffu, lo, src), shi = __shfl_sync(0xffffffffu, hi, src);
+                const uint32_t snch = __shfl_sync(0xffffffffu, nch, src);
+                const unsigned sat = __shfl_sync(0xffffffffu, at, src);
+                const uint32_t si = (uint32_t)(pw + src * 4 + k);
+                for (uint32_t c = lane; c < snch && sat + c < e.max_chunks; c += 32) {
+                  const long long st = base + slo + (long long)c * kRunChunk;
+                  e.chunks[sat + c] = make_uint4((uint32_t)st, (uint32_t)(st >> 32),
+                                                 min((uint32_t)kRunChunk, shi - slo - c * (uint32_t)kRunChunk), si);
+                }
               }
             }
           }
@@ -300,59 +308,15 @@ __device__ __forceinline__ void epoch_sys_assign(const EngineDev& e, unsigned* b
   grid_barrier(e, bar, gen);
 
   // ---------------------------------------------------------------- phase 5
-  // Warp block c of a filter covers merge diagonals [c*256, c*256 + 256):
-  // lane l walks 8 of them from diagonal c*256 + 8l, reading the offspring
-  // ends of particles [i0, i0 + 257) staged in the warp's window.
-  uint32_t* s_F = s_win + warp * kWindowWords;
-  for (int t = cb; t < ce;) {
-    const int f = __ldg(e.tile_filter + t);
-    const FilterDesc* fd = e.desc + f;
-    const FilterCtrl* fc = e.ctrl + f;
-    const int tb = fd->tile_begin, se = min(ce, tb + fd->n_tiles);
-    if (ld_cg_int(&fc->resample_flag)) {
-      const int n = fd->n;
-      const long long base = fd->p_off, n2 = 2ll * n;
+  // Heavy runs: chunk descriptors (first slot, length, ancestor), taken by
+  // the warps of the grid in turn, each written with coalesced stores.
+  const unsigned nchunks = min(ld_cg_u(bar + kBarChunks), e.max_chunks);
+  const int gw = (int)(blockIdx.x * (kThreads / 32)) + warp, nw = (int)(gridDim.x * (kThreads / 32));
 #pragma unroll 1
-      for (int g = t; g < se; ++g) {
-        const int c = (g - tb) * kSubTiles + warp;  // block index inside the filter
-        const long long d0 = (long long)c * kWarpDiag;
-        if (d0 >= n2) continue;  // warp-uniform
-        const int i0 = (int)__ldcg(e.mp_warp + (size_t)tb * kSubTiles + c);
-        if (i0 < 0 || i0 >= n) {  // cannot happen with valid weights; never index with it
-          if (lane == 0) atomicOr(e.err, ERR_BAD_WEIGHTS);
-          continue;
-        }
-        const int win = min(kWarpDiag + 1, n - i0);
-        __syncwarp();  // the window is free
-        for (int w = lane; w < win; w += 32) s_F[w] = __ldcg(e.offs + base + i0 + w);
-        __syncwarp();
-        const long long d = d0 + (long long)lane * (kWarpDiag / 32);
-        const long long dend = min(d0 + (long long)kWarpDiag, n2);
-        if (d < dend) {
-          int lo = 0, hi = (int)min((long long)(win - 1), d - d0);
-          while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if ((long long)(i0 + mid) + (long long)s_F[mid] >= d) hi = mid;
-            else lo = mid + 1;
-          }
-          int i = i0 + lo;
-          long long k = d - i;
-          const int steps = (int)min((long long)(kWarpDiag / 32), dend - d);
-#pragma unroll 1
-          for (int s = 0; s < steps; ++s) {
-            const int wi = i - i0;
-            if (wi >= win) break;
-            if (k < (long long)s_F[wi]) {
-              if (k >= 0 && k < n) e.anc[base + k] = i;
-              ++k;
-            } else {
-              ++i;
-            }
-          }
-        }
-      }
-    }
-    t = se;
+  for (unsigned c = gw; c < nchunks; c += nw) {
+    const uint4 d = __ldcg(e.chunks + c);
+    int* dst = e.anc + ((long long)d.y << 32 | d.x);
+    for (uint32_t j = lane; j < d.z; j += 32) dst[j] = (int)d.w;
   }
 }
 
@@ -361,7 +325,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
   constexpr int D = 3 + NCLK;
   constexpr int NV = 2 + D + 6;
   constexpr int kWarps = kThreads / 32;
-  extern __shared__ __align__(16) uint32_t s_win[];  // merge-path windows [kWarps][kWindowWords]
   __shared__ __align__(16) float2 s_sat[kSatStride * PF_MAX_SATS];
   __shared__ int s_grp[PF_MAX_CLK + 1];
   __shared__ unsigned char s_clk[PF_MAX_SATS];
@@ -375,7 +338,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
   // generation of the last barrier (every thread reads it before its CTA
   // first arrives, so no CTA can have moved it on yet)
   unsigned gen = ld_acquire(bar + 1);
-  if (threadIdx.x == 0 && blockIdx.x == 0) bar[2] = 0u;  // any-filter-resamples flag of this epoch
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    bar[2] = 0u;           // any-filter-resamples flag of this epoch
+    bar[kBarChunks] = 0u;  // queued offspring-run chunks of this epoch
+  }
   int cb, ce;
   cta_chunk(t0, count, cb, ce);
   for (int t = cb + (int)threadIdx.x; t < ce; t += kThreads) e.lb_agg[t] = 0ull;  // tile sums of phase 3
@@ -663,7 +629,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
       mego_tile(e, fd, ld_cg_u(&fc->epoch) - 1u, t);
     }
   } else {
-    epoch_sys_assign(e, bar, gen, cb, ce, s_u64, s_win);
+    epoch_sys_assign(e, bar, gen, cb, ce, s_u64);
   }
 }
 
