@@ -84,6 +84,7 @@ EXPORTED = [
     "pfe_get_ancestors", "pfe_get_resample_info", "pfe_error_word", "pfe_set_spin_limit",
     "pfe_last_launch_count", "pfe_get_anchor", "pfe_test_poison_lookback", "pfe_enable_timing",
     "pfe_read_timing", "pfe_result_bytes", "pfe_read_timing_kernels",
+    "pf_mlp_param_count", "pf_mlp_scratch_bytes", "pf_mlp_grad", "pf_mlp_adam_step", "pf_mlp_forward",
 ]
 
 _lib = None
@@ -148,11 +149,15 @@ def load():
     L.pfe_enable_timing.argtypes = [p, i, i]
     L.pfe_read_timing.argtypes = [p, C.POINTER(C.c_float), C.POINTER(C.c_float), i, C.POINTER(C.c_int)]
     L.pfe_read_timing_kernels.argtypes = [p, C.POINTER(C.c_float), i, C.POINTER(C.c_int)]
+    L.pf_mlp_grad.argtypes = [p, p, i, p, p, p, p, C.c_size_t, p]
+    L.pf_mlp_adam_step.argtypes = [p, p, i, p, p, p, i, f, p, p, C.c_size_t, p]
+    L.pf_mlp_forward.argtypes = [p, i, p, p, p]
     for name in EXPORTED:
         fn = getattr(L, name)
         if name not in ("pf_last_error",) and fn.restype is not C.c_char_p:
             if name != "pf_abi_version":
                 fn.restype = i
+    L.pf_mlp_scratch_bytes.restype = C.c_size_t
     _lib = L
     return L
 

@@ -14,8 +14,9 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIBDIR = PKG / "lib"
 LIB = LIBDIR / "libgnsspf_b200.so"
-SOURCES = ["pf_status.cu", "pf_engine.cu", "pf_compat.cu", "pf_noalloc.cu"]
-HEADERS = ["pf_common.cuh", "pf_engine_dev.cuh", "pf_engine_kernels.cuh", "pf_epoch_kernel.cuh", "pf_status.h"]
+SOURCES = ["pf_status.cu", "pf_engine.cu", "pf_compat.cu", "pf_noalloc.cu", "pf_mlp.cu"]
+HEADERS = ["pf_common.cuh", "pf_engine_dev.cuh", "pf_engine_kernels.cuh", "pf_epoch_kernel.cuh", "pf_mlp.cuh",
+           "pf_status.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
     "-O3", "-lineinfo", "-std=c++17",

@@ -324,6 +324,33 @@ int pfe_read_timing(pf_engine_t* eng, float* step_kernel_ms, float* whole_step_m
 int pfe_read_timing_kernels(pf_engine_t* eng, float* out_4_per_step,
                             int max_entries, int* count);
 
+/* ------------------------------------------------------------------------
+ * Learned NLOS likelihood: a per-satellite network 12 -> 64 -> 64 -> 2
+ * (ReLU; BF16 operands, FP32 accumulation on the tensor cores) giving the
+ * NLOS probability p = sigmoid(o0) and the NLOS bias mean mu = 20 m *
+ * softplus(o1).  No counterpart in the reference (its mixture likelihood,
+ * pf_device.cu:373-436, takes fixed mixture parameters).  Parameters are an
+ * FP32 array of pf_mlp_param_count() floats:
+ *   W1t[64][16] b1[64] W2t[64][64] b2[64] W3t[2][64] b3[2]  (Wt[out][in]).
+ * Inputs are n rows of 12 FP32 features; labels n rows of (nlos in {0,1},
+ * bias in m).  Every pointer is device memory; calls are asynchronous on
+ * `stream`.  Loss: mean over rows of BCE(p, nlos) + nlos ((mu - bias)/20)^2.
+ */
+int pf_mlp_param_count(void);
+size_t pf_mlp_scratch_bytes(void);
+/* Gradient of the mean loss (d_grad, param_count floats) and the loss. */
+int pf_mlp_grad(const float* d_x, const float* d_y, int n, const float* d_params,
+                float* d_grad, float* d_loss, void* d_scratch, size_t scratch_bytes,
+                void* stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8, step >= 1) on d_params with
+ * moments d_m, d_v over the batch. */
+int pf_mlp_adam_step(const float* d_x, const float* d_y, int n, float* d_params,
+                     float* d_m, float* d_v, int step, float lr, float* d_loss,
+                     void* d_scratch, size_t scratch_bytes, void* stream);
+/* (p_nlos, mu) per row into d_out (2 floats per row). */
+int pf_mlp_forward(const float* d_x, int n, const float* d_params, float* d_out,
+                   void* stream);
+
 #ifdef __cplusplus
 }
 #endif
