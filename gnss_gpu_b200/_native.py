@@ -20,7 +20,7 @@ PF_TILE = 1024
 PF_NOALLOC_MAX_PARTICLES = 1 << 22
 
 PF_RESAMPLE_SYSTEMATIC, PF_RESAMPLE_MEGOPOLIS = 0, 1
-PF_WEIGHT_GAUSSIAN, PF_WEIGHT_HUBER = 0, 1
+PF_WEIGHT_GAUSSIAN, PF_WEIGHT_HUBER, PF_WEIGHT_MIXTURE = 0, 1, 2
 PF_LW_OVERWRITE, PF_LW_ACCUMULATE = 0, 1
 PF_SYS_OFFSET_RANDOM, PF_SYS_OFFSET_REFERENCE = 0, 1
 PF_FLAG_COVARIANCE, PF_FLAG_RECENTER, PF_FLAG_KERNEL_CHAIN = 1, 2, 4
@@ -53,7 +53,7 @@ class FilterEpoch(C.Structure):
 class Sat(C.Structure):
     _fields_ = [
         ("x", C.c_double), ("y", C.c_double), ("z", C.c_double), ("pr", C.c_double),
-        ("w", C.c_double), ("clk", C.c_int), ("pad_", C.c_int),
+        ("w", C.c_double), ("clk", C.c_int), ("cn0", C.c_float), ("blocked", C.c_float), ("pad_", C.c_int),
     ]
 
 
@@ -69,9 +69,9 @@ class FilterResult(C.Structure):
 FILTER_EPOCH_DTYPE = np.dtype([("disp", "<f8", 3), ("n_sat", "<i4"), ("sat_offset", "<i4"),
                                ("flags", "<i4"), ("pad_", "<i4")])
 SAT_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("pr", "<f8"), ("w", "<f8"),
-                      ("clk", "<i4"), ("pad_", "<i4")])
+                      ("clk", "<i4"), ("cn0", "<f4"), ("blocked", "<f4"), ("pad_", "<i4")])
 assert FILTER_EPOCH_DTYPE.itemsize == C.sizeof(FilterEpoch) == 40
-assert SAT_DTYPE.itemsize == C.sizeof(Sat) == 48
+assert SAT_DTYPE.itemsize == C.sizeof(Sat) == 56
 
 EXPORTED = [
     "pf_last_error", "pf_abi_version",
@@ -85,6 +85,7 @@ EXPORTED = [
     "pfe_last_launch_count", "pfe_get_anchor", "pfe_test_poison_lookback", "pfe_enable_timing",
     "pfe_read_timing", "pfe_result_bytes", "pfe_read_timing_kernels",
     "pf_mlp_param_count", "pf_mlp_scratch_bytes", "pf_mlp_grad", "pf_mlp_adam_step", "pf_mlp_forward",
+    "pfe_set_mlp", "pfe_get_sat_debug",
 ]
 
 _lib = None
@@ -152,6 +153,8 @@ def load():
     L.pf_mlp_grad.argtypes = [p, p, i, p, p, p, p, C.c_size_t, p]
     L.pf_mlp_adam_step.argtypes = [p, p, i, p, p, p, i, f, p, p, C.c_size_t, p]
     L.pf_mlp_forward.argtypes = [p, i, p, p, p]
+    L.pfe_set_mlp.argtypes = [p, p]
+    L.pfe_get_sat_debug.argtypes = [p, i, p, i, C.POINTER(C.c_int)]
     for name in EXPORTED:
         fn = getattr(L, name)
         if name not in ("pf_last_error",) and fn.restype is not C.c_char_p:

@@ -40,6 +40,7 @@ struct pf_engine {
   cudaGraphExec_t gexec = nullptr;
   int resident[Q_COUNT];
   int epoch_resident = 0;     // co-resident CTAs of the cooperative epoch kernel
+  bool mlp_set = false;       // mixture mode: network parameters uploaded
   size_t epoch_smem = 0;      // its dynamic shared memory
   unsigned* bar = nullptr;    // grid barrier words (count, generation, any-resample)
   int sm_count = 0;
@@ -64,7 +65,7 @@ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
   size_t off_state0, off_state1, off_lw, off_anc, off_offs, off_mp, off_part, off_agg, off_inc,
-      off_flag, off_excl, off_wq, off_wsum, off_chunks, off_fmax, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
+      off_flag, off_excl, off_wq, off_wsum, off_chunks, off_fmax, off_mlp, off_satdbg, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
       total;
   size_t obs_slot_bytes;
   size_t max_chunks;
@@ -80,8 +81,11 @@ int validate_config(const pf_engine_config_t* cfg, const pf_filter_params_t* fp)
     return set_err(PF_EINVAL, "unknown resampler %d", cfg->resampler);
   if (cfg->resampler == PF_RESAMPLE_MEGOPOLIS && (cfg->megopolis_iters < 1 || cfg->megopolis_iters > 128))
     return set_err(PF_EINVAL, "megopolis_iters must be 1..128");
-  if (cfg->weight_mode != PF_WEIGHT_GAUSSIAN && cfg->weight_mode != PF_WEIGHT_HUBER)
+  if (cfg->weight_mode != PF_WEIGHT_GAUSSIAN && cfg->weight_mode != PF_WEIGHT_HUBER &&
+      cfg->weight_mode != PF_WEIGHT_MIXTURE)
     return set_err(PF_EINVAL, "unknown weight_mode %d", cfg->weight_mode);
+  if (cfg->weight_mode == PF_WEIGHT_MIXTURE && (cfg->flags & PF_FLAG_KERNEL_CHAIN))
+    return set_err(PF_EINVAL, "the mixture likelihood runs in the epoch kernel only (no PF_FLAG_KERNEL_CHAIN)");
   if (cfg->lw_mode != PF_LW_OVERWRITE && cfg->lw_mode != PF_LW_ACCUMULATE)
     return set_err(PF_EINVAL, "unknown lw_mode %d", cfg->lw_mode);
   if (cfg->sys_offset != PF_SYS_OFFSET_RANDOM && cfg->sys_offset != PF_SYS_OFFSET_REFERENCE)
@@ -91,7 +95,7 @@ int validate_config(const pf_engine_config_t* cfg, const pf_filter_params_t* fp)
   if (cfg->obs_slots < 1) return set_err(PF_EINVAL, "obs_slots must be >= 1");
   if (!(cfg->ess_threshold >= 0.0) || !isfinite(cfg->ess_threshold))
     return set_err(PF_EINVAL, "ess_threshold must be finite and >= 0");
-  if (cfg->weight_mode == PF_WEIGHT_HUBER && !(cfg->huber_k > 0.0))
+  if ((cfg->weight_mode == PF_WEIGHT_HUBER || cfg->weight_mode == PF_WEIGHT_MIXTURE) && !(cfg->huber_k > 0.0))
     return set_err(PF_EINVAL, "huber_k must be > 0");
   for (int f = 0; f < cfg->n_filters; ++f) {
     const pf_filter_params_t& p = fp[f];
@@ -147,6 +151,9 @@ Layout make_layout(const pf_engine_config_t* cfg, const pf_filter_params_t* fp) 
   L.max_chunks = (size_t)(P / kLightRun) + (size_t)T + 64;
   L.off_chunks = take(L.max_chunks * sizeof(uint4));
   L.off_fmax = take((size_t)cfg->n_filters * 4);
+  const bool mix = cfg->weight_mode == PF_WEIGHT_MIXTURE;
+  L.off_mlp = take(mix ? (size_t)kMlpParams * 4 : 0);
+  L.off_satdbg = take(mix ? (size_t)cfg->n_filters * cfg->max_sats * kSatDbg * 4 : 0);
   L.off_desc = take(sizeof(FilterDesc) * cfg->n_filters);
   L.off_ctrl = take(sizeof(FilterCtrl) * cfg->n_filters);
   L.off_tf = take((size_t)T * 4);
@@ -320,8 +327,9 @@ EpochKernel epoch_kernel_r(int resampler) {
 }
 template <int NCLK>
 EpochKernel epoch_kernel_w(int wmode, int resampler) {
-  return wmode == PF_WEIGHT_GAUSSIAN ? epoch_kernel_r<NCLK, PF_WEIGHT_GAUSSIAN>(resampler)
-                                     : epoch_kernel_r<NCLK, PF_WEIGHT_HUBER>(resampler);
+  if (wmode == PF_WEIGHT_GAUSSIAN) return epoch_kernel_r<NCLK, PF_WEIGHT_GAUSSIAN>(resampler);
+  if (wmode == PF_WEIGHT_HUBER) return epoch_kernel_r<NCLK, PF_WEIGHT_HUBER>(resampler);
+  return epoch_kernel_r<NCLK, PF_WEIGHT_MIXTURE>(resampler);
 }
 EpochKernel epoch_kernel(const pf_engine* eng) {
   const int w = eng->cfg.weight_mode, r = eng->cfg.resampler;
@@ -476,6 +484,8 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
   e.chunks = (uint4*)(w + L.off_chunks);
   e.max_chunks = (unsigned)L.max_chunks;
   e.fmax = (unsigned*)(w + L.off_fmax);
+  e.mlp = (const float*)(w + L.off_mlp);
+  e.sat_dbg = (float*)(w + L.off_satdbg);
   eng->desc_dev = (FilterDesc*)(w + L.off_desc);
   eng->ctrl_dev = (FilterCtrl*)(w + L.off_ctrl);
   e.desc = eng->desc_dev;
@@ -712,6 +722,8 @@ int pfe_step(pf_engine_t* eng) {
   if (!eng) return set_err(PF_EINVAL, "null engine");
   for (int f = 0; f < eng->cfg.n_filters; ++f)
     if (!eng->initialized[f]) return set_err(PF_ENOTINIT, "filter %d not initialized", f);
+  if (eng->cfg.weight_mode == PF_WEIGHT_MIXTURE && !eng->mlp_set)
+    return set_err(PF_ENOTINIT, "mixture likelihood: network parameters not set (pfe_set_mlp)");
   int n = 1;
   cudaEvent_t* ev = nullptr;
   if (eng->t_slots > 0) {
@@ -1043,6 +1055,38 @@ int pfe_error_word(pf_engine_t* eng, unsigned* word) {
   if (!eng || !word) return set_err(PF_EINVAL, "null argument");
   CK(cudaStreamSynchronize(eng->stream));
   CK(cudaMemcpy(word, eng->dev.err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  return PF_OK;
+}
+
+int pfe_set_mlp(pf_engine_t* eng, const float* params) {
+  clear_err();
+  if (!eng || !params) return set_err(PF_EINVAL, "null argument");
+  if (eng->cfg.weight_mode != PF_WEIGHT_MIXTURE) return set_err(PF_EINVAL, "engine is not in mixture mode");
+  for (int i = 0; i < kMlpParams; ++i)
+    if (!isfinite(params[i])) return set_err(PF_EINVAL, "network parameter %d is not finite", i);
+  CK(cudaMemcpyAsync((void*)eng->dev.mlp, params, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice, eng->stream));
+  CK(cudaStreamSynchronize(eng->stream));
+  eng->mlp_set = true;
+  return PF_OK;
+}
+
+int pfe_get_sat_debug(pf_engine_t* eng, int filter, float* out, int max_sats, int* n_sat) {
+  clear_err();
+  if (!eng || !out || !n_sat) return set_err(PF_EINVAL, "null argument");
+  if (eng->cfg.weight_mode != PF_WEIGHT_MIXTURE) return set_err(PF_EINVAL, "engine is not in mixture mode");
+  if (filter < 0 || filter >= eng->cfg.n_filters) return set_err(PF_EINVAL, "bad filter index");
+  CK(cudaStreamSynchronize(eng->stream));
+  FilterCtrl c;
+  CK(cudaMemcpy(&c, eng->ctrl_dev + filter, sizeof(c), cudaMemcpyDeviceToHost));
+  const unsigned ep = c.epoch == 0 ? 0 : c.epoch - 1;
+  const pf_filter_epoch_t* fe_dev = reinterpret_cast<const pf_filter_epoch_t*>(
+      eng->dev.obs + (size_t)(ep % (unsigned)eng->cfg.obs_slots) * eng->dev.obs_slot_bytes) + filter;
+  pf_filter_epoch_t fe;
+  CK(cudaMemcpy(&fe, fe_dev, sizeof(fe), cudaMemcpyDeviceToHost));
+  const int ns = std::max(0, std::min(std::min(fe.n_sat, eng->cfg.max_sats), max_sats));
+  CK(cudaMemcpy(out, eng->dev.sat_dbg + (size_t)filter * eng->cfg.max_sats * kSatDbg, sizeof(float) * ns * kSatDbg,
+                cudaMemcpyDeviceToHost));
+  *n_sat = ns;
   return PF_OK;
 }
 

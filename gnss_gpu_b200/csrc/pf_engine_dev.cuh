@@ -92,6 +92,8 @@ struct EngineDev {
   uint4* chunks;             // epoch kernel: queued offspring-run chunks (first slot lo/hi, length, ancestor)
   unsigned max_chunks;
   unsigned* fmax;            // epoch kernel: per filter, order-preserving code of the max log-weight
+  const float* mlp;          // mixture mode: network parameters (FP32)
+  float* sat_dbg;            // mixture mode: per filter and satellite, features and outputs
   unsigned* queue;
   unsigned* err;
   const unsigned char* obs;

@@ -33,6 +33,7 @@
 // blocks.
 #pragma once
 #include "pf_engine_kernels.cuh"
+#include "pf_learned.cuh"
 
 namespace pfb {
 
@@ -325,7 +326,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
   constexpr int D = 3 + NCLK;
   constexpr int NV = 2 + D + 6;
   constexpr int kWarps = kThreads / 32;
-  __shared__ __align__(16) float2 s_sat[kSatStride * PF_MAX_SATS];
+  constexpr int kStride = WMODE == PF_WEIGHT_MIXTURE ? kMixStride : kSatStride;
+  __shared__ __align__(16) float2 s_sat[kStride * PF_MAX_SATS];
   __shared__ int s_grp[PF_MAX_CLK + 1];
   __shared__ unsigned char s_clk[PF_MAX_SATS];
   __shared__ float s_wrow[2][kWarps][17];
@@ -369,7 +371,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
     const bool do_predict = (eflags & PF_EP_PREDICT) != 0;
     const bool do_weight = (eflags & PF_EP_WEIGHT) != 0;
 
-    if (f != cached) {  // satellite geometry of this filter (FP64 -> FP32 pairs)
+    if constexpr (WMODE == PF_WEIGHT_MIXTURE) {
+      if (f != cached) {
+        __shared__ MixSmem s_mix;
+        build_mixture_table<NCLK>(e, fd, fc, fe, sats, n_sat, do_weight, t == fd->tile_begin, f, s_sat, s_grp, s_clk,
+                                  s_mix);
+        cached = f;
+      }
+    }
+    if (WMODE != PF_WEIGHT_MIXTURE && f != cached) {  // satellite geometry of this filter (FP64 -> FP32 pairs)
       __syncthreads();   // nobody still reads the previous filter's table
       int my_c = 0;
       const pf_sat_t* sp = sats + fe->sat_offset + threadIdx.x;
@@ -490,8 +500,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int 
 #pragma unroll 2
           for (int s = s_grp[c]; s < s_end; ++s) {
 #pragma unroll
-            for (int p = 0; p < 2; ++p)
-              sat_pair_update<WMODE>(s_sat + kSatStride * s, dx[p], dy[p], dz[p], nbb[p], ncb[p], lwp[p], fd);
+            for (int p = 0; p < 2; ++p) {
+              if constexpr (WMODE == PF_WEIGHT_MIXTURE)
+                sat_pair_mixture(s_sat + kMixStride * s, dx[p], dy[p], dz[p], nbb[p], ncb[p], lwp[p], fd);
+              else
+                sat_pair_update<WMODE>(s_sat + kSatStride * s, dx[p], dy[p], dz[p], nbb[p], ncb[p], lwp[p], fd);
+            }
           }
         }
         lwv[0] = lwp[0].x; lwv[1] = lwp[0].y; lwv[2] = lwp[1].x; lwv[3] = lwp[1].y;

@@ -28,7 +28,7 @@ class EngineOptions:
     n_clk: int = 1
     resampler: str = "systematic"          # "systematic" | "megopolis"
     megopolis_iters: int = 15
-    weight_mode: str = "gaussian"          # "gaussian" | "huber"
+    weight_mode: str = "gaussian"          # "gaussian" | "huber" | "mixture" (learned, set_mlp)
     huber_k: float = 1.5
     lw_mode: str = "overwrite"             # "overwrite" (reference) | "accumulate"
     sys_offset: str = "random"             # "random" | "reference"
@@ -63,7 +63,8 @@ class Engine:
         cfg.n_clk = int(o.n_clk)
         cfg.resampler = {"systematic": N.PF_RESAMPLE_SYSTEMATIC, "megopolis": N.PF_RESAMPLE_MEGOPOLIS}[o.resampler]
         cfg.megopolis_iters = int(o.megopolis_iters)
-        cfg.weight_mode = {"gaussian": N.PF_WEIGHT_GAUSSIAN, "huber": N.PF_WEIGHT_HUBER}[o.weight_mode]
+        cfg.weight_mode = {"gaussian": N.PF_WEIGHT_GAUSSIAN, "huber": N.PF_WEIGHT_HUBER,
+                           "mixture": N.PF_WEIGHT_MIXTURE}[o.weight_mode]
         cfg.lw_mode = {"overwrite": N.PF_LW_OVERWRITE, "accumulate": N.PF_LW_ACCUMULATE}[o.lw_mode]
         cfg.sys_offset = {"random": N.PF_SYS_OFFSET_RANDOM, "reference": N.PF_SYS_OFFSET_REFERENCE}[o.sys_offset]
         cfg.max_sats = int(o.max_sats)
@@ -154,6 +155,10 @@ class Engine:
                 rec["w"] = 1.0 if w is None else np.asarray(w, dtype=np.float64).ravel()
                 clk = r.get("clk")
                 rec["clk"] = 0 if clk is None else np.asarray(clk, dtype=np.int32).ravel()
+                cn0 = r.get("cn0")
+                rec["cn0"] = 45.0 if cn0 is None else np.asarray(cn0, dtype=np.float32).ravel()
+                blk = r.get("blocked")
+                rec["blocked"] = 0.0 if blk is None else np.asarray(blk, dtype=np.float32).ravel()
                 chunks.append(rec)
             off += s
         sats_all = np.concatenate(chunks) if chunks else np.zeros(0, N.SAT_DTYPE)
@@ -166,6 +171,21 @@ class Engine:
                                         len(sats)))
 
     # ------------------------------------------------------------------ steps
+    def set_mlp(self, params):
+        """Upload the NLOS network's parameters (mixture mode)."""
+        prm = np.ascontiguousarray(params, dtype=np.float32)
+        if prm.size != self.lib.pf_mlp_param_count():
+            raise ValueError(f"expected {self.lib.pf_mlp_param_count()} parameters, got {prm.size}")
+        N.check(self.lib.pfe_set_mlp(self.h, N.vptr(prm)))
+
+    def sat_debug(self, k: int):
+        """(n_sat, 16) per satellite of filter k's last weighted epoch: the 12
+        features, p_nlos, mu, mode, residual against the prior mean."""
+        out = np.zeros((self.cfg.max_sats, 16), np.float32)
+        n = C.c_int(0)
+        N.check(self.lib.pfe_get_sat_debug(self.h, int(k), N.vptr(out), self.cfg.max_sats, C.byref(n)))
+        return out[: n.value]
+
     def step(self):
         N.check(self.lib.pfe_step(self.h))
 

@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define PF_ABI_VERSION 1
+#define PF_ABI_VERSION 2
 
 typedef enum {
   PF_OK = 0,
@@ -142,7 +142,12 @@ int pf_get_particles(const double* px, const double* py, const double* pz,
 #define PF_TILE 1024        /* particles per work tile                          */
 
 typedef enum { PF_RESAMPLE_SYSTEMATIC = 0, PF_RESAMPLE_MEGOPOLIS = 1 } pf_resampler_t;
-typedef enum { PF_WEIGHT_GAUSSIAN = 0, PF_WEIGHT_HUBER = 1 } pf_weight_mode_t;
+typedef enum {
+  PF_WEIGHT_GAUSSIAN = 0,
+  PF_WEIGHT_HUBER = 1,
+  PF_WEIGHT_MIXTURE = 2  /* learned LOS/NLOS mixture (pfe_set_mlp), Huber fallback;
+                            epoch-kernel path only */
+} pf_weight_mode_t;
 typedef enum { PF_LW_OVERWRITE = 0, PF_LW_ACCUMULATE = 1 } pf_lw_mode_t;
 typedef enum {
   PF_SYS_OFFSET_RANDOM = 0,    /* Philox draw per filter and epoch            */
@@ -197,6 +202,8 @@ typedef struct {
   double pr;             /* pseudorange, m                                    */
   double w;              /* per-satellite weight (1/sigma^2 scale), >= 0      */
   int clk;               /* clock state index, 0..n_clk-1                     */
+  float cn0;             /* C/N0, dB-Hz (PF_WEIGHT_MIXTURE features)          */
+  float blocked;         /* 1 if a ray trace at the prior mean says NLOS, else 0 */
   int pad_;
 } pf_sat_t;
 
@@ -323,6 +330,16 @@ int pfe_read_timing(pf_engine_t* eng, float* step_kernel_ms, float* whole_step_m
  * second entry holds all resampling kernels together and the rest are 0. */
 int pfe_read_timing_kernels(pf_engine_t* eng, float* out_4_per_step,
                             int max_entries, int* count);
+
+/* Network parameters of PF_WEIGHT_MIXTURE (host array of
+ * pf_mlp_param_count() floats, copied to the engine).  Required before the
+ * first step of a mixture engine. */
+int pfe_set_mlp(pf_engine_t* eng, const float* params);
+/* Per satellite of filter f's last weighted epoch (in upload order), 16
+ * floats: the 12 network features, p_nlos, mu, likelihood mode (0 mixture,
+ * 1 Huber fallback, 2 unused) and the residual against the prior mean.
+ * *n_sat receives the satellite count.  Mixture engines only. */
+int pfe_get_sat_debug(pf_engine_t* eng, int filter, float* out, int max_sats, int* n_sat);
 
 /* ------------------------------------------------------------------------
  * Learned NLOS likelihood: a per-satellite network 12 -> 64 -> 64 -> 2

@@ -51,10 +51,10 @@ def test_python_binding_covers_every_declared_function():
 
 def test_record_layouts(lib):
     from gnss_gpu_b200 import _native as N
-    assert C.sizeof(N.FilterEpoch) == 40 and C.sizeof(N.Sat) == 48
+    assert C.sizeof(N.FilterEpoch) == 40 and C.sizeof(N.Sat) == 56
     assert C.sizeof(N.EngineConfig) == 56
     assert C.sizeof(N.FilterParams) == 56
-    assert lib.pf_abi_version() == 1
+    assert lib.pf_abi_version() == 2
     assert lib.pf_last_error() == b""
 
 
