@@ -167,6 +167,37 @@ def weight(x, anchor, clk_anchor, rot, sats, clk, sigma_pr, mode=0, huber_k=1.5,
     return out
 
 
+def weight_mixture(x, anchor, clk_anchor, rot, sats, sigma_pr, p_nlos, mu, mode, huber_k=1.5):
+    """FP64 log-weights of the learned two-component likelihood (the epoch
+    kernel's PF_WEIGHT_MIXTURE, one clock state): per satellite with mode 0
+    log((1-p) N(r; 0, s2) + p N(r; mu, s2 + mu^2)) without the common
+    -log(2 pi)/2, with s2 = sigma_pr^2 / w; mode 1 the Huber term; mode 2
+    nothing.  x: (D, n) offsets about `anchor` in the E/N/U frame `rot`;
+    sats: (S, 5) rows x, y, z, pr, w."""
+    x = _f64(x)
+    sats = _f64(sats).reshape(-1, 5)
+    pos = _f64(anchor)[None, :] + x[:3].T @ _f64(rot)          # (n, 3) ECEF
+    cb = clk_anchor[0] + x[3]
+    lw = np.zeros(x.shape[1])
+    for s in range(len(sats)):
+        rng = np.linalg.norm(sats[s, :3][None, :] - pos, axis=1)
+        r = sats[s, 3] - rng - cb
+        w = sats[s, 4]
+        if mode[s] > 1.5 or w <= 0:
+            continue
+        if mode[s] > 0.5:
+            z = np.abs(r) / sigma_pr
+            rho = np.where(z < huber_k, 0.5 * z * z, huber_k * z - 0.5 * huber_k * huber_k)
+            lw -= w * rho
+            continue
+        s2 = sigma_pr * sigma_pr / w
+        sn2 = s2 + mu[s] ** 2
+        a = np.log1p(-p_nlos[s]) - 0.5 * np.log(s2) - r * r / (2 * s2)
+        b = np.log(p_nlos[s]) - 0.5 * np.log(sn2) - (r - mu[s]) ** 2 / (2 * sn2)
+        lw += np.logaddexp(a, b)
+    return lw
+
+
 def stats(x, lw, anchor, clk_anchor, rot):
     x = _f64(x)
     D, n = x.shape
