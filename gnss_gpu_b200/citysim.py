@@ -139,60 +139,88 @@ class CityTrajectory:
     rot: np.ndarray             # (3, 3) ECEF -> ENU
 
 
-def drive(city: City, n_epochs: int, seed: int, n_sat: int = 24, speed=(5.0, 15.0), dt: float = 1.0,
-          sigma_pr: float = 3.0, nlos_mean: float = 20.0, clk0: float = 3000.0, clk_drift: float = 0.5,
-          lla=S.ANCHOR_LLA) -> CityTrajectory:
-    """A receiver drives along the street grid (turning at random at
-    intersections) with GPS-like satellites: azimuth U[0, 2 pi), elevation
-    U[15, 85] deg, azimuth drift 0.008 deg/s."""
+def drive_many(city: City, n_traj: int, n_epochs: int, seed: int, n_sat: int = 24, speed=(5.0, 15.0),
+               dt: float = 1.0, sigma_pr: float = 3.0, nlos_mean: float = 20.0, clk0: float = 3000.0,
+               clk_drift: float = 0.5, lla=S.ANCHOR_LLA, sat_range=None) -> list:
+    """n_traj receivers drive along the street grid of one city (turning at
+    random at intersections), each with its own GPS-like constellation:
+    azimuth U[0, 2 pi), elevation U[15, 85] deg, azimuth drift 0.008 deg/s.
+    sat_range = (lo, hi) draws the number of satellites of every epoch
+    uniformly from lo..hi out of a pool of n_sat (all n_sat otherwise).
+    The ray tracing of every epoch is one call for all receivers."""
     rng = np.random.default_rng(seed)
     base = S.lla_to_ecef(*lla)
     rot = S.enu_rotation_lla(lla[0], lla[1])
     c = city.cell
-    # start on a street intersection away from the border
-    gx, gy = rng.integers(2, city.n - 2, 2)
-    pos = np.array([gx * c, gy * c, RX_HEIGHT])
-    heading = rng.integers(0, 4)  # 0 E, 1 N, 2 W, 3 S
+    R = n_traj
+    g = rng.integers(2, city.n - 2, (R, 2))
+    pos = np.column_stack([g[:, 0] * c, g[:, 1] * c, np.full(R, RX_HEIGHT)])
+    heading = rng.integers(0, 4, R)  # 0 E, 1 N, 2 W, 3 S
     dirs = np.array([[1.0, 0.0], [0.0, 1.0], [-1.0, 0.0], [0.0, -1.0]])
-    v = rng.uniform(*speed)
-    az0 = rng.uniform(0.0, 2.0 * np.pi, n_sat)
-    el_s = np.radians(rng.uniform(15.0, 85.0, n_sat))
+    v = rng.uniform(speed[0], speed[1], R)
+    az0 = rng.uniform(0.0, 2.0 * np.pi, (R, n_sat))
+    el_s = np.radians(rng.uniform(15.0, 85.0, (R, n_sat)))
     drift = np.radians(0.008) * dt
-    truth_enu, disp, sats, azs, els, prs, cn0s, nlos, biases, clks = [], [], [], [], [], [], [], [], [], []
+    rec = [dict(truth=[], disp=[], sats=[], az=[], el=[], pr=[], cn0=[], nlos=[], bias=[], clk=[]) for _ in range(R)]
     for t in range(n_epochs):
-        step = v * dt
         new = pos.copy()
-        new[:2] += dirs[heading] * step
-        # turn at an intersection crossed in this step; stay inside the city
-        cross = (np.floor(pos[:2] / c) != np.floor(new[:2] / c)).any()
-        if cross or not (c <= new[0] <= city.size - c and c <= new[1] <= city.size - c):
-            snapped = np.round(new[:2] / c) * c
-            new[:2] = np.clip(snapped, c, city.size - c)
-            choices = [h for h in range(4) if h != (heading + 2) % 4]
-            heading = int(rng.choice(choices))
+        new[:, :2] += dirs[heading] * (v * dt)[:, None]
+        cross = (np.floor(pos[:, :2] / c) != np.floor(new[:, :2] / c)).any(axis=1)
+        out = ~((new[:, 0] >= c) & (new[:, 0] <= city.size - c) & (new[:, 1] >= c) & (new[:, 1] <= city.size - c))
+        turn = cross | out
+        if turn.any():
+            snapped = np.clip(np.round(new[turn, :2] / c) * c, c, city.size - c)
+            new[turn, :2] = snapped
+            # a new heading other than straight back
+            step = rng.integers(1, 4, int(turn.sum()))
+            back = (heading[turn] + 2) % 4
+            heading[turn] = (back + step) % 4
         d = new - pos
         pos = new
-        az = az0 + drift * (t + 1)
-        p_ecef = base + pos @ rot
-        sp = S.sat_positions(p_ecef, rot, az, el_s)
-        blk = los_blocked(city, np.repeat(pos[None], n_sat, 0), az, el_s)
-        b = np.where(blk, rng.exponential(nlos_mean, n_sat), 0.0)
+        # satellites of this epoch
+        sel = []
+        for r in range(R):
+            if sat_range is None:
+                sel.append(np.arange(n_sat))
+            else:
+                k = int(rng.integers(sat_range[0], sat_range[1] + 1))
+                sel.append(np.sort(rng.choice(n_sat, min(k, n_sat), replace=False)))
+        az = [np.mod(az0[r, sel[r]] + drift * (t + 1), 2 * np.pi) for r in range(R)]
+        el = [el_s[r, sel[r]] for r in range(R)]
+        m = np.array([len(a) for a in az])
+        blk_all = los_blocked(city, np.repeat(pos, m, axis=0), np.concatenate(az), np.concatenate(el))
+        o = 0
         clk = clk0 + clk_drift * (t + 1)
-        pr = np.linalg.norm(sp - p_ecef, axis=1) + clk + rng.normal(0.0, sigma_pr, n_sat) + b
-        cn0 = np.where(blk, rng.normal(35.0, 5.0, n_sat), rng.normal(45.0, 4.0, n_sat))
-        truth_enu.append(pos.copy())
-        disp.append(d)
-        sats.append(sp)
-        azs.append(np.mod(az, 2 * np.pi))
-        els.append(el_s.copy())
-        prs.append(pr)
-        cn0s.append(cn0)
-        nlos.append(blk)
-        biases.append(b)
-        clks.append([clk])
-    te = np.array(truth_enu)
-    return CityTrajectory(city, te, base + te @ rot, np.array(clks), np.array(disp), sats, azs, els, prs, cn0s,
-                          nlos, biases, base, rot)
+        for r in range(R):
+            blk = blk_all[o:o + m[r]]
+            o += m[r]
+            p_ecef = base + pos[r] @ rot
+            sp = S.sat_positions(p_ecef, rot, az[r], el[r])
+            b = np.where(blk, rng.exponential(nlos_mean, m[r]), 0.0)
+            pr = np.linalg.norm(sp - p_ecef, axis=1) + clk + rng.normal(0.0, sigma_pr, m[r]) + b
+            cn0 = np.where(blk, rng.normal(35.0, 5.0, m[r]), rng.normal(45.0, 4.0, m[r]))
+            q = rec[r]
+            q["truth"].append(pos[r].copy())
+            q["disp"].append(d[r])
+            q["sats"].append(sp)
+            q["az"].append(az[r])
+            q["el"].append(np.array(el[r], copy=True))
+            q["pr"].append(pr)
+            q["cn0"].append(cn0)
+            q["nlos"].append(blk)
+            q["bias"].append(b)
+            q["clk"].append([clk])
+    out = []
+    for q in rec:
+        te = np.array(q["truth"])
+        out.append(CityTrajectory(city, te, base + te @ rot, np.array(q["clk"]), np.array(q["disp"]), q["sats"],
+                                  q["az"], q["el"], q["pr"], q["cn0"], q["nlos"], q["bias"], base, rot))
+    return out
+
+
+def drive(city: City, n_epochs: int, seed: int, **kw) -> CityTrajectory:
+    """One receiver (drive_many with n_traj = 1)."""
+    return drive_many(city, 1, n_epochs, seed, **kw)[0]
 
 
 def sat_az_el(rot: np.ndarray, p_ecef: np.ndarray, sats: np.ndarray):

@@ -96,17 +96,50 @@ class RunResult:
     steps_per_s: float         # particle-steps/s of the device steps (event-timed)
 
 
-def run_filters(trajs, n_particles: int, mode: str, params=None, seed: int = 0, keep_priors: bool = False,
-                init_spread=(5.0, 10.0)) -> RunResult:
+def prior_geometry_many(trajs, t: int, priors):
+    """prior_geometry for many filters at once (one ray-trace call per
+    city)."""
+    out = [None] * len(trajs)
+    by_city = {}
+    for k, tr in enumerate(trajs):
+        by_city.setdefault(id(tr.city), []).append(k)
+    for ks in by_city.values():
+        city = trajs[ks[0]].city
+        pts, azs, els, spans, geo = [], [], [], [], []
+        for k in ks:
+            tr = trajs[k]
+            pe, pc = priors[k]
+            v = tr.sats[t] - pe
+            rng = np.linalg.norm(v, axis=1)
+            e = (v / rng[:, None]) @ tr.rot.T
+            res = tr.pr[t] - rng - pc
+            p_enu = (pe - tr.anchor) @ tr.rot.T
+            pts.append(np.repeat(np.array([[p_enu[0], p_enu[1], CS.RX_HEIGHT]]), len(rng), 0))
+            azs.append(np.mod(np.arctan2(e[:, 0], e[:, 1]), 2 * np.pi))
+            els.append(np.arcsin(np.clip(e[:, 2], -1.0, 1.0)))
+            geo.append((e, res))
+            spans.append(len(rng))
+        blk = CS.los_blocked(city, np.concatenate(pts), np.concatenate(azs), np.concatenate(els)).astype(np.float32)
+        o = 0
+        for k, (e, res), m in zip(ks, geo, spans):
+            out[k] = (e, res, blk[o:o + m])
+            o += m
+    return out
+
+
+def run_filters(trajs, n_particles, mode: str, params=None, seed: int = 0, keep_priors: bool = False,
+                init_spread=(5.0, 10.0), max_sats=None) -> RunResult:
     """Run one filter per trajectory through all epochs on the GPU engine
     (batched, one launch per epoch); the prior of epoch t is the estimate of
-    epoch t-1 moved by the known displacement."""
-    import torch
+    epoch t-1 moved by the known displacement.  n_particles: one count or
+    one per trajectory."""
     F, E = len(trajs), len(trajs[0].pr)
-    specs = [FilterSpec(n_particles=n_particles, seed=seed * 1000 + k, sigma_pos=(1.0, 1.0, 0.5), sigma_clk=1.0,
+    counts = [int(n_particles)] * F if np.isscalar(n_particles) else [int(n) for n in n_particles]
+    specs = [FilterSpec(n_particles=counts[k], seed=seed * 1000 + k, sigma_pos=(1.0, 1.0, 0.5), sigma_clk=1.0,
                         sigma_pr=SIGMA_PR) for k in range(F)]
+    ms = max_sats or max(len(s) for tr in trajs for s in tr.sats)
     opts = EngineOptions(n_clk=1, resampler="systematic", weight_mode=mode, huber_k=HUBER_K,
-                         max_sats=max(len(s) for s in trajs[0].sats), obs_slots=1)
+                         max_sats=ms, obs_slots=1)
     eng = Engine(specs, opts)
     if mode == "mixture":
         eng.set_mlp(params)
@@ -120,13 +153,12 @@ def run_filters(trajs, n_particles: int, mode: str, params=None, seed: int = 0, 
     priors = [[] for _ in range(F)]
     eng.enable_timing(E + 1)
     for t in range(E):
+        geo = prior_geometry_many(trajs, t, prior)
         recs = []
         for k, tr in enumerate(trajs):
-            pe, pc = prior[k]
-            _, _, blk = prior_geometry(tr, t, pe, pc)
-            recs.append(epoch_record(tr, t, blk))
+            recs.append(epoch_record(tr, t, geo[k][2]))
             if keep_priors:
-                priors[k].append((pe.copy(), pc))
+                priors[k].append((prior[k][0].copy(), prior[k][1]))
         fe, sv = eng.pack_epoch(recs)
         eng.upload(0, fe, sv)
         eng.step()
@@ -139,7 +171,7 @@ def run_filters(trajs, n_particles: int, mode: str, params=None, seed: int = 0, 
             prior[k] = (est + tr.disp_enu[nxt] @ tr.rot, float(res[k]["est_clk"][0]))
     _, whole = eng.read_timing()
     eng.close()
-    sps = F * n_particles * len(whole) / max(float(np.sum(whole)) / 1e3, 1e-12)
+    sps = float(np.sum(counts)) * len(whole) / max(float(np.sum(whole)) / 1e3, 1e-12)
     return RunResult(err, priors, sps)
 
 
@@ -156,11 +188,14 @@ def training_set(trajs, priors):
     return np.concatenate(Xs), np.concatenate(Ys)
 
 
-def make_trajectories(n: int, n_epochs: int, seed: int, cities: int = 8, n_sat: int = 24):
+def make_trajectories(n: int, n_epochs: int, seed: int, cities: int = 8, n_sat: int = 24, sat_range=None):
+    """n drives spread over `cities` box cities (seeded)."""
     out = []
-    for k in range(n):
-        city = CS.make_city(seed * 1000 + k % cities)
-        out.append(CS.drive(city, n_epochs, seed=seed * 100_003 + k, n_sat=n_sat))
+    for c in range(cities):
+        m = len(range(c, n, cities))
+        if m:
+            out.extend(CS.drive_many(CS.make_city(seed * 1000 + c), m, n_epochs, seed=seed * 100_003 + c,
+                                     n_sat=n_sat, sat_range=sat_range))
     return out
 
 
