@@ -1000,40 +1000,53 @@ __device__ __forceinline__ void mego_tile(const EngineDev& e, const FilterDesc* 
   const uint32_t fid = (uint32_t)fd->filter_id;
   const int B = e.mego_iters;
   const float* lw = e.lw + base;
-#pragma unroll 1
-  for (int r = 0; r < 4; ++r) {
-    const int seg0 = j * kTile + r * kThreads + ((int)threadIdx.x & ~31);  // warp's first slot
-    if (seg0 >= n) continue;  // whole warp past the filter's end
-    const int k_real = seg0 + lane;
-    const bool valid = k_real < n;
-    const int k = valid ? k_real : seg0;  // lanes past the end shadow a valid slot
-    const uint32_t g = (uint32_t)(seg0 / 32);
-    // lane l draws the offsets of iterations 4l .. 4l+3 of this segment
-    const U4 ol = philox10(U4{g, epoch, TAG_MEGO_OFF | (uint32_t)lane, fid}, fd->key0, fd->key1);
-    int a = k;
-    float la = __ldcg(lw + k);
-#pragma unroll 1
-    for (int b0 = 0; b0 < B; b0 += 4) {
-      const U4 ur = philox10(U4{(uint32_t)k, epoch, TAG_MEGO_U | (uint32_t)(b0 >> 2), fid}, fd->key0, fd->key1);
-      const uint32_t uw[4] = {ur.x, ur.y, ur.z, ur.w};
+  // The warp's four 32-slot segments of the tile run their chains side by
+  // side (four independent dependency chains per lane).
+  int k[4], a[4];
+  float la[4];
+  bool valid[4];
+  U4 ol[4];
 #pragma unroll
-      for (int bb = 0; bb < 4; ++bb) {
-        if (b0 + bb >= B) break;
-        const int src_lane = (b0 + bb) >> 2;
-        const uint32_t ow = (bb == 0) ? ol.x : (bb == 1) ? ol.y : (bb == 2) ? ol.z : ol.w;
+  for (int r = 0; r < 4; ++r) {
+    const int seg0 = j * kTile + r * kThreads + ((int)threadIdx.x & ~31);  // segment's first slot
+    const bool act = seg0 < n;                                           // warp-uniform
+    const int k_real = seg0 + lane;
+    valid[r] = act && k_real < n;
+    k[r] = valid[r] ? k_real : (act ? seg0 : 0);  // lanes past the end shadow a valid slot
+    // lane l draws the offsets of iterations 4l .. 4l+3 of this segment
+    ol[r] = philox10(U4{(uint32_t)(seg0 / 32), epoch, TAG_MEGO_OFF | (uint32_t)lane, fid}, fd->key0, fd->key1);
+    a[r] = k[r];
+    la[r] = __ldcg(lw + k[r]);
+  }
+#pragma unroll 1
+  for (int b0 = 0; b0 < B; b0 += 4) {
+    U4 ur[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      ur[r] = philox10(U4{(uint32_t)k[r], epoch, TAG_MEGO_U | (uint32_t)(b0 >> 2), fid}, fd->key0, fd->key1);
+#pragma unroll
+    for (int bb = 0; bb < 4; ++bb) {
+      if (b0 + bb >= B) break;
+      const int src_lane = (b0 + bb) >> 2;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const uint32_t ow = (bb == 0) ? ol[r].x : (bb == 1) ? ol[r].y : (bb == 2) ? ol[r].z : ol[r].w;
+        const uint32_t uw = (bb == 0) ? ur[r].x : (bb == 1) ? ur[r].y : (bb == 2) ? ur[r].z : ur[r].w;
         const uint32_t o = __umulhi(__shfl_sync(0xffffffffu, ow, src_lane), (uint32_t)n);
-        int cand = k + (int)o;
+        int cand = k[r] + (int)o;
         if (cand >= n) cand -= n;
         const float lc = __ldcg(lw + cand);
-        const float lu = __logf(fmaf((float)uw[bb], 2.3283064365386963e-10f, 1.1641532182693481e-10f));
-        if (lc - la > lu) {
-          a = cand;
-          la = lc;
+        const float lu = __logf(fmaf((float)uw, 2.3283064365386963e-10f, 1.1641532182693481e-10f));
+        if (lc - la[r] > lu) {
+          a[r] = cand;
+          la[r] = lc;
         }
       }
     }
-    if (valid) e.anc[base + k] = a;
   }
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+    if (valid[r]) e.anc[base + k[r]] = a[r];
 }
 
 // k_mego: mego_tile over the launch's tiles.

@@ -321,8 +321,11 @@ __device__ __forceinline__ void epoch_sys_assign(const EngineDev& e, unsigned* b
   }
 }
 
+#ifndef PF_EPOCH_MINB
+#define PF_EPOCH_MINB 2  // resident CTAs per SM the epoch kernel is compiled for
+#endif
 template <int NCLK, int WMODE, int RESAMPLER>
-__global__ void __launch_bounds__(kThreads, 2) k_epoch(EngineDev e, int t0, int count, unsigned* bar) {
+__global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, int t0, int count, unsigned* bar) {
   constexpr int D = 3 + NCLK;
   constexpr int NV = 2 + D + 6;
   constexpr int kWarps = kThreads / 32;
