@@ -85,7 +85,7 @@ EXPORTED = [
     "pfe_last_launch_count", "pfe_get_anchor", "pfe_test_poison_lookback", "pfe_enable_timing",
     "pfe_read_timing", "pfe_result_bytes", "pfe_read_timing_kernels",
     "pf_mlp_param_count", "pf_mlp_scratch_bytes", "pf_mlp_grad", "pf_mlp_adam_step", "pf_mlp_forward",
-    "pfe_set_mlp", "pfe_get_sat_debug",
+    "pfe_set_mlp", "pfe_get_sat_debug", "pfe_set_epoch_ctas_per_sm",
 ]
 
 _lib = None
@@ -154,6 +154,7 @@ def load():
     L.pf_mlp_adam_step.argtypes = [p, p, i, p, p, p, i, f, p, p, C.c_size_t, p]
     L.pf_mlp_forward.argtypes = [p, i, p, p, p]
     L.pfe_set_mlp.argtypes = [p, p]
+    L.pfe_set_epoch_ctas_per_sm.argtypes = [p, i, C.POINTER(C.c_int)]
     L.pfe_get_sat_debug.argtypes = [p, i, p, i, C.POINTER(C.c_int)]
     for name in EXPORTED:
         fn = getattr(L, name)

@@ -41,6 +41,7 @@ struct pf_engine {
   int resident[Q_COUNT];
   int epoch_resident = 0;     // co-resident CTAs of the cooperative epoch kernel
   bool mlp_set = false;       // mixture mode: network parameters uploaded
+  int epoch_cap = 0;          // > 0: at most this many CTAs per launch of the epoch kernel (tuning)
   size_t epoch_smem = 0;      // its dynamic shared memory
   unsigned* bar = nullptr;    // grid barrier words (count, generation, any-resample)
   int sm_count = 0;
@@ -356,7 +357,9 @@ int prepare_epoch_kernel(pf_engine* eng) {
 // resident at once, which the grid barriers require (the driver refuses the
 // launch otherwise).
 int launch_epoch(pf_engine* eng, int t0, int count) {
-  const int grid = std::max(1, std::min(std::min(count, eng->epoch_resident), kMaxEpochGrid));
+  int cap = std::min(eng->epoch_resident, kMaxEpochGrid);
+  if (eng->epoch_cap > 0) cap = std::min(cap, eng->epoch_cap);
+  const int grid = std::max(1, std::min(count, cap));
   cudaLaunchConfig_t lc;
   memset(&lc, 0, sizeof(lc));
   lc.gridDim = dim3((unsigned)grid);
@@ -590,6 +593,17 @@ int pfe_set_stream(pf_engine_t* eng, void* stream) {
   clear_err();
   if (!eng) return set_err(PF_EINVAL, "null engine");
   eng->stream = (cudaStream_t)stream;
+  return PF_OK;
+}
+
+int pfe_set_epoch_ctas_per_sm(pf_engine_t* eng, int ctas_per_sm, int* resident_per_sm) {
+  clear_err();
+  if (!eng) return set_err(PF_EINVAL, "null engine");
+  const int per_sm = eng->sm_count > 0 ? eng->epoch_resident / eng->sm_count : 0;
+  if (resident_per_sm) *resident_per_sm = per_sm;
+  if (ctas_per_sm < 0 || ctas_per_sm > per_sm)
+    return set_err(PF_EINVAL, "ctas_per_sm must be 0 (all resident) .. %d", per_sm);
+  eng->epoch_cap = ctas_per_sm == 0 ? 0 : ctas_per_sm * eng->sm_count;
   return PF_OK;
 }
 

@@ -171,6 +171,13 @@ class Engine:
                                         len(sats)))
 
     # ------------------------------------------------------------------ steps
+    def set_epoch_ctas_per_sm(self, ctas_per_sm: int) -> int:
+        """Cap the epoch kernel's CTAs per SM (0 = all that fit); returns how
+        many fit."""
+        r = C.c_int(0)
+        N.check(self.lib.pfe_set_epoch_ctas_per_sm(self.h, int(ctas_per_sm), C.byref(r)))
+        return int(r.value)
+
     def set_mlp(self, params):
         """Upload the NLOS network's parameters (mixture mode)."""
         prm = np.ascontiguousarray(params, dtype=np.float32)

@@ -233,6 +233,10 @@ int pfe_create(const pf_engine_config_t* cfg,
                size_t workspace_bytes, void* stream, pf_engine_t** out);
 int pfe_destroy(pf_engine_t* eng);
 int pfe_set_stream(pf_engine_t* eng, void* stream);
+/* Tuning knob of the cooperative epoch kernel: launch at most ctas_per_sm
+ * CTAs per SM (0 = every CTA that fits, the default).  *resident_per_sm
+ * (optional) receives how many fit.  No counterpart in the reference. */
+int pfe_set_epoch_ctas_per_sm(pf_engine_t* eng, int ctas_per_sm, int* resident_per_sm);
 int pfe_set_filter_params(pf_engine_t* eng, int filter,
                           const pf_filter_params_t* params);
 
