@@ -20,11 +20,12 @@ PF_TILE = 1024
 PF_NOALLOC_MAX_PARTICLES = 1 << 22
 
 PF_RESAMPLE_SYSTEMATIC, PF_RESAMPLE_MEGOPOLIS = 0, 1
-PF_WEIGHT_GAUSSIAN, PF_WEIGHT_HUBER, PF_WEIGHT_MIXTURE = 0, 1, 2
+PF_WEIGHT_GAUSSIAN, PF_WEIGHT_HUBER, PF_WEIGHT_MIXTURE, PF_WEIGHT_GENERIC = 0, 1, 2, 3
+PF_LIK_GAUSSIAN, PF_LIK_STUDENT_T, PF_LIK_HUBER, PF_LIK_GMM = 0, 1, 2, 3
 PF_LW_OVERWRITE, PF_LW_ACCUMULATE = 0, 1
 PF_SYS_OFFSET_RANDOM, PF_SYS_OFFSET_REFERENCE = 0, 1
 PF_FLAG_COVARIANCE, PF_FLAG_RECENTER, PF_FLAG_KERNEL_CHAIN = 1, 2, 4
-PF_EP_PREDICT, PF_EP_WEIGHT, PF_EP_FORCE_RESAMPLE, PF_EP_NO_RESAMPLE = 1, 2, 4, 8
+PF_EP_PREDICT, PF_EP_WEIGHT, PF_EP_FORCE_RESAMPLE, PF_EP_NO_RESAMPLE, PF_EP_RESAMPLE_CHECK = 1, 2, 4, 8, 16
 
 
 class EngineConfig(C.Structure):
@@ -57,6 +58,11 @@ class Sat(C.Structure):
     ]
 
 
+class Likelihood(C.Structure):
+    _fields_ = [("type", C.c_int), ("pad_", C.c_int), ("nu", C.c_double), ("huber_k", C.c_double),
+                ("w_los", C.c_double), ("mu_nlos", C.c_double), ("sigma_nlos", C.c_double), ("gate_m", C.c_double)]
+
+
 class FilterResult(C.Structure):
     _fields_ = [
         ("est_ecef", C.c_double * 3), ("est_clk", C.c_double * PF_MAX_CLK), ("cov_enu", C.c_double * 6),
@@ -80,12 +86,14 @@ EXPORTED = [
     "pfe_workspace_bytes", "pfe_create", "pfe_destroy", "pfe_set_stream", "pfe_set_filter_params",
     "pfe_initialize", "pfe_get_frame", "pfe_upload_obs", "pfe_obs_slot_bytes", "pfe_step",
     "pfe_step_per_filter", "pfe_graph_capture", "pfe_graph_launch", "pfe_read_results",
-    "pfe_estimate", "pfe_get_ess", "pfe_get_particles", "pfe_get_state_f32", "pfe_set_state_f32",
+    "pfe_estimate", "pfe_get_ess", "pfe_current_ess", "pfe_position_spread", "pfe_get_particles",
+    "pfe_get_state_f32", "pfe_set_state_f32",
     "pfe_get_ancestors", "pfe_get_resample_info", "pfe_error_word", "pfe_set_spin_limit",
     "pfe_last_launch_count", "pfe_get_anchor", "pfe_test_poison_lookback", "pfe_enable_timing",
     "pfe_read_timing", "pfe_result_bytes", "pfe_read_timing_kernels",
     "pf_mlp_param_count", "pf_mlp_scratch_bytes", "pf_mlp_grad", "pf_mlp_adam_step", "pf_mlp_forward",
-    "pfe_set_mlp", "pfe_get_sat_debug", "pfe_set_epoch_ctas_per_sm",
+    "pfe_set_mlp", "pfe_get_sat_debug", "pfe_set_epoch_ctas_per_sm", "pfe_set_likelihood", "pfe_shift",
+    "pfe_add_position_term",
 ]
 
 _lib = None
@@ -135,6 +143,8 @@ def load():
     L.pfe_read_results.argtypes = [p, C.POINTER(FilterResult)]
     L.pfe_estimate.argtypes = [p, i, dp]
     L.pfe_get_ess.argtypes = [p, i, dp]
+    L.pfe_current_ess.argtypes = [p, i, dp]
+    L.pfe_position_spread.argtypes = [p, i, C.c_void_p, dp]
     L.pfe_get_particles.argtypes = [p, i, dp]
     L.pfe_get_state_f32.argtypes = [p, i, p, p, i]
     L.pfe_get_anchor.argtypes = [p, i, dp, dp, C.POINTER(C.c_float)]
@@ -155,6 +165,9 @@ def load():
     L.pf_mlp_forward.argtypes = [p, i, p, p, p]
     L.pfe_set_mlp.argtypes = [p, p]
     L.pfe_set_epoch_ctas_per_sm.argtypes = [p, i, C.POINTER(C.c_int)]
+    L.pfe_set_likelihood.argtypes = [p, C.POINTER(Likelihood)]
+    L.pfe_shift.argtypes = [p, i, dp, dp]
+    L.pfe_add_position_term.argtypes = [p, i, dp, dp, i, d]
     L.pfe_get_sat_debug.argtypes = [p, i, p, i, C.POINTER(C.c_int)]
     for name in EXPORTED:
         fn = getattr(L, name)

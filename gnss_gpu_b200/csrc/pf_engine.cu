@@ -1,5 +1,6 @@
 // pf_engine.cu -- host side of the resident engine (the pfe_* C ABI).
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
@@ -82,11 +83,11 @@ int validate_config(const pf_engine_config_t* cfg, const pf_filter_params_t* fp)
     return set_err(PF_EINVAL, "unknown resampler %d", cfg->resampler);
   if (cfg->resampler == PF_RESAMPLE_MEGOPOLIS && (cfg->megopolis_iters < 1 || cfg->megopolis_iters > 128))
     return set_err(PF_EINVAL, "megopolis_iters must be 1..128");
-  if (cfg->weight_mode != PF_WEIGHT_GAUSSIAN && cfg->weight_mode != PF_WEIGHT_HUBER &&
-      cfg->weight_mode != PF_WEIGHT_MIXTURE)
+  if (cfg->weight_mode < PF_WEIGHT_GAUSSIAN || cfg->weight_mode > PF_WEIGHT_GENERIC)
     return set_err(PF_EINVAL, "unknown weight_mode %d", cfg->weight_mode);
-  if (cfg->weight_mode == PF_WEIGHT_MIXTURE && (cfg->flags & PF_FLAG_KERNEL_CHAIN))
-    return set_err(PF_EINVAL, "the mixture likelihood runs in the epoch kernel only (no PF_FLAG_KERNEL_CHAIN)");
+  if ((cfg->weight_mode == PF_WEIGHT_MIXTURE || cfg->weight_mode == PF_WEIGHT_GENERIC) &&
+      (cfg->flags & PF_FLAG_KERNEL_CHAIN))
+    return set_err(PF_EINVAL, "this likelihood runs in the epoch kernel only (no PF_FLAG_KERNEL_CHAIN)");
   if (cfg->lw_mode != PF_LW_OVERWRITE && cfg->lw_mode != PF_LW_ACCUMULATE)
     return set_err(PF_EINVAL, "unknown lw_mode %d", cfg->lw_mode);
   if (cfg->sys_offset != PF_SYS_OFFSET_RANDOM && cfg->sys_offset != PF_SYS_OFFSET_REFERENCE)
@@ -330,7 +331,8 @@ template <int NCLK>
 EpochKernel epoch_kernel_w(int wmode, int resampler) {
   if (wmode == PF_WEIGHT_GAUSSIAN) return epoch_kernel_r<NCLK, PF_WEIGHT_GAUSSIAN>(resampler);
   if (wmode == PF_WEIGHT_HUBER) return epoch_kernel_r<NCLK, PF_WEIGHT_HUBER>(resampler);
-  return epoch_kernel_r<NCLK, PF_WEIGHT_MIXTURE>(resampler);
+  if (wmode == PF_WEIGHT_MIXTURE) return epoch_kernel_r<NCLK, PF_WEIGHT_MIXTURE>(resampler);
+  return epoch_kernel_r<NCLK, PF_WEIGHT_GENERIC>(resampler);
 }
 EpochKernel epoch_kernel(const pf_engine* eng) {
   const int w = eng->cfg.weight_mode, r = eng->cfg.resampler;
@@ -911,11 +913,11 @@ int pfe_result_bytes(pf_engine_t* eng, size_t* bytes) {
   return PF_OK;
 }
 
-int pfe_estimate(pf_engine_t* eng, int filter, double* out) {
-  clear_err();
+// One pass of k_estimate over filter f's current particles and weights;
+// leaves api_est / api_m2 in the host copy of the control block.
+static int run_estimate(pf_engine_t* eng, int filter) {
   int s = check_filter(eng, filter);
   if (s != PF_OK) return s;
-  if (!out) return set_err(PF_EINVAL, "null out");
   if (!eng->initialized[filter]) return set_err(PF_ENOTINIT, "filter %d not initialized", filter);
   const FilterDesc& d = eng->hdesc[filter];
   const int g = grid_for(eng, Q_EST, d.n_tiles);
@@ -926,8 +928,51 @@ int pfe_estimate(pf_engine_t* eng, int filter, double* out) {
     default: k_estimate<7><<<g, kThreads, 0, eng->stream>>>(eng->dev, d.tile_begin, d.n_tiles); break;
   }
   CK(cudaGetLastError());
-  if ((s = read_ctrl(eng)) != PF_OK) return s;
+  return read_ctrl(eng);
+}
+
+int pfe_estimate(pf_engine_t* eng, int filter, double* out) {
+  clear_err();
+  if (!out) return set_err(PF_EINVAL, "null out");
+  int s = run_estimate(eng, filter);
+  if (s != PF_OK) return s;
   for (int i = 0; i < eng->D; ++i) out[i] = eng->ctrl_host[filter].api_est[i];
+  return PF_OK;
+}
+
+int pfe_current_ess(pf_engine_t* eng, int filter, double* out) {
+  clear_err();
+  if (!out) return set_err(PF_EINVAL, "null out");
+  int s = run_estimate(eng, filter);
+  if (s != PF_OK) return s;
+  *out = eng->ctrl_host[filter].api_est[7];
+  return PF_OK;
+}
+
+int pfe_position_spread(pf_engine_t* eng, int filter, const double* center_ecef, double* out) {
+  clear_err();
+  if (!out) return set_err(PF_EINVAL, "null out");
+  if (center_ecef)
+    for (int i = 0; i < 3; ++i)
+      if (!isfinite(center_ecef[i])) return set_err(PF_EINVAL, "center must be finite");
+  int s = run_estimate(eng, filter);
+  if (s != PF_OK) return s;
+  const FilterCtrl& c = eng->ctrl_host[filter];
+  const double* rot = eng->hdesc[filter].rot;
+  // local mean m and local centre q (rows of rot are E, N, U in ECEF)
+  const double* ctr = center_ecef ? center_ecef : c.api_est;
+  double m[3], q[3];
+  for (int r = 0; r < 3; ++r) {
+    m[r] = q[r] = 0.0;
+    for (int i = 0; i < 3; ++i) {
+      m[r] += rot[3 * r + i] * (c.api_est[i] - c.anchor[i]);
+      q[r] += rot[3 * r + i] * (ctr[i] - c.anchor[i]);
+    }
+  }
+  // E|x - q|^2 = E|x|^2 - 2 q.m + |q|^2 (second moments about the anchor)
+  const double ex2 = c.api_m2[0] + c.api_m2[3] + c.api_m2[5];
+  const double v = ex2 - 2.0 * (q[0] * m[0] + q[1] * m[1] + q[2] * m[2]) + q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+  *out = sqrt(v > 0.0 ? v : 0.0);
   return PF_OK;
 }
 
@@ -1029,7 +1074,7 @@ int pfe_set_state_f32(pf_engine_t* eng, int filter, const float* state, const fl
                   cudaMemcpyHostToDevice));
   if (lw) {
     for (int k = 0; k < n; ++k)
-      if (!isfinite(lw[k])) return set_err(PF_EINVAL, "log-weights must be finite");
+      if (isnan(lw[k]) || lw[k] == INFINITY) return set_err(PF_EINVAL, "log-weights must be finite or -inf");
     CK(cudaMemcpy(eng->dev.lw + base, lw, sizeof(float) * n, cudaMemcpyHostToDevice));
   }
   c.resample_flag = 0;
@@ -1069,6 +1114,97 @@ int pfe_error_word(pf_engine_t* eng, unsigned* word) {
   if (!eng || !word) return set_err(PF_EINVAL, "null argument");
   CK(cudaStreamSynchronize(eng->stream));
   CK(cudaMemcpy(word, eng->dev.err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  return PF_OK;
+}
+
+int pfe_set_likelihood(pf_engine_t* eng, const pf_likelihood_t* lik) {
+  clear_err();
+  if (!eng || !lik) return set_err(PF_EINVAL, "null argument");
+  if (eng->cfg.weight_mode != PF_WEIGHT_GENERIC) return set_err(PF_EINVAL, "engine is not in generic mode");
+  switch (lik->type) {
+    case PF_LIK_GAUSSIAN: break;
+    case PF_LIK_STUDENT_T:
+      if (!(lik->nu > 0.0) || !isfinite(lik->nu)) return set_err(PF_EINVAL, "Student's t needs nu > 0");
+      break;
+    case PF_LIK_HUBER:
+      if (!(lik->huber_k > 0.0) || !isfinite(lik->huber_k)) return set_err(PF_EINVAL, "Huber needs k > 0");
+      break;
+    case PF_LIK_GMM:
+      if (!(lik->w_los > 0.0 && lik->w_los < 1.0)) return set_err(PF_EINVAL, "GMM needs 0 < w_los < 1");
+      if (!(lik->sigma_nlos > 0.0) || !isfinite(lik->sigma_nlos) || !isfinite(lik->mu_nlos))
+        return set_err(PF_EINVAL, "GMM needs a finite mu_nlos and sigma_nlos > 0");
+      break;
+    default: return set_err(PF_EINVAL, "unknown likelihood type %d", lik->type);
+  }
+  if (!(lik->gate_m >= 0.0) || !isfinite(lik->gate_m)) return set_err(PF_EINVAL, "gate_m must be finite and >= 0");
+  eng->dev.lk_type = lik->type;
+  eng->dev.lk_nu = (float)lik->nu;
+  eng->dev.lk_huber_k = (float)lik->huber_k;
+  eng->dev.lk_w_los = (float)lik->w_los;
+  eng->dev.lk_mu_nlos = (float)lik->mu_nlos;
+  eng->dev.lk_sigma_nlos = (float)lik->sigma_nlos;
+  eng->dev.lk_gate_m = (float)lik->gate_m;
+  return PF_OK;
+}
+
+int pfe_shift(pf_engine_t* eng, int filter, const double dpos_ecef[3], const double* dclk) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!dpos_ecef) return set_err(PF_EINVAL, "null displacement");
+  for (int i = 0; i < 3; ++i)
+    if (!isfinite(dpos_ecef[i])) return set_err(PF_EINVAL, "displacement not finite");
+  if ((s = read_ctrl(eng)) != PF_OK) return s;
+  FilterCtrl c = eng->ctrl_host[filter];
+  for (int i = 0; i < 3; ++i) c.anchor[i] += dpos_ecef[i];
+  if (dclk)
+    for (int k = 0; k < eng->cfg.n_clk; ++k) {
+      if (!isfinite(dclk[k])) return set_err(PF_EINVAL, "clock shift not finite");
+      c.clk_anchor[k] += dclk[k];
+    }
+  CK(cudaMemcpyAsync(eng->ctrl_dev + filter, &c, sizeof(c), cudaMemcpyHostToDevice, eng->stream));
+  CK(cudaStreamSynchronize(eng->stream));
+  eng->ctrl_host[filter] = c;
+  return PF_OK;
+}
+
+int pfe_add_position_term(pf_engine_t* eng, int filter, const double* refs_ecef, const double* log_pi, int K,
+                          double sigma) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!eng->initialized[filter]) return set_err(PF_ENOTINIT, "filter %d not initialized", filter);
+  if (!refs_ecef || K < 1 || K > kMaxPosRefs) return set_err(PF_EINVAL, "need 1..%d references", kMaxPosRefs);
+  if (!(sigma > 0.0) || !isfinite(sigma)) return set_err(PF_EINVAL, "sigma must be > 0");
+  if ((s = read_ctrl(eng)) != PF_OK) return s;
+  const FilterCtrl& c = eng->ctrl_host[filter];
+  const FilterDesc& d = eng->hdesc[filter];
+  PosTerm pt;
+  memset(&pt, 0, sizeof(pt));
+  pt.K = K;
+  pt.inv_2s2 = (float)(0.5 / (sigma * sigma));
+  for (int j = 0; j < K; ++j) {
+    double v[3];
+    for (int i = 0; i < 3; ++i) {
+      if (!isfinite(refs_ecef[3 * j + i])) return set_err(PF_EINVAL, "reference not finite");
+      v[i] = refs_ecef[3 * j + i] - c.anchor[i];
+    }
+    for (int r = 0; r < 3; ++r) pt.ref[j][r] = (float)(d.rot[3 * r] * v[0] + d.rot[3 * r + 1] * v[1] + d.rot[3 * r + 2] * v[2]);
+    pt.logpi[j] = (float)(log_pi ? log_pi[j] : -log((double)K));
+  }
+  const int g = std::max(1, std::min(eng->sm_count * 4, (d.n + kTile - 1) / kTile));
+  switch (eng->D) {
+    case 4: k_position_term<4><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, pt); break;
+    case 5: k_position_term<5><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, pt); break;
+    case 6: k_position_term<6><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, pt); break;
+    default: k_position_term<7><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, pt); break;
+  }
+  CK(cudaGetLastError());
+  // the weights are explicit now
+  const int zero = 0;
+  CK(cudaMemcpyAsync(reinterpret_cast<char*>(eng->ctrl_dev + filter) + offsetof(FilterCtrl, lw_zero), &zero,
+                     sizeof(int), cudaMemcpyHostToDevice, eng->stream));
+  CK(cudaStreamSynchronize(eng->stream));
   return PF_OK;
 }
 

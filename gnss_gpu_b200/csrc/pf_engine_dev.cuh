@@ -58,6 +58,7 @@ struct FilterCtrl {
   double ess;
   double sum_w;
   double api_est[8];      // output of the on-demand estimate kernel
+  double api_m2[6];       // its weighted second moments E[x_i x_j] of the local offsets
   unsigned long long wq_total;
   float shift[8];         // pending re-centring, applied by the next predict
   float max_lw;
@@ -93,6 +94,8 @@ struct EngineDev {
   unsigned max_chunks;
   unsigned* fmax;            // epoch kernel: per filter, order-preserving code of the max log-weight
   const float* mlp;          // mixture mode: network parameters (FP32)
+  int lk_type;               // generic mode: pf_likelihood_type_t and its parameters
+  float lk_nu, lk_huber_k, lk_w_los, lk_mu_nlos, lk_sigma_nlos, lk_gate_m;
   float* sat_dbg;            // mixture mode: per filter and satellite, features and outputs
   unsigned* queue;
   unsigned* err;

@@ -434,7 +434,7 @@ __device__ __forceinline__ void finalize_filter(const EngineDev& e, const Filter
   const bool recenter = (e.flags & PF_FLAG_RECENTER) != 0 && W > 0.0;
 #pragma unroll
   for (int d = 0; d < 8; ++d) fc->shift[d] = (recenter && d < D) ? (float)mu[d] : 0.f;
-  bool rs = do_weight && !(eflags & PF_EP_NO_RESAMPLE) &&
+  bool rs = (do_weight || (eflags & PF_EP_RESAMPLE_CHECK)) && !(eflags & PF_EP_NO_RESAMPLE) &&
             ((eflags & PF_EP_FORCE_RESAMPLE) || ess < (double)e.ess_threshold * (double)n);
   if (!(W > 0.0) || !(ms.max_lw > -INFINITY)) {
     if (do_weight) atomicOr(e.err, ERR_BAD_WEIGHTS);
@@ -649,6 +649,10 @@ __global__ void __launch_bounds__(kThreads, PF_KSTEP_MINB) k_step(EngineDev e, i
       } else {
 #pragma unroll
         for (int k = 0; k < 4; ++k) lwv[k] = lw0[k];
+        // reset weights live only in the control block: a resample test of
+        // them (no weight pass) reads the array, so it is zeroed first
+        if (lw_zero && (eflags & PF_EP_RESAMPLE_CHECK) && !(eflags & PF_EP_NO_RESAMPLE))
+          __stcs(reinterpret_cast<float4*>(e.lw + base + p0), make_float4(0.f, 0.f, 0.f, 0.f));
       }
 #pragma unroll
       for (int k = 0; k < 4; ++k)
@@ -1117,7 +1121,9 @@ __global__ void __launch_bounds__(kThreads) k_init(EngineDev e, int t0, int coun
 // -------------------------------------------------------------------------
 // k_estimate: weighted mean over the current particle set with the current
 // log-weights (zeros after a resample) -- the reference's pf_estimate
-// semantics (weight.cu:163-220,301-321) -- plus the ESS of those weights.
+// semantics (weight.cu:163-220,301-321) -- plus the ESS of those weights
+// (pf_device.cu:924) and the weighted second moments of the local position
+// offsets (for the position spread, pf_device.cu:1025).
 template <int D>
 __global__ void __launch_bounds__(kThreads) k_estimate(EngineDev e, int t0, int count) {
   __shared__ float s_red[kThreads / 32][kPartStride];
@@ -1158,7 +1164,7 @@ __global__ void __launch_bounds__(kThreads) k_estimate(EngineDev e, int t0, int 
     } else {
       lwv[0] = lwv[1] = lwv[2] = lwv[3] = -INFINITY;
     }
-    tile_stats<D>(x, lwv, false, e.part + (size_t)t * kPartStride, s_maxtmp, s_red);
+    tile_stats<D>(x, lwv, true, e.part + (size_t)t * kPartStride, s_maxtmp, s_red);
     if (threadIdx.x == 0) {
       __threadfence();
       unsigned old = atomicAdd(&fc->est_ticket, 1u);
@@ -1178,6 +1184,8 @@ __global__ void __launch_bounds__(kThreads) k_estimate(EngineDev e, int t0, int 
 #pragma unroll
         for (int c = 0; c < D - 3; ++c) fc->api_est[3 + c] = fc->clk_anchor[c] + ms.sx[3 + c] / W;
         fc->api_est[7] = (ms.w2 > 0.0) ? W * W / ms.w2 : 0.0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) fc->api_m2[i] = ms.sxx[i] / W;
         fc->est_ticket = 0u;
         __threadfence();
       }
@@ -1185,6 +1193,53 @@ __global__ void __launch_bounds__(kThreads) k_estimate(EngineDev e, int t0, int 
     }
   }
   queue_exit(q);
+}
+
+// -------------------------------------------------------------------------
+// k_position_term: adds log sum_j pi_j exp(-|p - ref_j|^2 / (2 sigma^2)) to
+// the log-weights of filter f's current particles (gathered through the
+// last resample, if any; weights read as zero when the filter's weights
+// were reset).  References are in the filter's local frame relative to its
+// anchor (pf_device.cu:889-900 for one reference).
+constexpr int kMaxPosRefs = 64;
+struct PosTerm {
+  float ref[kMaxPosRefs][3];
+  float logpi[kMaxPosRefs];
+  int K;
+  float inv_2s2;
+};
+
+template <int D>
+__global__ void __launch_bounds__(kThreads) k_position_term(EngineDev e, int f, PosTerm pt) {
+  const FilterDesc* fd = e.desc + f;
+  const FilterCtrl* fc = e.ctrl + f;
+  const int n = fd->n;
+  const long long base = fd->p_off;
+  const float* src = fc->parity ? e.state1 : e.state0;
+  const bool zero = fc->lw_zero != 0;
+  for (int p0 = (blockIdx.x * kThreads + threadIdx.x) * 4; p0 < n; p0 += gridDim.x * kThreads * 4) {
+    float x[D][4];
+    load_particles<D>(e, src, base, p0, n, fc->resample_flag != 0, x);
+    float4 l = zero ? make_float4(0.f, 0.f, 0.f, 0.f) : *reinterpret_cast<const float4*>(e.lw + base + p0);
+    float lv[4] = {l.x, l.y, l.z, l.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      float m = -INFINITY, acc = 0.f;
+      for (int j = 0; j < pt.K; ++j) {
+        const float dx = x[0][k] - pt.ref[j][0], dy = x[1][k] - pt.ref[j][1], dz = x[2][k] - pt.ref[j][2];
+        const float v = pt.logpi[j] - pt.inv_2s2 * (dx * dx + dy * dy + dz * dz);
+        if (!(v > -INFINITY)) continue;  // a component of weight zero
+        if (v > m) {
+          acc = acc * __expf(m - v) + 1.f;
+          m = v;
+        } else {
+          acc += __expf(v - m);
+        }
+      }
+      lv[k] += (m > -INFINITY) ? m + __logf(acc) : -INFINITY;
+    }
+    *reinterpret_cast<float4*>(e.lw + base + p0) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+  }
 }
 
 // -------------------------------------------------------------------------

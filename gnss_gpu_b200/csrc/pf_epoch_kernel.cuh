@@ -34,6 +34,7 @@
 #pragma once
 #include "pf_engine_kernels.cuh"
 #include "pf_learned.cuh"
+#include "pf_generic.cuh"
 
 namespace pfb {
 
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
   constexpr int D = 3 + NCLK;
   constexpr int NV = 2 + D + 6;
   constexpr int kWarps = kThreads / 32;
-  constexpr int kStride = WMODE == PF_WEIGHT_MIXTURE ? kMixStride : kSatStride;
+  constexpr int kStride = (WMODE == PF_WEIGHT_MIXTURE || WMODE == PF_WEIGHT_GENERIC) ? kMixStride : kSatStride;
   __shared__ __align__(16) float2 s_sat[kStride * PF_MAX_SATS];
   __shared__ int s_grp[PF_MAX_CLK + 1];
   __shared__ unsigned char s_clk[PF_MAX_SATS];
@@ -413,7 +414,10 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
           const int c2 = s_clk[s2];
           rank += (c2 < c) || (c2 == c && s2 < (int)threadIdx.x);
         }
-        write_sat_entry(s_sat + kSatStride * rank, eE, eN, eU, g, y, wq);
+        if constexpr (WMODE == PF_WEIGHT_GENERIC)
+          write_generic_entry(s_sat + kMixStride * rank, e, fd->sigma_pr, eE, eN, eU, g, y, (float)sp->w);
+        else
+          write_sat_entry(s_sat + kSatStride * rank, eE, eN, eU, g, y, wq);
       }
       if (threadIdx.x <= NCLK) {
         int cnt = 0;
@@ -496,8 +500,28 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
           bb = __ffma2_rn(dz[p], dz[p], bb);
           nbb[p] = f2(-bb.x, -bb.y);
         }
+        if constexpr (WMODE == PF_WEIGHT_GENERIC) {
+          bool gated[4] = {false, false, false, false};
+          const float gate = e.lk_gate_m;
+          if (gate > 0.f) {  // per-particle NLOS gate: drop |r| > gate unless too few satellites remain
+            int kept[4] = {0, 0, 0, 0}, used = 0;
 #pragma unroll
-        for (int c = 0; c < NCLK; ++c) {
+            for (int c = 0; c < NCLK; ++c) {
+              const float2 ncb[2] = {f2(-x[3 + c][0], -x[3 + c][1]), f2(-x[3 + c][2], -x[3 + c][3])};
+              generic_kept(s_sat, s_grp[c], s_grp[c + 1], dx, dy, dz, nbb, ncb, kept, used, gate);
+            }
+            const int need = used < 4 ? used : 4;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) gated[k] = kept[k] >= need;
+          }
+#pragma unroll
+          for (int c = 0; c < NCLK; ++c) {
+            const float2 ncb[2] = {f2(-x[3 + c][0], -x[3 + c][1]), f2(-x[3 + c][2], -x[3 + c][3])};
+            generic_pairs(s_sat, s_grp[c], s_grp[c + 1], dx, dy, dz, nbb, ncb, lwp, gated, gate);
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < NCLK && WMODE != PF_WEIGHT_GENERIC; ++c) {
           const float2 ncb[2] = {f2(-x[3 + c][0], -x[3 + c][1]), f2(-x[3 + c][2], -x[3 + c][3])};
           const int s_end = s_grp[c + 1];
 #pragma unroll 2
@@ -516,6 +540,10 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
       } else {
 #pragma unroll
         for (int k = 0; k < 4; ++k) lwv[k] = lw0[k];
+        // reset weights live only in the control block: a resample test of
+        // them (no weight pass) reads the array, so it is zeroed first
+        if (lw_zero && (eflags & PF_EP_RESAMPLE_CHECK) && !(eflags & PF_EP_NO_RESAMPLE))
+          __stcs(reinterpret_cast<float4*>(e.lw + base + p0), make_float4(0.f, 0.f, 0.f, 0.f));
       }
 #pragma unroll
       for (int k = 0; k < 4; ++k)
@@ -588,7 +616,8 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
           row[0] = tm;
           // filter maximum for the one-pass merge and the quantiser, kept
           // only when the filter may resample this epoch
-          if (tm > -INFINITY && do_weight && !(eflags & PF_EP_NO_RESAMPLE)) atomicMax(e.fmax + f, ord_code(tm));
+          if (tm > -INFINITY && (do_weight || (eflags & PF_EP_RESAMPLE_CHECK)) && !(eflags & PF_EP_NO_RESAMPLE))
+            atomicMax(e.fmax + f, ord_code(tm));
         }
         if (it + 2 < ce - cb) {  // buffer b is free again
           if (b) named_arrive<4>();

@@ -28,7 +28,7 @@ class EngineOptions:
     n_clk: int = 1
     resampler: str = "systematic"          # "systematic" | "megopolis"
     megopolis_iters: int = 15
-    weight_mode: str = "gaussian"          # "gaussian" | "huber" | "mixture" (learned, set_mlp)
+    weight_mode: str = "gaussian"          # "gaussian" | "huber" | "mixture" (learned, set_mlp) | "generic"
     huber_k: float = 1.5
     lw_mode: str = "overwrite"             # "overwrite" (reference) | "accumulate"
     sys_offset: str = "random"             # "random" | "reference"
@@ -64,7 +64,7 @@ class Engine:
         cfg.resampler = {"systematic": N.PF_RESAMPLE_SYSTEMATIC, "megopolis": N.PF_RESAMPLE_MEGOPOLIS}[o.resampler]
         cfg.megopolis_iters = int(o.megopolis_iters)
         cfg.weight_mode = {"gaussian": N.PF_WEIGHT_GAUSSIAN, "huber": N.PF_WEIGHT_HUBER,
-                           "mixture": N.PF_WEIGHT_MIXTURE}[o.weight_mode]
+                           "mixture": N.PF_WEIGHT_MIXTURE, "generic": N.PF_WEIGHT_GENERIC}[o.weight_mode]
         cfg.lw_mode = {"overwrite": N.PF_LW_OVERWRITE, "accumulate": N.PF_LW_ACCUMULATE}[o.lw_mode]
         cfg.sys_offset = {"random": N.PF_SYS_OFFSET_RANDOM, "reference": N.PF_SYS_OFFSET_REFERENCE}[o.sys_offset]
         cfg.max_sats = int(o.max_sats)
@@ -178,6 +178,34 @@ class Engine:
         N.check(self.lib.pfe_set_epoch_ctas_per_sm(self.h, int(ctas_per_sm), C.byref(r)))
         return int(r.value)
 
+    def set_likelihood(self, kind: str = "gaussian", nu: float = 0.0, huber_k: float = 1.5, w_los: float = 0.7,
+                       mu_nlos: float = 15.0, sigma_nlos: float = 30.0, gate_m: float = 0.0):
+        """Likelihood of a "generic" engine for the following steps: "gaussian",
+        "student_t" (nu), "huber" (huber_k) or "gmm" (w_los, mu_nlos,
+        sigma_nlos); gate_m > 0 adds the per-particle NLOS gate."""
+        lk = N.Likelihood()
+        lk.type = {"gaussian": N.PF_LIK_GAUSSIAN, "student_t": N.PF_LIK_STUDENT_T, "huber": N.PF_LIK_HUBER,
+                   "gmm": N.PF_LIK_GMM}[kind]
+        lk.nu, lk.huber_k, lk.w_los, lk.mu_nlos, lk.sigma_nlos, lk.gate_m = (
+            float(nu), float(huber_k), float(w_los), float(mu_nlos), float(sigma_nlos), float(gate_m))
+        N.check(self.lib.pfe_set_likelihood(self.h, C.byref(lk)))
+
+    def shift(self, k: int, dpos_ecef, dclk=None):
+        """Move every particle of filter k by dpos_ecef and its clocks by dclk."""
+        dp = np.ascontiguousarray(dpos_ecef, dtype=np.float64).reshape(3)
+        dc = None if dclk is None else np.ascontiguousarray(np.broadcast_to(np.asarray(dclk, np.float64),
+                                                                              (self.cfg.n_clk,)))
+        N.check(self.lib.pfe_shift(self.h, int(k), dp.ctypes.data_as(C.POINTER(C.c_double)),
+                                   None if dc is None else dc.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def add_position_term(self, k: int, refs_ecef, sigma: float, log_pi=None):
+        """log-weights += log sum_j pi_j N(p; ref_j, sigma^2 I) for filter k."""
+        refs = np.ascontiguousarray(refs_ecef, dtype=np.float64).reshape(-1, 3)
+        lp = None if log_pi is None else np.ascontiguousarray(log_pi, dtype=np.float64).ravel()
+        N.check(self.lib.pfe_add_position_term(self.h, int(k), refs.ctypes.data_as(C.POINTER(C.c_double)),
+                                               None if lp is None else lp.ctypes.data_as(C.POINTER(C.c_double)),
+                                               len(refs), float(sigma)))
+
     def set_mlp(self, params):
         """Upload the NLOS network's parameters (mixture mode)."""
         prm = np.ascontiguousarray(params, dtype=np.float32)
@@ -238,6 +266,20 @@ class Engine:
     def ess(self, k: int) -> float:
         v = C.c_double(0)
         N.check(self.lib.pfe_get_ess(self.h, k, C.byref(v)))
+        return float(v.value)
+
+    def current_ess(self, k: int) -> float:
+        """ESS of filter k's current log-weights, recomputed on the device."""
+        v = C.c_double(0)
+        N.check(self.lib.pfe_current_ess(self.h, k, C.byref(v)))
+        return float(v.value)
+
+    def position_spread(self, k: int, center_ecef=None) -> float:
+        """Weighted RMS distance of filter k's particles from center_ecef
+        (default: their weighted mean), computed on the device."""
+        v = C.c_double(0)
+        c = None if center_ecef is None else np.ascontiguousarray(center_ecef, dtype=np.float64).reshape(3)
+        N.check(self.lib.pfe_position_spread(self.h, k, None if c is None else N.vptr(c), C.byref(v)))
         return float(v.value)
 
     def particles(self, k: int) -> np.ndarray:

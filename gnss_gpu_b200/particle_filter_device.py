@@ -1,0 +1,389 @@
+"""Drop-in ParticleFilterDevice for python/gnss_gpu/particle_filter_device.py.
+
+The reference's device-resident filter keeps (x, y, z, clock) per particle
+on the GPU and offers robust likelihoods (Student's t, Huber, a per-particle
+NLOS gate), a fixed two-component GMM, position-domain constraints, clock
+and position shifts, and access to particle states, log-weights and
+resampling ancestors.  This class offers the same constructor and those
+methods on the engine's sm_100a kernels (weight mode "generic"):
+
+* predict() records the motion; the next update() fuses it with the weight
+  pass.  update()/update_gmm() overwrite the log-weights as the reference
+  does (pf_device.cu:278) and, with resample=True, resample on the device
+  when ESS < ess_threshold * N.
+* position_update(), position_mixture_update() add a position term to the
+  log-weights on the device; shift_clock_bias(), recenter_position() and
+  correct_clock_bias() move the filter's anchor (O(1), no particle pass).
+* resample_if_needed() tests the ESS of the current weights on the device
+  and resamples when needed.
+
+Not built: the velocity states (sigma_vel > 0, velocity_guide_alpha != 1,
+rbpf_velocity_kf), the double-difference / carrier-phase / Doppler
+likelihoods and the forward-backward smoother; their methods raise
+NotImplementedError.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _native as N
+from .engine import Engine, EngineOptions, FilterSpec
+
+
+class ParticleFilterDevice:
+    """GPU-resident GNSS particle filter (reference constructor arguments)."""
+
+    def __init__(self, n_particles=1_000_000, sigma_pos=1.0, sigma_cb=300.0,
+                 sigma_pr=5.0, nu=0.0, resampling="megopolis", ess_threshold=0.5,
+                 seed=42, per_particle_nlos_gate=False,
+                 per_particle_nlos_dd_pr_threshold_m=10.0,
+                 per_particle_nlos_dd_carrier_threshold_cycles=0.5,
+                 per_particle_nlos_undiff_pr_threshold_m=30.0,
+                 per_particle_huber=False,
+                 per_particle_huber_dd_pr_k=1.5,
+                 per_particle_huber_dd_carrier_k=1.5,
+                 per_particle_huber_undiff_pr_k=1.5,
+                 sigma_vel=0.0,
+                 velocity_guide_alpha=1.0,
+                 rbpf_velocity_kf=False,
+                 velocity_process_noise=0.0, *, megopolis_iterations=15, max_sats=N.PF_MAX_SATS):
+        N.load()
+        if float(sigma_vel) != 0.0 or float(velocity_guide_alpha) != 1.0 or bool(rbpf_velocity_kf) \
+                or float(velocity_process_noise) != 0.0:
+            raise NotImplementedError("per-particle velocity states are not built: use sigma_vel=0, "
+                                      "velocity_guide_alpha=1, rbpf_velocity_kf=False")
+        self.n_particles = n_particles
+        self.sigma_pos = sigma_pos
+        self.sigma_cb = sigma_cb
+        self.sigma_pr = sigma_pr
+        self.nu = nu
+        self.resampling = resampling
+        self.ess_threshold = ess_threshold
+        self.seed = seed
+        self.per_particle_nlos_gate = bool(per_particle_nlos_gate)
+        self.per_particle_nlos_dd_pr_threshold_m = float(per_particle_nlos_dd_pr_threshold_m)
+        self.per_particle_nlos_dd_carrier_threshold_cycles = float(per_particle_nlos_dd_carrier_threshold_cycles)
+        self.per_particle_nlos_undiff_pr_threshold_m = float(per_particle_nlos_undiff_pr_threshold_m)
+        self.per_particle_huber = bool(per_particle_huber)
+        self.per_particle_huber_dd_pr_k = float(per_particle_huber_dd_pr_k)
+        self.per_particle_huber_dd_carrier_k = float(per_particle_huber_dd_carrier_k)
+        self.per_particle_huber_undiff_pr_k = float(per_particle_huber_undiff_pr_k)
+        self.sigma_vel = float(sigma_vel)
+        self.velocity_guide_alpha = float(velocity_guide_alpha)
+        self.rbpf_velocity_kf = bool(rbpf_velocity_kf)
+        self.velocity_process_noise = float(velocity_process_noise)
+        self.megopolis_iterations = int(megopolis_iterations)
+        self.max_sats = int(max_sats)
+        self._engine = None
+        self._initialized = False
+        self._step = 0
+        self._pending = None        # (disp_local, sigma_pos) of a recorded predict
+        self._spec = None
+        self._rot = None
+
+    # ------------------------------------------------------------------
+    def _require_init(self):
+        if not self._initialized:
+            raise RuntimeError("ParticleFilterDevice not initialized. Call initialize() first.")
+
+    def _gate(self):
+        if not self.per_particle_nlos_gate:
+            return 0.0
+        v = self.per_particle_nlos_undiff_pr_threshold_m
+        return v if np.isfinite(v) and v > 0.0 else 0.0
+
+    def _huber_k(self):
+        v = self.per_particle_huber_undiff_pr_k
+        return v if np.isfinite(v) and v > 0.0 else 1.5
+
+    def _spec_for(self, sigma_pos, sigma_pr):
+        sp = float(self.sigma_pos if sigma_pos is None else sigma_pos)
+        return FilterSpec(n_particles=int(self.n_particles), seed=int(self.seed), sigma_pos=(sp, sp, sp),
+                          sigma_clk=float(self.sigma_cb),
+                          sigma_pr=float(self.sigma_pr if sigma_pr is None else sigma_pr))
+
+    def _set_spec(self, spec):
+        if spec != self._spec:
+            self._engine.set_filter_params(0, spec)
+            self._spec = spec
+
+    def _launch(self, disp_local, flags, sats=None, pr=None, w=None):
+        rec = {"disp": disp_local, "flags": flags}
+        if sats is not None:
+            rec.update(sats=sats, pr=pr, w=w)
+        fe, sv = self._engine.pack_epoch([rec])
+        self._engine.upload(0, fe, sv)
+        self._engine.step()
+
+    def _flush(self):
+        """Apply a recorded predict on its own (no weighting, no resampling)."""
+        if self._pending is not None:
+            disp, sp = self._pending
+            self._pending = None
+            self._set_spec(self._spec_for(sp, None))
+            self._launch(disp, N.PF_EP_PREDICT)
+
+    def _refresh(self, flags=0):
+        """A step without motion or satellites: statistics of the current
+        weights (and with PF_EP_RESAMPLE_CHECK the resample test)."""
+        self._flush()
+        self._launch(np.zeros(3), flags)
+
+    # ------------------------------------------------------------------
+    def initialize(self, position_ecef, clock_bias=0.0, spread_pos=100.0,
+                   spread_cb=1000.0, velocity=None, spread_vel=0.0,
+                   velocity_init_sigma=0.0):
+        """Scatter particles N(position, spread_pos) / N(clock_bias, spread_cb)."""
+        if (velocity is not None and np.any(np.asarray(velocity, dtype=np.float64) != 0.0)) \
+                or float(spread_vel) != 0.0 or float(velocity_init_sigma) != 0.0:
+            raise NotImplementedError("per-particle velocity states are not built")
+        pos = np.asarray(position_ecef, dtype=np.float64).ravel()
+        if pos.size < 3 or not np.all(np.isfinite(pos[:3])):
+            raise ValueError("position_ecef must hold 3 finite values")
+        if self.resampling not in ("megopolis", "systematic"):
+            raise ValueError(f"unknown resampling method {self.resampling!r}")
+        if self._engine is not None:
+            self._engine.close()
+        opts = EngineOptions(n_clk=1, resampler=self.resampling, megopolis_iters=self.megopolis_iterations,
+                             weight_mode="generic", huber_k=self._huber_k(), lw_mode="overwrite",
+                             sys_offset="reference", max_sats=self.max_sats, obs_slots=1, covariance=True,
+                             recenter=True, ess_threshold=float(self.ess_threshold))
+        self._spec = self._spec_for(None, None)
+        self._engine = Engine([self._spec], opts)
+        self._engine.initialize(0, pos[:3], float(clock_bias), float(spread_pos), float(spread_cb))
+        self._rot, _ = self._engine.frame(0)
+        self._initialized = True
+        self._step = 0
+        self._pending = None
+
+    def predict(self, velocity=None, dt=1.0, sigma_pos=None, sigma_vel=None, velocity_guide_alpha=None,
+                rbpf_velocity_kf=None, velocity_process_noise=None):
+        """Constant-velocity motion (ECEF m/s) plus N(0, sigma_pos) / N(0, sigma_cb)."""
+        self._require_init()
+        if (sigma_vel not in (None, 0.0)) or (velocity_guide_alpha not in (None, 1.0)) or rbpf_velocity_kf \
+                or (velocity_process_noise not in (None, 0.0)):
+            raise NotImplementedError("per-particle velocity states are not built")
+        vel = np.zeros(3) if velocity is None else np.asarray(velocity, dtype=np.float64).ravel()[:3]
+        if vel.size < 3 or not np.all(np.isfinite(vel)) or not np.isfinite(dt):
+            raise ValueError("velocity must hold 3 finite values and dt must be finite")
+        self._flush()
+        self._step += 1
+        self._pending = (self._rot @ (vel * float(dt)), sigma_pos)
+
+    def _weight(self, sat_ecef, pseudoranges, weights, sigma_pr, resample, **lik):
+        self._require_init()
+        sat = np.asarray(sat_ecef, dtype=np.float64).reshape(-1, 3)
+        pr = np.asarray(pseudoranges, dtype=np.float64).ravel()
+        if len(sat) != len(pr):
+            raise ValueError("sat_ecef and pseudoranges disagree on the satellite count")
+        w = np.ones(len(pr)) if weights is None else np.asarray(weights, dtype=np.float64).ravel()
+        self._engine.set_likelihood(**lik)
+        flags = N.PF_EP_WEIGHT | (0 if resample else N.PF_EP_NO_RESAMPLE)
+        disp, sp = np.zeros(3), None
+        if self._pending is not None:
+            disp, sp = self._pending
+            self._pending = None
+            flags |= N.PF_EP_PREDICT
+        self._set_spec(self._spec_for(sp, sigma_pr))
+        self._launch(disp, flags, sat, pr, w)
+
+    def update(self, sat_ecef, pseudoranges, weights=None, sigma_pr=None, resample=True):
+        """Pseudorange likelihood: Student's t when nu > 0, else Huber when
+        per_particle_huber, else Gaussian; per-particle NLOS gate when
+        per_particle_nlos_gate.  Overwrites the log-weights."""
+        if float(self.nu) > 0.0:
+            lik = dict(kind="student_t", nu=float(self.nu))
+        elif self.per_particle_huber:
+            lik = dict(kind="huber", huber_k=self._huber_k())
+        else:
+            lik = dict(kind="gaussian")
+        self._weight(sat_ecef, pseudoranges, weights, sigma_pr, resample, gate_m=self._gate(), **lik)
+
+    def update_gmm(self, sat_ecef, pseudoranges, weights=None, sigma_pr=None,
+                   w_los=0.7, mu_nlos=15.0, sigma_nlos=30.0, resample=True):
+        """LOS/NLOS Gaussian-mixture likelihood (pf_device.cu:373-436)."""
+        self._weight(sat_ecef, pseudoranges, weights, sigma_pr, resample, kind="gmm", w_los=float(w_los),
+                     mu_nlos=float(mu_nlos), sigma_nlos=float(sigma_nlos))
+
+    def update_dd_pseudorange(self, *a, **k):
+        raise NotImplementedError("double-difference pseudorange likelihood is not built")
+
+    def update_carrier_afv(self, *a, **k):
+        raise NotImplementedError("carrier-phase AFV likelihood is not built")
+
+    def update_dd_carrier_afv(self, *a, **k):
+        raise NotImplementedError("double-difference carrier-phase likelihood is not built")
+
+    def update_doppler(self, *a, **k):
+        raise NotImplementedError("Doppler likelihood is not built")
+
+    def update_doppler_kf(self, *a, **k):
+        raise NotImplementedError("Doppler velocity Kalman update is not built")
+
+    def enable_smoothing(self):
+        raise NotImplementedError("forward-backward smoothing is not built")
+
+    def store_epoch(self, *a, **k):
+        raise NotImplementedError("forward-backward smoothing is not built")
+
+    def smooth(self, *a, **k):
+        raise NotImplementedError("forward-backward smoothing is not built")
+
+    # ------------------------------------------------------------------
+    def position_update(self, ref_ecef, sigma_pos=30.0):
+        """log-weights += -|p - ref|^2 / (2 sigma_pos^2) (pf_device.cu:889-900)."""
+        self._require_init()
+        ref = np.asarray(ref_ecef, dtype=np.float64).ravel()[:3]
+        self._flush()
+        self._engine.add_position_term(0, ref[None, :], float(sigma_pos))
+
+    def position_mixture_update(self, refs_ecef, sigma_pos=1.0, mixture_weights=None):
+        """log-weights += log sum_j pi_j exp(-|p - ref_j|^2 / (2 sigma^2)),
+        pi normalised (at most 64 references, one device pass)."""
+        self._require_init()
+        refs = np.asarray(refs_ecef, dtype=np.float64).reshape(-1, 3)
+        refs_ok = np.all(np.isfinite(refs), axis=1)
+        if mixture_weights is None:
+            mix = np.full(len(refs), 1.0 / max(1, len(refs)))
+        else:
+            mix = np.asarray(mixture_weights, dtype=np.float64).reshape(-1)
+            if mix.size != len(refs):
+                raise ValueError("mixture_weights length must match refs_ecef")
+        refs, mix = refs[refs_ok], mix[refs_ok]
+        if len(refs) == 0:
+            return
+        mix = np.where(np.isfinite(mix) & (mix > 0.0), mix, 0.0)
+        mix = mix / mix.sum() if mix.sum() > 0 else np.full(len(refs), 1.0 / len(refs))
+        if len(refs) > 64:
+            raise ValueError("at most 64 mixture references are supported")
+        keep = mix > 0
+        self._flush()
+        with np.errstate(divide="ignore"):
+            self._engine.add_position_term(0, refs[keep], max(float(sigma_pos), 1.0e-6), np.log(mix[keep]))
+
+    def shift_clock_bias(self, shift: float):
+        """Add `shift` (m) to every particle's clock bias."""
+        self._require_init()
+        self._flush()
+        self._engine.shift(0, np.zeros(3), [float(shift)])
+
+    def recenter_position(self, ref_ecef, max_shift_m=10000.0):
+        """Move the cloud's weighted mean to ref_ecef when within the cap;
+        returns (shift norm, applied)."""
+        self._require_init()
+        ref = np.asarray(ref_ecef, dtype=np.float64).ravel()
+        if ref.size != 3:
+            raise ValueError("ref_ecef must have shape (3,)")
+        if not np.all(np.isfinite(ref)):
+            return float("inf"), False
+        est = self.estimate()
+        delta = ref - est[:3]
+        norm = float(np.linalg.norm(delta))
+        if float(max_shift_m) > 0.0 and norm > float(max_shift_m):
+            return norm, False
+        self._engine.shift(0, delta)
+        return norm, True
+
+    def correct_clock_bias(self, sat_ecef, pseudoranges, quantile=0.5):
+        """Shift every clock bias so the estimate's clock equals the chosen
+        quantile of the pseudorange residuals at the estimated position."""
+        self._require_init()
+        est = self.estimate()
+        sat = np.asarray(sat_ecef, dtype=np.float64).reshape(-1, 3)
+        pr = np.asarray(pseudoranges, dtype=np.float64).ravel()
+        res = pr - np.linalg.norm(sat - est[:3], axis=1)
+        expected = float(np.quantile(res, float(np.clip(quantile, 0.0, 1.0))))
+        self._engine.shift(0, np.zeros(3), [expected - est[3]])
+
+    def _resample(self):
+        """Resample now, whatever the ESS."""
+        self._require_init()
+        self._refresh(N.PF_EP_RESAMPLE_CHECK | N.PF_EP_FORCE_RESAMPLE)
+
+    def resample_if_needed(self):
+        """Resample when the ESS of the current weights is below
+        ess_threshold * n_particles; returns whether it did."""
+        self._require_init()
+        self._refresh(N.PF_EP_RESAMPLE_CHECK)
+        return bool(self._engine.results()[0]["resampled"])
+
+    # ------------------------------------------------------------------
+    def estimate(self):
+        """Weighted mean [x, y, z, clock_bias] (ECEF, m) of the current particles."""
+        self._require_init()
+        self._flush()
+        return self._engine.estimate(0)
+
+    def get_particles(self):
+        """All particles as an (n_particles, 4) FP64 array [x, y, z, clock_bias]."""
+        self._require_init()
+        self._flush()
+        return self._engine.particles(0)
+
+    def get_particle_states(self):
+        """(n_particles, 16) rows [x, y, z, clock_bias, 12 zeros]: the
+        reference's layout, whose velocity columns this filter does not model."""
+        p = self.get_particles()
+        out = np.zeros((len(p), 16))
+        out[:, :4] = p
+        return out
+
+    def set_particle_states(self, states):
+        """Replace the particles (rows [x, y, z, clock_bias, ...]) and reset
+        the weights."""
+        self._require_init()
+        arr = np.asarray(states, dtype=np.float64)
+        if arr.ndim != 2 or arr.shape[0] != self.n_particles or arr.shape[1] not in (4, 16):
+            raise ValueError(f"states shape {arr.shape} != ({self.n_particles}, 16)")
+        self._flush()
+        anchor, clk, _ = self._engine.anchor(0)
+        st = np.empty((4, self.n_particles), np.float32)
+        st[:3] = ((arr[:, :3] - anchor) @ self._rot.T).T
+        st[3] = arr[:, 3] - clk[0]
+        self._engine.set_state_f32(0, st, np.zeros(self.n_particles, np.float32))
+
+    def get_log_weights(self):
+        """Current log-weights as FP64."""
+        self._require_init()
+        self._flush()
+        _, lw = self._engine.state_f32(0)
+        return lw.astype(np.float64)
+
+    def set_log_weights(self, log_weights):
+        """Replace the log-weights of the current particles."""
+        self._require_init()
+        lw = np.asarray(log_weights, dtype=np.float64).reshape(-1)
+        if lw.size != self.n_particles:
+            raise ValueError(f"log_weights size {lw.size} != {self.n_particles}")
+        self._flush()
+        st, _ = self._engine.state_f32(0)
+        self._engine.set_state_f32(0, st, lw.astype(np.float32))
+
+    def get_resample_ancestors(self):
+        """Slot j of the last systematic resample copied particle out[j]."""
+        self._require_init()
+        if self.resampling != "systematic":
+            raise RuntimeError("get_resample_ancestors requires resampling='systematic'")
+        return self._engine.ancestors(0)
+
+    def get_ess(self):
+        """Effective sample size of the current log-weights (device pass)."""
+        self._require_init()
+        self._flush()
+        return self._engine.current_ess(0)
+
+    def get_position_spread(self, center=None):
+        """Weighted RMS distance of the particles from `center` (default: the
+        weighted mean), m, from one device pass."""
+        self._require_init()
+        c = None
+        if center is not None:
+            c = np.asarray(center, dtype=np.float64).ravel()
+            if c.size != 3:
+                raise ValueError("center must have shape (3,)")
+        self._flush()
+        return self._engine.position_spread(0, c)
+
+    def sync(self):
+        if self._engine is not None:
+            self._engine.synchronize()

@@ -145,9 +145,30 @@ typedef enum { PF_RESAMPLE_SYSTEMATIC = 0, PF_RESAMPLE_MEGOPOLIS = 1 } pf_resamp
 typedef enum {
   PF_WEIGHT_GAUSSIAN = 0,
   PF_WEIGHT_HUBER = 1,
-  PF_WEIGHT_MIXTURE = 2  /* learned LOS/NLOS mixture (pfe_set_mlp), Huber fallback;
+  PF_WEIGHT_MIXTURE = 2, /* learned LOS/NLOS mixture (pfe_set_mlp), Huber fallback;
+                            epoch-kernel path only */
+  PF_WEIGHT_GENERIC = 3  /* the device filter's likelihoods (pfe_set_likelihood);
                             epoch-kernel path only */
 } pf_weight_mode_t;
+
+/* Likelihood of PF_WEIGHT_GENERIC engines (pf_device.cu:189-276,373-436). */
+typedef enum {
+  PF_LIK_GAUSSIAN = 0,
+  PF_LIK_STUDENT_T = 1,  /* nu > 0 */
+  PF_LIK_HUBER = 2,      /* huber_k > 0 */
+  PF_LIK_GMM = 3         /* w_los, mu_nlos, sigma_nlos */
+} pf_likelihood_type_t;
+
+typedef struct {
+  int type;              /* pf_likelihood_type_t                              */
+  int pad_;
+  double nu;             /* Student's t degrees of freedom                    */
+  double huber_k;        /* Huber threshold in sigmas                         */
+  double w_los;          /* GMM: weight of the LOS component, in (0, 1)       */
+  double mu_nlos;        /* GMM: mean of the NLOS component, m                */
+  double sigma_nlos;     /* GMM: std of the NLOS component, m                 */
+  double gate_m;         /* > 0: per-particle NLOS gate on |residual|, m      */
+} pf_likelihood_t;
 typedef enum { PF_LW_OVERWRITE = 0, PF_LW_ACCUMULATE = 1 } pf_lw_mode_t;
 typedef enum {
   PF_SYS_OFFSET_RANDOM = 0,    /* Philox draw per filter and epoch            */
@@ -189,6 +210,8 @@ typedef struct {
 #define PF_EP_WEIGHT 2         /* evaluate the likelihood (else keep lw)   */
 #define PF_EP_FORCE_RESAMPLE 4 /* resample regardless of ESS               */
 #define PF_EP_NO_RESAMPLE 8    /* never resample this epoch                */
+#define PF_EP_RESAMPLE_CHECK 16 /* without PF_EP_WEIGHT: still test the ESS of
+                                   the current weights and resample if needed */
 typedef struct {
   double disp[3];        /* displacement in the filter's local E/N/U frame, m */
   int n_sat;
@@ -277,8 +300,17 @@ int pfe_result_bytes(pf_engine_t* eng, size_t* bytes);
  * (zero after a resample), as the reference's pf_estimate.  out is
  * [3 + n_clk] in ECEF / m.  Synchronous. */
 int pfe_estimate(pf_engine_t* eng, int filter, double* out);
-/* ESS of the current log-weights (N after a resample).  Synchronous. */
+/* ESS of the log-weights of the last step (N after a resample): no kernel,
+ * one control-block read.  Synchronous. */
 int pfe_get_ess(pf_engine_t* eng, int filter, double* out);
+/* ESS of the current log-weights, recomputed on the device (one estimate
+ * pass): also right after pfe_add_position_term / pfe_set_state_f32
+ * (pf_device.cu:1722 pf_device_ess).  Synchronous. */
+int pfe_current_ess(pf_engine_t* eng, int filter, double* out);
+/* Weighted RMS distance (m) of the current particles from center_ecef (null:
+ * from their weighted mean), from one device pass over the particles
+ * (pf_device.cu:1764 pf_device_position_spread).  Synchronous. */
+int pfe_position_spread(pf_engine_t* eng, int filter, const double* center_ecef, double* out);
 /* Export particles as FP64 ECEF rows [N][3 + n_clk] into host memory. */
 int pfe_get_particles(pf_engine_t* eng, int filter, double* out_host);
 /* Local-frame FP32 state [D][N] and FP32 log-weights of a filter.
@@ -292,8 +324,10 @@ int pfe_get_state_f32(pf_engine_t* eng, int filter, float* out_host_DxN,
  * re-centring shift [8] that the next step subtracts. */
 int pfe_get_anchor(pf_engine_t* eng, int filter, double anchor_ecef[3],
                    double clk_anchor[PF_MAX_CLK], float shift[8]);
-/* Replace a filter's state: offsets [D][N] (FP32, local frame), lw (may be
- * NULL = zeros).  Used for checkpoint/restore and tests. */
+/* Replace a filter's state: offsets [D][N] (FP32, local frame about the
+ * committed anchor; the pending shift is cleared), lw (may be NULL = zeros;
+ * finite or -inf, PF_EINVAL for NaN / +inf).  Used for checkpoint/restore,
+ * ParticleFilterDevice.set_particle_states / set_log_weights and tests. */
 int pfe_set_state_f32(pf_engine_t* eng, int filter, const float* state_DxN,
                       const float* lw_or_null);
 /* Ancestor indices written by the last resample (host copy, N ints). */
@@ -334,6 +368,23 @@ int pfe_read_timing(pf_engine_t* eng, float* step_kernel_ms, float* whole_step_m
  * second entry holds all resampling kernels together and the rest are 0. */
 int pfe_read_timing_kernels(pf_engine_t* eng, float* out_4_per_step,
                             int max_entries, int* count);
+
+/* Likelihood of a PF_WEIGHT_GENERIC engine for the following steps. */
+int pfe_set_likelihood(pf_engine_t* eng, const pf_likelihood_t* lik);
+/* Moves every particle of filter f by dpos_ecef (m) and its clock states by
+ * dclk[0..n_clk-1] (m; may be null): an O(1) change of the filter's anchor
+ * (pf_device.cu:902-921). */
+int pfe_shift(pf_engine_t* eng, int filter, const double dpos_ecef[3], const double* dclk);
+/* Adds to the log-weights of filter f the position term
+ *   log sum_j pi_j exp(-|p - ref_j|^2 / (2 sigma^2))   (1 <= K <= 64
+ * references; log_pi may be null for equal pi_j = 1/K, and entries of -inf
+ * drop a reference; K = 1 is
+ * pf_device.cu:889-900) over the current particles (gathered through the
+ * last resample, if any).  The filter's statistics (estimate, ESS) follow at
+ * its next step; a step with flags PF_EP_RESAMPLE_CHECK (or 0) and no
+ * satellites recomputes them and resamples if needed. */
+int pfe_add_position_term(pf_engine_t* eng, int filter, const double* refs_ecef, const double* log_pi,
+                          int K, double sigma);
 
 /* Network parameters of PF_WEIGHT_MIXTURE (host array of
  * pf_mlp_param_count() floats, copied to the engine).  Required before the

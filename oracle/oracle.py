@@ -198,6 +198,55 @@ def weight_mixture(x, anchor, clk_anchor, rot, sats, sigma_pr, p_nlos, mu, mode,
     return lw
 
 
+def weight_generic(x, anchor, clk_anchor, rot, sats, sigma_pr, kind="gaussian", nu=0.0, huber_k=1.5,
+                   w_los=0.7, mu_nlos=15.0, sigma_nlos=30.0, gate_m=0.0):
+    """FP64 log-weights of the device filter's likelihoods, one clock state.
+
+    Per satellite with residual r = pr - |sat - p| - cb and weight w:
+      gaussian   -w r^2 / (2 sigma^2)                          pf_device.cu:273-275
+      student_t  -(nu + 1)/2 log(1 + w r^2 / (nu sigma^2))      pf_device.cu:265-266
+      huber      -w rho_k(|r| / sigma)                         pf_device.cu:19-26,267-268
+      gmm        log(w_los/sigma exp(-w r^2/(2 sigma^2))
+                     + (1-w_los)/sigma_nlos exp(-w (r-mu)^2/(2 sigma_nlos^2)))
+                                                               pf_device.cu:415-428
+    gate_m > 0: a particle drops the satellites with |r| > gate_m unless
+    fewer than min(n_sat, 4) would remain (pf_device.cu:236-258).
+    Satellites of weight <= 0 are skipped.  x: (D, n) offsets about
+    `anchor` in the E/N/U frame `rot`; sats: (S, 5) rows x, y, z, pr, w.
+    Also returns the (S, n) residuals."""
+    x = _f64(x)
+    sats = _f64(sats).reshape(-1, 5)
+    pos = _f64(anchor)[None, :] + x[:3].T @ _f64(rot)
+    cb = clk_anchor[0] + x[3]
+    S = len(sats)
+    res = np.empty((S, x.shape[1]))
+    for s in range(S):
+        res[s] = sats[s, 3] - np.linalg.norm(sats[s, :3][None, :] - pos, axis=1) - cb
+    use = np.ones_like(res, dtype=bool)
+    if gate_m > 0.0:
+        inside = np.abs(res) <= gate_m
+        gate_on = inside.sum(axis=0) >= min(S, 4)
+        use = inside | ~gate_on[None, :]
+    lw = np.zeros(x.shape[1])
+    for s in range(S):
+        r, w = res[s], sats[s, 4]
+        if w <= 0.0:
+            continue
+        if kind == "student_t":
+            t = -0.5 * (nu + 1.0) * np.log1p(w * r * r / (nu * sigma_pr * sigma_pr))
+        elif kind == "huber":
+            z = np.abs(r) / sigma_pr
+            t = -w * np.where(z < huber_k, 0.5 * z * z, huber_k * z - 0.5 * huber_k * huber_k)
+        elif kind == "gmm":
+            a = np.log(w_los) - np.log(sigma_pr) - 0.5 * w * r * r / (sigma_pr * sigma_pr)
+            b = np.log(1.0 - w_los) - np.log(sigma_nlos) - 0.5 * w * (r - mu_nlos) ** 2 / (sigma_nlos * sigma_nlos)
+            t = np.logaddexp(a, b)
+        else:
+            t = -0.5 * w * r * r / (sigma_pr * sigma_pr)
+        lw += np.where(use[s], t, 0.0)
+    return lw, res
+
+
 def stats(x, lw, anchor, clk_anchor, rot):
     x = _f64(x)
     D, n = x.shape

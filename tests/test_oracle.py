@@ -185,3 +185,62 @@ def test_reference_megopolis_chain_prefers_heavy_particles():
     lw[: n // 4] = 0.0
     anc = O.pf_megopolis_ref_ancestors(lw, 20, 12345)
     assert np.mean(anc < n // 4) > 0.9
+
+
+# ------------------------------------------------ device-filter likelihoods
+def _outlier_case(n_out, n_sat=5):
+    sats = TOKYO_SATS[:n_sat]
+    pr = np.linalg.norm(sats - TOKYO_TRUE_POS, axis=1) + TOKYO_TRUE_CB
+    pr[:n_out] += 100.0
+    return np.column_stack([sats, pr, np.ones(n_sat)])
+
+
+def _generic(rows, x=None, **kw):
+    x = np.zeros((4, 1)) if x is None else x
+    lw, _ = O.weight_generic(x, TOKYO_TRUE_POS, [TOKYO_TRUE_CB], np.eye(3), rows, 5.0, **kw)
+    return lw
+
+
+def test_generic_gaussian_and_huber_match_pinned_oracle():
+    """weight_generic agrees with the C oracle (pinned against the
+    reference) on a cloud of particles, Gaussian and Huber."""
+    rng = np.random.default_rng(5)
+    x = np.vstack([rng.normal(0, 30, (3, 500)), rng.normal(0, 20, (1, 500))])
+    rows = np.column_stack([TOKYO_SATS, TOKYO_PR, rng.uniform(0.5, 2.0, len(TOKYO_PR))])
+    clk = np.zeros(len(rows), np.int32)
+    for kind, mode in (("gaussian", 0), ("huber", 1)):
+        want = O.weight(x, TOKYO_TRUE_POS, [TOKYO_TRUE_CB], np.eye(3), rows, clk, 5.0, mode=mode, huber_k=1.5)
+        got, _ = O.weight_generic(x, TOKYO_TRUE_POS, [TOKYO_TRUE_CB], np.eye(3), rows, 5.0, kind=kind, huber_k=1.5)
+        np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-7)
+
+
+def test_generic_known_answers():
+    """A 100 m outlier at sigma 5 (reference tests/test_cuda_streams.py:
+    668-693 for Gaussian / Huber, 569-600 for the gate); Student's t and the
+    GMM from their closed forms (pf_device.cu:265-266, 415-428)."""
+    one = _outlier_case(1)
+    assert _generic(one, kind="gaussian")[0] == pytest.approx(-200.0, abs=1e-6)
+    assert _generic(one, kind="huber", huber_k=1.5)[0] == pytest.approx(-28.875, abs=1e-6)
+    assert _generic(one, kind="student_t", nu=4.0)[0] == pytest.approx(-2.5 * np.log(101.0), abs=1e-9)
+    a = np.log(0.7) - np.log(5.0)
+    gmm_clean = np.logaddexp(a, np.log(0.3) - np.log(30.0) - 0.5 * 15.0 ** 2 / 900.0)
+    gmm_out = np.logaddexp(a - 0.5 * 100.0 ** 2 / 25.0, np.log(0.3) - np.log(30.0) - 0.5 * 85.0 ** 2 / 900.0)
+    want = 4 * gmm_clean + gmm_out
+    got = _generic(one, kind="gmm", w_los=0.7, mu_nlos=15.0, sigma_nlos=30.0)[0]
+    assert got == pytest.approx(want, abs=1e-6)
+    # gate: one outlier of five is dropped, five of five keep the gate off
+    assert abs(_generic(one, kind="gaussian", gate_m=30.0)[0]) < 1e-6
+    assert _generic(_outlier_case(5), kind="gaussian", gate_m=30.0)[0] < -900.0
+    # two outliers of five: three inside < min(5, 4), gate off
+    assert _generic(_outlier_case(2), kind="gaussian", gate_m=30.0)[0] == pytest.approx(-400.0, abs=1e-6)
+    # three satellites: min(3, 4) = 3 must stay inside
+    assert _generic(_outlier_case(1, 3), kind="gaussian", gate_m=30.0)[0] == pytest.approx(-200.0, abs=1e-6)
+
+
+def test_generic_weight_zero_satellite_contributes_nothing():
+    rows = _outlier_case(1)
+    rows[0, 4] = 0.0
+    for kind in ("gaussian", "student_t", "huber", "gmm"):
+        full = _generic(rows, kind=kind, nu=3.0)
+        drop = _generic(rows[1:], kind=kind, nu=3.0)
+        assert full[0] == pytest.approx(drop[0], abs=1e-12)

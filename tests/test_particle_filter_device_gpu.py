@@ -1,0 +1,367 @@
+"""ParticleFilterDevice drop-in: the reference's wrapper tests
+(tests/test_cuda_streams.py of the reference project, the parts this
+filter models) and FP64 parity of every likelihood, position term, shift
+and statistic with the oracle."""
+import numpy as np
+import pytest
+
+from conftest import TOKYO_SATS, TOKYO_PR, TOKYO_TRUE_POS, TOKYO_TRUE_CB
+from oracle import oracle as O
+from pfhelp import lw_close, EST_TOL_M, ESS_RTOL
+
+pytestmark = pytest.mark.gpu
+
+SEED = 42
+ORIGIN = np.array([0.0, 0.0, 0.0])
+ORIGIN_CB = 100.0
+
+
+def _origin_sats(n_sat=8):
+    """Satellites of the reference's stream tests: receiver at the ECEF
+    origin, 20,000 km away in seeded random directions."""
+    rng = np.random.RandomState(123)
+    d = rng.randn(n_sat, 3)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    sat = d * 20_000_000.0
+    pr = np.linalg.norm(sat - ORIGIN, axis=1) + ORIGIN_CB
+    return sat, pr, np.ones(n_sat)
+
+
+@pytest.fixture(scope="module")
+def PFD():
+    from gnss_gpu_b200 import ParticleFilterDevice
+    return ParticleFilterDevice
+
+
+def _cloud(pf):
+    """(offsets (4, n) FP64, anchor, clock anchor, rot) of the current
+    particles -- the frame the device weighted them in."""
+    eng = pf._engine
+    x, _ = eng.state_f32(0)
+    anchor, clk, _ = eng.anchor(0)
+    rot, _ = eng.frame(0)
+    return x.astype(np.float64), anchor, clk, rot
+
+
+# ------------------------------------------------ reference tests, ported
+class TestWrapper:
+    def test_sync_method_exists(self, PFD):
+        pf = PFD(n_particles=1000, seed=SEED)
+        pf.initialize(position_ecef=ORIGIN, clock_bias=ORIGIN_CB, spread_pos=50.0, spread_cb=200.0)
+        pf.sync()
+
+    def test_full_pipeline_with_sync(self, PFD):
+        sat, pr, w = _origin_sats()
+        pf = PFD(n_particles=100_000, sigma_pos=1.0, sigma_cb=300.0, sigma_pr=5.0, resampling="systematic",
+                 seed=SEED)
+        pf.initialize(position_ecef=ORIGIN, clock_bias=ORIGIN_CB, spread_pos=50.0, spread_cb=200.0)
+        for _ in range(3):
+            pf.predict(dt=1.0)
+            pf.update(sat, pr, w)
+        pf.sync()
+        res = pf.estimate()
+        assert res.shape == (4,)
+        assert np.all(np.isfinite(res))
+
+    def test_get_log_weights_shape(self, PFD):
+        sat, pr, w = _origin_sats()
+        pf = PFD(n_particles=1024, sigma_pos=1.0, sigma_cb=300.0, sigma_pr=5.0, resampling="systematic", seed=SEED)
+        pf.initialize(position_ecef=ORIGIN, clock_bias=ORIGIN_CB, spread_pos=50.0, spread_cb=200.0)
+        pf.predict(dt=1.0)
+        pf.update(sat, pr, w, resample=False)
+        lw = pf.get_log_weights()
+        assert lw.shape == (1024,)
+        assert np.all(np.isfinite(lw))
+        pf.resample_if_needed()
+
+    def test_get_particle_states_shape(self, PFD):
+        pf = PFD(n_particles=2048, seed=SEED)
+        pf.initialize(position_ecef=ORIGIN, clock_bias=ORIGIN_CB, spread_pos=0.0, spread_cb=0.0)
+        st = pf.get_particle_states()
+        assert st.shape == (2048, 16)
+        np.testing.assert_allclose(st[:, :3], 0.0, atol=1e-9)
+        np.testing.assert_allclose(st[:, 3], ORIGIN_CB, atol=1e-9)
+        assert pf.estimate().shape == (4,)
+
+    def test_get_position_spread_shrinks_after_update(self, PFD):
+        sat, pr, w = _origin_sats()
+        pf = PFD(n_particles=50_000, sigma_pos=1.0, sigma_cb=300.0, sigma_pr=5.0, resampling="systematic", seed=SEED)
+        pf.initialize(position_ecef=ORIGIN, clock_bias=ORIGIN_CB, spread_pos=80.0, spread_cb=200.0)
+        s0 = pf.get_position_spread(center=ORIGIN)
+        pf.update(sat, pr, w, resample=False)
+        s1 = pf.get_position_spread()
+        assert np.isfinite(s0) and np.isfinite(s1)
+        assert s1 < s0
+
+    def test_per_particle_nlos_gate_skips_outlier_residuals(self, PFD):
+        sat, pr, w = _origin_sats(5)
+        out = pr.copy()
+        out[0] += 100.0
+        kw = dict(n_particles=1024, sigma_pos=1.0, sigma_cb=300.0, sigma_pr=5.0, resampling="systematic", seed=SEED,
+                  per_particle_nlos_gate=True, per_particle_nlos_undiff_pr_threshold_m=30.0)
+        pf = PFD(**kw)
+        pf.initialize(ORIGIN, clock_bias=ORIGIN_CB, spread_pos=0.0, spread_cb=0.0)
+        pf.update(sat, out, w, resample=False)
+        assert float(np.max(np.abs(pf.get_log_weights()))) < 1e-6
+        pf2 = PFD(**kw)
+        pf2.initialize(ORIGIN, clock_bias=ORIGIN_CB, spread_pos=0.0, spread_cb=0.0)
+        pf2.update(sat, pr + 100.0, w, resample=False)
+        assert float(np.max(pf2.get_log_weights())) < -900.0
+
+    def test_per_particle_huber_softens_outlier_cost_without_rejecting(self, PFD):
+        sat, pr, w = _origin_sats(5)
+        out = pr.copy()
+        out[0] += 100.0
+
+        def lw0(huber):
+            pf = PFD(n_particles=1024, sigma_pos=1.0, sigma_cb=300.0, sigma_pr=5.0, resampling="systematic",
+                     seed=SEED, per_particle_huber=huber, per_particle_huber_undiff_pr_k=1.5)
+            pf.initialize(ORIGIN, clock_bias=ORIGIN_CB, spread_pos=0.0, spread_cb=0.0)
+            pf.update(sat, out, w, resample=False)
+            return float(pf.get_log_weights()[0])
+
+        g, h = lw0(False), lw0(True)
+        assert g == pytest.approx(-200.0)
+        assert h == pytest.approx(-28.875)
+        assert g < h < 0.0
+
+    def test_get_resample_ancestors_after_systematic(self, PFD):
+        sat, pr, w = _origin_sats()
+        pf = PFD(n_particles=512, sigma_pos=1.0, sigma_cb=300.0, sigma_pr=5.0, resampling="systematic", seed=SEED)
+        pf.initialize(position_ecef=ORIGIN, clock_bias=ORIGIN_CB, spread_pos=50.0, spread_cb=200.0)
+        pf.predict(dt=1.0)
+        pf.update(sat, pr, w)
+        pf._resample()
+        anc = pf.get_resample_ancestors()
+        assert anc.shape == (512,) and anc.dtype == np.int32
+        assert np.all(anc >= 0) and np.all(anc < 512)
+
+    @pytest.mark.parametrize("method", ["systematic", "megopolis"])
+    def test_convergence_near_truth(self, PFD, method):
+        sat, pr, w = _origin_sats()
+        pf = PFD(n_particles=100_000, sigma_pos=1.0, sigma_cb=300.0, sigma_pr=5.0, resampling=method,
+                 ess_threshold=0.5, seed=SEED)
+        pf.initialize(position_ecef=ORIGIN, clock_bias=ORIGIN_CB, spread_pos=20.0, spread_cb=200.0)
+        for _ in range(5):
+            pf.predict(dt=0.0)
+            pf.update(sat, pr, w)
+        assert np.linalg.norm(pf.estimate()[:3] - ORIGIN) < 100.0
+
+    def test_not_built_paths_raise(self, PFD):
+        with pytest.raises(NotImplementedError):
+            PFD(n_particles=1024, sigma_vel=1.0)
+        with pytest.raises(NotImplementedError):
+            PFD(n_particles=1024, rbpf_velocity_kf=True)
+        pf = PFD(n_particles=1024)
+        with pytest.raises(RuntimeError):
+            pf.predict()
+        pf.initialize(ORIGIN, clock_bias=ORIGIN_CB)
+        for name in ("update_dd_pseudorange", "update_carrier_afv", "update_dd_carrier_afv", "update_doppler",
+                     "update_doppler_kf", "store_epoch", "smooth"):
+            with pytest.raises(NotImplementedError):
+                getattr(pf, name)(None)
+        with pytest.raises(RuntimeError):
+            pf.get_resample_ancestors()  # megopolis
+
+
+# ------------------------------------------------------ FP64 parity
+LIKELIHOODS = [
+    ("gaussian", dict(), dict(kind="gaussian")),
+    ("student_t", dict(nu=4.0), dict(kind="student_t", nu=4.0)),
+    ("huber", dict(per_particle_huber=True, per_particle_huber_undiff_pr_k=1.5), dict(kind="huber", huber_k=1.5)),
+    ("gate", dict(per_particle_nlos_gate=True, per_particle_nlos_undiff_pr_threshold_m=20.0),
+     dict(kind="gaussian", gate_m=20.0)),
+    ("student_t_gate", dict(nu=3.0, per_particle_nlos_gate=True, per_particle_nlos_undiff_pr_threshold_m=25.0),
+     dict(kind="student_t", nu=3.0, gate_m=25.0)),
+]
+
+
+def _nlos_pr(seed=9):
+    rng = np.random.default_rng(seed)
+    pr = TOKYO_PR.copy()
+    pr[[1, 4]] += rng.uniform(20.0, 60.0, 2)  # two NLOS delays
+    w = rng.uniform(0.5, 2.0, len(pr))
+    return pr, w
+
+
+@pytest.mark.parametrize("name,ctor,lik", LIKELIHOODS, ids=[l[0] for l in LIKELIHOODS])
+@pytest.mark.parametrize("method", ["systematic", "megopolis"])
+def test_update_log_weights_match_oracle(PFD, name, ctor, lik, method):
+    pr, w = _nlos_pr()
+    pf = PFD(n_particles=60_000, sigma_pos=2.0, sigma_cb=3.0, sigma_pr=5.0, resampling=method, seed=7, **ctor)
+    pf.initialize(TOKYO_TRUE_POS + 15.0, clock_bias=TOKYO_TRUE_CB, spread_pos=40.0, spread_cb=30.0)
+    for t in range(3):
+        pf.predict(velocity=np.array([1.0, -0.5, 0.2]), dt=1.0)
+        pf.update(TOKYO_SATS, pr, w, resample=(t < 2))
+        if t == 2:
+            x, anchor, clk, rot = _cloud(pf)
+            rows = np.column_stack([TOKYO_SATS, pr, w])
+            want, res = O.weight_generic(x, anchor, clk, rot, rows, 5.0, **lik)
+            got = pf.get_log_weights()
+            ok, rel = lw_close(got, want)
+            if lik.get("gate_m", 0.0) > 0.0:
+                # particles with a residual within 2 cm of the gate may fall
+                # either side in FP32
+                ok |= np.any(np.abs(np.abs(res) - lik["gate_m"]) < 0.02, axis=0)
+                assert np.mean(ok) == 1.0
+            assert ok.all(), f"{name}: worst {rel.max():.2e}"
+            # estimate and ESS of the same weights
+            pos = anchor[None, :] + x[:3].T @ rot
+            wt = np.exp(want - want.max())
+            est = np.concatenate([(wt[:, None] * pos).sum(0), [(wt * (clk[0] + x[3])).sum()]]) / wt.sum()
+            assert np.max(np.abs(pf.estimate() - est)) <= EST_TOL_M
+            ess = wt.sum() ** 2 / (wt * wt).sum()
+            assert pf.get_ess() == pytest.approx(ess, rel=ESS_RTOL)
+
+
+def test_update_gmm_log_weights_match_oracle(PFD):
+    pr, w = _nlos_pr(3)
+    pf = PFD(n_particles=50_000, sigma_pos=2.0, sigma_cb=3.0, sigma_pr=4.0, resampling="systematic", seed=11)
+    pf.initialize(TOKYO_TRUE_POS, clock_bias=TOKYO_TRUE_CB, spread_pos=30.0, spread_cb=20.0)
+    pf.predict(dt=1.0)
+    pf.update_gmm(TOKYO_SATS, pr, w, w_los=0.8, mu_nlos=20.0, sigma_nlos=25.0, resample=False)
+    x, anchor, clk, rot = _cloud(pf)
+    want, _ = O.weight_generic(x, anchor, clk, rot, np.column_stack([TOKYO_SATS, pr, w]), 4.0, kind="gmm",
+                               w_los=0.8, mu_nlos=20.0, sigma_nlos=25.0)
+    ok, rel = lw_close(pf.get_log_weights(), want)
+    assert ok.all(), f"worst {rel.max():.2e}"
+
+
+def test_sigma_pr_override_and_zero_weight_satellite(PFD):
+    pr, w = _nlos_pr(4)
+    w[2] = 0.0
+    pf = PFD(n_particles=20_000, sigma_pr=5.0, nu=5.0, seed=3)
+    pf.initialize(TOKYO_TRUE_POS, clock_bias=TOKYO_TRUE_CB, spread_pos=20.0, spread_cb=20.0)
+    pf.update(TOKYO_SATS, pr, w, sigma_pr=2.5, resample=False)
+    x, anchor, clk, rot = _cloud(pf)
+    want, _ = O.weight_generic(x, anchor, clk, rot, np.column_stack([TOKYO_SATS, pr, w]), 2.5, kind="student_t",
+                               nu=5.0)
+    ok, rel = lw_close(pf.get_log_weights(), want)
+    assert ok.all(), f"worst {rel.max():.2e}"
+
+
+# ------------------------------------------------ position terms, shifts
+def _weighted(pf, n=40_000, seed=5):
+    pf.initialize(TOKYO_TRUE_POS, clock_bias=TOKYO_TRUE_CB, spread_pos=25.0, spread_cb=15.0)
+    pf.predict(dt=1.0)
+    pf.update(TOKYO_SATS, TOKYO_PR, None, resample=False)
+    return pf
+
+
+def test_position_update_matches_oracle(PFD):
+    pf = _weighted(PFD(n_particles=40_000, resampling="systematic", seed=2))
+    before = pf.get_log_weights()
+    p = pf.get_particles()
+    ref = TOKYO_TRUE_POS + np.array([3.0, -4.0, 2.0])
+    pf.position_update(ref, sigma_pos=30.0)
+    want = before - 0.5 * np.sum((p[:, :3] - ref) ** 2, axis=1) / 900.0
+    ok, rel = lw_close(pf.get_log_weights(), want)
+    assert ok.all(), f"worst {rel.max():.2e}"
+    wt = np.exp(want - want.max())
+    assert pf.get_ess() == pytest.approx(wt.sum() ** 2 / (wt * wt).sum(), rel=ESS_RTOL)
+    est = (wt[:, None] * p).sum(0) / wt.sum()
+    assert np.max(np.abs(pf.estimate() - est)) <= EST_TOL_M
+
+
+@pytest.mark.parametrize("K", [1, 3, 8, 40])
+def test_position_mixture_update_matches_oracle(PFD, K):
+    pf = _weighted(PFD(n_particles=40_000, resampling="systematic", seed=4))
+    before = pf.get_log_weights()
+    p = pf.get_particles()
+    rng = np.random.default_rng(K)
+    refs = TOKYO_TRUE_POS + rng.normal(0, 10.0, (K, 3))
+    mix = rng.uniform(0.0, 1.0, K)
+    if K > 1:
+        mix[0] = 0.0  # a zero-weight component
+    pf.position_mixture_update(refs, sigma_pos=6.0, mixture_weights=mix)
+    m = mix / mix.sum()
+    with np.errstate(divide="ignore"):
+        comp = np.log(m)[None, :] - 0.5 * np.sum((p[:, None, :3] - refs[None]) ** 2, axis=2) / 36.0
+    mx = comp.max(1)
+    want = before + mx + np.log(np.exp(comp - mx[:, None]).sum(1))
+    ok, rel = lw_close(pf.get_log_weights(), want)
+    assert ok.all(), f"worst {rel.max():.2e}"
+
+
+def test_position_update_after_resample_and_resample_if_needed(PFD):
+    pf = PFD(n_particles=30_000, resampling="systematic", seed=8, ess_threshold=0.5)
+    pf.initialize(TOKYO_TRUE_POS, clock_bias=TOKYO_TRUE_CB, spread_pos=60.0, spread_cb=30.0)
+    pf.update(TOKYO_SATS, TOKYO_PR, None)            # resamples: weights reset
+    assert pf.get_ess() == pytest.approx(30_000.0)
+    assert np.all(pf.get_log_weights() == 0.0)
+    p = pf.get_particles()
+    ref = TOKYO_TRUE_POS + np.array([20.0, 0.0, 0.0])
+    pf.position_update(ref, sigma_pos=2.0)            # sharp: ESS falls
+    want = -0.5 * np.sum((p[:, :3] - ref) ** 2, axis=1) / 4.0
+    ok, rel = lw_close(pf.get_log_weights(), want)
+    assert ok.all(), f"worst {rel.max():.2e}"
+    wt = np.exp(want - want.max())
+    ess = wt.sum() ** 2 / (wt * wt).sum()
+    assert ess < 15_000
+    assert pf.get_ess() == pytest.approx(ess, rel=ESS_RTOL)
+    assert pf.resample_if_needed() is True
+    assert pf.get_ess() == pytest.approx(30_000.0)
+    anc = pf.get_resample_ancestors()
+    np.testing.assert_array_equal(np.sort(anc), anc)  # systematic: ancestors ascending
+    np.testing.assert_allclose(pf.get_particles(), p[anc], atol=1e-4)  # FP32 offsets re-centred
+    assert pf.resample_if_needed() is False
+
+
+def test_shifts_move_every_particle(PFD):
+    pf = _weighted(PFD(n_particles=20_000, resampling="megopolis", seed=6))
+    p0 = pf.get_particles()
+    lw0 = pf.get_log_weights()
+    pf.shift_clock_bias(12.5)
+    p1 = pf.get_particles()
+    np.testing.assert_allclose(p1[:, 3] - p0[:, 3], 12.5, atol=1e-6)
+    np.testing.assert_allclose(p1[:, :3], p0[:, :3], atol=1e-9)
+    est = pf.estimate()
+    target = est[:3] + np.array([5.0, -3.0, 1.0])
+    norm, applied = pf.recenter_position(target, max_shift_m=100.0)
+    assert applied and norm == pytest.approx(np.sqrt(35.0), rel=1e-9)
+    np.testing.assert_allclose(pf.estimate()[:3], target, atol=EST_TOL_M)
+    norm, applied = pf.recenter_position(target + 1e4, max_shift_m=100.0)
+    assert not applied
+    assert pf.recenter_position(np.array([np.nan, 0.0, 0.0])) == (float("inf"), False)
+    np.testing.assert_array_equal(pf.get_log_weights(), lw0)
+    # clock re-centring on the residual median at the estimate
+    est = pf.estimate()
+    res = TOKYO_PR - np.linalg.norm(TOKYO_SATS - est[:3], axis=1)
+    pf.correct_clock_bias(TOKYO_SATS, TOKYO_PR, quantile=0.5)
+    assert pf.estimate()[3] == pytest.approx(np.median(res), abs=EST_TOL_M)
+
+
+def test_state_and_weight_roundtrip(PFD):
+    pf = _weighted(PFD(n_particles=10_000, resampling="systematic", seed=12))
+    rng = np.random.default_rng(1)
+    st = np.zeros((10_000, 16))
+    st[:, :3] = TOKYO_TRUE_POS + rng.normal(0, 30.0, (10_000, 3))
+    st[:, 3] = TOKYO_TRUE_CB + rng.normal(0, 10.0, 10_000)
+    pf.set_particle_states(st)
+    assert np.all(pf.get_log_weights() == 0.0)
+    assert pf.get_ess() == pytest.approx(10_000.0)
+    np.testing.assert_allclose(pf.get_particles(), st[:, :4], atol=1e-4)
+    np.testing.assert_allclose(pf.get_particle_states()[:, 4:], 0.0)
+    lw = rng.normal(0, 2.0, 10_000)
+    lw[:10] = -np.inf
+    pf.set_log_weights(lw)
+    got = pf.get_log_weights()
+    np.testing.assert_array_equal(got[:10], -np.inf)
+    np.testing.assert_allclose(got[10:], lw[10:].astype(np.float32), rtol=0, atol=0)
+    wt = np.exp(lw - lw.max())
+    assert pf.get_ess() == pytest.approx(wt.sum() ** 2 / (wt * wt).sum(), rel=ESS_RTOL)
+    c = TOKYO_TRUE_POS + np.array([4.0, 4.0, -2.0])
+    want = np.sqrt(np.sum(wt * np.sum((st[:, :3] - c) ** 2, axis=1)) / wt.sum())
+    assert pf.get_position_spread(center=c) == pytest.approx(want, rel=1e-5)
+    est = (wt[:, None] * st[:, :4]).sum(0) / wt.sum()
+    np.testing.assert_allclose(pf.estimate(), est, atol=EST_TOL_M)
+    want0 = np.sqrt(np.sum(wt * np.sum((st[:, :3] - est[:3]) ** 2, axis=1)) / wt.sum())
+    assert pf.get_position_spread() == pytest.approx(want0, rel=1e-5)
+    # the filter steps on from the restored state
+    pf.predict(dt=1.0)
+    pf.update(TOKYO_SATS, TOKYO_PR)
+    assert np.all(np.isfinite(pf.estimate()))
+    with pytest.raises(ValueError):
+        pf.set_particle_states(st[:10])
+    with pytest.raises(ValueError):
+        pf.set_log_weights(lw[:10])
