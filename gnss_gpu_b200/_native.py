@@ -22,6 +22,8 @@ PF_NOALLOC_MAX_PARTICLES = 1 << 22
 PF_RESAMPLE_SYSTEMATIC, PF_RESAMPLE_MEGOPOLIS = 0, 1
 PF_WEIGHT_GAUSSIAN, PF_WEIGHT_HUBER, PF_WEIGHT_MIXTURE, PF_WEIGHT_GENERIC = 0, 1, 2, 3
 PF_LIK_GAUSSIAN, PF_LIK_STUDENT_T, PF_LIK_HUBER, PF_LIK_GMM = 0, 1, 2, 3
+PF_OBS_DD_PSEUDORANGE, PF_OBS_CARRIER_AFV, PF_OBS_DD_CARRIER_AFV = 0, 1, 2
+PF_MAX_OBS_ROWS = 128
 PF_LW_OVERWRITE, PF_LW_ACCUMULATE = 0, 1
 PF_SYS_OFFSET_RANDOM, PF_SYS_OFFSET_REFERENCE = 0, 1
 PF_FLAG_COVARIANCE, PF_FLAG_RECENTER, PF_FLAG_KERNEL_CHAIN = 1, 2, 4
@@ -63,6 +65,11 @@ class Likelihood(C.Structure):
                 ("w_los", C.c_double), ("mu_nlos", C.c_double), ("sigma_nlos", C.c_double), ("gate_m", C.c_double)]
 
 
+# pf_obs_row_t
+OBS_ROW_DTYPE = np.dtype([("sat_k", "<f8", 3), ("sat_ref", "<f8", 3), ("obs", "<f8"), ("base_k", "<f8"),
+                          ("base_ref", "<f8"), ("weight", "<f8"), ("wavelength", "<f8")])
+
+
 class FilterResult(C.Structure):
     _fields_ = [
         ("est_ecef", C.c_double * 3), ("est_clk", C.c_double * PF_MAX_CLK), ("cov_enu", C.c_double * 6),
@@ -93,7 +100,7 @@ EXPORTED = [
     "pfe_read_timing", "pfe_result_bytes", "pfe_read_timing_kernels",
     "pf_mlp_param_count", "pf_mlp_scratch_bytes", "pf_mlp_grad", "pf_mlp_adam_step", "pf_mlp_forward",
     "pfe_set_mlp", "pfe_get_sat_debug", "pfe_set_epoch_ctas_per_sm", "pfe_set_likelihood", "pfe_shift",
-    "pfe_add_position_term",
+    "pfe_add_position_term", "pfe_add_obs_term",
 ]
 
 _lib = None
@@ -168,6 +175,7 @@ def load():
     L.pfe_set_likelihood.argtypes = [p, C.POINTER(Likelihood)]
     L.pfe_shift.argtypes = [p, i, dp, dp]
     L.pfe_add_position_term.argtypes = [p, i, dp, dp, i, d]
+    L.pfe_add_obs_term.argtypes = [p, i, i, C.c_void_p, i, d, d, d, i]
     L.pfe_get_sat_debug.argtypes = [p, i, p, i, C.POINTER(C.c_int)]
     for name in EXPORTED:
         fn = getattr(L, name)

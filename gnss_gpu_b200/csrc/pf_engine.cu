@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "pf_epoch_kernel.cuh"
+#include "pf_obs_terms.cuh"
 #include "pf_status.h"
 
 using namespace pfb;
@@ -45,6 +46,7 @@ struct pf_engine {
   int epoch_cap = 0;          // > 0: at most this many CTAs per launch of the epoch kernel (tuning)
   size_t epoch_smem = 0;      // its dynamic shared memory
   unsigned* bar = nullptr;    // grid barrier words (count, generation, any-resample)
+  ObsRow* obs_rows = nullptr; // rows of pfe_add_obs_term
   int sm_count = 0;
   int last_launches = 0;
   std::vector<int> initialized;
@@ -67,7 +69,7 @@ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
   size_t off_state0, off_state1, off_lw, off_anc, off_offs, off_mp, off_part, off_agg, off_inc,
-      off_flag, off_excl, off_wq, off_wsum, off_chunks, off_fmax, off_mlp, off_satdbg, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
+      off_flag, off_excl, off_wq, off_wsum, off_chunks, off_fmax, off_mlp, off_satdbg, off_obsrows, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
       total;
   size_t obs_slot_bytes;
   size_t max_chunks;
@@ -156,6 +158,7 @@ Layout make_layout(const pf_engine_config_t* cfg, const pf_filter_params_t* fp) 
   const bool mix = cfg->weight_mode == PF_WEIGHT_MIXTURE;
   L.off_mlp = take(mix ? (size_t)kMlpParams * 4 : 0);
   L.off_satdbg = take(mix ? (size_t)cfg->n_filters * cfg->max_sats * kSatDbg * 4 : 0);
+  L.off_obsrows = take(sizeof(ObsRow) * kMaxObsRows);
   L.off_desc = take(sizeof(FilterDesc) * cfg->n_filters);
   L.off_ctrl = take(sizeof(FilterCtrl) * cfg->n_filters);
   L.off_tf = take((size_t)T * 4);
@@ -491,6 +494,7 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
   e.fmax = (unsigned*)(w + L.off_fmax);
   e.mlp = (const float*)(w + L.off_mlp);
   e.sat_dbg = (float*)(w + L.off_satdbg);
+  eng->obs_rows = (ObsRow*)(w + L.off_obsrows);
   eng->desc_dev = (FilterDesc*)(w + L.off_desc);
   eng->ctrl_dev = (FilterCtrl*)(w + L.off_ctrl);
   e.desc = eng->desc_dev;
@@ -1201,6 +1205,81 @@ int pfe_add_position_term(pf_engine_t* eng, int filter, const double* refs_ecef,
   }
   CK(cudaGetLastError());
   // the weights are explicit now
+  const int zero = 0;
+  CK(cudaMemcpyAsync(reinterpret_cast<char*>(eng->ctrl_dev + filter) + offsetof(FilterCtrl, lw_zero), &zero,
+                     sizeof(int), cudaMemcpyHostToDevice, eng->stream));
+  CK(cudaStreamSynchronize(eng->stream));
+  return PF_OK;
+}
+
+int pfe_add_obs_term(pf_engine_t* eng, int filter, int kind, const pf_obs_row_t* rows, int n_rows, double sigma,
+                     double gate, double huber_k, int accumulate) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!eng->initialized[filter]) return set_err(PF_ENOTINIT, "filter %d not initialized", filter);
+  if (kind < PF_OBS_DD_PSEUDORANGE || kind > PF_OBS_DD_CARRIER_AFV) return set_err(PF_EINVAL, "unknown kind %d", kind);
+  if (n_rows < 0 || n_rows > kMaxObsRows) return set_err(PF_ECAP, "need 0..%d rows", kMaxObsRows);
+  if (n_rows > 0 && !rows) return set_err(PF_EINVAL, "null rows");
+  if (!(sigma > 0.0) || !isfinite(sigma)) return set_err(PF_EINVAL, "sigma must be > 0");
+  if (!(gate >= 0.0) || !isfinite(gate)) return set_err(PF_EINVAL, "gate must be finite and >= 0");
+  if (kind == PF_OBS_CARRIER_AFV && gate > 0.0) return set_err(PF_EINVAL, "the undifferenced carrier term has no gate");
+  if (!(huber_k >= 0.0) || !isfinite(huber_k)) return set_err(PF_EINVAL, "huber_k must be finite and >= 0");
+  if ((s = read_ctrl(eng)) != PF_OK) return s;
+  const FilterCtrl& c = eng->ctrl_host[filter];
+  const FilterDesc& d = eng->hdesc[filter];
+  std::vector<ObsRow> host((size_t)std::max(n_rows, 1));
+  const bool dd = kind != PF_OBS_CARRIER_AFV;
+  for (int i = 0; i < n_rows; ++i) {
+    const pf_obs_row_t& r = rows[i];
+    bool ok = isfinite(r.obs) && isfinite(r.weight);
+    for (int j = 0; j < 3; ++j) ok = ok && isfinite(r.sat_k[j]) && (!dd || isfinite(r.sat_ref[j]));
+    if (dd) ok = ok && isfinite(r.base_k) && isfinite(r.base_ref);
+    if (!ok) return set_err(PF_EINVAL, "row %d not finite", i);
+    const bool carrier = kind != PF_OBS_DD_PSEUDORANGE;
+    if (carrier && !(r.wavelength > 0.0 && isfinite(r.wavelength)))
+      return set_err(PF_EINVAL, "row %d: wavelength must be > 0", i);
+    ObsRow& o = host[i];
+    memset(&o, 0, sizeof(o));
+    double vk[3], vr[3];
+    for (int j = 0; j < 3; ++j) {
+      vk[j] = r.sat_k[j] - c.anchor[j];
+      vr[j] = dd ? r.sat_ref[j] - c.anchor[j] : 0.0;
+    }
+    for (int q = 0; q < 3; ++q) {
+      o.sk[q] = d.rot[3 * q] * vk[0] + d.rot[3 * q + 1] * vk[1] + d.rot[3 * q + 2] * vk[2];
+      o.sr[q] = d.rot[3 * q] * vr[0] + d.rot[3 * q + 1] * vr[1] + d.rot[3 * q + 2] * vr[2];
+    }
+    o.w = r.weight;
+    o.inv_wl = carrier ? 1.0 / r.wavelength : 1.0;
+    if (kind == PF_OBS_DD_PSEUDORANGE)
+      o.c = r.obs + r.base_k - r.base_ref;
+    else if (kind == PF_OBS_CARRIER_AFV)
+      o.c = r.obs - c.clk_anchor[0] * o.inv_wl;
+    else
+      o.c = r.obs + (r.base_k - r.base_ref) * o.inv_wl;
+  }
+  if (n_rows == 0 && accumulate) return PF_OK;
+  ObsBlock b;
+  memset(&b, 0, sizeof(b));
+  b.n = n_rows;
+  b.kind = kind;
+  b.accumulate = accumulate ? 1 : 0;
+  b.gate_min = std::min(n_rows, 3);
+  b.inv_sigma2 = 1.0 / (sigma * sigma);
+  b.inv_sigma = 1.0 / sigma;
+  b.gate = gate;
+  b.huber_k = huber_k;
+  if (n_rows > 0)
+    CK(cudaMemcpyAsync(eng->obs_rows, host.data(), sizeof(ObsRow) * n_rows, cudaMemcpyHostToDevice, eng->stream));
+  const int g = std::max(1, std::min(eng->sm_count * 4, (d.n + kTile - 1) / kTile));
+  switch (eng->D) {
+    case 4: k_obs_term<4><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, b, eng->obs_rows); break;
+    case 5: k_obs_term<5><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, b, eng->obs_rows); break;
+    case 6: k_obs_term<6><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, b, eng->obs_rows); break;
+    default: k_obs_term<7><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, b, eng->obs_rows); break;
+  }
+  CK(cudaGetLastError());
   const int zero = 0;
   CK(cudaMemcpyAsync(reinterpret_cast<char*>(eng->ctrl_dev + filter) + offsetof(FilterCtrl, lw_zero), &zero,
                      sizeof(int), cudaMemcpyHostToDevice, eng->stream));

@@ -206,6 +206,15 @@ class Engine:
                                                None if lp is None else lp.ctypes.data_as(C.POINTER(C.c_double)),
                                                len(refs), float(sigma)))
 
+    def add_obs_term(self, k: int, kind: int, rows, sigma: float, gate: float = 0.0, huber_k: float = 0.0,
+                     accumulate: bool = True):
+        """Differenced / carrier-phase observation term over filter k's
+        current particles (FP64 on the device).  rows: structured array of
+        N.OBS_ROW_DTYPE."""
+        r = np.ascontiguousarray(rows, dtype=N.OBS_ROW_DTYPE)
+        N.check(self.lib.pfe_add_obs_term(self.h, int(k), int(kind), N.vptr(r) if len(r) else None, len(r),
+                                          float(sigma), float(gate), float(huber_k), 1 if accumulate else 0))
+
     def set_mlp(self, params):
         """Upload the NLOS network's parameters (mixture mode)."""
         prm = np.ascontiguousarray(params, dtype=np.float32)

@@ -17,10 +17,12 @@ methods on the engine's sm_100a kernels (weight mode "generic"):
 * resample_if_needed() tests the ESS of the current weights on the device
   and resamples when needed.
 
+* update_dd_pseudorange(), update_carrier_afv(), update_dd_carrier_afv()
+  evaluate the differenced / carrier-phase terms in FP64 on the device.
+
 Not built: the velocity states (sigma_vel > 0, velocity_guide_alpha != 1,
-rbpf_velocity_kf), the double-difference / carrier-phase / Doppler
-likelihoods and the forward-backward smoother; their methods raise
-NotImplementedError.
+rbpf_velocity_kf), the Doppler likelihoods that need them and the
+forward-backward smoother; their methods raise NotImplementedError.
 """
 from __future__ import annotations
 
@@ -86,15 +88,22 @@ class ParticleFilterDevice:
         if not self._initialized:
             raise RuntimeError("ParticleFilterDevice not initialized. Call initialize() first.")
 
-    def _gate(self):
+    def _per_particle_threshold(self, value):
         if not self.per_particle_nlos_gate:
             return 0.0
-        v = self.per_particle_nlos_undiff_pr_threshold_m
-        return v if np.isfinite(v) and v > 0.0 else 0.0
+        value = float(value)
+        return value if np.isfinite(value) and value > 0.0 else 0.0
+
+    @staticmethod
+    def _per_particle_huber_k(value):
+        value = float(value)
+        return value if np.isfinite(value) and value > 0.0 else 1.5
+
+    def _gate(self):
+        return self._per_particle_threshold(self.per_particle_nlos_undiff_pr_threshold_m)
 
     def _huber_k(self):
-        v = self.per_particle_huber_undiff_pr_k
-        return v if np.isfinite(v) and v > 0.0 else 1.5
+        return self._per_particle_huber_k(self.per_particle_huber_undiff_pr_k)
 
     def _spec_for(self, sigma_pos, sigma_pr):
         sp = float(self.sigma_pos if sigma_pos is None else sigma_pos)
@@ -205,14 +214,65 @@ class ParticleFilterDevice:
         self._weight(sat_ecef, pseudoranges, weights, sigma_pr, resample, kind="gmm", w_los=float(w_los),
                      mu_nlos=float(mu_nlos), sigma_nlos=float(sigma_nlos))
 
-    def update_dd_pseudorange(self, *a, **k):
-        raise NotImplementedError("double-difference pseudorange likelihood is not built")
+    @staticmethod
+    def _dd_rows(dd_result, obs, wavelengths=None):
+        n = int(dd_result.n_dd)
+        rows = np.zeros(n, N.OBS_ROW_DTYPE)
+        rows["sat_k"] = np.asarray(dd_result.sat_ecef_k, dtype=np.float64).reshape(-1, 3)[:n]
+        rows["sat_ref"] = np.asarray(dd_result.sat_ecef_ref, dtype=np.float64).reshape(-1, 3)[:n]
+        rows["obs"] = np.asarray(obs, dtype=np.float64).ravel()[:n]
+        rows["base_k"] = np.asarray(dd_result.base_range_k, dtype=np.float64).ravel()[:n]
+        rows["base_ref"] = np.asarray(dd_result.base_range_ref, dtype=np.float64).ravel()[:n]
+        rows["weight"] = np.asarray(dd_result.dd_weights, dtype=np.float64).ravel()[:n]
+        rows["wavelength"] = 1.0 if wavelengths is None else np.asarray(wavelengths, dtype=np.float64).ravel()[:n]
+        return rows
 
-    def update_carrier_afv(self, *a, **k):
-        raise NotImplementedError("carrier-phase AFV likelihood is not built")
+    def _obs_update(self, kind, rows, sigma, gate, huber_k, accumulate, resample):
+        self._require_init()
+        self._flush()
+        self._engine.add_obs_term(0, kind, rows, sigma, gate, huber_k, accumulate)
+        if resample:
+            self.resample_if_needed()
 
-    def update_dd_carrier_afv(self, *a, **k):
-        raise NotImplementedError("double-difference carrier-phase likelihood is not built")
+    def update_dd_pseudorange(self, dd_result, sigma_pr=0.75, resample=True):
+        """Double-differenced pseudorange likelihood (clock-free); overwrites
+        the log-weights (pf_device.cu:282-368).  dd_result: the reference's
+        DDPseudorangeResult fields (sat_ecef_k, sat_ecef_ref,
+        dd_pseudorange_m, base_range_k, base_range_ref, dd_weights, n_dd)."""
+        rows = self._dd_rows(dd_result, dd_result.dd_pseudorange_m)
+        huber = self._per_particle_huber_k(self.per_particle_huber_dd_pr_k) if self.per_particle_huber else 0.0
+        self._obs_update(N.PF_OBS_DD_PSEUDORANGE, rows, float(sigma_pr),
+                         self._per_particle_threshold(self.per_particle_nlos_dd_pr_threshold_m), huber, False,
+                         resample)
+
+    def update_carrier_afv(self, sat_ecef, carrier_phase_cycles, weights=None, wavelength=0.190293673,
+                           sigma_cycles=0.05, resample=True):
+        """Carrier-phase ambiguity-function likelihood on the fractional cycle
+        residual; adds to the log-weights (pf_device.cu:439-494)."""
+        sat = np.asarray(sat_ecef, dtype=np.float64).reshape(-1, 3)
+        cp = np.asarray(carrier_phase_cycles, dtype=np.float64).ravel()
+        rows = np.zeros(len(cp), N.OBS_ROW_DTYPE)
+        rows["sat_k"] = sat
+        rows["obs"] = cp
+        rows["weight"] = 1.0 if weights is None else np.asarray(weights, dtype=np.float64).ravel()
+        rows["wavelength"] = float(wavelength)
+        self._obs_update(N.PF_OBS_CARRIER_AFV, rows, float(sigma_cycles), 0.0, 0.0, True, resample)
+
+    def update_dd_carrier_afv(self, dd_result, wavelength=None, sigma_cycles=0.05, resample=True):
+        """Double-differenced carrier-phase AFV likelihood; adds to the
+        log-weights (pf_device.cu:496-604).  Per-pair wavelengths come from
+        dd_result.wavelengths_m unless `wavelength` overrides them."""
+        n = int(dd_result.n_dd)
+        if wavelength is None:
+            wl = getattr(dd_result, "wavelengths_m", None)
+            wl = np.full(n, 0.190293673) if wl is None else np.asarray(wl, dtype=np.float64).ravel()
+        else:
+            wl = np.full(n, float(wavelength))
+        rows = self._dd_rows(dd_result, dd_result.dd_carrier_cycles, wl)
+        huber = self._per_particle_huber_k(self.per_particle_huber_dd_carrier_k) if self.per_particle_huber else 0.0
+        self._obs_update(N.PF_OBS_DD_CARRIER_AFV, rows, float(sigma_cycles),
+                         self._per_particle_threshold(self.per_particle_nlos_dd_carrier_threshold_cycles), huber,
+                         True, resample)
 
     def update_doppler(self, *a, **k):
         raise NotImplementedError("Doppler likelihood is not built")

@@ -169,6 +169,25 @@ typedef struct {
   double sigma_nlos;     /* GMM: std of the NLOS component, m                 */
   double gate_m;         /* > 0: per-particle NLOS gate on |residual|, m      */
 } pf_likelihood_t;
+
+/* Differenced and carrier-phase observation terms (pfe_add_obs_term). */
+typedef enum {
+  PF_OBS_DD_PSEUDORANGE = 0,  /* pf_device.cu:282-368 (m)                    */
+  PF_OBS_CARRIER_AFV = 1,     /* pf_device.cu:439-494 (cycles; uses clock 0)  */
+  PF_OBS_DD_CARRIER_AFV = 2   /* pf_device.cu:496-604 (cycles)                */
+} pf_obs_kind_t;
+
+typedef struct {
+  double sat_k[3];    /* ECEF m: the satellite, or satellite k of a DD pair     */
+  double sat_ref[3];  /* ECEF m: the pair's reference satellite (DD kinds)      */
+  double obs;         /* DD pseudorange (m) / carrier phase / DD carrier (cycles) */
+  double base_k;      /* base-station range to sat_k, m (DD kinds)              */
+  double base_ref;    /* base-station range to sat_ref, m (DD kinds)            */
+  double weight;      /* row weight                                             */
+  double wavelength;  /* m (carrier kinds)                                      */
+} pf_obs_row_t;
+#define PF_MAX_OBS_ROWS 128
+
 typedef enum { PF_LW_OVERWRITE = 0, PF_LW_ACCUMULATE = 1 } pf_lw_mode_t;
 typedef enum {
   PF_SYS_OFFSET_RANDOM = 0,    /* Philox draw per filter and epoch            */
@@ -385,6 +404,17 @@ int pfe_shift(pf_engine_t* eng, int filter, const double dpos_ecef[3], const dou
  * satellites recomputes them and resamples if needed. */
 int pfe_add_position_term(pf_engine_t* eng, int filter, const double* refs_ecef, const double* log_pi,
                           int K, double sigma);
+/* One pass over filter f's current particles (gathered through the last
+ * resample, if any) evaluating n_rows (0..PF_MAX_OBS_ROWS) observation rows
+ * of one kind in FP64: per row -w r^2 / (2 sigma^2), or with huber_k > 0
+ * the Huber cost -w rho_k(|r| / sigma); for the DD kinds gate > 0 drops rows
+ * with |r| > gate unless fewer than min(n_rows, 3) would remain (gate must
+ * be 0 for PF_OBS_CARRIER_AFV).  accumulate != 0 adds the sum to the
+ * current log-weights (the reference's carrier kernels), 0 overwrites them
+ * (its DD pseudorange kernel).  Statistics follow as for
+ * pfe_add_position_term. */
+int pfe_add_obs_term(pf_engine_t* eng, int filter, int kind, const pf_obs_row_t* rows, int n_rows,
+                     double sigma, double gate, double huber_k, int accumulate);
 
 /* Network parameters of PF_WEIGHT_MIXTURE (host array of
  * pf_mlp_param_count() floats, copied to the engine).  Required before the

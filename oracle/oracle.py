@@ -247,6 +247,57 @@ def weight_generic(x, anchor, clk_anchor, rot, sats, sigma_pr, kind="gaussian", 
     return lw, res
 
 
+OBS_DD_PSEUDORANGE, OBS_CARRIER_AFV, OBS_DD_CARRIER_AFV = 0, 1, 2
+
+
+def obs_term(x, anchor, clk_anchor, rot, kind, sat_k, obs, weight, sat_ref=None, base_k=None, base_ref=None,
+             wavelength=None, sigma=1.0, gate=0.0, huber_k=0.0):
+    """FP64 sum over rows of the differenced / carrier-phase terms, per
+    particle, in ECEF as the reference computes them:
+      DD pseudorange   r = dd - (|p - s_k| - |p - s_ref| - b_k + b_ref)        pf_device.cu:282-368
+      carrier AFV      a = afv(cp - (|p - s| + cb) / lambda)                   pf_device.cu:439-494
+      DD carrier AFV   a = afv(dd - (|p - s_k| - |p - s_ref| - b_k + b_ref) / lambda)
+                                                                               pf_device.cu:496-604
+    afv(v) = v - rint(v); cost w r^2 / (2 sigma^2) or the Huber cost
+    (huber_k > 0, pf_device.cu:19-26); DD kinds: gate > 0 drops rows with
+    |r| > gate unless fewer than min(n, 3) remain.  Returns (-sum of costs,
+    residuals (n_rows, n))."""
+    x = _f64(x)
+    pos = _f64(anchor)[None, :] + x[:3].T @ _f64(rot)
+    cb = clk_anchor[0] + x[3]
+    sat_k = _f64(sat_k).reshape(-1, 3)
+    n_rows = len(sat_k)
+    res = np.empty((n_rows, x.shape[1]))
+    for i in range(n_rows):
+        rk = np.linalg.norm(pos - sat_k[i][None, :], axis=1)
+        if kind == OBS_CARRIER_AFV:
+            v = obs[i] - (rk + cb) / wavelength[i]
+            res[i] = v - np.rint(v)
+            continue
+        rr = np.linalg.norm(pos - _f64(sat_ref).reshape(-1, 3)[i][None, :], axis=1)
+        dd_expected = rk - rr - base_k[i] + base_ref[i]
+        if kind == OBS_DD_PSEUDORANGE:
+            res[i] = obs[i] - dd_expected
+        else:
+            v = obs[i] - dd_expected / wavelength[i]
+            res[i] = v - np.rint(v)
+    use = np.ones_like(res, dtype=bool)
+    if gate > 0.0 and kind != OBS_CARRIER_AFV:
+        inside = np.abs(res) <= gate
+        on = inside.sum(axis=0) >= min(n_rows, 3)
+        use = inside | ~on[None, :]
+    lw = np.zeros(x.shape[1])
+    for i in range(n_rows):
+        v = res[i]
+        if huber_k > 0.0:
+            z = np.abs(v) / sigma
+            cost = weight[i] * np.where(z < huber_k, 0.5 * z * z, huber_k * z - 0.5 * huber_k * huber_k)
+        else:
+            cost = 0.5 * weight[i] * v * v / (sigma * sigma)
+        lw -= np.where(use[i], cost, 0.0)
+    return lw, res
+
+
 def stats(x, lw, anchor, clk_anchor, rot):
     x = _f64(x)
     D, n = x.shape

@@ -244,3 +244,53 @@ def test_generic_weight_zero_satellite_contributes_nothing():
         full = _generic(rows, kind=kind, nu=3.0)
         drop = _generic(rows[1:], kind=kind, nu=3.0)
         assert full[0] == pytest.approx(drop[0], abs=1e-12)
+
+
+# ------------------------------------ differenced / carrier-phase terms
+def _dd_case(outlier, carrier=False):
+    """Receiver at the ECEF origin, base 120/-35/18 m away, 5 satellites
+    20,000 km out; pair 0 carries the outlier (reference
+    tests/test_cuda_streams.py:600-660, 694-773)."""
+    rng = np.random.RandomState(123)
+    d = rng.randn(5, 3)
+    sats = d / np.linalg.norm(d, axis=1, keepdims=True) * 20_000_000.0
+    rover = np.zeros(3)
+    base = np.array([120.0, -35.0, 18.0])
+    rr = np.linalg.norm(sats - rover, axis=1)
+    br = np.linalg.norm(sats - base, axis=1)
+    dd = (rr[1:] - rr[0]) - (br[1:] - br[0])
+    wl = np.full(4, 0.190293673)
+    if carrier:
+        dd = dd / wl
+    dd[0] += outlier
+    return dict(sat_k=sats[1:], sat_ref=np.repeat(sats[[0]], 4, axis=0), obs=dd, weight=np.ones(4),
+                base_k=br[1:], base_ref=np.repeat(br[0], 4), wavelength=wl)
+
+
+def _obs(kind, case, **kw):
+    lw, _ = O.obs_term(np.zeros((4, 1)), np.zeros(3), [0.0], np.eye(3), kind, **case, **kw)
+    return lw[0]
+
+
+def test_obs_term_known_answers():
+    pr = _dd_case(50.0)
+    assert _obs(O.OBS_DD_PSEUDORANGE, pr, sigma=0.5) == pytest.approx(-5000.0, rel=1e-9)
+    assert _obs(O.OBS_DD_PSEUDORANGE, pr, sigma=0.5, huber_k=1.5) == pytest.approx(-148.875, rel=1e-9)
+    assert abs(_obs(O.OBS_DD_PSEUDORANGE, pr, sigma=0.5, gate=10.0)) < 1e-6
+    cp = _dd_case(0.45, carrier=True)
+    assert _obs(O.OBS_DD_CARRIER_AFV, cp, sigma=0.05) == pytest.approx(-40.5, abs=1e-6)
+    assert _obs(O.OBS_DD_CARRIER_AFV, cp, sigma=0.05, huber_k=1.5) == pytest.approx(-12.375, abs=1e-6)
+    assert abs(_obs(O.OBS_DD_CARRIER_AFV, cp, sigma=0.05, gate=0.3)) < 1e-6
+    # integer cycle slips leave the fractional residual unchanged
+    slip = dict(cp, obs=cp["obs"] + np.array([0.0, 7.0, -3.0, 120.0]))
+    assert _obs(O.OBS_DD_CARRIER_AFV, slip, sigma=0.05) == pytest.approx(-40.5, abs=1e-6)
+    # undifferenced carrier at the true clock: only the planted fraction costs
+    rng = np.random.RandomState(123)
+    d = rng.randn(5, 3)
+    sats = d / np.linalg.norm(d, axis=1, keepdims=True) * 20_000_000.0
+    wl = np.full(5, 0.190293673)
+    cb = 100.0
+    cyc = (np.linalg.norm(sats, axis=1) + cb) / wl + np.array([0.2, 3.0, -8.0, 0.0, 1e6])
+    lw, _ = O.obs_term(np.zeros((4, 1)), np.zeros(3), [cb], np.eye(3), O.OBS_CARRIER_AFV, sat_k=sats, obs=cyc,
+                       weight=np.ones(5), wavelength=wl, sigma=0.05)
+    assert lw[0] == pytest.approx(-0.5 * 0.2 ** 2 / 0.05 ** 2, abs=1e-5)

@@ -2,6 +2,8 @@
 (tests/test_cuda_streams.py of the reference project, the parts this
 filter models) and FP64 parity of every likelihood, position term, shift
 and statistic with the oracle."""
+from types import SimpleNamespace
+
 import numpy as np
 import pytest
 
@@ -147,6 +149,87 @@ class TestWrapper:
             pf.update(sat, pr, w)
         assert np.linalg.norm(pf.estimate()[:3] - ORIGIN) < 100.0
 
+    @staticmethod
+    def _dd(outlier, carrier=False, n_sat=5):
+        sat, _, _ = _origin_sats(n_sat)
+        base = np.array([120.0, -35.0, 18.0])
+        rr = np.linalg.norm(sat - ORIGIN, axis=1)
+        br = np.linalg.norm(sat - base, axis=1)
+        dd = (rr[1:] - rr[0]) - (br[1:] - br[0])
+        wl = np.full(n_sat - 1, 0.190293673)
+        if carrier:
+            dd = dd / wl
+        dd[0] += outlier
+        return SimpleNamespace(dd_pseudorange_m=dd, dd_carrier_cycles=dd, sat_ecef_k=sat[1:],
+                               sat_ecef_ref=np.repeat(sat[[0]], n_sat - 1, axis=0), base_range_k=br[1:],
+                               base_range_ref=np.repeat(br[0], n_sat - 1), dd_weights=np.ones(n_sat - 1),
+                               wavelengths_m=wl, n_dd=n_sat - 1)
+
+    @pytest.mark.parametrize("huber,want", [(False, -5000.0), (True, -148.875)])
+    def test_dd_pseudorange_huber_known_answers(self, PFD, huber, want):
+        pf = PFD(n_particles=1024, sigma_pos=1.0, sigma_cb=300.0, sigma_pr=5.0, resampling="systematic", seed=SEED,
+                 per_particle_huber=huber, per_particle_huber_dd_pr_k=1.5)
+        pf.initialize(ORIGIN, clock_bias=0.0, spread_pos=0.0, spread_cb=0.0)
+        pf.update_dd_pseudorange(self._dd(50.0), sigma_pr=0.5, resample=False)
+        assert float(pf.get_log_weights()[0]) == pytest.approx(want)
+
+    @pytest.mark.parametrize("huber,want", [(False, -40.5), (True, -12.375)])
+    def test_dd_carrier_huber_known_answers(self, PFD, huber, want):
+        pf = PFD(n_particles=1024, sigma_pos=1.0, sigma_cb=300.0, sigma_pr=5.0, resampling="systematic", seed=SEED,
+                 per_particle_huber=huber, per_particle_huber_dd_carrier_k=1.5)
+        pf.initialize(ORIGIN, clock_bias=0.0, spread_pos=0.0, spread_cb=0.0)
+        pf.update_dd_carrier_afv(self._dd(0.45, carrier=True), sigma_cycles=0.05, resample=False)
+        assert float(pf.get_log_weights()[0]) == pytest.approx(want, abs=1e-5)
+
+    def test_dd_gates_skip_outlier_pairs(self, PFD):
+        kw = dict(n_particles=1024, sigma_pos=1.0, sigma_cb=300.0, sigma_pr=5.0, resampling="systematic", seed=SEED,
+                  per_particle_nlos_gate=True, per_particle_nlos_dd_pr_threshold_m=10.0,
+                  per_particle_nlos_dd_carrier_threshold_cycles=0.3)
+        pf = PFD(**kw)
+        pf.initialize(ORIGIN, clock_bias=0.0, spread_pos=0.0, spread_cb=0.0)
+        pf.update_dd_pseudorange(self._dd(50.0), sigma_pr=0.5, resample=False)
+        assert float(np.max(np.abs(pf.get_log_weights()))) < 1e-6
+        pf2 = PFD(**kw)
+        pf2.initialize(ORIGIN, clock_bias=0.0, spread_pos=0.0, spread_cb=0.0)
+        pf2.update_dd_carrier_afv(self._dd(0.45, carrier=True), sigma_cycles=0.05, resample=False)
+        assert float(np.max(np.abs(pf2.get_log_weights()))) < 1e-6
+
+    def test_update_dd_pseudorange_smoke(self, PFD):
+        rng = np.random.RandomState(321)
+        d = rng.randn(5, 3)
+        sat = d / np.linalg.norm(d, axis=1, keepdims=True) * 20_000_000.0
+        base = np.array([120.0, -35.0, 18.0])
+        rr = np.linalg.norm(sat, axis=1)
+        br = np.linalg.norm(sat - base, axis=1)
+        res = SimpleNamespace(dd_pseudorange_m=(rr[1:] - rr[0]) - (br[1:] - br[0]), sat_ecef_k=sat[1:],
+                              sat_ecef_ref=np.repeat(sat[[0]], 4, axis=0), base_range_k=br[1:],
+                              base_range_ref=np.repeat(br[0], 4), dd_weights=np.ones(4), n_dd=4)
+        pf = PFD(n_particles=50_000, sigma_pos=1.0, sigma_cb=300.0, sigma_pr=5.0, resampling="systematic", seed=SEED)
+        pf.initialize(ORIGIN, clock_bias=250.0, spread_pos=30.0, spread_cb=200.0)
+        pf.update_dd_pseudorange(res, sigma_pr=0.5)
+        pf.sync()
+        est = pf.estimate()
+        assert np.all(np.isfinite(est)) and np.linalg.norm(est[:3]) < 10.0
+
+    def test_update_dd_carrier_afv_smoke(self, PFD):
+        sat = np.array([[20_200_000.0, 0.0, 0.0], [0.0, 21_000_000.0, 0.0], [0.0, 0.0, 20_600_000.0],
+                        [-20_800_000.0, 2_000_000.0, 1_000_000.0]])
+        rover = np.array([0.3, -0.2, 0.1])
+        base = np.array([120.0, -35.0, 18.0])
+        rr = np.linalg.norm(sat - rover, axis=1)
+        br = np.linalg.norm(sat - base, axis=1)
+        wl = np.array([0.190293673, 0.192039486, 0.190293673])
+        refs, ks = np.array([0, 2, 2]), np.array([1, 3, 1])
+        res = SimpleNamespace(dd_carrier_cycles=((rr[ks] - rr[refs]) - (br[ks] - br[refs])) / wl, sat_ecef_k=sat[ks],
+                              sat_ecef_ref=sat[refs], base_range_k=br[ks], base_range_ref=br[refs],
+                              dd_weights=np.ones(3), wavelengths_m=wl, n_dd=3)
+        pf = PFD(n_particles=30_000, sigma_pos=0.1, sigma_cb=300.0, sigma_pr=5.0, resampling="systematic", seed=SEED)
+        pf.initialize(position_ecef=rover, clock_bias=0.0, spread_pos=0.2, spread_cb=10.0)
+        pf.update_dd_carrier_afv(res, sigma_cycles=0.05)
+        pf.sync()
+        est = pf.estimate()
+        assert np.all(np.isfinite(est)) and np.linalg.norm(est[:3] - rover) < 2.0
+
     def test_not_built_paths_raise(self, PFD):
         with pytest.raises(NotImplementedError):
             PFD(n_particles=1024, sigma_vel=1.0)
@@ -156,8 +239,7 @@ class TestWrapper:
         with pytest.raises(RuntimeError):
             pf.predict()
         pf.initialize(ORIGIN, clock_bias=ORIGIN_CB)
-        for name in ("update_dd_pseudorange", "update_carrier_afv", "update_dd_carrier_afv", "update_doppler",
-                     "update_doppler_kf", "store_epoch", "smooth"):
+        for name in ("update_doppler", "update_doppler_kf", "store_epoch", "smooth"):
             with pytest.raises(NotImplementedError):
                 getattr(pf, name)(None)
         with pytest.raises(RuntimeError):
@@ -365,3 +447,110 @@ def test_state_and_weight_roundtrip(PFD):
         pf.set_particle_states(st[:10])
     with pytest.raises(ValueError):
         pf.set_log_weights(lw[:10])
+
+
+# --------------------------------- differenced / carrier terms, FP64 parity
+def _dd_tokyo(rng, n_pairs, carrier=False, nlos=()):
+    base = TOKYO_TRUE_POS + np.array([800.0, -450.0, 30.0])
+    sats = TOKYO_SATS[: n_pairs + 1]
+    rr = np.linalg.norm(sats - TOKYO_TRUE_POS, axis=1)
+    br = np.linalg.norm(sats - base, axis=1)
+    refs = np.zeros(n_pairs, int)
+    ks = np.arange(1, n_pairs + 1)
+    wl = rng.choice([0.190293673, 0.244210213, 0.254828049], n_pairs)
+    dd = (rr[ks] - rr[refs]) - (br[ks] - br[refs])
+    if carrier:
+        dd = dd / wl + rng.normal(0, 0.02, n_pairs) + rng.integers(-50, 50, n_pairs)
+    else:
+        dd = dd + rng.normal(0, 0.5, n_pairs)
+    for i in nlos:
+        dd[i] += 25.0 if not carrier else 0.4
+    return SimpleNamespace(dd_pseudorange_m=dd, dd_carrier_cycles=dd, sat_ecef_k=sats[ks], sat_ecef_ref=sats[refs],
+                           base_range_k=br[ks], base_range_ref=br[refs], dd_weights=rng.uniform(0.5, 2.0, n_pairs),
+                           wavelengths_m=wl, n_dd=n_pairs)
+
+
+def _obs_want(pf, kind, res, obs, sigma, gate=0.0, huber_k=0.0, wl=None):
+    x, anchor, clk, rot = _cloud(pf)
+    return O.obs_term(x, anchor, clk, rot, kind, res.sat_ecef_k, obs, res.dd_weights, res.sat_ecef_ref,
+                      res.base_range_k, res.base_range_ref, wl, sigma, gate, huber_k)
+
+
+def _mask_edges(ok, r, gate, afv):
+    if gate > 0:
+        ok |= np.any(np.abs(np.abs(r) - gate) < 1e-6, axis=0)
+    if afv:
+        ok |= np.any(np.abs(np.abs(r) - 0.5) < 1e-6, axis=0)
+    return ok
+
+
+DD_CASES = [("gauss", dict(), 0.0, 0.0), ("huber", dict(per_particle_huber=True, per_particle_huber_dd_pr_k=1.2), 0.0, 1.2),
+            ("gate", dict(per_particle_nlos_gate=True, per_particle_nlos_dd_pr_threshold_m=8.0), 8.0, 0.0)]
+
+
+@pytest.mark.parametrize("name,ctor,gate,hk", DD_CASES, ids=[c[0] for c in DD_CASES])
+def test_dd_pseudorange_matches_oracle(PFD, name, ctor, gate, hk):
+    rng = np.random.default_rng(21)
+    res = _dd_tokyo(rng, 7, nlos=(2,))
+    pf = PFD(n_particles=40_000, resampling="systematic", seed=5, **ctor)
+    pf.initialize(TOKYO_TRUE_POS, clock_bias=TOKYO_TRUE_CB, spread_pos=15.0, spread_cb=20.0)
+    pf.predict(dt=1.0)
+    pf.update(TOKYO_SATS, TOKYO_PR, None, resample=True)     # a gathered cloud underneath
+    pf.update_dd_pseudorange(res, sigma_pr=0.8, resample=False)
+    want, r = _obs_want(pf, O.OBS_DD_PSEUDORANGE, res, res.dd_pseudorange_m, 0.8, gate, hk)
+    ok, rel = lw_close(pf.get_log_weights(), want, rtol=1e-6)
+    ok = _mask_edges(ok, r, gate, False)
+    assert ok.all(), f"worst {rel.max():.2e}"
+
+
+@pytest.mark.parametrize("gate,hk", [(0.0, 0.0), (0.25, 0.0), (0.0, 1.5)])
+def test_dd_carrier_accumulates_and_matches_oracle(PFD, gate, hk):
+    rng = np.random.default_rng(22)
+    res = _dd_tokyo(rng, 7, carrier=True, nlos=(4,))
+    ctor = dict(per_particle_nlos_gate=gate > 0, per_particle_nlos_dd_carrier_threshold_cycles=gate or 0.5,
+                per_particle_huber=hk > 0, per_particle_huber_dd_carrier_k=hk or 1.5)
+    pf = PFD(n_particles=40_000, resampling="megopolis", seed=6, **ctor)
+    pf.initialize(TOKYO_TRUE_POS, clock_bias=TOKYO_TRUE_CB, spread_pos=0.5, spread_cb=5.0)
+    pf.update(TOKYO_SATS, TOKYO_PR, None, resample=False)
+    before = pf.get_log_weights()
+    pf.update_dd_carrier_afv(res, sigma_cycles=0.05, resample=False)
+    term, r = _obs_want(pf, O.OBS_DD_CARRIER_AFV, res, res.dd_carrier_cycles, 0.05, gate, hk, res.wavelengths_m)
+    ok, rel = lw_close(pf.get_log_weights(), before + term)
+    ok = _mask_edges(ok, r, gate, True)
+    assert ok.all(), f"worst {rel.max():.2e}"
+
+
+def test_carrier_afv_matches_oracle_and_resamples(PFD):
+    rng = np.random.default_rng(23)
+    wl = 0.190293673
+    rng_true = np.linalg.norm(TOKYO_SATS - TOKYO_TRUE_POS, axis=1)
+    cyc = (rng_true + TOKYO_TRUE_CB) / wl + rng.normal(0, 0.02, len(rng_true)) + rng.integers(-1_000_000, 1_000_000, len(rng_true))
+    w = rng.uniform(0.5, 1.5, len(cyc))
+    pf = PFD(n_particles=50_000, resampling="systematic", seed=9, ess_threshold=0.5)
+    pf.initialize(TOKYO_TRUE_POS, clock_bias=TOKYO_TRUE_CB, spread_pos=0.3, spread_cb=0.3)
+    pf.update_carrier_afv(TOKYO_SATS, cyc, w, wavelength=wl, sigma_cycles=0.05, resample=False)
+    x, anchor, clk, rot = _cloud(pf)
+    want, r = O.obs_term(x, anchor, clk, rot, O.OBS_CARRIER_AFV, TOKYO_SATS, cyc, w, wavelength=np.full(len(cyc), wl),
+                         sigma=0.05)
+    ok, rel = lw_close(pf.get_log_weights(), want)
+    ok = _mask_edges(ok, r, 0.0, True)
+    assert ok.all(), f"worst {rel.max():.2e}"
+    wt = np.exp(want - want.max())
+    ess = wt.sum() ** 2 / (wt * wt).sum()
+    assert pf.get_ess() == pytest.approx(ess, rel=ESS_RTOL)
+    assert pf.resample_if_needed() == bool(ess < 25_000)
+
+
+def test_obs_term_rejects_bad_rows(PFD):
+    pf = PFD(n_particles=1024)
+    pf.initialize(TOKYO_TRUE_POS, clock_bias=TOKYO_TRUE_CB)
+    res = _dd_tokyo(np.random.default_rng(1), 4, carrier=True)
+    res.wavelengths_m = np.array([0.19, 0.0, 0.19, 0.19])
+    with pytest.raises(ValueError):
+        pf.update_dd_carrier_afv(res)
+    res.wavelengths_m = np.full(4, 0.19)
+    res.dd_carrier_cycles = np.array([1.0, np.nan, 2.0, 3.0])
+    with pytest.raises(ValueError):
+        pf.update_dd_carrier_afv(res)
+    with pytest.raises(ValueError):
+        pf.update_dd_pseudorange(res, sigma_pr=0.0)
