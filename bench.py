@@ -12,7 +12,8 @@ independent replica of the workload (the path shards across independent
 filters with no exchange), timed on the device, max over ranks.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--workload cfg1-systematic|cfg1-megopolis|cfg2-batched]
+                  [--workload cfg1-systematic|cfg1-megopolis|cfg2-batched|cfg3-learned|
+                              cfg4-batched-learned|device-filter]
 """
 from __future__ import annotations
 
@@ -43,7 +44,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="cfg1-systematic",
                     choices=["cfg1-systematic", "cfg1-megopolis", "cfg2-batched", "cfg3-learned",
-                             "cfg4-batched-learned"])
+                             "cfg4-batched-learned", "device-filter"])
     ap.add_argument("--epochs", type=int, default=0, help="cfg3/cfg4: evaluated epochs (default 600 / 120)")
     ap.add_argument("--n-particles", type=int, default=1_000_000)
     ap.add_argument("--path", default="epoch", choices=["epoch", "chain"],
@@ -268,25 +269,27 @@ def run_b200(args, world, rank, local, pg):
         eng2.initialize(0, tr.truth_ecef[0], tr.truth_clk[0], 10.0, 30.0)
         s_ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + W)]
         e_ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + W)]
+        # each epoch's inputs as the C-ABI records (pf_filter_epoch_t + pf_sat_t) in host memory
+        host_in = [eng2.pack_epoch([epoch_record(tr, i % len(tr.pr), flags)]) for i in range(K + W)]
         h2d = 0
+        est = np.zeros((K + W, 3))
         for i in range(K + W):
-            t = i % len(tr.pr)
+            fe, sv = host_in[i]
             with torch.cuda.stream(eng2.stream):
                 flush.fill_(i & 0xFF)
                 s_ev[i].record(eng2.stream)
-            fe, sv = eng2.pack_epoch([epoch_record(tr, t, flags)])  # host inputs
-            eng2.upload(0, fe, sv)                                   # pinned H2D
-            eng2.step()
-            eng2.results()                                           # D2H + sync
+            res = eng2.step_io(fe, sv)      # staged pinned H2D + step + D2H of the results + sync
             with torch.cuda.stream(eng2.stream):
                 e_ev[i].record(eng2.stream)
+            est[i] = res[0].est_ecef[:]
             h2d = fe.nbytes + sv.nbytes
         torch.cuda.synchronize()
+        assert np.all(np.isfinite(est))
         e2e_s = sum(s_ev[i].elapsed_time(e_ev[i]) for i in range(W, W + K)) / 1e3
         e2e_s = reduce_max(pg, e2e_s)
         e2e = {"value": n * K * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(eng2.result_bytes()), "ms_per_step": e2e_s / K * 1e3,
-               "api": "gnss_gpu_b200.Engine pack_epoch/upload/step/results per step"}
+               "api": "gnss_gpu_b200.Engine.step_io per step (pfe_step_io: upload, step, read results)"}
         eng2.close()
 
     peak, peak_kind = peaks()
@@ -510,6 +513,129 @@ def run_learned(args, world, rank, local, pg, cfg4: bool):
     }
 
 
+# --------------------------------------- ParticleFilterDevice drop-in
+def cpu_baseline_d4(n: int, epochs: int, seed: int, sats, pr):
+    """The oracle's FP64 step (OpenMP) with D = 4 and the given satellites:
+    predict, Gaussian weight, ESS, systematic resample, estimate."""
+    from oracle import oracle as O
+    D = 4
+    x = np.ascontiguousarray(O.init_state(n, D, 50.0, 200.0, 4242).reshape(-1))
+    xt = np.zeros_like(x)
+    lw = np.zeros(n)
+    lw32 = np.zeros(n, np.float32)
+    anc = np.zeros(n, np.int32)
+    anchor = np.zeros(3)
+    ca = np.array([100.0, 0.0, 0.0, 0.0])
+    rot = np.ascontiguousarray(np.eye(3).ravel())
+    sigma = np.array([1, 1, 1, 300, 0, 0, 0, 0], np.float32)
+    stats = np.zeros(24)
+    rows = np.ascontiguousarray(np.column_stack([sats, pr, np.ones(len(pr))]).ravel())
+    ci = np.zeros(len(pr), np.int32)
+    L = O.lib()
+    t0 = time.perf_counter()
+    for t in range(epochs):
+        L.orc_epoch(n, D, x, xt, lw, lw32, anc, anchor, ca, rot, np.zeros(3), sigma, 4242, 0, t + 1, len(pr), rows,
+                    ci, 5.0, 0.5, stats)
+    dt = time.perf_counter() - t0
+    return n * epochs / dt, O.num_threads(), dt
+
+
+def run_device_filter(args, world, rank, local, pg):
+    """ParticleFilterDevice, the reference's device-resident filter API:
+    the predict + update cycle of its stream benchmark (8 satellites 20,000 km
+    from a receiver at the ECEF origin, systematic resampling), at N
+    particles, for three likelihoods.  value: device time of the cycles
+    (CUDA events on the filter's stream, L2 flushed between cycles); e2e:
+    the same cycles plus estimate() to the host, timed around the host calls."""
+    import torch
+    from gnss_gpu_b200 import ParticleFilterDevice
+    torch.cuda.set_device(local)
+    W, K = args.warmup, args.steps
+    n = args.n_particles
+    rng = np.random.RandomState(123)
+    d = rng.randn(8, 3)
+    sats = d / np.linalg.norm(d, axis=1, keepdims=True) * 20_000_000.0
+    pr = np.linalg.norm(sats, axis=1) + 100.0
+    pr[[1, 5]] += (30.0, 12.0)  # two NLOS-like delays
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=torch.device("cuda", local))
+    variants = {"gaussian": dict(), "student_t_gate": dict(nu=4.0, per_particle_nlos_gate=True,
+                                                            per_particle_nlos_undiff_pr_threshold_m=20.0),
+                "gmm": dict()}
+    res = {}
+    clocks = ClockSampler(local)
+    clocks.start()
+    for name, kw in variants.items():
+        pf = ParticleFilterDevice(n_particles=n, sigma_pos=1.0, sigma_cb=300.0, sigma_pr=5.0,
+                                  resampling="systematic", seed=42 + rank, **kw)
+        pf.initialize(np.zeros(3), clock_bias=100.0, spread_pos=50.0, spread_cb=200.0)
+        stream = pf._engine.stream
+        upd = (lambda: pf.update_gmm(sats, pr, None)) if name == "gmm" else (lambda: pf.update(sats, pr, None))
+        for i in range(W):
+            pf.predict(dt=1.0)
+            upd()
+        pf.sync()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(2 * K)]
+        for i in range(K):  # device time of the cycle
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 0xFF)
+                ev[i][0].record(stream)
+            pf.predict(dt=1.0)
+            upd()
+            with torch.cuda.stream(stream):
+                ev[i][1].record(stream)
+        pf.sync()
+        est = []
+        for i in range(K):  # e2e: cycle + estimate to the host
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 0xFF)
+                ev[K + i][0].record(stream)
+            pf.predict(dt=1.0)
+            upd()
+            est.append(pf.estimate())
+            with torch.cuda.stream(stream):
+                ev[K + i][1].record(stream)
+        pf.sync()
+        dev_s = sum(a.elapsed_time(b) for a, b in ev[:K]) / 1e3
+        e2e_s = sum(a.elapsed_time(b) for a, b in ev[K:]) / 1e3
+        res[name] = {"value": n * K / reduce_max(pg, dev_s), "ms_per_cycle": dev_s / K * 1e3,
+                     "e2e": n * K / reduce_max(pg, e2e_s), "e2e_ms_per_cycle": e2e_s / K * 1e3,
+                     "launches_per_cycle": pf._engine.last_launch_count(),
+                     "final_error_m": float(np.linalg.norm(est[-1][:3]))}
+        pf._engine.close()
+    clk = clocks.stop()
+    peak, peak_kind = peaks()
+    D = 4
+    b_alg = 2 * D * 4 + 4 + 4 + 4
+    g = res["gaussian"]
+    achieved = g["value"] * b_alg / 1e9
+    out = {
+        "metric": "ParticleFilterDevice particle-steps/s (predict + update cycle, 8 satellites)",
+        "value": g["value"] * world, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": g["ms_per_cycle"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 state / f64 anchor", "data": "synthetic (the reference stream benchmark's geometry)",
+        "config": {"workload": f"device-filter: ParticleFilterDevice, {n} particles x 8 satellites, D=4, "
+                               "sigma_pr 5 m, systematic resampling when ESS<N/2",
+                   "particles": n, "satellites": 8, "parallelism": f"replicas x{world}",
+                   "l2": "flushed between cycles (outside the event intervals)"},
+        "gpu_launches": K * g["launches_per_cycle"],
+        "likelihoods": res,
+        "e2e": {"value": g["e2e"] * world, "unit": UNIT, "h2d_bytes_per_step": 56 * 8 + 64,
+                "d2h_bytes_per_step": 8 * 4, "api": "ParticleFilterDevice.predict/update/estimate per cycle"},
+        "roofline": {"bound": "hbm", "kernel": "k_epoch<generic> (+ k_estimate in e2e)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",
+                     "algorithmic_bytes_per_launch": b_alg * n, "traffic": None},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        _, _, dt1 = cpu_baseline_d4(n, 1, 7, sats, pr)
+        epochs = int(max(2, min(400, 10.0 / max(dt1, 1e-3))))
+        v, cores, dt = cpu_baseline_d4(n, epochs, 7, sats, pr)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                               "sample": f"oracle FP64 C port (OpenMP), Gaussian, {n} particles x 8 satellites, "
+                                         f"{epochs} epochs, {dt:.1f} s"}
+    return out
+
+
 # ------------------------------------------------------- reference arm
 def run_reference(args, world, rank):
     if rank != 0:
@@ -545,6 +671,8 @@ def main():
         out = run_reference(args, world, rank)
     elif args.workload == "cfg2-batched":
         out = run_cfg2(args, world, rank, local, pg)
+    elif args.workload == "device-filter":
+        out = run_device_filter(args, world, rank, local, pg)
     elif args.workload in ("cfg3-learned", "cfg4-batched-learned"):
         out = run_learned(args, world, rank, local, pg, args.workload == "cfg4-batched-learned")
     else:

@@ -100,7 +100,7 @@ EXPORTED = [
     "pfe_read_timing", "pfe_result_bytes", "pfe_read_timing_kernels",
     "pf_mlp_param_count", "pf_mlp_scratch_bytes", "pf_mlp_grad", "pf_mlp_adam_step", "pf_mlp_forward",
     "pfe_set_mlp", "pfe_get_sat_debug", "pfe_set_epoch_ctas_per_sm", "pfe_set_likelihood", "pfe_shift",
-    "pfe_add_position_term", "pfe_add_obs_term",
+    "pfe_add_position_term", "pfe_add_obs_term", "pfe_step_io",
 ]
 
 _lib = None
@@ -176,6 +176,7 @@ def load():
     L.pfe_shift.argtypes = [p, i, dp, dp]
     L.pfe_add_position_term.argtypes = [p, i, dp, dp, i, d]
     L.pfe_add_obs_term.argtypes = [p, i, i, C.c_void_p, i, d, d, d, i]
+    L.pfe_step_io.argtypes = [p, C.c_void_p, C.c_void_p, i, C.c_void_p]
     L.pfe_get_sat_debug.argtypes = [p, i, p, i, C.POINTER(C.c_int)]
     for name in EXPORTED:
         fn = getattr(L, name)

@@ -37,6 +37,7 @@ struct pf_engine {
   cudaEvent_t pin_ev[2] = {nullptr, nullptr};
   int pin_cur = 0;
   FilterCtrl* ctrl_host = nullptr;  // pinned mirror
+  unsigned* err_host = nullptr;     // pinned copy of the device error word
   size_t obs_slot_bytes = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -384,9 +385,10 @@ int launch_epoch(pf_engine* eng, int t0, int count) {
 bool use_chain(const pf_engine* eng) { return (eng->cfg.flags & PF_FLAG_KERNEL_CHAIN) != 0; }
 
 int sync_and_check(pf_engine* eng) {
+  // the error word rides on the same stream as the caller's reads: one sync
+  CK(cudaMemcpyAsync(eng->err_host, eng->dev.err, sizeof(unsigned), cudaMemcpyDeviceToHost, eng->stream));
   CK(cudaStreamSynchronize(eng->stream));
-  unsigned w = 0;
-  CK(cudaMemcpy(&w, eng->dev.err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  const unsigned w = *eng->err_host;
   if (w & ERR_LOOKBACK_TIMEOUT) return set_err(PF_ETIMEOUT, "device look-back spin limit reached (error word 0x%x)", w);
   if (w & ERR_BARRIER_TIMEOUT) return set_err(PF_ETIMEOUT, "device grid-barrier spin limit reached (error word 0x%x)", w);
   if (w & ERR_SAT_CAP) return set_err(PF_ECAP, "n_sat above max_sats (error word 0x%x)", w);
@@ -549,7 +551,8 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
       return fail(PF_ECUDA);
   }
   if (check_cuda(cudaHostAlloc((void**)&eng->ctrl_host, sizeof(FilterCtrl) * cfg->n_filters, cudaHostAllocDefault),
-                 "pinned ctrl") != PF_OK)
+                 "pinned ctrl") != PF_OK ||
+      check_cuda(cudaHostAlloc((void**)&eng->err_host, 64, cudaHostAllocDefault), "pinned error word") != PF_OK)
     return fail(PF_ENOMEM);
 
   // Device tables and zeroed control blocks.
@@ -590,6 +593,7 @@ int pfe_destroy(pf_engine_t* eng) {
     if (eng->pin_ev[i]) cudaEventDestroy(eng->pin_ev[i]);
   }
   if (eng->ctrl_host) cudaFreeHost(eng->ctrl_host);
+  if (eng->err_host) cudaFreeHost(eng->err_host);
   for (cudaEvent_t e : eng->tev) cudaEventDestroy(e);
   delete eng;
   return PF_OK;
@@ -908,6 +912,17 @@ int pfe_read_results(pf_engine_t* eng, pf_filter_result_t* out) {
     r.initialized = eng->initialized[f];
   }
   return PF_OK;
+}
+
+int pfe_step_io(pf_engine_t* eng, const pf_filter_epoch_t* fe, const pf_sat_t* sats, int n_sats_total,
+                pf_filter_result_t* out) {
+  clear_err();
+  if (!eng || !fe || !out) return set_err(PF_EINVAL, "null argument");
+  if (eng->cfg.obs_slots != 1) return set_err(PF_EINVAL, "pfe_step_io needs an engine with obs_slots == 1");
+  int s = pfe_upload_obs(eng, 0, fe, sats, n_sats_total);
+  if (s != PF_OK) return s;
+  if ((s = pfe_step(eng)) != PF_OK) return s;
+  return pfe_read_results(eng, out);
 }
 
 int pfe_result_bytes(pf_engine_t* eng, size_t* bytes) {

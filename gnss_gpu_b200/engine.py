@@ -233,6 +233,14 @@ class Engine:
     def step(self):
         N.check(self.lib.pfe_step(self.h))
 
+    def step_io(self, fe: np.ndarray, sats: np.ndarray):
+        """One epoch from host records to host results in one library call
+        (upload into slot 0, step, read); returns the raw per-filter
+        N.FilterResult array (reused by the next call).  Needs obs_slots == 1."""
+        N.check(self.lib.pfe_step_io(self.h, N.vptr(fe), N.vptr(sats) if len(sats) else None, len(sats),
+                                     C.byref(self._results)))
+        return self._results
+
     def step_per_filter(self):
         N.check(self.lib.pfe_step_per_filter(self.h))
 

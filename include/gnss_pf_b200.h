@@ -304,6 +304,11 @@ int pfe_obs_slot_bytes(pf_engine_t* eng, size_t* bytes);
 int pfe_step(pf_engine_t* eng);
 /* The same kernels launched once per filter (comparison path). */
 int pfe_step_per_filter(pf_engine_t* eng);
+/* One epoch from host memory to host memory, the call of a real-time
+ * caller: pfe_upload_obs into slot 0, pfe_step, pfe_read_results into
+ * out[n_filters] (synchronises).  Needs obs_slots == 1. */
+int pfe_step_io(pf_engine_t* eng, const pf_filter_epoch_t* fe, const pf_sat_t* sats, int n_sats_total,
+                pf_filter_result_t* out);
 
 /* Capture one epoch (pfe_step, or pfe_step_per_filter if per_filter != 0)
  * into a CUDA graph; pfe_graph_launch replays it n_epochs times. */

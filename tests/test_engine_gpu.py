@@ -224,6 +224,36 @@ def test_determinism_same_seed_bit_identical():
     assert np.array_equal(s1[0], s2[0])
 
 
+def test_step_io_equals_separate_calls():
+    """pfe_step_io (upload, step, read in one call) gives the same results
+    and state as the three calls."""
+    tr = S.config0()
+
+    def run(io):
+        eng = H.make_engine([20_000, 3000], seeds=[5, 6])
+        for k in range(2):
+            eng.initialize(k, tr.anchor, tr.truth_clk[0], 10.0, 30.0)
+        for t in range(4):
+            fe, sv = eng.pack_epoch([_epoch_rec(tr, t)] * 2)
+            if io:
+                raw = eng.step_io(fe, sv)
+                assert raw[1].epoch == t + 1
+            else:
+                eng.upload(0, fe, sv)
+                eng.step()
+        return eng.results(), eng.state_f32(0)
+
+    (ra, sa), (rb, sb) = run(True), run(False)
+    for k in range(2):
+        assert np.array_equal(ra[k]["est_ecef"], rb[k]["est_ecef"]) and ra[k]["ess"] == rb[k]["ess"]
+    assert np.array_equal(sa[0], sb[0]) and np.array_equal(sa[1], sb[1])
+    eng = H.make_engine([1000], obs_slots=2)
+    eng.initialize(0, tr.anchor, tr.truth_clk[0], 10.0, 30.0)
+    fe, sv = eng.pack_epoch([_epoch_rec(tr, 0)])
+    with pytest.raises(ValueError):
+        eng.step_io(fe, sv)
+
+
 def test_degenerate_weights_single_survivor():
     """One particle carries all the weight: the ESS is 1 and every slot
     descends from it (merge path with one particle owning all N slots)."""
