@@ -267,29 +267,29 @@ def run_b200(args, world, rank, local, pg):
                                             max_sats=32, obs_slots=1, kernel_chain=args.path == "chain"),
                       device=local)
         eng2.initialize(0, tr.truth_ecef[0], tr.truth_clk[0], 10.0, 30.0)
-        s_ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + W)]
-        e_ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + W)]
         # each epoch's inputs as the C-ABI records (pf_filter_epoch_t + pf_sat_t) in host memory
         host_in = [eng2.pack_epoch([epoch_record(tr, i % len(tr.pr), flags)]) for i in range(K + W)]
         h2d = 0
         est = np.zeros((K + W, 3))
+        wall = []
         for i in range(K + W):
             fe, sv = host_in[i]
             with torch.cuda.stream(eng2.stream):
-                flush.fill_(i & 0xFF)
-                s_ev[i].record(eng2.stream)
+                flush.fill_(i & 0xFF)      # evict L2, then let the device go idle: outside the timer
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
             res = eng2.step_io(fe, sv)      # staged pinned H2D + step + D2H of the results + sync
-            with torch.cuda.stream(eng2.stream):
-                e_ev[i].record(eng2.stream)
+            wall.append(time.perf_counter() - t0)
             est[i] = res[0].est_ecef[:]
             h2d = fe.nbytes + sv.nbytes
-        torch.cuda.synchronize()
         assert np.all(np.isfinite(est))
-        e2e_s = sum(s_ev[i].elapsed_time(e_ev[i]) for i in range(W, W + K)) / 1e3
+        e2e_s = float(np.sum(wall[W:]))
         e2e_s = reduce_max(pg, e2e_s)
         e2e = {"value": n * K * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(eng2.result_bytes()), "ms_per_step": e2e_s / K * 1e3,
-               "api": "gnss_gpu_b200.Engine.step_io per step (pfe_step_io: upload, step, read results)"}
+               "api": "gnss_gpu_b200.Engine.step_io per step (pfe_step_io: upload, step, read results)",
+               "timing": "host clock around each call, from host inputs to host results; the L2 flush and a "
+                         "device synchronize run before each timer starts"}
         eng2.close()
 
     peak, peak_kind = peaks()

@@ -24,6 +24,7 @@ PF_WEIGHT_GAUSSIAN, PF_WEIGHT_HUBER, PF_WEIGHT_MIXTURE, PF_WEIGHT_GENERIC = 0, 1
 PF_LIK_GAUSSIAN, PF_LIK_STUDENT_T, PF_LIK_HUBER, PF_LIK_GMM = 0, 1, 2, 3
 PF_OBS_DD_PSEUDORANGE, PF_OBS_CARRIER_AFV, PF_OBS_DD_CARRIER_AFV = 0, 1, 2
 PF_MAX_OBS_ROWS = 128
+PF_MAX_DOPPLER_ROWS = 64
 PF_LW_OVERWRITE, PF_LW_ACCUMULATE = 0, 1
 PF_SYS_OFFSET_RANDOM, PF_SYS_OFFSET_REFERENCE = 0, 1
 PF_FLAG_COVARIANCE, PF_FLAG_RECENTER, PF_FLAG_KERNEL_CHAIN = 1, 2, 4
@@ -70,6 +71,14 @@ OBS_ROW_DTYPE = np.dtype([("sat_k", "<f8", 3), ("sat_ref", "<f8", 3), ("obs", "<
                           ("base_ref", "<f8"), ("weight", "<f8"), ("wavelength", "<f8")])
 
 
+class VelState(C.Structure):
+    _fields_ = [("buf", C.c_void_p), ("sel", C.c_int), ("seq", C.c_uint)]
+
+
+# pf_doppler_row_t
+DOPPLER_ROW_DTYPE = np.dtype([("sat", "<f8", 3), ("sat_vel", "<f8", 3), ("doppler_hz", "<f8"), ("weight", "<f8")])
+
+
 class FilterResult(C.Structure):
     _fields_ = [
         ("est_ecef", C.c_double * 3), ("est_clk", C.c_double * PF_MAX_CLK), ("cov_enu", C.c_double * 6),
@@ -100,7 +109,8 @@ EXPORTED = [
     "pfe_read_timing", "pfe_result_bytes", "pfe_read_timing_kernels",
     "pf_mlp_param_count", "pf_mlp_scratch_bytes", "pf_mlp_grad", "pf_mlp_adam_step", "pf_mlp_forward",
     "pfe_set_mlp", "pfe_get_sat_debug", "pfe_set_epoch_ctas_per_sm", "pfe_set_likelihood", "pfe_shift",
-    "pfe_add_position_term", "pfe_add_obs_term", "pfe_step_io",
+    "pfe_add_position_term", "pfe_add_obs_term", "pfe_step_io", "pfe_vel_init", "pfe_vel_follow",
+    "pfe_vel_predict", "pfe_vel_doppler",
 ]
 
 _lib = None
@@ -177,6 +187,11 @@ def load():
     L.pfe_add_position_term.argtypes = [p, i, dp, dp, i, d]
     L.pfe_add_obs_term.argtypes = [p, i, i, C.c_void_p, i, d, d, d, i]
     L.pfe_step_io.argtypes = [p, C.c_void_p, C.c_void_p, i, C.c_void_p]
+    vs = C.POINTER(VelState)
+    L.pfe_vel_init.argtypes = [p, i, vs, dp, d, d, C.c_uint]
+    L.pfe_vel_follow.argtypes = [p, i, vs]
+    L.pfe_vel_predict.argtypes = [p, i, vs, dp, d, d, d, d, i, d, C.c_uint]
+    L.pfe_vel_doppler.argtypes = [p, i, vs, C.c_void_p, i, d, d, d, d, i]
     L.pfe_get_sat_debug.argtypes = [p, i, p, i, C.POINTER(C.c_int)]
     for name in EXPORTED:
         fn = getattr(L, name)

@@ -13,6 +13,7 @@
 
 #include "pf_epoch_kernel.cuh"
 #include "pf_obs_terms.cuh"
+#include "pf_velocity.cuh"
 #include "pf_status.h"
 
 using namespace pfb;
@@ -1300,6 +1301,141 @@ int pfe_add_obs_term(pf_engine_t* eng, int filter, int kind, const pf_obs_row_t*
                      sizeof(int), cudaMemcpyHostToDevice, eng->stream));
   CK(cudaStreamSynchronize(eng->stream));
   return PF_OK;
+}
+
+static int vel_check(pf_engine_t* eng, int filter, pf_vel_state_t* vs) {
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!vs || !vs->buf) return set_err(PF_EINVAL, "null velocity state");
+  if (vs->sel != 0 && vs->sel != 1) return set_err(PF_EINVAL, "velocity state: sel must be 0 or 1");
+  if (!eng->initialized[filter]) return set_err(PF_ENOTINIT, "filter %d not initialized", filter);
+  return PF_OK;
+}
+
+static int vel_grid(pf_engine_t* eng, int n, int per_thread) {
+  return std::max(1, std::min(eng->sm_count * 8, (n + kThreads * per_thread - 1) / (kThreads * per_thread)));
+}
+
+int pfe_vel_init(pf_engine_t* eng, int filter, pf_vel_state_t* vs, const double v0_ecef[3], double spread_vel,
+                 double init_sigma, unsigned step) {
+  clear_err();
+  int s = vel_check(eng, filter, vs);
+  if (s != PF_OK) return s;
+  if (!v0_ecef) return set_err(PF_EINVAL, "null v0");
+  for (int i = 0; i < 3; ++i)
+    if (!isfinite(v0_ecef[i])) return set_err(PF_EINVAL, "v0 not finite");
+  if (!(spread_vel >= 0.0) || !isfinite(spread_vel) || !isfinite(init_sigma))
+    return set_err(PF_EINVAL, "spread_vel must be finite and >= 0");
+  if ((s = read_ctrl(eng)) != PF_OK) return s;
+  const int n = eng->hdesc[filter].n;
+  k_vel_init<<<vel_grid(eng, n, 1), kThreads, 0, eng->stream>>>(eng->dev, filter, vs->buf, v0_ecef[0], v0_ecef[1],
+                                                                  v0_ecef[2], spread_vel, init_sigma * init_sigma, step);
+  CK(cudaGetLastError());
+  vs->sel = 0;
+  vs->seq = eng->ctrl_host[filter].rs_seq;
+  return sync_and_check(eng);
+}
+
+int pfe_vel_follow(pf_engine_t* eng, int filter, pf_vel_state_t* vs) {
+  clear_err();
+  int s = vel_check(eng, filter, vs);
+  if (s != PF_OK) return s;
+  if ((s = read_ctrl(eng)) != PF_OK) return s;
+  const FilterCtrl& c = eng->ctrl_host[filter];
+  if (!c.resample_flag || c.rs_seq == vs->seq) return PF_OK;
+  const int n = eng->hdesc[filter].n;
+  const double* in = vs->buf + (size_t)vs->sel * kVelComp * n;
+  double* out = vs->buf + (size_t)(vs->sel ^ 1) * kVelComp * n;
+  k_vel_gather<<<vel_grid(eng, n, 1), kThreads, 0, eng->stream>>>(eng->dev, filter, in, out);
+  CK(cudaGetLastError());
+  vs->sel ^= 1;
+  vs->seq = c.rs_seq;
+  return sync_and_check(eng);
+}
+
+int pfe_vel_predict(pf_engine_t* eng, int filter, pf_vel_state_t* vs, const double guide_ecef[3], double dt,
+                    double sigma_pos, double sigma_vel, double alpha, int kf, double q, unsigned step) {
+  clear_err();
+  int s = pfe_vel_follow(eng, filter, vs);
+  if (s != PF_OK) return s;
+  if (!guide_ecef) return set_err(PF_EINVAL, "null guide velocity");
+  for (int i = 0; i < 3; ++i)
+    if (!isfinite(guide_ecef[i])) return set_err(PF_EINVAL, "guide velocity not finite");
+  if (!isfinite(dt) || !isfinite(sigma_pos) || !isfinite(sigma_vel) || !isfinite(alpha) || !isfinite(q) ||
+      sigma_pos < 0.0 || sigma_vel < 0.0)
+    return set_err(PF_EINVAL, "predict parameters must be finite, sigmas >= 0");
+  FilterCtrl c = eng->ctrl_host[filter];  // read by the follow above
+  const FilterDesc& d = eng->hdesc[filter];
+  VelPredict vp;
+  memset(&vp, 0, sizeof(vp));
+  for (int i = 0; i < 3; ++i) vp.guide[i] = guide_ecef[i];
+  for (int i = 0; i < 9; ++i) vp.rot[i] = d.rot[i];
+  vp.dt = dt;
+  vp.sigma_pos = sigma_pos;
+  vp.sigma_vel = sigma_vel;
+  vp.alpha = alpha;
+  vp.q = q;
+  vp.kf = kf ? 1 : 0;
+  vp.step = step;
+  double* vb = vs->buf + (size_t)vs->sel * kVelComp * d.n;
+  const int g = vel_grid(eng, d.n, 4);
+  switch (eng->D) {
+    case 4: k_vel_predict<4><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, vb, vp); break;
+    case 5: k_vel_predict<5><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, vb, vp); break;
+    case 6: k_vel_predict<6><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, vb, vp); break;
+    default: k_vel_predict<7><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, vb, vp); break;
+  }
+  CK(cudaGetLastError());
+  // the particles now sit, gathered, in the other buffer
+  c.parity ^= 1;
+  c.resample_flag = 0;
+  CK(cudaMemcpyAsync(eng->ctrl_dev + filter, &c, sizeof(c), cudaMemcpyHostToDevice, eng->stream));
+  CK(cudaStreamSynchronize(eng->stream));
+  eng->ctrl_host[filter] = c;
+  return sync_and_check(eng);
+}
+
+int pfe_vel_doppler(pf_engine_t* eng, int filter, pf_vel_state_t* vs, const pf_doppler_row_t* rows, int n_rows,
+                    double wavelength, double sigma_mps, double gain, double max_update, int kf) {
+  clear_err();
+  int s = pfe_vel_follow(eng, filter, vs);
+  if (s != PF_OK) return s;
+  if (n_rows < 1 || n_rows > kMaxDopplerRows || !rows) return set_err(PF_ECAP, "need 1..%d rows", kMaxDopplerRows);
+  if (!(wavelength > 0.0) || !isfinite(wavelength) || !(sigma_mps > 0.0) || !isfinite(sigma_mps) || !isfinite(gain) ||
+      !isfinite(max_update))
+    return set_err(PF_EINVAL, "wavelength and sigma must be > 0, gain and cap finite");
+  for (int i = 0; i < n_rows; ++i) {
+    bool ok = isfinite(rows[i].doppler_hz) && isfinite(rows[i].weight);
+    for (int k = 0; k < 3; ++k) ok = ok && isfinite(rows[i].sat[k]) && isfinite(rows[i].sat_vel[k]);
+    if (!ok) return set_err(PF_EINVAL, "row %d not finite", i);
+  }
+  static_assert(sizeof(DopplerRow) == sizeof(pf_doppler_row_t), "row layout");
+  // the rows ride in the observation-term scratch (128 x 80 bytes)
+  static_assert(sizeof(DopplerRow) * kMaxDopplerRows <= sizeof(ObsRow) * kMaxObsRows, "scratch size");
+  CK(cudaMemcpyAsync(eng->obs_rows, rows, sizeof(DopplerRow) * n_rows, cudaMemcpyHostToDevice, eng->stream));
+  DopplerArgs a;
+  memset(&a, 0, sizeof(a));
+  a.n_sat = n_rows;
+  a.kf = kf ? 1 : 0;
+  a.wavelength = wavelength;
+  a.sigma = sigma_mps;
+  a.gain = gain;
+  a.max_update = max_update;
+  const FilterDesc& d = eng->hdesc[filter];
+  double* vb = vs->buf + (size_t)vs->sel * kVelComp * d.n;
+  const DopplerRow* dr = reinterpret_cast<const DopplerRow*>(eng->obs_rows);
+  const int g = vel_grid(eng, d.n, 4);
+  switch (eng->D) {
+    case 4: k_doppler<4><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, vb, dr, a); break;
+    case 5: k_doppler<5><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, vb, dr, a); break;
+    case 6: k_doppler<6><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, vb, dr, a); break;
+    default: k_doppler<7><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, vb, dr, a); break;
+  }
+  CK(cudaGetLastError());
+  const int zero = 0;
+  CK(cudaMemcpyAsync(reinterpret_cast<char*>(eng->ctrl_dev + filter) + offsetof(FilterCtrl, lw_zero), &zero,
+                     sizeof(int), cudaMemcpyHostToDevice, eng->stream));
+  return sync_and_check(eng);
 }
 
 int pfe_set_mlp(pf_engine_t* eng, const float* params) {

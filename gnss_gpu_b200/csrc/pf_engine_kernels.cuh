@@ -295,18 +295,27 @@ __device__ __forceinline__ MergedStats merge_tiles_at(const float* part, int tb,
   double acc[16];
 #pragma unroll
   for (int i = 0; i < 16; ++i) acc[i] = 0.0;
-  if (M > -INFINITY) {
-    for (int i = threadIdx.x; i < nt; i += kThreads) {
-      const float4* row4 = reinterpret_cast<const float4*>(part + (size_t)(tb + i) * kPartStride);
-      const float4 a0 = __ldcg(row4), a1 = __ldcg(row4 + 1), a2 = __ldcg(row4 + 2), a3 = __ldcg(row4 + 3);
-      const float r[16] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w,
-                           a2.x, a2.y, a2.z, a2.w, a3.x, a3.y, a3.z, a3.w};
-      if (!(r[0] > -INFINITY)) continue;
-      const double sc = exp((double)r[0] - (double)M);
-      acc[0] += sc * (double)r[1];
-      acc[1] += sc * sc * (double)r[2];
+  auto fold = [&](const float4 a0, const float4 a1, const float4 a2, const float4 a3) {
+    const float r[16] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w,
+                         a2.x, a2.y, a2.z, a2.w, a3.x, a3.y, a3.z, a3.w};
+    if (!(r[0] > -INFINITY)) return;
+    const double sc = exp((double)r[0] - (double)M);
+    acc[0] += sc * (double)r[1];
+    acc[1] += sc * sc * (double)r[2];
 #pragma unroll
-      for (int v = 2; v < NV; ++v) acc[v] += sc * (double)r[1 + v];
+    for (int v = 2; v < NV; ++v) acc[v] += sc * (double)r[1 + v];
+  };
+  if (M > -INFINITY) {
+    // two rows in flight per thread (rows i and i + kThreads, folded in
+    // that order, the order of the plain loop)
+    for (int i = threadIdx.x; i < nt; i += 2 * kThreads) {
+      const int j = i + kThreads;
+      const float4* ra = reinterpret_cast<const float4*>(part + (size_t)(tb + i) * kPartStride);
+      const float4* rb = reinterpret_cast<const float4*>(part + (size_t)(tb + (j < nt ? j : i)) * kPartStride);
+      const float4 a0 = __ldcg(ra), a1 = __ldcg(ra + 1), a2 = __ldcg(ra + 2), a3 = __ldcg(ra + 3);
+      const float4 b0 = __ldcg(rb), b1 = __ldcg(rb + 1), b2 = __ldcg(rb + 2), b3 = __ldcg(rb + 3);
+      fold(a0, a1, a2, a3);
+      if (j < nt) fold(b0, b1, b2, b3);
     }
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

@@ -215,6 +215,12 @@ class Engine:
         N.check(self.lib.pfe_add_obs_term(self.h, int(k), int(kind), N.vptr(r) if len(r) else None, len(r),
                                           float(sigma), float(gate), float(huber_k), 1 if accumulate else 0))
 
+    # ------------------------------------------------------ velocity states
+    def velocity_states(self, k: int) -> "VelocityStates":
+        """Per-particle velocity states of filter k (device memory allocated
+        here, initialised by VelocityStates.init)."""
+        return VelocityStates(self, k)
+
     def set_mlp(self, params):
         """Upload the NLOS network's parameters (mixture mode)."""
         prm = np.ascontiguousarray(params, dtype=np.float32)
@@ -374,3 +380,62 @@ class Engine:
         c = C.c_int(0)
         N.check(self.lib.pfe_read_timing_kernels(self.h, a, n, C.byref(c)))
         return np.array(a[: 4 * c.value]).reshape(-1, 4)
+
+
+class VelocityStates:
+    """Per-particle ECEF velocity and 3x3 covariance (FP64) of one engine
+    filter, in device memory beside the engine's particles (pfe_vel_*)."""
+
+    NCOMP = 12
+
+    def __init__(self, eng: Engine, k: int):
+        torch = eng._torch
+        self.eng, self.k = eng, int(k)
+        self.n = eng.filters[k].n_particles
+        # no fill: init() writes buffer 0, the resample gather writes buffer 1
+        self.buf = torch.empty(2 * self.NCOMP * self.n, dtype=torch.float64, device=eng.device)
+        self.vs = N.VelState()
+        self.vs.buf = C.c_void_p(self.buf.data_ptr())
+        self.vs.sel = 0
+        self.vs.seq = 0
+
+    def init(self, v0_ecef, spread_vel=0.0, init_sigma=0.0, step=0):
+        v = np.ascontiguousarray(v0_ecef, dtype=np.float64).reshape(3)
+        N.check(self.eng.lib.pfe_vel_init(self.eng.h, self.k, C.byref(self.vs), N.dptr(v), float(spread_vel),
+                                          float(init_sigma), int(step) & 0xFFFFFFFF))
+
+    def follow(self):
+        N.check(self.eng.lib.pfe_vel_follow(self.eng.h, self.k, C.byref(self.vs)))
+
+    def predict(self, guide_ecef, dt, sigma_pos, sigma_vel, alpha, kf, q, step):
+        g = np.ascontiguousarray(guide_ecef, dtype=np.float64).reshape(3)
+        N.check(self.eng.lib.pfe_vel_predict(self.eng.h, self.k, C.byref(self.vs), N.dptr(g), float(dt),
+                                             float(sigma_pos), float(sigma_vel), float(alpha), 1 if kf else 0,
+                                             float(q), int(step) & 0xFFFFFFFF))
+
+    def doppler(self, sat_ecef, sat_vel, doppler_hz, weights, wavelength, sigma_mps, gain=0.0, max_update=0.0,
+                kf=False):
+        rows = np.zeros(len(doppler_hz), N.DOPPLER_ROW_DTYPE)
+        rows["sat"] = np.asarray(sat_ecef, dtype=np.float64).reshape(-1, 3)
+        rows["sat_vel"] = np.asarray(sat_vel, dtype=np.float64).reshape(-1, 3)
+        rows["doppler_hz"] = np.asarray(doppler_hz, dtype=np.float64).ravel()
+        rows["weight"] = np.asarray(weights, dtype=np.float64).ravel()
+        N.check(self.eng.lib.pfe_vel_doppler(self.eng.h, self.k, C.byref(self.vs), N.vptr(rows), len(rows),
+                                             float(wavelength), float(sigma_mps), float(gain), float(max_update),
+                                             1 if kf else 0))
+
+    def host(self):
+        """(n, 12) FP64: velocity (3) then covariance row-major (9), current
+        particle order (call follow() first after a resampling step)."""
+        self.eng.synchronize()
+        cur = self.buf[self.vs.sel * self.NCOMP * self.n:(self.vs.sel + 1) * self.NCOMP * self.n]
+        return cur.view(self.NCOMP, self.n).t().cpu().numpy().copy()
+
+    def set_host(self, arr):
+        a = np.ascontiguousarray(np.asarray(arr, dtype=np.float64).reshape(self.n, self.NCOMP).T)
+        torch = self.eng._torch
+        cur = self.buf[self.vs.sel * self.NCOMP * self.n:(self.vs.sel + 1) * self.NCOMP * self.n]
+        src = torch.from_numpy(a.reshape(-1))
+        with torch.cuda.stream(self.eng.stream):
+            cur.copy_(src.to(cur.device, non_blocking=False))
+        self.eng.synchronize()

@@ -20,9 +20,14 @@ methods on the engine's sm_100a kernels (weight mode "generic"):
 * update_dd_pseudorange(), update_carrier_afv(), update_dd_carrier_afv()
   evaluate the differenced / carrier-phase terms in FP64 on the device.
 
-Not built: the velocity states (sigma_vel > 0, velocity_guide_alpha != 1,
-rbpf_velocity_kf), the Doppler likelihoods that need them and the
-forward-backward smoother; their methods raise NotImplementedError.
+* Per-particle velocity states (velocity and its covariance, FP64) come into
+  being when a call needs them (sigma_vel > 0, velocity_guide_alpha < 1,
+  rbpf_velocity_kf, a velocity spread, a Doppler update); until then every
+  particle's velocity is the last guide.  update_doppler() and
+  update_doppler_kf() work on them.
+
+Not built: the forward-backward smoother (enable_smoothing, store_epoch,
+smooth raise NotImplementedError).
 """
 from __future__ import annotations
 
@@ -50,10 +55,6 @@ class ParticleFilterDevice:
                  rbpf_velocity_kf=False,
                  velocity_process_noise=0.0, *, megopolis_iterations=15, max_sats=N.PF_MAX_SATS):
         N.load()
-        if float(sigma_vel) != 0.0 or float(velocity_guide_alpha) != 1.0 or bool(rbpf_velocity_kf) \
-                or float(velocity_process_noise) != 0.0:
-            raise NotImplementedError("per-particle velocity states are not built: use sigma_vel=0, "
-                                      "velocity_guide_alpha=1, rbpf_velocity_kf=False")
         self.n_particles = n_particles
         self.sigma_pos = sigma_pos
         self.sigma_cb = sigma_cb
@@ -82,6 +83,9 @@ class ParticleFilterDevice:
         self._pending = None        # (disp_local, sigma_pos) of a recorded predict
         self._spec = None
         self._rot = None
+        self._vel = None            # per-particle velocity states, once any call needs them
+        self._v_shared = np.zeros(3)
+        self._var_shared = 0.0
 
     # ------------------------------------------------------------------
     def _require_init(self):
@@ -123,6 +127,8 @@ class ParticleFilterDevice:
         fe, sv = self._engine.pack_epoch([rec])
         self._engine.upload(0, fe, sv)
         self._engine.step()
+        if self._vel is not None:
+            self._vel.follow()
 
     def _flush(self):
         """Apply a recorded predict on its own (no weighting, no resampling)."""
@@ -142,10 +148,12 @@ class ParticleFilterDevice:
     def initialize(self, position_ecef, clock_bias=0.0, spread_pos=100.0,
                    spread_cb=1000.0, velocity=None, spread_vel=0.0,
                    velocity_init_sigma=0.0):
-        """Scatter particles N(position, spread_pos) / N(clock_bias, spread_cb)."""
-        if (velocity is not None and np.any(np.asarray(velocity, dtype=np.float64) != 0.0)) \
-                or float(spread_vel) != 0.0 or float(velocity_init_sigma) != 0.0:
-            raise NotImplementedError("per-particle velocity states are not built")
+        """Scatter particles N(position, spread_pos) / N(clock_bias, spread_cb);
+        velocities `velocity` (+ N(0, spread_vel)), velocity covariance
+        velocity_init_sigma^2 I."""
+        v0 = np.zeros(3) if velocity is None else np.asarray(velocity, dtype=np.float64).ravel()[:3]
+        if v0.size < 3 or not np.all(np.isfinite(v0)) or not (float(spread_vel) >= 0.0):
+            raise ValueError("velocity must hold 3 finite values and spread_vel must be >= 0")
         pos = np.asarray(position_ecef, dtype=np.float64).ravel()
         if pos.size < 3 or not np.all(np.isfinite(pos[:3])):
             raise ValueError("position_ecef must hold 3 finite values")
@@ -164,20 +172,51 @@ class ParticleFilterDevice:
         self._initialized = True
         self._step = 0
         self._pending = None
+        self._vel = None
+        self._v_shared = v0.copy()
+        self._var_shared = float(velocity_init_sigma) ** 2
+        if float(spread_vel) > 0.0 or self._per_particle_velocity():
+            self._ensure_vel(spread_vel)
+
+    def _per_particle_velocity(self, sigma_vel=None, alpha=None, kf=None):
+        sv = self.sigma_vel if sigma_vel is None else float(sigma_vel)
+        a = self.velocity_guide_alpha if alpha is None else float(alpha)
+        k = self.rbpf_velocity_kf if kf is None else bool(kf)
+        return sv > 0.0 or a != 1.0 or k
+
+    def _ensure_vel(self, spread_vel=0.0):
+        """Per-particle velocity states, started from the shared velocity and
+        covariance every particle has had so far."""
+        if self._vel is None:
+            self._vel = self._engine.velocity_states(0)
+            self._vel.init(self._v_shared, float(spread_vel), np.sqrt(self._var_shared), step=0)
+        return self._vel
 
     def predict(self, velocity=None, dt=1.0, sigma_pos=None, sigma_vel=None, velocity_guide_alpha=None,
                 rbpf_velocity_kf=None, velocity_process_noise=None):
-        """Constant-velocity motion (ECEF m/s) plus N(0, sigma_pos) / N(0, sigma_cb)."""
+        """Motion with the velocity guide (ECEF m/s) plus N(0, sigma_pos) /
+        N(0, sigma_cb).  With per-particle velocities (sigma_vel > 0,
+        velocity_guide_alpha < 1, rbpf_velocity_kf, a Doppler update, a
+        velocity spread) every particle moves by its own velocity
+        (pf_device.cu:106-187); otherwise every particle's velocity is the
+        guide and the motion is fused into the next update."""
         self._require_init()
-        if (sigma_vel not in (None, 0.0)) or (velocity_guide_alpha not in (None, 1.0)) or rbpf_velocity_kf \
-                or (velocity_process_noise not in (None, 0.0)):
-            raise NotImplementedError("per-particle velocity states are not built")
         vel = np.zeros(3) if velocity is None else np.asarray(velocity, dtype=np.float64).ravel()[:3]
         if vel.size < 3 or not np.all(np.isfinite(vel)) or not np.isfinite(dt):
             raise ValueError("velocity must hold 3 finite values and dt must be finite")
         self._flush()
         self._step += 1
-        self._pending = (self._rot @ (vel * float(dt)), sigma_pos)
+        sp = float(self.sigma_pos if sigma_pos is None else sigma_pos)
+        if self._vel is None and not self._per_particle_velocity(sigma_vel, velocity_guide_alpha, rbpf_velocity_kf):
+            self._v_shared = vel.copy()
+            self._pending = (self._rot @ (vel * float(dt)), sp)
+            return
+        sv = self.sigma_vel if sigma_vel is None else float(sigma_vel)
+        a = self.velocity_guide_alpha if velocity_guide_alpha is None else float(velocity_guide_alpha)
+        kf = self.rbpf_velocity_kf if rbpf_velocity_kf is None else bool(rbpf_velocity_kf)
+        q = self.velocity_process_noise if velocity_process_noise is None else float(velocity_process_noise)
+        self._ensure_vel().predict(vel, float(dt), sp, sv, a, kf, q, self._step)
+        self._pending = (np.zeros(3), 0.0)  # the clocks' noise rides on the next update
 
     def _weight(self, sat_ecef, pseudoranges, weights, sigma_pr, resample, **lik):
         self._require_init()
@@ -274,11 +313,43 @@ class ParticleFilterDevice:
                          self._per_particle_threshold(self.per_particle_nlos_dd_carrier_threshold_cycles), huber,
                          True, resample)
 
-    def update_doppler(self, *a, **k):
-        raise NotImplementedError("Doppler likelihood is not built")
+    def _doppler_args(self, sat_ecef, sat_vel, doppler_hz, weights):
+        sat = np.asarray(sat_ecef, dtype=np.float64).reshape(-1, 3)
+        sv = np.asarray(sat_vel, dtype=np.float64).reshape(-1, 3)
+        dop = np.asarray(doppler_hz, dtype=np.float64).ravel()
+        if sat.shape != sv.shape:
+            raise ValueError("sat_ecef and sat_vel must have the same shape")
+        if dop.size != len(sat):
+            raise ValueError("doppler_hz length must match sat_ecef rows")
+        w = np.ones(dop.size) if weights is None else np.asarray(weights, dtype=np.float64).ravel()
+        if w.size != dop.size:
+            raise ValueError("weights length must match doppler_hz")
+        return sat, sv, dop, w
 
-    def update_doppler_kf(self, *a, **k):
-        raise NotImplementedError("Doppler velocity Kalman update is not built")
+    def update_doppler(self, sat_ecef, sat_vel, doppler_hz, weights=None, wavelength=0.19029367279836488,
+                       sigma_mps=0.5, velocity_update_gain=0.25, max_velocity_update_mps=10.0, resample=True):
+        """Doppler likelihood of each particle's velocity (with its own clock
+        drift), then a blend of velocity_update_gain toward its Doppler WLS
+        velocity (pf_device.cu:610-748); adds to the log-weights."""
+        self._require_init()
+        sat, sv, dop, w = self._doppler_args(sat_ecef, sat_vel, doppler_hz, weights)
+        self._flush()
+        self._ensure_vel().doppler(sat, sv, dop, w, float(wavelength), float(sigma_mps),
+                                   float(velocity_update_gain), float(max_velocity_update_mps), kf=False)
+        if resample:
+            self.resample_if_needed()
+
+    def update_doppler_kf(self, sat_ecef, sat_vel, doppler_hz, weights=None, wavelength=0.19029367279836488,
+                          sigma_mps=0.5, resample=True):
+        """Sequential Kalman update of each particle's velocity by the
+        Doppler rows, with the innovation likelihood added to the
+        log-weights (pf_device.cu:750-887)."""
+        self._require_init()
+        sat, sv, dop, w = self._doppler_args(sat_ecef, sat_vel, doppler_hz, weights)
+        self._flush()
+        self._ensure_vel().doppler(sat, sv, dop, w, float(wavelength), float(sigma_mps), kf=True)
+        if resample:
+            self.resample_if_needed()
 
     def enable_smoothing(self):
         raise NotImplementedError("forward-backward smoothing is not built")
@@ -381,11 +452,17 @@ class ParticleFilterDevice:
         return self._engine.particles(0)
 
     def get_particle_states(self):
-        """(n_particles, 16) rows [x, y, z, clock_bias, 12 zeros]: the
-        reference's layout, whose velocity columns this filter does not model."""
+        """(n_particles, 16) rows [x, y, z, clock_bias, vx, vy, vz, 3x3
+        velocity covariance row-major] (ECEF, m, m/s)."""
         p = self.get_particles()
         out = np.zeros((len(p), 16))
         out[:, :4] = p
+        if self._vel is not None:
+            self._vel.follow()
+            out[:, 4:] = self._vel.host()
+        else:
+            out[:, 4:7] = self._v_shared
+            out[:, [7, 11, 15]] = self._var_shared
         return out
 
     def set_particle_states(self, states):
@@ -401,6 +478,8 @@ class ParticleFilterDevice:
         st[:3] = ((arr[:, :3] - anchor) @ self._rot.T).T
         st[3] = arr[:, 3] - clk[0]
         self._engine.set_state_f32(0, st, np.zeros(self.n_particles, np.float32))
+        if arr.shape[1] == 16:
+            self._ensure_vel().set_host(arr[:, 4:])
 
     def get_log_weights(self):
         """Current log-weights as FP64."""

@@ -188,6 +188,27 @@ typedef struct {
 } pf_obs_row_t;
 #define PF_MAX_OBS_ROWS 128
 
+/* Per-particle velocity states (pfe_vel_*): caller-owned device memory of
+ * 2 x 12 x n doubles (n = the filter's particles): two buffers, component c
+ * of particle j at buf[c * n + j] with c = 0..2 the ECEF velocity (m/s) and
+ * 3..11 its 3x3 covariance row-major.  `sel` is the buffer holding the
+ * current states and `seq` the resample already followed; both are kept by
+ * the calls (initialise by pfe_vel_init). */
+typedef struct {
+  double* buf;
+  int sel;
+  unsigned seq;
+} pf_vel_state_t;
+
+/* One Doppler observation (pfe_vel_doppler). */
+typedef struct {
+  double sat[3];      /* satellite ECEF position, m      */
+  double sat_vel[3];  /* satellite ECEF velocity, m/s    */
+  double doppler_hz;  /* range rate = -doppler * lambda  */
+  double weight;
+} pf_doppler_row_t;
+#define PF_MAX_DOPPLER_ROWS 64
+
 typedef enum { PF_LW_OVERWRITE = 0, PF_LW_ACCUMULATE = 1 } pf_lw_mode_t;
 typedef enum {
   PF_SYS_OFFSET_RANDOM = 0,    /* Philox draw per filter and epoch            */
@@ -420,6 +441,31 @@ int pfe_add_position_term(pf_engine_t* eng, int filter, const double* refs_ecef,
  * pfe_add_position_term. */
 int pfe_add_obs_term(pf_engine_t* eng, int filter, int kind, const pf_obs_row_t* rows, int n_rows,
                      double sigma, double gate, double huber_k, int accumulate);
+
+/* Velocity states of filter f (pf_device.cu:67-100): v = v0 (+ spread_vel
+ * N(0, 1) per axis when > 0), covariance init_sigma^2 I, in buffer 0.
+ * `step` keys the random draws. */
+int pfe_vel_init(pf_engine_t* eng, int filter, pf_vel_state_t* vs, const double v0_ecef[3], double spread_vel,
+                 double init_sigma, unsigned step);
+/* Follows the filter's last resample (gathers the states through its
+ * ancestors) unless already followed.  Call after every step that may
+ * resample, before the next one. */
+int pfe_vel_follow(pf_engine_t* eng, int filter, pf_vel_state_t* vs);
+/* Velocity predict (pf_device.cu:106-187): v = (1 - alpha) v + alpha guide
+ * (+ sigma_vel noise unless kf), positions += v dt + noise, the noise
+ * N(0, sigma_pos^2 I + dt^2 P_v) when kf != 0 (and P_v += q dt I), else
+ * N(0, sigma_pos^2 I).  Clocks are not moved: the next pfe_step (flags
+ * PF_EP_PREDICT, zero displacement) adds their noise.  Follows a pending
+ * resample first; materialises the particles' gather. */
+int pfe_vel_predict(pf_engine_t* eng, int filter, pf_vel_state_t* vs, const double guide_ecef[3], double dt,
+                    double sigma_pos, double sigma_vel, double alpha, int kf, double q, unsigned step);
+/* Doppler likelihood over the current particles and their velocities,
+ * added to the log-weights: kf == 0 is pf_device.cu:610-748 (clock drift
+ * per particle, then a blend of gain toward the particle's WLS velocity,
+ * capped at max_update m/s when > 0); kf != 0 is pf_device.cu:750-887
+ * (sequential velocity Kalman update, innovation likelihood).  1..64 rows. */
+int pfe_vel_doppler(pf_engine_t* eng, int filter, pf_vel_state_t* vs, const pf_doppler_row_t* rows, int n_rows,
+                    double wavelength, double sigma_mps, double gain, double max_update, int kf);
 
 /* Network parameters of PF_WEIGHT_MIXTURE (host array of
  * pf_mlp_param_count() floats, copied to the engine).  Required before the

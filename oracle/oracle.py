@@ -298,6 +298,155 @@ def obs_term(x, anchor, clk_anchor, rot, kind, sat_k, obs, weight, sat_ref=None,
     return lw, res
 
 
+# ------------------------------------------------ per-particle velocity
+TAG_VEL_INIT, TAG_VEL_PREDICT = 0x06000000, 0x07000000
+
+
+def vel_normals(j, step, tag, seed, filter_id=0):
+    """The eight standard normals of particle slot j for a velocity draw:
+    Philox4x32-10 blocks (j, step, tag, filter) and (j, step, tag | 1,
+    filter), Box-Muller in FP64 (u1 = (a + 1/2) 2^-32, u2 = b 2^-32 - 1/2)."""
+    k = seed_key(seed)
+    w = np.concatenate([philox10([j, step, tag, filter_id], k), philox10([j, step, tag | 1, filter_id], k)])
+    z = np.empty(8)
+    for i in range(4):
+        u1 = (float(w[2 * i]) + 0.5) * 2.0 ** -32
+        u2 = float(w[2 * i + 1]) * 2.0 ** -32 - 0.5
+        r = np.sqrt(-2.0 * np.log(u1))
+        z[2 * i], z[2 * i + 1] = r * np.cos(2.0 * np.pi * u2), r * np.sin(2.0 * np.pi * u2)
+    return z
+
+
+def vel_predict(pos, v, P, guide, dt, sigma_pos, sigma_vel, alpha, kf, q, step, seed):
+    """Velocity predict of pf_device.cu:106-187 with this project's draws:
+    v = (1 - a) v + a g (+ sigma_vel z[0:3] unless kf); positions += v dt +
+    noise, the noise L z[0:3] with L the Cholesky factor of
+    sigma_pos^2 I + dt^2 P (kf; then P += q dt I) or sigma_pos z[k:k+3].
+    pos, v: (n, 3) ECEF; P: (n, 9) row-major.  Returns new copies."""
+    pos, v, P = np.array(pos, float), np.array(v, float), np.array(P, float)
+    a = min(1.0, max(0.0, alpha))
+    for j in range(len(pos)):
+        z = vel_normals(j, step, TAG_VEL_PREDICT, seed)
+        vj = (1.0 - a) * v[j] + a * np.asarray(guide, float)
+        zi = 0
+        if not kf and sigma_vel > 0.0:
+            vj = vj + z[0:3] * sigma_vel
+            zi = 3
+        v[j] = vj
+        if kf:
+            Pj = P[j]
+            dt2, s2 = dt * dt, sigma_pos * sigma_pos
+            a00, a01, a02 = s2 + dt2 * Pj[0], dt2 * Pj[1], dt2 * Pj[2]
+            a11, a12, a22 = s2 + dt2 * Pj[4], dt2 * Pj[5], s2 + dt2 * Pj[8]
+            l00 = np.sqrt(max(a00, 0.0))
+            l10 = a01 / l00 if l00 > 1e-12 else 0.0
+            l20 = a02 / l00 if l00 > 1e-12 else 0.0
+            l11 = np.sqrt(max(a11 - l10 * l10, 0.0))
+            l21 = (a12 - l20 * l10) / l11 if l11 > 1e-12 else 0.0
+            l22 = np.sqrt(max(a22 - l20 * l20 - l21 * l21, 0.0))
+            nz = np.array([l00 * z[0], l10 * z[0] + l11 * z[1], l20 * z[0] + l21 * z[1] + l22 * z[2]])
+            qdt = max(q, 0.0) * max(dt, 0.0)
+            P[j, [0, 4, 8]] += qdt
+        else:
+            nz = z[zi:zi + 3] * sigma_pos
+        pos[j] = pos[j] + vj * dt + nz
+    return pos, v, P
+
+
+def _solve4(A):
+    A = A.copy()
+    for col in range(4):
+        mr = col
+        for row in range(col + 1, 4):
+            if abs(A[row, col]) > abs(A[mr, col]):
+                mr = row
+        if mr != col:
+            A[[col, mr]] = A[[mr, col]]
+        if abs(A[col, col]) < 1e-12:
+            return None
+        for row in range(col + 1, 4):
+            f = A[row, col] / A[col, col]
+            A[row, col:] -= f * A[col, col:]
+    x = np.zeros(4)
+    for row in range(3, -1, -1):
+        x[row] = (A[row, 4] - A[row, row + 1:4] @ x[row + 1:4]) / A[row, row]
+    return x
+
+
+def doppler(pos, v, P, sat, sat_vel, doppler_hz, weights, wavelength, sigma, gain=0.0, max_update=0.0, kf=False):
+    """Per-particle Doppler terms in FP64: pf_device.cu:610-748 (kf False:
+    clock drift per particle, Gaussian likelihood, blend toward the WLS
+    velocity) and pf_device.cu:750-887 (kf True: sequential velocity KF,
+    innovation likelihood).  Returns (log_w (n,), v, P) copies."""
+    pos, v, P = np.array(pos, float), np.array(v, float), np.array(P, float)
+    n = len(pos)
+    lw = np.zeros(n)
+    obs = -np.asarray(doppler_hz, float) * wavelength
+    w_all = np.maximum(np.asarray(weights, float), 0.0)
+    for j in range(n):
+        d = sat - pos[j]
+        r = np.linalg.norm(d, axis=1)
+        ok = r >= 1.0
+        los = d / np.where(ok, r, 1.0)[:, None]
+        svr = np.sum(sat_vel * los, axis=1)
+        if not kf:
+            rxr = los @ v[j]
+            wsum = float(np.sum(w_all[ok]))
+            if wsum <= 0.0:
+                continue
+            cd = float(np.sum((w_all * (obs - svr + rxr))[ok])) / wsum
+            pred = np.sum((sat_vel - v[j]) * los, axis=1) + cd
+            res = obs - pred
+            lw[j] = float(np.sum((-0.5 * w_all * res * res / (sigma * sigma))[ok]))
+            g = min(1.0, max(0.0, gain))
+            if g <= 0.0 or len(obs) < 4:
+                continue
+            A = np.zeros((4, 5))
+            for s in np.nonzero(ok)[0]:
+                h = np.array([-los[s, 0], -los[s, 1], -los[s, 2], 1.0])
+                rhs = obs[s] - svr[s]
+                A[:, 4] += h * w_all[s] * rhs
+                A[:, :4] += np.outer(h, h) * w_all[s]
+            A[range(4), range(4)] += 1e-9
+            sol = _solve4(A)
+            if sol is None:
+                continue
+            dv = sol[:3] - v[j]
+            nrm = np.linalg.norm(dv)
+            if max_update > 0.0 and nrm > max_update:
+                dv = dv * (max_update / max(nrm, 1e-9))
+            v[j] = v[j] + g * dv
+        else:
+            use = ok & (w_all > 0.0)
+            wsum = float(np.sum(w_all[use]))
+            if wsum <= 0.0:
+                continue
+            hm = np.sum(-los[use] * w_all[use, None], axis=0) / wsum
+            ym = float(np.sum(w_all[use] * (obs - svr)[use])) / wsum
+            Pj = P[j].reshape(3, 3).copy()
+            mu = v[j].copy()
+            for s in np.nonzero(use)[0]:
+                h = -los[s] - hm
+                yc = (obs[s] - svr[s]) - ym
+                ph = Pj @ h
+                S = float(h @ ph) + sigma * sigma / w_all[s]
+                if not (S > 1e-18) or not np.isfinite(S):
+                    continue
+                innov = yc - float(h @ mu)
+                K = ph / S
+                mu = mu + K * innov
+                Pj = Pj - np.outer(K, h @ Pj)
+                for a_, b_ in ((0, 1), (0, 2), (1, 2)):
+                    m = 0.5 * (Pj[a_, b_] + Pj[b_, a_])
+                    Pj[a_, b_] = Pj[b_, a_] = m if np.isfinite(m) else 0.0
+                for a_ in range(3):
+                    Pj[a_, a_] = Pj[a_, a_] if (np.isfinite(Pj[a_, a_]) and Pj[a_, a_] > 1e-12) else 1e-12
+                lw[j] += -0.5 * (innov * innov / S + np.log(S))
+            v[j] = mu
+            P[j] = Pj.reshape(9)
+    return lw, v, P
+
+
 def stats(x, lw, anchor, clk_anchor, rot):
     x = _f64(x)
     D, n = x.shape

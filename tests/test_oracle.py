@@ -294,3 +294,58 @@ def test_obs_term_known_answers():
     lw, _ = O.obs_term(np.zeros((4, 1)), np.zeros(3), [cb], np.eye(3), O.OBS_CARRIER_AFV, sat_k=sats, obs=cyc,
                        weight=np.ones(5), wavelength=wl, sigma=0.05)
     assert lw[0] == pytest.approx(-0.5 * 0.2 ** 2 / 0.05 ** 2, abs=1e-5)
+
+
+# ---------------------------------------------- velocity states, Doppler
+L1 = 0.19029367279836488
+
+
+def doppler_case():
+    """Receiver, satellites and a known receiver velocity and clock drift
+    (reference tests/test_cuda_streams.py:61-88)."""
+    rx = np.array([-3957199.0, 3310205.0, 3737911.0])
+    true_vel = np.array([0.3, -0.5, 0.8])
+    sat = np.array([[-14985000.0, -3988000.0, 21474000.0], [-9575000.0, 15498000.0, 19457000.0],
+                    [7624000.0, -16218000.0, 19843000.0], [16305000.0, 12037000.0, 17183000.0],
+                    [-20889000.0, 13759000.0, 8291000.0], [5463000.0, 24413000.0, 8934000.0]])
+    sv = np.array([[1200.0, -2800.0, 500.0], [-800.0, 1500.0, -2700.0], [2500.0, 1800.0, -900.0],
+                   [-1100.0, -2200.0, 2100.0], [600.0, 2900.0, 1300.0], [-2600.0, 400.0, -1800.0]])
+    los = (sat - rx) / np.linalg.norm(sat - rx, axis=1)[:, None]
+    dop = -(np.sum((sv - true_vel) * los, axis=1) + 5.0) / L1
+    return rx, sat, sv, dop, true_vel
+
+
+def test_doppler_oracle_known_answers():
+    """The reference's Doppler tests (tests/test_cuda_streams.py:285-337):
+    WLS blend with gain 1 recovers the velocity to 1e-3, the velocity KF
+    from sigma 10 to 2e-2 with the variances shrinking."""
+    rx, sat, sv, dop, tv = doppler_case()
+    pos = np.tile(rx, (4, 1))
+    _, v, _ = O.doppler(pos, np.zeros((4, 3)), np.zeros((4, 9)), sat, sv, dop, np.ones(6), L1, 0.5, gain=1.0,
+                        max_update=100.0)
+    np.testing.assert_allclose(v, np.tile(tv, (4, 1)), atol=1e-3)
+    lw, v, P = O.doppler(pos, np.zeros((4, 3)), np.tile(100.0 * np.eye(3).ravel(), (4, 1)), sat, sv, dop, np.ones(6),
+                         L1, 0.5, kf=True)
+    np.testing.assert_allclose(v, np.tile(tv, (4, 1)), atol=2e-2)
+    assert np.all(P[:, [0, 4, 8]] < 100.0) and np.all(P[:, [0, 4, 8]] > 0.0)
+    # the likelihood prefers the true velocity
+    lw_true, _, _ = O.doppler(pos[:1], tv[None], np.zeros((1, 9)), sat, sv, dop, np.ones(6), L1, 0.5)
+    lw_off, _, _ = O.doppler(pos[:1], (tv + 1.0)[None], np.zeros((1, 9)), sat, sv, dop, np.ones(6), L1, 0.5)
+    assert lw_true[0] == pytest.approx(0.0, abs=1e-9) and lw_off[0] < -1.0
+
+
+def test_velocity_predict_oracle_known_answers():
+    """Reference tests/test_cuda_streams.py:239-283: the guide becomes every
+    particle's velocity and moves it by v dt; in KF mode the positions spread
+    by sqrt(sigma_pos^2 + dt^2 var) and the variances grow by q dt."""
+    n = 400
+    pos, v, P = O.vel_predict(np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 9)), [2.0, -1.0, 0.5], 0.25, 0.0, 0.0,
+                              1.0, False, 0.0, 1, 42)
+    np.testing.assert_allclose(pos, np.tile([0.5, -0.25, 0.125], (n, 1)), atol=1e-12)
+    np.testing.assert_allclose(v, np.tile([2.0, -1.0, 0.5], (n, 1)))
+    P0 = np.tile(4.0 * np.eye(3).ravel(), (n, 1))
+    pos, v, P = O.vel_predict(np.zeros((n, 3)), np.tile([1.0, 0, 0], (n, 1)), P0, [1.0, 0.0, 0.0], 1.0, 1.0, 100.0,
+                              1.0, True, 0.5, 1, 42)
+    np.testing.assert_allclose(v, np.tile([1.0, 0.0, 0.0], (n, 1)))
+    assert 1.9 < np.std(pos[:, 0] - 1.0) < 2.6 and 1.9 < np.std(pos[:, 1]) < 2.6
+    np.testing.assert_allclose(P[:, [0, 4, 8]], 4.5)

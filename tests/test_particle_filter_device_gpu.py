@@ -231,15 +231,11 @@ class TestWrapper:
         assert np.all(np.isfinite(est)) and np.linalg.norm(est[:3] - rover) < 2.0
 
     def test_not_built_paths_raise(self, PFD):
-        with pytest.raises(NotImplementedError):
-            PFD(n_particles=1024, sigma_vel=1.0)
-        with pytest.raises(NotImplementedError):
-            PFD(n_particles=1024, rbpf_velocity_kf=True)
         pf = PFD(n_particles=1024)
         with pytest.raises(RuntimeError):
             pf.predict()
         pf.initialize(ORIGIN, clock_bias=ORIGIN_CB)
-        for name in ("update_doppler", "update_doppler_kf", "store_epoch", "smooth"):
+        for name in ("store_epoch", "smooth"):
             with pytest.raises(NotImplementedError):
                 getattr(pf, name)(None)
         with pytest.raises(RuntimeError):
@@ -554,3 +550,131 @@ def test_obs_term_rejects_bad_rows(PFD):
         pf.update_dd_carrier_afv(res)
     with pytest.raises(ValueError):
         pf.update_dd_pseudorange(res, sigma_pr=0.0)
+
+
+# ------------------------------------------------- velocity states, Doppler
+from test_oracle import doppler_case, L1  # noqa: E402
+
+
+class TestVelocityWrapper:
+    """The reference's velocity-state tests (tests/test_cuda_streams.py:
+    216-337, 406-505), through the drop-in."""
+
+    def test_states_include_velocity_and_covariance(self, PFD):
+        pf = PFD(n_particles=2048, seed=SEED)
+        pf.initialize(np.array([10.0, 20.0, 30.0]), clock_bias=ORIGIN_CB, spread_pos=0.0, spread_cb=0.0,
+                      velocity=np.array([1.5, -2.0, 0.25]), spread_vel=0.0, velocity_init_sigma=2.0)
+        st = pf.get_particle_states()
+        assert st.shape == (2048, 16)
+        np.testing.assert_allclose(st[:, :3], np.tile([10.0, 20.0, 30.0], (2048, 1)), atol=1e-5)
+        np.testing.assert_allclose(st[:, 4:7], np.tile([1.5, -2.0, 0.25], (2048, 1)))
+        np.testing.assert_allclose(st[:, [7, 11, 15]], 4.0)
+        np.testing.assert_allclose(st[:, [8, 9, 10, 12, 13, 14]], 0.0)
+
+    def test_predict_moves_by_the_guide(self, PFD):
+        pf = PFD(n_particles=2048, seed=SEED, velocity_guide_alpha=0.999999999)
+        pf.initialize(ORIGIN, clock_bias=ORIGIN_CB, spread_pos=0.0, spread_cb=0.0)
+        pf.predict(velocity=np.array([2.0, -1.0, 0.5]), dt=0.25, sigma_pos=0.0)
+        st = pf.get_particle_states()
+        np.testing.assert_allclose(st[:, :3], np.tile([0.5, -0.25, 0.125], (2048, 1)), atol=1e-5)
+        np.testing.assert_allclose(st[:, 4:7], np.tile([2.0, -1.0, 0.5], (2048, 1)), atol=1e-8)
+
+    def test_rbpf_predict_spreads_by_velocity_covariance(self, PFD):
+        pf = PFD(n_particles=20_000, seed=SEED, rbpf_velocity_kf=True, velocity_process_noise=0.5)
+        pf.initialize(ORIGIN, clock_bias=ORIGIN_CB, spread_pos=0.0, spread_cb=0.0, velocity=np.array([1.0, 0, 0]),
+                      velocity_init_sigma=2.0)
+        pf.predict(velocity=np.array([1.0, 0.0, 0.0]), dt=1.0, sigma_pos=1.0)
+        st = pf.get_particle_states()
+        np.testing.assert_allclose(st[:, 4:7], np.tile([1.0, 0.0, 0.0], (20_000, 1)))
+        for i, c in enumerate((1.0, 0.0, 0.0)):
+            assert 1.6 < float(np.std(st[:, i] - c)) < 2.4
+        np.testing.assert_allclose(st[:, [7, 11, 15]], 4.5)
+
+    def test_wrapper_rbpf_predict_controls(self, PFD):
+        pf = PFD(n_particles=4096, seed=SEED, rbpf_velocity_kf=True, velocity_process_noise=0.25)
+        pf.initialize(ORIGIN, clock_bias=ORIGIN_CB, spread_pos=0.0, spread_cb=0.0, velocity=np.array([0.5, -0.25, 0.0]),
+                      velocity_init_sigma=1.0)
+        pf.predict(velocity=np.array([0.5, -0.25, 0.0]), dt=2.0, sigma_pos=0.0)
+        st = pf.get_particle_states()
+        np.testing.assert_allclose(st[:, 4:7], np.tile([0.5, -0.25, 0.0], (4096, 1)))
+        np.testing.assert_allclose(st[:, [7, 11, 15]], 1.5)
+
+    def test_update_doppler_moves_velocity(self, PFD):
+        rx, sat, sv, dop, tv = doppler_case()
+        pf = PFD(n_particles=2048, seed=SEED, resampling="systematic")
+        pf.initialize(rx, clock_bias=ORIGIN_CB, spread_pos=0.0, spread_cb=0.0, velocity=np.zeros(3))
+        pf.update_doppler(sat, sv, dop, weights=np.ones(6), sigma_mps=0.5, velocity_update_gain=1.0,
+                          max_velocity_update_mps=100.0, resample=False)
+        np.testing.assert_allclose(pf.get_particle_states()[:, 4:7], np.tile(tv, (2048, 1)), atol=1e-3)
+
+    def test_update_doppler_kf_moves_velocity(self, PFD):
+        rx, sat, sv, dop, tv = doppler_case()
+        pf = PFD(n_particles=2048, seed=SEED, resampling="systematic")
+        pf.initialize(rx, clock_bias=ORIGIN_CB, spread_pos=0.0, spread_cb=0.0, velocity=np.zeros(3),
+                      velocity_init_sigma=10.0)
+        pf.update_doppler_kf(sat, sv, dop, weights=np.ones(6), sigma_mps=0.5, resample=False)
+        st = pf.get_particle_states()
+        np.testing.assert_allclose(st[:, 4:7], np.tile(tv, (2048, 1)), atol=2e-2)
+        assert np.all(st[:, [7, 11, 15]] < 100.0) and np.all(st[:, [7, 11, 15]] > 0.0)
+
+
+@pytest.mark.parametrize("kf", [False, True])
+def test_velocity_predict_matches_oracle(PFD, kf):
+    n = 3000
+    pf = PFD(n_particles=n, seed=77, resampling="systematic", sigma_vel=0.0 if kf else 0.7,
+             velocity_guide_alpha=0.6, rbpf_velocity_kf=kf, velocity_process_noise=0.3)
+    pf.initialize(TOKYO_TRUE_POS, clock_bias=TOKYO_TRUE_CB, spread_pos=5.0, spread_cb=3.0,
+                  velocity=np.array([3.0, -1.0, 0.5]), spread_vel=1.5, velocity_init_sigma=0.8)
+    st0 = pf.get_particle_states()
+    guide = np.array([2.0, 1.0, -0.5])
+    pf.predict(velocity=guide, dt=0.5, sigma_pos=0.4)
+    st1 = pf.get_particle_states()
+    pos, v, P = O.vel_predict(st0[:, :3], st0[:, 4:7], st0[:, 7:], guide, 0.5, 0.4, 0.0 if kf else 0.7, 0.6, kf, 0.3,
+                              pf._step, 77)
+    np.testing.assert_allclose(st1[:, 4:7], v, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(st1[:, 7:], P, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(st1[:, :3], pos, rtol=0, atol=2e-5)  # FP32 offsets about the anchor
+
+
+@pytest.mark.parametrize("kf", [False, True])
+def test_doppler_matches_oracle(PFD, kf):
+    rx, sat, sv, dop, tv = doppler_case()
+    rng = np.random.default_rng(3)
+    dop = dop + rng.normal(0, 2.0, len(dop))
+    w = rng.uniform(0.5, 2.0, len(dop))
+    n = 2000
+    pf = PFD(n_particles=n, seed=5, resampling="systematic", rbpf_velocity_kf=kf)
+    pf.initialize(rx, clock_bias=ORIGIN_CB, spread_pos=20.0, spread_cb=10.0, velocity=np.array([0.5, 0.0, -0.2]),
+                  spread_vel=1.0, velocity_init_sigma=3.0)
+    pf.update(sat, np.linalg.norm(sat - rx, axis=1) + ORIGIN_CB, None, resample=False)
+    before = pf.get_log_weights()
+    st0 = pf.get_particle_states()
+    if kf:
+        pf.update_doppler_kf(sat, sv, dop, weights=w, sigma_mps=0.4, resample=False)
+    else:
+        pf.update_doppler(sat, sv, dop, weights=w, sigma_mps=0.4, velocity_update_gain=0.5,
+                          max_velocity_update_mps=2.0, resample=False)
+    st1 = pf.get_particle_states()
+    # positions the device used: the FP32 offsets about the anchor, in FP64
+    x, anchor, clk, rot = _cloud(pf)
+    pos = anchor[None, :] + x[:3].T @ rot
+    lw, v, P = O.doppler(pos, st0[:, 4:7], st0[:, 7:], sat, sv, dop, w, L1, 0.4, gain=0.5, max_update=2.0, kf=kf)
+    ok, rel = lw_close(pf.get_log_weights(), before + lw, rtol=1e-6)
+    assert ok.all(), f"worst {rel.max():.2e}"
+    np.testing.assert_allclose(st1[:, 4:7], v, rtol=1e-9, atol=1e-9)
+    np.testing.assert_allclose(st1[:, 7:], P, rtol=1e-9, atol=1e-12)
+
+
+def test_velocities_follow_resampling(PFD):
+    pf = PFD(n_particles=5000, seed=9, resampling="systematic", sigma_vel=0.5, ess_threshold=0.99)
+    pf.initialize(TOKYO_TRUE_POS, clock_bias=TOKYO_TRUE_CB, spread_pos=30.0, spread_cb=20.0,
+                  velocity=np.zeros(3), spread_vel=2.0)
+    before = pf.get_particle_states()
+    pf.update(TOKYO_SATS, TOKYO_PR, None, resample=True)       # resamples (threshold 0.99)
+    anc = pf.get_resample_ancestors()
+    after = pf.get_particle_states()
+    np.testing.assert_array_equal(after[:, 4:], before[anc, 4:])
+    np.testing.assert_allclose(after[:, :3], before[anc, :3], atol=1e-4)
+    pf.predict(velocity=np.array([1.0, 0, 0]), dt=1.0)
+    pf.update(TOKYO_SATS, TOKYO_PR, None)
+    assert np.all(np.isfinite(pf.estimate()))
