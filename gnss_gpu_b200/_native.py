@@ -71,6 +71,11 @@ OBS_ROW_DTYPE = np.dtype([("sat_k", "<f8", 3), ("sat_ref", "<f8", 3), ("obs", "<
                           ("base_ref", "<f8"), ("weight", "<f8"), ("wavelength", "<f8")])
 
 
+class Mesh(C.Structure):
+    _fields_ = [("nodes", C.c_void_p), ("tris", C.c_void_p), ("n_nodes", C.c_int), ("n_tris", C.c_int),
+                ("origin", C.c_double * 3), ("rot", C.c_double * 9)]
+
+
 class VelState(C.Structure):
     _fields_ = [("buf", C.c_void_p), ("sel", C.c_int), ("seq", C.c_uint)]
 
@@ -110,7 +115,8 @@ EXPORTED = [
     "pf_mlp_param_count", "pf_mlp_scratch_bytes", "pf_mlp_grad", "pf_mlp_adam_step", "pf_mlp_forward",
     "pfe_set_mlp", "pfe_get_sat_debug", "pfe_set_epoch_ctas_per_sm", "pfe_set_likelihood", "pfe_shift",
     "pfe_add_position_term", "pfe_add_obs_term", "pfe_step_io", "pfe_vel_init", "pfe_vel_follow",
-    "pfe_vel_predict", "pfe_vel_doppler",
+    "pfe_vel_predict", "pfe_vel_doppler", "pf_mesh_build", "pf_mesh_los", "pfe_add_3d_term",
+    "pf_weight_3d",
 ]
 
 _lib = None
@@ -192,6 +198,10 @@ def load():
     L.pfe_vel_follow.argtypes = [p, i, vs]
     L.pfe_vel_predict.argtypes = [p, i, vs, dp, d, d, d, d, i, d, C.c_uint]
     L.pfe_vel_doppler.argtypes = [p, i, vs, C.c_void_p, i, d, d, d, d, i]
+    L.pf_mesh_build.argtypes = [dp, i, C.c_void_p, C.c_void_p, C.POINTER(C.c_int), dp, dp]
+    L.pf_mesh_los.argtypes = [C.POINTER(Mesh), C.c_void_p, C.c_void_p, i, i, C.c_void_p, C.c_void_p]
+    L.pfe_add_3d_term.argtypes = [p, i, C.POINTER(Mesh), dp, i, d, d, d, d, d, i]
+    L.pf_weight_3d.argtypes = [dp, dp, dp, dp, dp, dp, dp, dp, i, dp, i, i, d, d, d, d, d]
     L.pfe_get_sat_debug.argtypes = [p, i, p, i, C.POINTER(C.c_int)]
     for name in EXPORTED:
         fn = getattr(L, name)

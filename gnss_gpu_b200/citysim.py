@@ -229,3 +229,23 @@ def sat_az_el(rot: np.ndarray, p_ecef: np.ndarray, sats: np.ndarray):
     u = u / np.linalg.norm(u, axis=1, keepdims=True)
     e = u @ rot.T
     return np.mod(np.arctan2(e[:, 0], e[:, 1]), 2 * np.pi), np.arcsin(np.clip(e[:, 2], -1.0, 1.0))
+
+
+def city_triangles(city: City, anchor_ecef, rot) -> np.ndarray:
+    """The city's buildings as a triangle mesh (T, 3, 3) in ECEF: per
+    building four walls and a roof, two triangles each.  anchor_ecef is the
+    city origin, rot the ECEF -> local E/N/U rotation."""
+    ix, iy = np.nonzero(city.occ)
+    x0, x1 = city.box[ix, iy, 0], city.box[ix, iy, 1]
+    y0, y1 = city.box[ix, iy, 2], city.box[ix, iy, 3]
+    h = city.height[ix, iy]
+    z = np.zeros_like(h)
+    # corners: 0..3 at the ground, 4..7 at the roof (x0y0, x1y0, x1y1, x0y1)
+    cx = np.stack([x0, x1, x1, x0, x0, x1, x1, x0], axis=1)
+    cy = np.stack([y0, y0, y1, y1, y0, y0, y1, y1], axis=1)
+    cz = np.stack([z, z, z, z, h, h, h, h], axis=1)
+    corners = np.stack([cx, cy, cz], axis=-1)                   # (B, 8, 3) local
+    faces = np.array([[0, 1, 5], [0, 5, 4], [1, 2, 6], [1, 6, 5], [2, 3, 7], [2, 7, 6], [3, 0, 4], [3, 4, 7],
+                      [4, 5, 6], [4, 6, 7]])
+    tri_local = corners[:, faces, :].reshape(-1, 3, 3)
+    return np.asarray(anchor_ecef, dtype=np.float64) + tri_local @ np.asarray(rot, dtype=np.float64)

@@ -16,6 +16,7 @@
 #include <mutex>
 #include <vector>
 
+#include "pf_bvh.cuh"
 #include "pf_common.cuh"
 #include "pf_status.h"
 
@@ -86,6 +87,32 @@ struct Carve {
 inline int grid_of(int n) { return (n + kB - 1) / kB; }
 
 // --------------------------------------------------------------- kernels
+// Building-aware likelihood of FP64 particle arrays (weight_3d.cu:86-177):
+// one thread per particle, a ray per satellite through the mesh hierarchy.
+__global__ void c_weight_3d(const double* px, const double* py, const double* pz, const double* pcb,
+                            pfb::MeshDev m, const pfb::Sat3d* sats, pfb::Weight3dArgs a, double* lw, int n) {
+  __shared__ pfb::Sat3d s_sat[pfb::kMax3dSats];
+  for (int i = threadIdx.x; i < a.n_sat; i += blockDim.x) s_sat[i] = sats[i];
+  __syncthreads();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const double p[3] = {px[j], py[j], pz[j]};
+  const float3 o = pfb::mesh_origin(m, p);
+  double acc = 0.0;
+  for (int s = 0; s < a.n_sat; ++s) {
+    const pfb::Sat3d& sv = s_sat[s];
+    const double v[3] = {sv.sat[0] - p[0], sv.sat[1] - p[1], sv.sat[2] - p[2]};
+    const double L = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    const bool blocked = pfb::bvh_blocked(m, o, pfb::mesh_dir(m, v, L), (float)L);
+    const double r = sv.pr - (L + pcb[j]);
+    const double los = -0.5 * sv.w * r * r * a.inv_s2_los;
+    const double rn = r > 0.0 ? r - a.nlos_bias : r;
+    const double nlos = -0.5 * sv.w * rn * rn * a.inv_s2_nlos;
+    acc += pfb::mix_loglik(los, nlos, blocked ? a.p_blocked : a.p_clear);
+  }
+  lw[j] = acc;
+}
+
 __global__ void c_init(double* px, double* py, double* pz, double* pcb, double ix, double iy,
                        double iz, double icb, double sp, double scb, int n, uint32_t k0,
                        uint32_t k1) {
@@ -546,6 +573,73 @@ int pf_resample_megopolis(double* px, double* py, double* pz, double* pcb, const
   CK(cudaMemcpyAsync(py, oy, nb, cudaMemcpyDeviceToHost, w->stream));
   CK(cudaMemcpyAsync(pz, oz, nb, cudaMemcpyDeviceToHost, w->stream));
   CK(cudaMemcpyAsync(pcb, ocb, nb, cudaMemcpyDeviceToHost, w->stream));
+  return finish(w);
+}
+
+int pf_weight_3d(const double* px, const double* py, const double* pz, const double* pcb, const double* sat_ecef,
+                 const double* pseudoranges, const double* weights_sat, const double* triangles, int n_tri,
+                 double* log_weights, int n_particles, int n_sat, double sigma_los, double sigma_nlos,
+                 double nlos_bias, double blocked_nlos_prob, double clear_nlos_prob) {
+  clear_err();
+  int s = check_n(n_particles);
+  if (s != PF_OK) return s;
+  if (n_sat <= 0 || n_sat > pfb::kMax3dSats) return set_err(PF_ECAP, "need 1..%d satellites", pfb::kMax3dSats);
+  if (n_tri < 0 || (n_tri > 0 && !triangles)) return set_err(PF_EINVAL, "bad triangles");
+  if (!px || !py || !pz || !pcb || !sat_ecef || !pseudoranges || !weights_sat || !log_weights)
+    return set_err(PF_EINVAL, "null array");
+  if (!(sigma_los > 0.0) || !(sigma_nlos > 0.0) || !isfinite(sigma_los) || !isfinite(sigma_nlos) ||
+      !isfinite(nlos_bias) || !isfinite(blocked_nlos_prob) || !isfinite(clear_nlos_prob))
+    return set_err(PF_EINVAL, "sigmas must be > 0 and all parameters finite");
+  std::vector<float> nodes((size_t)std::max(1, 2 * n_tri) * 8), tris((size_t)std::max(1, n_tri) * 12);
+  int n_nodes = 0;
+  double origin[3], rot[9];
+  if ((s = pf_mesh_build(triangles, n_tri, nodes.data(), tris.data(), &n_nodes, origin, rot)) != PF_OK) return s;
+  std::vector<pfb::Sat3d> sv(n_sat);
+  for (int i = 0; i < n_sat; ++i) {
+    for (int k = 0; k < 3; ++k) sv[i].sat[k] = sat_ecef[3 * i + k];
+    sv[i].pr = pseudoranges[i];
+    sv[i].w = weights_sat[i];
+  }
+  std::lock_guard<std::mutex> lk(g_mu);
+  const size_t nb = (size_t)n_particles * 8;
+  const size_t nodes_b = sizeof(float) * nodes.size(), tris_b = sizeof(float) * tris.size();
+  Workspace* w;
+  if ((s = workspace(5 * align_up(nb, 256) + align_up(sizeof(pfb::Sat3d) * n_sat, 256) + align_up(nodes_b, 256) +
+                         align_up(tris_b, 256),
+                     &w)) != PF_OK)
+    return s;
+  Carve c{(unsigned char*)w->buf};
+  double *dx = c.take<double>(n_particles), *dy = c.take<double>(n_particles),
+         *dz = c.take<double>(n_particles), *dcb = c.take<double>(n_particles),
+         *dlw = c.take<double>(n_particles);
+  pfb::Sat3d* dsat = c.take<pfb::Sat3d>(n_sat);
+  float* dnodes = c.take<float>(nodes.size());
+  float* dtris = c.take<float>(tris.size());
+  CK(cudaMemcpyAsync(dx, px, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dy, py, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dz, pz, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dcb, pcb, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dsat, sv.data(), sizeof(pfb::Sat3d) * n_sat, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dnodes, nodes.data(), nodes_b, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dtris, tris.data(), tris_b, cudaMemcpyHostToDevice, w->stream));
+  pfb::MeshDev m;
+  memset(&m, 0, sizeof(m));
+  m.nodes = reinterpret_cast<const float4*>(dnodes);
+  m.tris = reinterpret_cast<const float4*>(dtris);
+  m.n_nodes = n_nodes;
+  m.n_tris = n_tri;
+  for (int k = 0; k < 3; ++k) m.origin[k] = origin[k];
+  for (int k = 0; k < 9; ++k) m.rot[k] = rot[k];
+  pfb::Weight3dArgs a;
+  memset(&a, 0, sizeof(a));
+  a.n_sat = n_sat;
+  a.inv_s2_los = 1.0 / (sigma_los * sigma_los);
+  a.inv_s2_nlos = 1.0 / (sigma_nlos * sigma_nlos);
+  a.nlos_bias = nlos_bias;
+  a.p_blocked = blocked_nlos_prob;
+  a.p_clear = clear_nlos_prob;
+  c_weight_3d<<<grid_of(n_particles), kB, 0, w->stream>>>(dx, dy, dz, dcb, m, dsat, a, dlw, n_particles);
+  CK(cudaMemcpyAsync(log_weights, dlw, nb, cudaMemcpyDeviceToHost, w->stream));
   return finish(w);
 }
 

@@ -14,6 +14,7 @@
 #include "pf_epoch_kernel.cuh"
 #include "pf_obs_terms.cuh"
 #include "pf_velocity.cuh"
+#include "pf_weight3d.cuh"
 #include "pf_status.h"
 
 using namespace pfb;
@@ -1430,6 +1431,113 @@ int pfe_vel_doppler(pf_engine_t* eng, int filter, pf_vel_state_t* vs, const pf_d
     case 5: k_doppler<5><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, vb, dr, a); break;
     case 6: k_doppler<6><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, vb, dr, a); break;
     default: k_doppler<7><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, vb, dr, a); break;
+  }
+  CK(cudaGetLastError());
+  const int zero = 0;
+  CK(cudaMemcpyAsync(reinterpret_cast<char*>(eng->ctrl_dev + filter) + offsetof(FilterCtrl, lw_zero), &zero,
+                     sizeof(int), cudaMemcpyHostToDevice, eng->stream));
+  return sync_and_check(eng);
+}
+
+static int mesh_dev(const pf_mesh_t* mesh, MeshDev& m) {
+  if (!mesh) return set_err(PF_EINVAL, "null mesh");
+  if (mesh->n_nodes < 0 || mesh->n_tris < 0 || (mesh->n_nodes > 0 && (!mesh->nodes || !mesh->tris)))
+    return set_err(PF_EINVAL, "mesh: bad node or triangle arrays");
+  if (mesh->n_nodes > 2 * mesh->n_tris) return set_err(PF_EINVAL, "mesh: more nodes than the builder makes");
+  memset(&m, 0, sizeof(m));
+  m.nodes = static_cast<const float4*>(mesh->nodes);
+  m.tris = static_cast<const float4*>(mesh->tris);
+  m.n_nodes = mesh->n_nodes;
+  m.n_tris = mesh->n_tris;
+  for (int i = 0; i < 3; ++i) m.origin[i] = mesh->origin[i];
+  for (int i = 0; i < 9; ++i) m.rot[i] = mesh->rot[i];
+  return PF_OK;
+}
+
+int pf_mesh_build(const double* tris_ecef, int n_tri, float* nodes_out, float* tris_out, int* n_nodes,
+                  double origin[3], double rot[9]) {
+  clear_err();
+  if (n_tri < 0 || (n_tri > 0 && (!tris_ecef || !nodes_out || !tris_out)) || !n_nodes || !origin || !rot)
+    return set_err(PF_EINVAL, "null argument");
+  double o[3] = {0.0, 0.0, 0.0};
+  for (int i = 0; i < n_tri * 9; ++i) {
+    if (!isfinite(tris_ecef[i])) return set_err(PF_EINVAL, "triangle coordinate %d not finite", i);
+    o[i % 3] += tris_ecef[i];
+  }
+  if (n_tri > 0)
+    for (int a = 0; a < 3; ++a) o[a] /= 3.0 * n_tri;
+  double R[9];
+  enu_rotation(o, R);
+  std::vector<double> tm((size_t)n_tri * 9);
+  for (int i = 0; i < n_tri * 3; ++i) {
+    const double v[3] = {tris_ecef[3 * (size_t)i] - o[0], tris_ecef[3 * (size_t)i + 1] - o[1],
+                         tris_ecef[3 * (size_t)i + 2] - o[2]};
+    for (int r = 0; r < 3; ++r) tm[3 * (size_t)i + r] = R[3 * r] * v[0] + R[3 * r + 1] * v[1] + R[3 * r + 2] * v[2];
+  }
+  HostBvh h;
+  build_bvh(tm, n_tri, h);
+  if (h.n_nodes > 2 * n_tri) return set_err(PF_ECUDA, "internal: node count above 2 n");
+  if (h.n_nodes) memcpy(nodes_out, h.nodes.data(), sizeof(float) * h.nodes.size());
+  if (n_tri) memcpy(tris_out, h.tris.data(), sizeof(float) * h.tris.size());
+  *n_nodes = h.n_nodes;
+  for (int a = 0; a < 3; ++a) origin[a] = o[a];
+  for (int a = 0; a < 9; ++a) rot[a] = R[a];
+  return PF_OK;
+}
+
+int pf_mesh_los(const pf_mesh_t* mesh, const double* d_rx, const double* d_sat, int n_rx, int n_sat,
+                unsigned char* d_los_out, void* stream) {
+  clear_err();
+  MeshDev m;
+  int s = mesh_dev(mesh, m);
+  if (s != PF_OK) return s;
+  if (n_rx < 0 || n_sat < 0) return set_err(PF_EINVAL, "negative sizes");
+  const long long total = (long long)n_rx * n_sat;
+  if (total == 0) return PF_OK;
+  if (!d_rx || !d_sat || !d_los_out) return set_err(PF_EINVAL, "null argument");
+  int dev = 0, sms = 148;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int g = (int)std::max(1LL, std::min((long long)sms * 8, (total + kThreads - 1) / kThreads));
+  k_bvh_los<<<g, kThreads, 0, (cudaStream_t)stream>>>(m, d_rx, d_sat, n_rx, n_sat, d_los_out);
+  CK(cudaGetLastError());
+  return PF_OK;
+}
+
+int pfe_add_3d_term(pf_engine_t* eng, int filter, const pf_mesh_t* mesh, const double* sats, int n_sat,
+                    double sigma_los, double sigma_nlos, double nlos_bias, double p_blocked, double p_clear,
+                    int accumulate) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!eng->initialized[filter]) return set_err(PF_ENOTINIT, "filter %d not initialized", filter);
+  MeshDev m;
+  if ((s = mesh_dev(mesh, m)) != PF_OK) return s;
+  if (n_sat < 1 || n_sat > kMax3dSats || !sats) return set_err(PF_ECAP, "need 1..%d satellites", kMax3dSats);
+  for (int i = 0; i < 5 * n_sat; ++i)
+    if (!isfinite(sats[i])) return set_err(PF_EINVAL, "satellite value %d not finite", i);
+  if (!(sigma_los > 0.0) || !(sigma_nlos > 0.0) || !isfinite(sigma_los) || !isfinite(sigma_nlos) ||
+      !isfinite(nlos_bias) || !isfinite(p_blocked) || !isfinite(p_clear))
+    return set_err(PF_EINVAL, "sigmas must be > 0 and all parameters finite");
+  static_assert(sizeof(Sat3d) * kMax3dSats <= sizeof(ObsRow) * kMaxObsRows, "scratch size");
+  CK(cudaMemcpyAsync(eng->obs_rows, sats, sizeof(Sat3d) * n_sat, cudaMemcpyHostToDevice, eng->stream));
+  Weight3dArgs a;
+  memset(&a, 0, sizeof(a));
+  a.n_sat = n_sat;
+  a.accumulate = accumulate ? 1 : 0;
+  a.inv_s2_los = 1.0 / (sigma_los * sigma_los);
+  a.inv_s2_nlos = 1.0 / (sigma_nlos * sigma_nlos);
+  a.nlos_bias = nlos_bias;
+  a.p_blocked = p_blocked;
+  a.p_clear = p_clear;
+  const FilterDesc& d = eng->hdesc[filter];
+  const Sat3d* sv = reinterpret_cast<const Sat3d*>(eng->obs_rows);
+  const int g = std::max(1, std::min(eng->sm_count * 16, (d.n + kThreads - 1) / kThreads));
+  switch (eng->D) {
+    case 4: k_weight_3d<4><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, m, sv, a); break;
+    case 5: k_weight_3d<5><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, m, sv, a); break;
+    case 6: k_weight_3d<6><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, m, sv, a); break;
+    default: k_weight_3d<7><<<g, kThreads, 0, eng->stream>>>(eng->dev, filter, m, sv, a); break;
   }
   CK(cudaGetLastError());
   const int zero = 0;

@@ -1,0 +1,80 @@
+// pf_weight3d.cuh -- the engine's building-aware likelihood and the
+// line-of-sight queries over a device mesh (hierarchy and traversal in
+// pf_bvh.cuh).
+#pragma once
+#include "pf_bvh.cuh"
+#include "pf_engine_kernels.cuh"
+
+namespace pfb {
+
+// Building-aware pseudorange likelihood (weight_3d.cu:86-177): per
+// satellite a ray from the particle; blocked rays use the NLOS-prior
+// p_blocked, clear ones p_clear, in a mixture of a tight LOS Gaussian and a
+// wide NLOS Gaussian whose positive residuals are reduced by nlos_bias.
+template <int D>
+__global__ void __launch_bounds__(kThreads) k_weight_3d(EngineDev e, int f, MeshDev m, const Sat3d* sats,
+                                                        Weight3dArgs a) {
+  __shared__ Sat3d s_sat[kMax3dSats];
+  for (int i = threadIdx.x; i < a.n_sat; i += kThreads) s_sat[i] = sats[i];
+  __syncthreads();
+  const FilterDesc* fd = e.desc + f;
+  const FilterCtrl* fc = e.ctrl + f;
+  const int n = fd->n;
+  const long long base = fd->p_off;
+  const float* src = fc->parity ? e.state1 : e.state0;
+  const bool keep = a.accumulate && fc->lw_zero == 0;
+  const bool gather = fc->resample_flag != 0;
+  // one particle per thread: the traversals are latency bound, so many
+  // threads in flight matter more than per-thread reuse
+  for (int j = blockIdx.x * kThreads + threadIdx.x; j < n; j += gridDim.x * kThreads) {
+    int src_j = j;
+    if (gather) {
+      src_j = __ldcg(e.anc + base + j);
+      if ((unsigned)src_j >= (unsigned)n) src_j = j;
+    }
+    const float* sp = src + base + src_j;
+    const float x0 = __ldcg(sp), x1 = __ldcg(sp + e.p_total), x2 = __ldcg(sp + 2 * e.p_total),
+                x3 = __ldcg(sp + 3 * e.p_total);
+    double p[3];
+    local_to_ecef(fd->rot, fc->anchor, (double)x0, (double)x1, (double)x2, p);
+    const double cb = fc->clk_anchor[0] + (double)x3;
+    const float3 o = mesh_origin(m, p);
+    double acc = 0.0;
+    for (int s = 0; s < a.n_sat; ++s) {
+      const Sat3d& sv = s_sat[s];
+      const double v[3] = {sv.sat[0] - p[0], sv.sat[1] - p[1], sv.sat[2] - p[2]};
+      const double L = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      const bool blocked = bvh_blocked(m, o, mesh_dir(m, v, L), (float)L);
+      const double r = sv.pr - (L + cb);
+      const double los = -0.5 * sv.w * r * r * a.inv_s2_los;
+      const double rn = r > 0.0 ? r - a.nlos_bias : r;
+      const double nlos = -0.5 * sv.w * rn * rn * a.inv_s2_nlos;
+      acc += mix_loglik(los, nlos, blocked ? a.p_blocked : a.p_clear);
+    }
+    const float l0 = keep ? e.lw[base + j] : 0.f;
+    e.lw[base + j] = (float)((double)l0 + acc);
+  }
+}
+
+// Line of sight of n_ray rays: receiver rx[i / n_sat] to satellite
+// sat[i] (ECEF, FP64); los[i] = 1 when clear.  Non-finite inputs give 0.
+__global__ void __launch_bounds__(kThreads) k_bvh_los(MeshDev m, const double* rx, const double* sat, int n_rx,
+                                                      int n_sat, unsigned char* los) {
+  const long long total = (long long)n_rx * n_sat;
+  for (long long i = blockIdx.x * (long long)kThreads + threadIdx.x; i < total; i += (long long)gridDim.x * kThreads) {
+    const long long r = i / n_sat;
+    const double p[3] = {rx[3 * r], rx[3 * r + 1], rx[3 * r + 2]};
+    const double s[3] = {sat[3 * i], sat[3 * i + 1], sat[3 * i + 2]};
+    bool ok = true;
+    for (int a = 0; a < 3; ++a) ok = ok && isfinite(p[a]) && isfinite(s[a]);
+    if (!ok) {
+      los[i] = 0;
+      continue;
+    }
+    const double v[3] = {s[0] - p[0], s[1] - p[1], s[2] - p[2]};
+    const double L = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    los[i] = bvh_blocked(m, mesh_origin(m, p), mesh_dir(m, v, L), (float)L) ? 0 : 1;
+  }
+}
+
+}  // namespace pfb

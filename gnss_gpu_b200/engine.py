@@ -215,6 +215,18 @@ class Engine:
         N.check(self.lib.pfe_add_obs_term(self.h, int(k), int(kind), N.vptr(r) if len(r) else None, len(r),
                                           float(sigma), float(gate), float(huber_k), 1 if accumulate else 0))
 
+    def add_3d_term(self, k: int, mesh, sats_ecef, pr, w, sigma_los: float, sigma_nlos: float, nlos_bias: float,
+                    p_blocked: float, p_clear: float, accumulate: bool = False):
+        """Building-aware pseudorange likelihood of filter k through `mesh`
+        (an N.Mesh of a BVHAccelerator); overwrites the log-weights unless
+        accumulate."""
+        sats = np.ascontiguousarray(np.column_stack([np.asarray(sats_ecef, np.float64).reshape(-1, 3),
+                                                     np.asarray(pr, np.float64).ravel(),
+                                                     np.asarray(w, np.float64).ravel()]))
+        N.check(self.lib.pfe_add_3d_term(self.h, int(k), C.byref(mesh), N.dptr(sats.reshape(-1)), len(sats),
+                                         float(sigma_los), float(sigma_nlos), float(nlos_bias), float(p_blocked),
+                                         float(p_clear), 1 if accumulate else 0))
+
     # ------------------------------------------------------ velocity states
     def velocity_states(self, k: int) -> "VelocityStates":
         """Per-particle velocity states of filter k (device memory allocated

@@ -209,6 +209,20 @@ typedef struct {
 } pf_doppler_row_t;
 #define PF_MAX_DOPPLER_ROWS 64
 
+/* A triangle mesh with its bounding-volume hierarchy on the device
+ * (pf_mesh_build fills the host side; the caller copies nodes and tris to
+ * device memory and sets the pointers).  nodes: n_nodes x 8 floats;
+ * tris: n_tris x 12 floats; coordinates in the mesh frame: East/North/Up at
+ * `origin` (ECEF, m), rot the ECEF -> mesh rotation (rows E, N, U). */
+typedef struct {
+  const void* nodes;
+  const void* tris;
+  int n_nodes;
+  int n_tris;
+  double origin[3];
+  double rot[9];
+} pf_mesh_t;
+
 typedef enum { PF_LW_OVERWRITE = 0, PF_LW_ACCUMULATE = 1 } pf_lw_mode_t;
 typedef enum {
   PF_SYS_OFFSET_RANDOM = 0,    /* Philox draw per filter and epoch            */
@@ -466,6 +480,38 @@ int pfe_vel_predict(pf_engine_t* eng, int filter, pf_vel_state_t* vs, const doub
  * (sequential velocity Kalman update, innovation likelihood).  1..64 rows. */
 int pfe_vel_doppler(pf_engine_t* eng, int filter, pf_vel_state_t* vs, const pf_doppler_row_t* rows, int n_rows,
                     double wavelength, double sigma_mps, double gain, double max_update, int kf);
+
+/* Builds the hierarchy of n_tri triangles (ECEF, m; n_tri x 9 doubles:
+ * v0, v1, v2) into host arrays: nodes_out (capacity 2 * n_tri x 8 floats),
+ * tris_out (n_tri x 12 floats), the node count, the mesh frame's origin and
+ * rotation (python/gnss_gpu/bvh.py BVHAccelerator, src/raytrace/bvh.cu). */
+int pf_mesh_build(const double* tris_ecef, int n_tri, float* nodes_out, float* tris_out, int* n_nodes,
+                  double origin[3], double rot[9]);
+/* Stateless building-aware likelihood of FP64 host particle arrays, the
+ * reference's _gnss_gpu_pf3d.pf_weight_3d (weight_3d.cu:182-253; px..pcb
+ * n_particles each, sat_ecef n_sat x 3, triangles n_tri x 9 ECEF):
+ * log_weights[i] = sum over satellites of the LOS/NLOS mixture term. */
+int pf_weight_3d(const double* px, const double* py, const double* pz, const double* pcb, const double* sat_ecef,
+                 const double* pseudoranges, const double* weights_sat, const double* triangles, int n_tri,
+                 double* log_weights, int n_particles, int n_sat, double sigma_los, double sigma_nlos,
+                 double nlos_bias, double blocked_nlos_prob, double clear_nlos_prob);
+/* Line of sight of n_rx x n_sat rays, receiver rx[i] (device, n_rx x 3
+ * doubles) to satellite sat[i][s] (device, n_rx x n_sat x 3 doubles):
+ * los_out (device, n_rx x n_sat bytes) 1 when clear, 0 when blocked or not
+ * finite.  Asynchronous on `stream` (BVHAccelerator.check_los_batch). */
+int pf_mesh_los(const pf_mesh_t* mesh, const double* d_rx, const double* d_sat, int n_rx, int n_sat,
+                unsigned char* d_los_out, void* stream);
+/* Building-aware pseudorange likelihood over filter f's current particles
+ * (weight_3d.cu:86-177, weight_3d_bvh.cu): per satellite (sats: n_sat x 5
+ * doubles x, y, z, pseudorange, weight; 1..64) a ray through the mesh;
+ * blocked rays use the NLOS prior p_blocked, clear ones p_clear, in the
+ * mixture of N(r; 0, sigma_los) and N(r'; 0, sigma_nlos) with r' = r -
+ * nlos_bias for r > 0.  accumulate != 0 adds to the log-weights, 0
+ * overwrites them (the reference).  Statistics follow as for
+ * pfe_add_position_term. */
+int pfe_add_3d_term(pf_engine_t* eng, int filter, const pf_mesh_t* mesh, const double* sats, int n_sat,
+                    double sigma_los, double sigma_nlos, double nlos_bias, double p_blocked, double p_clear,
+                    int accumulate);
 
 /* Network parameters of PF_WEIGHT_MIXTURE (host array of
  * pf_mlp_param_count() floats, copied to the engine).  Required before the

@@ -73,6 +73,9 @@ def lib():
         L.orc_pf_megopolis_ref_ancestors.argtypes = [F64, i32, i32, C.c_ulonglong, I32]
         L.orc_num_threads.restype = i32
         L.orc_set_threads.argtypes = [i32]
+        U8 = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+        L.orc_los.argtypes = [F64, F64, i32, i32, F64, i32, U8]
+        L.orc_weight_3d.argtypes = [i32, F64, F64, i32, F64, F64, i32, f64, f64, f64, f64, f64, F64, P]
         _lib = L
     return _lib
 
@@ -445,6 +448,34 @@ def doppler(pos, v, P, sat, sat_vel, doppler_hz, weights, wavelength, sigma, gai
             v[j] = mu
             P[j] = Pj.reshape(9)
     return lw, v, P
+
+
+# ------------------------------------------------ building-aware likelihood
+def los(rx, sat, tris):
+    """Line of sight by brute-force FP64 ray casting (weight_3d.cu:14-48):
+    rx (R, 3), sat (R, S, 3), tris (T, 3, 3) ECEF -> (R, S) bool."""
+    rx = _f64(rx).reshape(-1, 3)
+    sat = _f64(sat).reshape(len(rx), -1, 3)
+    tri = _f64(tris).reshape(-1, 9)
+    out = np.zeros(sat.shape[:2], np.uint8)
+    lib().orc_los(rx, sat.reshape(-1), len(rx), sat.shape[1], tri.reshape(-1), len(tri), out.reshape(-1))
+    return out.astype(bool)
+
+
+def weight_3d(pos, cb, sats, tris, sigma_los, sigma_nlos, nlos_bias, p_blocked, p_clear):
+    """FP64 log-weights of the building-aware likelihood (weight_3d.cu:86-177)
+    and the (n, S) blocked flags.  pos (n, 3) ECEF, cb (n,), sats (S, 5)
+    rows x, y, z, pr, w, tris (T, 3, 3)."""
+    pos = _f64(pos).reshape(-1, 3)
+    n = len(pos)
+    sv = _f64(sats).reshape(-1, 5)
+    tri = _f64(tris).reshape(-1, 9)
+    lw = np.zeros(n)
+    blk = np.zeros((n, len(sv)), np.uint8)
+    lib().orc_weight_3d(n, pos.reshape(-1), _f64(cb).reshape(-1), len(sv), sv.reshape(-1), tri.reshape(-1), len(tri),
+                        float(sigma_los), float(sigma_nlos), float(nlos_bias), float(p_blocked), float(p_clear), lw,
+                        blk.ctypes.data)
+    return lw, blk.astype(bool)
 
 
 def stats(x, lw, anchor, clk_anchor, rot):

@@ -15,6 +15,8 @@
  *   resampling.cu:175-272  reference Megopolis -> orc_pf_megopolis_ref
  *   Chesser et al. arXiv:2109.13504, canonical Megopolis -> orc_megopolis
  *   particle_filter.py:129-175 update order   -> orc_epoch
+ *   weight_3d.cu:14-177    building-aware likelihood (brute-force ray
+ *                          casting, LOS/NLOS mixture) -> orc_los, orc_weight_3d
  * Random numbers: Philox4x32-10 from Salmon et al., SC'11, with this
  * project's counter layout (particle, epoch, tag, filter), so the oracle and
  * the CUDA path draw identical 32-bit words.  Normals: Box-Muller in FP64.
@@ -523,4 +525,74 @@ void orc_set_threads(int n) {
 #else
   (void)n;
 #endif
+}
+
+/* ----------------------------------------------------------------------
+ * Building-aware likelihood (weight_3d.cu:14-177): Moller-Trumbore in FP64
+ * against every triangle, then the LOS/NLOS mixture per satellite.
+ * tris: n_tri x 9 (v0, v1, v2, ECEF). */
+static int orc_tri_hit(const double o[3], const double d[3], const double* t, double max_t) {
+  const double e1[3] = {t[3] - t[0], t[4] - t[1], t[5] - t[2]};
+  const double e2[3] = {t[6] - t[0], t[7] - t[1], t[8] - t[2]};
+  const double h[3] = {d[1] * e2[2] - d[2] * e2[1], d[2] * e2[0] - d[0] * e2[2], d[0] * e2[1] - d[1] * e2[0]};
+  const double a = e1[0] * h[0] + e1[1] * h[1] + e1[2] * h[2];
+  if (fabs(a) < 1e-12) return 0;
+  const double f = 1.0 / a;
+  const double s[3] = {o[0] - t[0], o[1] - t[1], o[2] - t[2]};
+  const double u = f * (s[0] * h[0] + s[1] * h[1] + s[2] * h[2]);
+  if (u < 0.0 || u > 1.0) return 0;
+  const double q[3] = {s[1] * e1[2] - s[2] * e1[1], s[2] * e1[0] - s[0] * e1[2], s[0] * e1[1] - s[1] * e1[0]};
+  const double v = f * (d[0] * q[0] + d[1] * q[1] + d[2] * q[2]);
+  if (v < 0.0 || u + v > 1.0) return 0;
+  const double tt = f * (e2[0] * q[0] + e2[1] * q[1] + e2[2] * q[2]);
+  return tt > 1e-6 && tt < max_t;
+}
+
+static int orc_blocked(const double p[3], const double sat[3], const double* tris, int n_tri) {
+  const double v[3] = {sat[0] - p[0], sat[1] - p[1], sat[2] - p[2]};
+  const double dist = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  const double d[3] = {v[0] / dist, v[1] / dist, v[2] / dist};
+  for (int t = 0; t < n_tri; ++t)
+    if (orc_tri_hit(p, d, tris + 9 * (size_t)t, dist)) return 1;
+  return 0;
+}
+
+/* los[r * n_sat + s] = 1 when rx[r] sees sat[r * n_sat + s]. */
+void orc_los(const double* rx, const double* sat, int n_rx, int n_sat, const double* tris, int n_tri,
+             unsigned char* los) {
+#pragma omp parallel for schedule(dynamic, 16)
+  for (long long i = 0; i < (long long)n_rx * n_sat; ++i)
+    los[i] = orc_blocked(rx + 3 * (i / n_sat), sat + 3 * i, tris, n_tri) ? 0 : 1;
+}
+
+static double orc_mix(double los, double nlos, double p) {
+  if (p <= 0.0) return los;
+  if (p >= 1.0) return nlos;
+  const double a = log(1.0 - p) + los, b = log(p) + nlos;
+  const double m = a > b ? a : b;
+  return m + log(exp(a - m) + exp(b - m));
+}
+
+/* pos: n x 3 ECEF, cb: n; sats: n_sat x 5 (x, y, z, pr, w).  lw_out: n;
+ * blocked_out (n x n_sat, may be NULL). */
+void orc_weight_3d(int n, const double* pos, const double* cb, int n_sat, const double* sats, const double* tris,
+                   int n_tri, double sigma_los, double sigma_nlos, double nlos_bias, double p_blocked,
+                   double p_clear, double* lw_out, unsigned char* blocked_out) {
+  const double il = 1.0 / (sigma_los * sigma_los), in = 1.0 / (sigma_nlos * sigma_nlos);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int j = 0; j < n; ++j) {
+    double acc = 0.0;
+    for (int s = 0; s < n_sat; ++s) {
+      const double* sv = sats + 5 * (size_t)s;
+      const int blk = orc_blocked(pos + 3 * (size_t)j, sv, tris, n_tri);
+      if (blocked_out) blocked_out[(size_t)j * n_sat + s] = (unsigned char)blk;
+      const double dx = pos[3 * j] - sv[0], dy = pos[3 * j + 1] - sv[1], dz = pos[3 * j + 2] - sv[2];
+      const double r = sv[3] - (sqrt(dx * dx + dy * dy + dz * dz) + cb[j]);
+      const double los = -0.5 * sv[4] * r * r * il;
+      const double rn = r > 0.0 ? r - nlos_bias : r;
+      const double nlos = -0.5 * sv[4] * rn * rn * in;
+      acc += orc_mix(los, nlos, blk ? p_blocked : p_clear);
+    }
+    lw_out[j] = acc;
+  }
 }
