@@ -3,7 +3,8 @@
 `BuildingModel` holds a triangle mesh (ECEF, m); `BVHAccelerator` builds its
 hierarchy in the library (pf_mesh_build: median splits, leaves of at most 4
 triangles, stored in FP32 in an East/North/Up frame about the mesh's mean
-vertex) and keeps nodes and triangles in device memory.  They mirror
+vertex, each node holding the boxes of its two children) and keeps nodes
+and triangles in device memory.  They mirror
 python/gnss_gpu/raytrace.py BuildingModel and python/gnss_gpu/bvh.py
 BVHAccelerator of the reference for the parts the 3D particle filters use:
 construction from triangles or a Wavefront OBJ file and line-of-sight
@@ -78,7 +79,7 @@ class BVHAccelerator:
         lib = N.load()
         torch = _torch()
         n = len(tri)
-        nodes = np.zeros((max(1, 2 * n), 8), np.float32)
+        nodes = np.zeros((max(1, n), 16), np.float32)
         tris = np.zeros((max(1, n), 12), np.float32)
         n_nodes = C.c_int(0)
         origin = np.zeros(3)

@@ -9,15 +9,16 @@
 // the FP32 traversal keeps sub-millimetre precision across a city.
 //
 // Layout (device):
-//   nodes  2 x float4 per node: (bmin, a) (bmax, b) with a, b bit-cast ints;
-//          a >= 0: inner node with children a and b; a < 0: leaf holding
-//          triangles [-a - 1, -a - 1 + b).
+//   nodes  4 x float4 per inner node, the boxes of its two children:
+//          (left bmin, left ref) (left bmax, right ref) (right bmin, -)
+//          (right bmax, -), refs bit-cast ints: >= 0 an inner node, < 0 a
+//          leaf ~(first triangle << 3 | count - 1).  Node 0 is the root.
 //   tris   3 x float4 per triangle: v0, e1 = v1 - v0, e2 = v2 - v0.
-// The builder splits at the median centroid along the widest centroid
-// extent (leaves of at most kBvhLeaf triangles), so the depth stays below
-// log2(n / kBvhLeaf) + 2 and the traversal stack of kBvhStack entries
-// (at most depth + 1 are live) cannot overflow for any mesh the 32-bit
-// indices can hold.
+// The builder splits by the binned surface-area heuristic down to depth 32
+// and at the median centroid below that (leaves of at most kBvhLeaf
+// triangles), so the depth stays below 32 + log2(n / kBvhLeaf) + 2 and the
+// traversal stack of kBvhStack entries (at most depth + 1 are live) cannot
+// overflow for any mesh the 32-bit indices can hold.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -30,7 +31,7 @@
 namespace pfb {
 
 constexpr int kBvhLeaf = 4;
-constexpr int kBvhStack = 32;  // >= depth + 1 for any 32-bit triangle count
+constexpr int kBvhStack = 64;  // >= depth + 1: surface-area splits to depth 32, median below
 
 // ---------------------------------------------------------------- host
 struct HostBvh {
@@ -38,6 +39,85 @@ struct HostBvh {
   std::vector<float> tris;   // 12 floats per triangle
   int n_nodes = 0;
 };
+
+#ifndef PF_BVH_SAH
+#define PF_BVH_SAH 1
+#endif
+constexpr int kSahBins = 16;
+constexpr int kBvhSahDepth = 32;  // deeper subtrees split at the median (keeps the depth bounded)
+
+inline float half_area(const float* mn, const float* mx) {
+  const float dx = mx[0] - mn[0], dy = mx[1] - mn[1], dz = mx[2] - mn[2];
+  return dx * dy + dy * dz + dz * dx;
+}
+
+// Binned surface-area split of idx[b, e): the axis and bin boundary with
+// the least sum over children of (triangles x box surface).  Reorders
+// idx[b, e) around the boundary and returns it in mid; false when every
+// centroid falls into one bin (the caller splits at the median).
+inline bool sah_split(std::vector<int>& idx, const std::vector<float>& cen, const std::vector<float>& lo,
+                      const std::vector<float>& hi, int b, int e, const float* cmn, const float* cmx, int& mid) {
+  float best = INFINITY;
+  int best_ax = -1, best_k = 0;
+  for (int ax = 0; ax < 3; ++ax) {
+    const float ext = cmx[ax] - cmn[ax];
+    if (!(ext > 0.f)) continue;
+    const float scale = kSahBins / ext;
+    int cnt[kSahBins] = {0};
+    float bmn[kSahBins][3], bmx[kSahBins][3];
+    for (int k = 0; k < kSahBins; ++k)
+      for (int a = 0; a < 3; ++a) {
+        bmn[k][a] = INFINITY;
+        bmx[k][a] = -INFINITY;
+      }
+    for (int q = b; q < e; ++q) {
+      const int i = idx[q];
+      const int k = std::min(kSahBins - 1, (int)((cen[3 * (size_t)i + ax] - cmn[ax]) * scale));
+      ++cnt[k];
+      for (int a = 0; a < 3; ++a) {
+        bmn[k][a] = std::min(bmn[k][a], lo[3 * (size_t)i + a]);
+        bmx[k][a] = std::max(bmx[k][a], hi[3 * (size_t)i + a]);
+      }
+    }
+    // sweep: right-side prefix areas, then left to right
+    float rarea[kSahBins];
+    int rcnt[kSahBins];
+    float rmn[3] = {INFINITY, INFINITY, INFINITY}, rmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    int rc = 0;
+    for (int k = kSahBins - 1; k > 0; --k) {
+      rc += cnt[k];
+      for (int a = 0; a < 3; ++a) {
+        rmn[a] = std::min(rmn[a], bmn[k][a]);
+        rmx[a] = std::max(rmx[a], bmx[k][a]);
+      }
+      rcnt[k] = rc;
+      rarea[k] = rc ? half_area(rmn, rmx) : 0.f;
+    }
+    float lmn[3] = {INFINITY, INFINITY, INFINITY}, lmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    int lc = 0;
+    for (int k = 0; k < kSahBins - 1; ++k) {
+      lc += cnt[k];
+      for (int a = 0; a < 3; ++a) {
+        lmn[a] = std::min(lmn[a], bmn[k][a]);
+        lmx[a] = std::max(lmx[a], bmx[k][a]);
+      }
+      if (lc == 0 || rcnt[k + 1] == 0) continue;
+      const float c = lc * half_area(lmn, lmx) + rcnt[k + 1] * rarea[k + 1];
+      if (c < best) {
+        best = c;
+        best_ax = ax;
+        best_k = k;
+      }
+    }
+  }
+  if (best_ax < 0) return false;
+  const float scale = kSahBins / (cmx[best_ax] - cmn[best_ax]);
+  auto it = std::partition(idx.begin() + b, idx.begin() + e, [&](int i) {
+    return std::min(kSahBins - 1, (int)((cen[3 * (size_t)i + best_ax] - cmn[best_ax]) * scale)) <= best_k;
+  });
+  mid = (int)(it - idx.begin());
+  return mid > b && mid < e;
+}
 
 // tris_m: n x 9 doubles already in the mesh frame.
 inline void build_bvh(const std::vector<double>& tris_m, int n, HostBvh& out) {
@@ -54,7 +134,7 @@ inline void build_bvh(const std::vector<double>& tris_m, int n, HostBvh& out) {
       cen[3 * (size_t)i + a] = (float)((v0 + v1 + v2) / 3.0);
     }
   }
-  struct Item { int node, b, e; };
+  struct Item { int node, b, e, depth; };
   std::vector<float>& nodes = out.nodes;
   nodes.clear();
   auto new_node = [&]() {
@@ -62,7 +142,7 @@ inline void build_bvh(const std::vector<double>& tris_m, int n, HostBvh& out) {
     return (int)(nodes.size() / 8) - 1;
   };
   std::vector<Item> stack;
-  if (n > 0) stack.push_back({new_node(), 0, n});
+  if (n > 0) stack.push_back({new_node(), 0, n, 0});
   while (!stack.empty()) {
     const Item it = stack.back();
     stack.pop_back();
@@ -90,22 +170,69 @@ inline void build_bvh(const std::vector<double>& tris_m, int n, HostBvh& out) {
       int ax = 0;
       for (int a = 1; a < 3; ++a)
         if (cmx[a] - cmn[a] > cmx[ax] - cmn[ax]) ax = a;
-      const int mid = (it.b + it.e) / 2;
-      std::nth_element(idx.begin() + it.b, idx.begin() + mid, idx.begin() + it.e, [&](int p, int q) {
-        const float cp = cen[3 * (size_t)p + ax], cq = cen[3 * (size_t)q + ax];
-        return cp < cq || (cp == cq && p < q);
-      });
+      int mid = (it.b + it.e) / 2;
+      bool done = false;
+      if (PF_BVH_SAH && it.depth < kBvhSahDepth) done = sah_split(idx, cen, lo, hi, it.b, it.e, cmn, cmx, mid);
+      if (!done)
+        std::nth_element(idx.begin() + it.b, idx.begin() + mid, idx.begin() + it.e, [&](int p, int q) {
+          const float cp = cen[3 * (size_t)p + ax], cq = cen[3 * (size_t)q + ax];
+          return cp < cq || (cp == cq && p < q);
+        });
       const int l = new_node(), r = new_node();
       nd = &nodes[8 * (size_t)it.node];  // the vector may have moved
       ia = l;
       ib = r;
-      stack.push_back({r, mid, it.e});
-      stack.push_back({l, it.b, mid});
+      stack.push_back({r, mid, it.e, it.depth + 1});
+      stack.push_back({l, it.b, mid, it.depth + 1});
     }
     memcpy(&nd[3], &ia, 4);
     memcpy(&nd[7], &ib, 4);
   }
-  out.n_nodes = (int)(nodes.size() / 8);
+  // Child-box layout: each inner node of the binary tree becomes one node
+  // holding its two children's boxes, so a traversal tests both children
+  // at the parent, visits the nearer and never pops a missed node.
+  const int nb = (int)(nodes.size() / 8);
+  auto ia_of = [&](int k) { int v; memcpy(&v, &nodes[8 * (size_t)k + 3], 4); return v; };
+  auto ib_of = [&](int k) { int v; memcpy(&v, &nodes[8 * (size_t)k + 7], 4); return v; };
+  std::vector<int> inner_id(nb, -1);
+  int n_inner = 0;
+  for (int k = 0; k < nb; ++k)
+    if (ia_of(k) >= 0) inner_id[k] = n_inner++;
+  auto child_ref = [&](int k) {
+    const int a = ia_of(k);
+    return a >= 0 ? inner_id[k] : ~(((-a - 1) << 3) | (ib_of(k) - 1));
+  };
+  // child k's box and reference into the left (side 0) or right (side 1)
+  // slots of a node: boxes at [0..2]/[4..6] and [8..10]/[12..14], references
+  // at [3] and [7]
+  auto put_child = [&](float* dst, int side, int k) {
+    const int ref = child_ref(k);
+    for (int a = 0; a < 3; ++a) {
+      dst[8 * side + a] = nodes[8 * (size_t)k + a];
+      dst[8 * side + 4 + a] = nodes[8 * (size_t)k + 4 + a];
+    }
+    memcpy(&dst[side == 0 ? 3 : 7], &ref, 4);
+  };
+  std::vector<float> wide;
+  if (nb > 0) {
+    wide.assign((size_t)std::max(n_inner, 1) * 16, 0.f);
+    if (n_inner == 0) {  // the whole mesh is one leaf: a root with it on the left and, on the right,
+      n_inner = 1;       // a point box far outside any ray's reach
+      put_child(&wide[0], 0, 0);
+      for (int a = 0; a < 3; ++a) wide[8 + a] = wide[12 + a] = 1e30f;
+      const int none = ~0;
+      memcpy(&wide[7], &none, 4);
+    } else {
+      for (int k = 0; k < nb; ++k) {
+        if (inner_id[k] < 0) continue;
+        float* dst = &wide[16 * (size_t)inner_id[k]];
+        put_child(dst, 0, ia_of(k));
+        put_child(dst, 1, ib_of(k));
+      }
+    }
+  }
+  nodes.swap(wide);
+  out.n_nodes = nb > 0 ? n_inner : 0;
   out.tris.assign((size_t)n * 12, 0.f);
   for (int k = 0; k < n; ++k) {
     const int i = idx[k];
@@ -146,43 +273,71 @@ __device__ __forceinline__ bool tri_hit(const float3 o, const float3 d, const fl
   return t > 1e-6f && t < tmax;
 }
 
-// Is any triangle between o and o + tmax d (d unit)?  Any-hit traversal,
-// left child first; a full stack (impossible with the builder's depth
-// bound) would end the walk early and report the ray clear.
+__device__ __forceinline__ bool slab(const float4 mn, const float4 mx, const float3 o, const float3 inv, float tmax,
+                                     float& tin) {
+  float a = (mn.x - o.x) * inv.x, b = (mx.x - o.x) * inv.x;
+  float t0 = fmaxf(0.f, fminf(a, b)), t1 = fminf(tmax, fmaxf(a, b));
+  a = (mn.y - o.y) * inv.y;
+  b = (mx.y - o.y) * inv.y;
+  t0 = fmaxf(t0, fminf(a, b));
+  t1 = fminf(t1, fmaxf(a, b));
+  a = (mn.z - o.z) * inv.z;
+  b = (mx.z - o.z) * inv.z;
+  t0 = fmaxf(t0, fminf(a, b));
+  t1 = fminf(t1, fmaxf(a, b));
+  tin = t0;
+  return t0 <= t1;
+}
+
+// Triangles of leaf reference `ref` (~(start << 3 | count - 1)).
+__device__ __forceinline__ bool leaf_hit(const MeshDev& m, int ref, const float3 o, const float3 d, float tmax) {
+  const int code = ~ref, s0 = code >> 3, c = (code & 7) + 1;
+  if (s0 + c > m.n_tris) return false;  // malformed reference
+  for (int k = 0; k < c; ++k) {
+    const float4* t = m.tris + 3 * (s0 + k);
+    if (tri_hit(o, d, __ldg(t), __ldg(t + 1), __ldg(t + 2), tmax)) return true;
+  }
+  return false;
+}
+
+// Is any triangle between o and o + tmax d (d unit)?  Any-hit traversal of
+// the child-box layout: both children tested at the parent, leaves
+// intersected at once, the nearer inner child visited first, the other
+// stacked.  A full stack (impossible with the builder's depth bound) would
+// drop the farther child and could report a blocked ray clear.
 __device__ __forceinline__ bool bvh_blocked(const MeshDev& m, const float3 o, const float3 d, float tmax) {
   if (m.n_nodes <= 0) return false;
   const float3 inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
   int stack[kBvhStack];
-  int sp = 0;
-  stack[sp++] = 0;
-  while (sp > 0) {
-    const int ni = stack[--sp];
-    const float4 n0 = __ldg(m.nodes + 2 * ni), n1 = __ldg(m.nodes + 2 * ni + 1);
-    float t0 = 0.f, t1 = tmax;
-    {
-      float a = (n0.x - o.x) * inv.x, b = (n1.x - o.x) * inv.x;
-      t0 = fmaxf(t0, fminf(a, b));
-      t1 = fminf(t1, fmaxf(a, b));
-      a = (n0.y - o.y) * inv.y;
-      b = (n1.y - o.y) * inv.y;
-      t0 = fmaxf(t0, fminf(a, b));
-      t1 = fminf(t1, fmaxf(a, b));
-      a = (n0.z - o.z) * inv.z;
-      b = (n1.z - o.z) * inv.z;
-      t0 = fmaxf(t0, fminf(a, b));
-      t1 = fminf(t1, fmaxf(a, b));
+  int sp = 0, node = 0;
+  // a tree visits each node at most once: the bound only guards against a
+  // malformed mesh description (which would otherwise loop)
+  for (int visits = 0; visits <= m.n_nodes; ++visits) {
+    if ((unsigned)node >= (unsigned)m.n_nodes) return false;
+    const float4* nd = m.nodes + 4 * node;
+    const float4 l0 = __ldg(nd), l1 = __ldg(nd + 1), r0 = __ldg(nd + 2), r1 = __ldg(nd + 3);
+    float tl, tr;
+    bool hl = slab(l0, l1, o, inv, tmax, tl), hr = slab(r0, r1, o, inv, tmax, tr);
+    const int cl = __float_as_int(l0.w), cr = __float_as_int(l1.w);
+    if (hl && cl < 0) {
+      if (leaf_hit(m, cl, o, d, tmax)) return true;
+      hl = false;
     }
-    if (t0 > t1) continue;
-    const int ia = __float_as_int(n0.w), ib = __float_as_int(n1.w);
-    if (ia < 0) {
-      const int s = -ia - 1;
-      for (int k = 0; k < ib; ++k) {
-        const float4* t = m.tris + 3 * (s + k);
-        if (tri_hit(o, d, __ldg(t), __ldg(t + 1), __ldg(t + 2), tmax)) return true;
-      }
-    } else if (sp + 2 <= kBvhStack) {
-      stack[sp++] = ib;
-      stack[sp++] = ia;
+    if (hr && cr < 0) {
+      if (leaf_hit(m, cr, o, d, tmax)) return true;
+      hr = false;
+    }
+    if (hl && hr) {
+      const bool lf = tl <= tr;
+      if (sp < kBvhStack) stack[sp++] = lf ? cr : cl;
+      node = lf ? cl : cr;
+    } else if (hl) {
+      node = cl;
+    } else if (hr) {
+      node = cr;
+    } else {
+      if (sp == 0) return false;
+      node = stack[--sp];
     }
   }
   return false;

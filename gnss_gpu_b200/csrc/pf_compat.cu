@@ -590,7 +590,7 @@ int pf_weight_3d(const double* px, const double* py, const double* pz, const dou
   if (!(sigma_los > 0.0) || !(sigma_nlos > 0.0) || !isfinite(sigma_los) || !isfinite(sigma_nlos) ||
       !isfinite(nlos_bias) || !isfinite(blocked_nlos_prob) || !isfinite(clear_nlos_prob))
     return set_err(PF_EINVAL, "sigmas must be > 0 and all parameters finite");
-  std::vector<float> nodes((size_t)std::max(1, 2 * n_tri) * 8), tris((size_t)std::max(1, n_tri) * 12);
+  std::vector<float> nodes((size_t)std::max(1, n_tri) * 16), tris((size_t)std::max(1, n_tri) * 12);
   int n_nodes = 0;
   double origin[3], rot[9];
   if ((s = pf_mesh_build(triangles, n_tri, nodes.data(), tris.data(), &n_nodes, origin, rot)) != PF_OK) return s;

@@ -1443,7 +1443,7 @@ static int mesh_dev(const pf_mesh_t* mesh, MeshDev& m) {
   if (!mesh) return set_err(PF_EINVAL, "null mesh");
   if (mesh->n_nodes < 0 || mesh->n_tris < 0 || (mesh->n_nodes > 0 && (!mesh->nodes || !mesh->tris)))
     return set_err(PF_EINVAL, "mesh: bad node or triangle arrays");
-  if (mesh->n_nodes > 2 * mesh->n_tris) return set_err(PF_EINVAL, "mesh: more nodes than the builder makes");
+  if (mesh->n_nodes > std::max(1, mesh->n_tris)) return set_err(PF_EINVAL, "mesh: more nodes than the builder makes");
   memset(&m, 0, sizeof(m));
   m.nodes = static_cast<const float4*>(mesh->nodes);
   m.tris = static_cast<const float4*>(mesh->tris);
@@ -1459,6 +1459,7 @@ int pf_mesh_build(const double* tris_ecef, int n_tri, float* nodes_out, float* t
   clear_err();
   if (n_tri < 0 || (n_tri > 0 && (!tris_ecef || !nodes_out || !tris_out)) || !n_nodes || !origin || !rot)
     return set_err(PF_EINVAL, "null argument");
+  if (n_tri >= (1 << 28)) return set_err(PF_ECAP, "at most 2^28 - 1 triangles");
   double o[3] = {0.0, 0.0, 0.0};
   for (int i = 0; i < n_tri * 9; ++i) {
     if (!isfinite(tris_ecef[i])) return set_err(PF_EINVAL, "triangle coordinate %d not finite", i);
@@ -1476,7 +1477,7 @@ int pf_mesh_build(const double* tris_ecef, int n_tri, float* nodes_out, float* t
   }
   HostBvh h;
   build_bvh(tm, n_tri, h);
-  if (h.n_nodes > 2 * n_tri) return set_err(PF_ECUDA, "internal: node count above 2 n");
+  if (h.n_nodes > std::max(1, n_tri)) return set_err(PF_ECUDA, "internal: node count above n");
   if (h.n_nodes) memcpy(nodes_out, h.nodes.data(), sizeof(float) * h.nodes.size());
   if (n_tri) memcpy(tris_out, h.tris.data(), sizeof(float) * h.tris.size());
   *n_nodes = h.n_nodes;

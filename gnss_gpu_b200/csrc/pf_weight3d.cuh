@@ -25,7 +25,9 @@ __global__ void __launch_bounds__(kThreads) k_weight_3d(EngineDev e, int f, Mesh
   const bool keep = a.accumulate && fc->lw_zero == 0;
   const bool gather = fc->resample_flag != 0;
   // one particle per thread: the traversals are latency bound, so many
-  // threads in flight matter more than per-thread reuse
+  // threads in flight matter more than per-thread reuse.  (A warp-wide walk
+  // on a shared stack, one control path per warp, measured slower: 2.4 vs
+  // 2.0 ms at 1M particles within 2 m, 15.5 vs 5.1 ms within 100 m.)
   for (int j = blockIdx.x * kThreads + threadIdx.x; j < n; j += gridDim.x * kThreads) {
     int src_j = j;
     if (gather) {

@@ -211,8 +211,8 @@ typedef struct {
 
 /* A triangle mesh with its bounding-volume hierarchy on the device
  * (pf_mesh_build fills the host side; the caller copies nodes and tris to
- * device memory and sets the pointers).  nodes: n_nodes x 8 floats;
- * tris: n_tris x 12 floats; coordinates in the mesh frame: East/North/Up at
+ * device memory and sets the pointers).  nodes: n_nodes x 16 floats (each
+ * the boxes of two children); tris: n_tris x 12 floats; coordinates in the mesh frame: East/North/Up at
  * `origin` (ECEF, m), rot the ECEF -> mesh rotation (rows E, N, U). */
 typedef struct {
   const void* nodes;
@@ -482,7 +482,8 @@ int pfe_vel_doppler(pf_engine_t* eng, int filter, pf_vel_state_t* vs, const pf_d
                     double wavelength, double sigma_mps, double gain, double max_update, int kf);
 
 /* Builds the hierarchy of n_tri triangles (ECEF, m; n_tri x 9 doubles:
- * v0, v1, v2) into host arrays: nodes_out (capacity 2 * n_tri x 8 floats),
+ * v0, v1, v2; fewer than 2^28) into host arrays: nodes_out (capacity
+ * max(1, n_tri) x 16 floats),
  * tris_out (n_tri x 12 floats), the node count, the mesh frame's origin and
  * rotation (python/gnss_gpu/bvh.py BVHAccelerator, src/raytrace/bvh.cu). */
 int pf_mesh_build(const double* tris_ecef, int n_tri, float* nodes_out, float* tris_out, int* n_nodes,

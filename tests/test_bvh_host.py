@@ -16,7 +16,7 @@ from oracle import oracle as O
 def _build(tri):
     L = N.load()
     n = len(tri)
-    nodes = np.zeros((max(1, 2 * n), 8), np.float32)
+    nodes = np.zeros((max(1, n), 16), np.float32)
     tris = np.zeros((max(1, n), 12), np.float32)
     nn = C.c_int(0)
     origin, rot = np.zeros(3), np.zeros(9)
@@ -33,29 +33,38 @@ def city_mesh(seed=1, size=600.0):
 
 
 def test_hierarchy_is_valid():
+    """Every triangle in exactly one leaf; every child box holds the child's
+    contents; a tree rooted at node 0 reaching every node; bounded depth."""
     tri, _, _, _ = city_mesh()
     nodes, tris, origin, rot = _build(tri)
     n = len(tri)
-    assert 0 < len(nodes) <= 2 * n
-    ia = nodes[:, 3].view(np.int32)
-    ib = nodes[:, 7].view(np.int32)
+    assert 0 < len(nodes) <= n
     covered = np.zeros(n, int)
-    depth = np.zeros(len(nodes), int)
-    for k in range(len(nodes)):
-        lo, hi = nodes[k, :3], nodes[k, 4:7]
-        if ia[k] < 0:
-            s, c = -ia[k] - 1, ib[k]
-            assert 1 <= c <= 4
-            covered[s:s + c] += 1
-            v0 = tris[s:s + c, 0:3]
-            for v in (v0, v0 + tris[s:s + c, 4:7], v0 + tris[s:s + c, 8:11]):
-                assert np.all(v >= lo - 1e-3) and np.all(v <= hi + 1e-3)
-        else:
-            for ch in (ia[k], ib[k]):
-                assert np.all(nodes[ch, :3] >= lo) and np.all(nodes[ch, 4:7] <= hi)
-                depth[ch] = depth[k] + 1
+    seen = np.zeros(len(nodes), int)
+    depth_max = 0
+    stack = [(0, 0)]
+    while stack:
+        k, dep = stack.pop()
+        seen[k] += 1
+        depth_max = max(depth_max, dep)
+        for off in (0, 8):
+            lo, hi = nodes[k, off:off + 3], nodes[k, off + 4:off + 7]
+            ref = nodes[k, 3 if off == 0 else 7].view(np.int32)
+            if ref >= 0:
+                for o2 in (0, 8):
+                    assert np.all(nodes[ref, o2:o2 + 3] >= lo) and np.all(nodes[ref, o2 + 4:o2 + 7] <= hi)
+                stack.append((int(ref), dep + 1))
+            else:
+                code = ~int(ref)
+                s, c = code >> 3, (code & 7) + 1
+                assert 1 <= c <= 4
+                covered[s:s + c] += 1
+                v0 = tris[s:s + c, 0:3]
+                for v in (v0, v0 + tris[s:s + c, 4:7], v0 + tris[s:s + c, 8:11]):
+                    assert np.all(v >= lo - 1e-3) and np.all(v <= hi + 1e-3)
     assert np.all(covered == 1)
-    assert depth.max() <= np.log2(n / 4) + 2
+    assert np.all(seen == 1)
+    assert depth_max < 64  # the traversal stack: surface-area splits to depth 32, median splits below
     # the stored triangles are the input, in the mesh frame
     back = origin + (tris[:, 0:3].astype(np.float64)) @ rot
     assert np.allclose(np.sort(back[:, 0]), np.sort(tri[:, 0, 0]), atol=1e-2)
@@ -65,7 +74,9 @@ def test_empty_and_single_triangle_meshes():
     nodes, tris, _, _ = _build(np.zeros((0, 3, 3)))
     assert len(nodes) == 0
     nodes, tris, _, _ = _build(BuildingModel.create_box([0, 0, 0], 2, 2, 2).triangles[:1])
-    assert len(nodes) == 1 and nodes[0, 3].view(np.int32) == -1
+    # one leaf: a root with the leaf (triangle 0, count 1) on the left and a far point box on the right
+    assert len(nodes) == 1 and ~int(nodes[0, 3].view(np.int32)) == 0
+    assert np.all(nodes[0, 8:11] == 1e30) and np.all(nodes[0, 12:15] == 1e30)
 
 
 def test_box_and_los_oracle():
