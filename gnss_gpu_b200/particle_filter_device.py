@@ -26,8 +26,9 @@ methods on the engine's sm_100a kernels (weight mode "generic"):
   particle's velocity is the last guide.  update_doppler() and
   update_doppler_kf() work on them.
 
-Not built: the forward-backward smoother (enable_smoothing, store_epoch,
-smooth raise NotImplementedError).
+* enable_smoothing(), store_epoch() and smooth() run the reference's
+  forward-backward scheme: a second filter over the stored epochs in
+  reverse, averaged with the forward estimates.
 """
 from __future__ import annotations
 
@@ -351,14 +352,135 @@ class ParticleFilterDevice:
         if resample:
             self.resample_if_needed()
 
+    # ------------------------------------------------ forward-backward smoothing
     def enable_smoothing(self):
-        raise NotImplementedError("forward-backward smoothing is not built")
+        """Store each epoch's observations for an offline forward-backward
+        pass (particle_filter_device.py:892-899): call before the forward
+        pass, store_epoch() after each epoch, smooth() at the end."""
+        self._smooth_epochs = []
+        self._smooth_enabled = True
 
-    def store_epoch(self, *a, **k):
-        raise NotImplementedError("forward-backward smoothing is not built")
+    @staticmethod
+    def _f64(a):
+        return None if a is None else np.array(a, dtype=np.float64, copy=True)
 
-    def smooth(self, *a, **k):
-        raise NotImplementedError("forward-backward smoothing is not built")
+    def store_epoch(self, sat_ecef, pseudoranges, weights, velocity, dt, spp_ref=None, dd_pseudorange=None,
+                    dd_pseudorange_sigma=None, dd_pseudorange_source=None, dd_carrier=None, dd_carrier_sigma=None,
+                    carrier_anchor_pseudorange=None, carrier_anchor_sigma=None, carrier_afv=None,
+                    carrier_afv_sigma=None, carrier_afv_wavelength=None, doppler_update=None, doppler_sigma_mps=None,
+                    doppler_velocity_update_gain=None, doppler_max_velocity_update_mps=None):
+        """Record the epoch just processed (the arrays given to update(), the
+        predict velocity and dt, optional references and the other
+        observation updates) with the current estimate
+        (particle_filter_device.py:901-1070)."""
+        if not getattr(self, "_smooth_enabled", False):
+            return
+        f = self._f64
+
+        def dd(res, extra):
+            if res is None:
+                return None
+            d = {k: f(getattr(res, k)) for k in ("sat_ecef_k", "sat_ecef_ref", "base_range_k", "base_range_ref",
+                                                 "dd_weights") + extra}
+            d["ref_sat_ids"] = tuple(getattr(res, "ref_sat_ids", ()))
+            d["n_dd"] = int(res.n_dd)
+            return d
+
+        def rows(src, keys):
+            return None if src is None else {k: f(src[k]) for k in keys}
+
+        dop = rows(doppler_update, ("sat_ecef", "sat_vel", "doppler_hz", "weights"))
+        if dop is not None:
+            dop["wavelength_m"] = float(doppler_update.get("wavelength_m", 0.19029367279836488))
+        opt = lambda v: None if v is None else float(v)  # noqa: E731
+        self._smooth_epochs.append({
+            "estimate": np.asarray(self.estimate(), dtype=np.float64)[:3].copy(),
+            "sat_ecef": f(sat_ecef), "pseudoranges": f(pseudoranges), "weights": f(weights),
+            "velocity": f(velocity), "dt": float(dt), "spp_ref": f(spp_ref),
+            "dd_pseudorange": dd(dd_pseudorange, ("dd_pseudorange_m",)),
+            "dd_pseudorange_sigma": opt(dd_pseudorange_sigma),
+            "dd_pseudorange_source": None if dd_pseudorange_source is None else str(dd_pseudorange_source),
+            "dd_carrier": dd(dd_carrier, ("dd_carrier_cycles", "wavelengths_m")),
+            "dd_carrier_sigma": opt(dd_carrier_sigma),
+            "carrier_anchor_pseudorange": rows(carrier_anchor_pseudorange, ("sat_ecef", "pseudoranges", "weights")),
+            "carrier_anchor_sigma": opt(carrier_anchor_sigma),
+            "carrier_afv": rows(carrier_afv, ("sat_ecef", "carrier_phase_cycles", "weights")),
+            "carrier_afv_sigma": opt(carrier_afv_sigma), "carrier_afv_wavelength": opt(carrier_afv_wavelength),
+            "doppler_update": dop, "doppler_sigma_mps": opt(doppler_sigma_mps),
+            "doppler_velocity_update_gain": opt(doppler_velocity_update_gain),
+            "doppler_max_velocity_update_mps": opt(doppler_max_velocity_update_mps),
+        })
+
+    def smooth(self, position_update_sigma=None, skip_widelane_dd_pseudorange=False):
+        """Backward pass over the stored epochs with a second filter (seed +
+        1, reversed velocities, the same updates in the same order), then the
+        equal-weight average of forward and backward estimates
+        (particle_filter_device.py:1072-1251).  Returns (smoothed, forward),
+        each (n_epochs, 3) ECEF."""
+        from types import SimpleNamespace
+        if not getattr(self, "_smooth_enabled", False) or not self._smooth_epochs:
+            raise RuntimeError("No stored epochs. Call enable_smoothing() before forward pass.")
+        stored = self._smooth_epochs
+        n_ep = len(stored)
+        forward = np.array([e["estimate"] for e in stored])
+        last = stored[-1]
+        init_cb = float(np.median(last["pseudoranges"] - np.linalg.norm(
+            last["sat_ecef"].reshape(-1, 3) - last["estimate"], axis=1)))
+        bwd = ParticleFilterDevice(
+            n_particles=self.n_particles, sigma_pos=self.sigma_pos, sigma_cb=self.sigma_cb, sigma_pr=self.sigma_pr,
+            nu=self.nu, resampling=self.resampling, ess_threshold=self.ess_threshold, seed=self.seed + 1,
+            per_particle_nlos_gate=self.per_particle_nlos_gate,
+            per_particle_nlos_dd_pr_threshold_m=self.per_particle_nlos_dd_pr_threshold_m,
+            per_particle_nlos_dd_carrier_threshold_cycles=self.per_particle_nlos_dd_carrier_threshold_cycles,
+            per_particle_nlos_undiff_pr_threshold_m=self.per_particle_nlos_undiff_pr_threshold_m,
+            per_particle_huber=self.per_particle_huber, per_particle_huber_dd_pr_k=self.per_particle_huber_dd_pr_k,
+            per_particle_huber_dd_carrier_k=self.per_particle_huber_dd_carrier_k,
+            per_particle_huber_undiff_pr_k=self.per_particle_huber_undiff_pr_k, sigma_vel=self.sigma_vel,
+            velocity_guide_alpha=self.velocity_guide_alpha, rbpf_velocity_kf=self.rbpf_velocity_kf,
+            velocity_process_noise=self.velocity_process_noise, megopolis_iterations=self.megopolis_iterations,
+            max_sats=self.max_sats)
+        bwd.initialize(last["estimate"], clock_bias=init_cb, spread_pos=10.0, spread_cb=100.0,
+                       velocity_init_sigma=np.sqrt(self._var_shared) if self._vel is None else 0.0)
+        backward = np.zeros((n_ep, 3))
+        for i in range(n_ep - 1, -1, -1):
+            ep = stored[i]
+            bwd.predict(velocity=None if ep["velocity"] is None else -ep["velocity"], dt=ep["dt"])
+            sat, pr, w = ep["sat_ecef"].reshape(-1, 3), ep["pseudoranges"], ep["weights"]
+            dd_ep = ep["dd_pseudorange"]
+            if dd_ep is not None and not (skip_widelane_dd_pseudorange and ep["dd_pseudorange_source"] == "widelane"):
+                bwd.update_dd_pseudorange(SimpleNamespace(**dd_ep), sigma_pr=(
+                    ep["dd_pseudorange_sigma"] if ep["dd_pseudorange_sigma"] is not None else self.sigma_pr))
+            else:
+                bwd.correct_clock_bias(sat, pr)
+                bwd.update(sat, pr, weights=w)
+            if ep["dd_carrier"] is not None:
+                bwd.resample_if_needed()
+                bwd.update_dd_carrier_afv(SimpleNamespace(**ep["dd_carrier"]), sigma_cycles=(
+                    ep["dd_carrier_sigma"] if ep["dd_carrier_sigma"] is not None else 0.05))
+            ca = ep["carrier_anchor_pseudorange"]
+            if ca is not None:
+                bwd.update(ca["sat_ecef"], ca["pseudoranges"], weights=ca["weights"], sigma_pr=(
+                    ep["carrier_anchor_sigma"] if ep["carrier_anchor_sigma"] is not None else self.sigma_pr))
+            cafv = ep["carrier_afv"]
+            if cafv is not None:
+                bwd.resample_if_needed()
+                bwd.update_carrier_afv(cafv["sat_ecef"], cafv["carrier_phase_cycles"], weights=cafv["weights"],
+                                       wavelength=(ep["carrier_afv_wavelength"]
+                                                   if ep["carrier_afv_wavelength"] is not None else 0.190293673),
+                                       sigma_cycles=ep["carrier_afv_sigma"] if ep["carrier_afv_sigma"] is not None
+                                       else 0.05)
+            # Doppler rows constrain the forward-time velocity: the backward
+            # filter runs with reversed velocities, so (as in the reference)
+            # they are not replayed
+            if position_update_sigma is not None and ep["spp_ref"] is not None:
+                bwd.position_update(ep["spp_ref"][:3], sigma_pos=position_update_sigma)
+            backward[i] = bwd.estimate()[:3]
+        smoothed = (forward + backward) / 2.0
+        self._smooth_enabled = False
+        self._smooth_epochs = []
+        if bwd._engine is not None:
+            bwd._engine.close()
+        return smoothed, forward
 
     # ------------------------------------------------------------------
     def position_update(self, ref_ecef, sigma_pos=30.0):

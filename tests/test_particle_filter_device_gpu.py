@@ -235,9 +235,8 @@ class TestWrapper:
         with pytest.raises(RuntimeError):
             pf.predict()
         pf.initialize(ORIGIN, clock_bias=ORIGIN_CB)
-        for name in ("store_epoch", "smooth"):
-            with pytest.raises(NotImplementedError):
-                getattr(pf, name)(None)
+        with pytest.raises(RuntimeError):
+            pf.smooth()  # no stored epochs
         with pytest.raises(RuntimeError):
             pf.get_resample_ancestors()  # megopolis
 
@@ -678,3 +677,60 @@ def test_velocities_follow_resampling(PFD):
     pf.predict(velocity=np.array([1.0, 0, 0]), dt=1.0)
     pf.update(TOKYO_SATS, TOKYO_PR, None)
     assert np.all(np.isfinite(pf.estimate()))
+
+
+# ------------------------------------------------ forward-backward smoothing
+class TestSmoothing:
+    def test_smooth_with_dd_pseudorange_and_carrier_smoke(self, PFD):
+        """Reference tests/test_cuda_streams.py:775-831, 1002-1079."""
+        sat = np.array([[20_200_000.0, 0.0, 0.0], [0.0, 21_000_000.0, 0.0], [0.0, 0.0, 20_600_000.0],
+                        [-20_800_000.0, 2_000_000.0, 1_000_000.0]])
+        rover = np.array([0.3, -0.2, 0.1])
+        base = np.array([120.0, -35.0, 18.0])
+        rr, br = np.linalg.norm(sat - rover, axis=1), np.linalg.norm(sat - base, axis=1)
+        dd_pr = SimpleNamespace(dd_pseudorange_m=(rr[1:] - rr[0]) - (br[1:] - br[0]), sat_ecef_k=sat[1:],
+                                sat_ecef_ref=np.repeat(sat[[0]], 3, axis=0), base_range_k=br[1:],
+                                base_range_ref=np.repeat(br[0], 3), dd_weights=np.ones(3), ref_sat_ids=("G01",) * 3,
+                                n_dd=3)
+        ks, rs = np.array([1, 3, 1]), np.array([0, 2, 2])
+        wl = np.array([0.190293673, 0.192039486, 0.190293673])
+        dd_cp = SimpleNamespace(dd_carrier_cycles=((rr[ks] - rr[rs]) - (br[ks] - br[rs])) / wl, sat_ecef_k=sat[ks],
+                                sat_ecef_ref=sat[rs], base_range_k=br[ks], base_range_ref=br[rs], dd_weights=np.ones(3),
+                                wavelengths_m=wl, ref_sat_ids=("G01", "E03", "G03"), n_dd=3)
+        pf = PFD(n_particles=20_000, sigma_pos=0.1, sigma_cb=300.0, sigma_pr=5.0, resampling="systematic", seed=SEED)
+        pf.initialize(position_ecef=rover, clock_bias=0.0, spread_pos=0.2, spread_cb=10.0)
+        pf.enable_smoothing()
+        for _ in range(3):
+            pf.predict(dt=1.0)
+            pf.update_dd_pseudorange(dd_pr, sigma_pr=0.5)
+            pf.resample_if_needed()
+            pf.update_dd_carrier_afv(dd_cp, sigma_cycles=0.05)
+            pf.store_epoch(sat, rr, np.ones(4), None, 1.0, spp_ref=None, dd_pseudorange=dd_pr,
+                           dd_pseudorange_sigma=0.5, dd_carrier=dd_cp, dd_carrier_sigma=0.05)
+        smoothed, forward = pf.smooth(position_update_sigma=None)
+        assert smoothed.shape == (3, 3) and forward.shape == (3, 3)
+        assert np.all(np.isfinite(smoothed)) and np.all(np.isfinite(forward))
+        with pytest.raises(RuntimeError):
+            pf.smooth()  # the stored epochs are consumed
+
+    def test_smoothing_runs_a_noisy_drive(self, PFD):
+        rng = np.random.default_rng(11)
+        sat, _, _ = _origin_sats(8)
+        v = np.array([1.0, 0.5, 0.0])
+        truth = [ORIGIN + v * t for t in range(30)]
+        pf = PFD(n_particles=50_000, sigma_pos=0.5, sigma_cb=2.0, sigma_pr=5.0, resampling="systematic", seed=5)
+        pf.initialize(truth[0], clock_bias=ORIGIN_CB, spread_pos=5.0, spread_cb=5.0)
+        pf.enable_smoothing()
+        for t, p in enumerate(truth):
+            if t:
+                pf.predict(velocity=v, dt=1.0)
+            pr = np.linalg.norm(sat - p, axis=1) + ORIGIN_CB + rng.normal(0, 5.0, len(sat))
+            pf.update(sat, pr)
+            pf.store_epoch(sat, pr, np.ones(len(sat)), v, 1.0)
+        smoothed, forward = pf.smooth()
+        assert smoothed.shape == forward.shape == (30, 3)
+        err_f = np.linalg.norm(forward - np.array(truth), axis=1)
+        err_s = np.linalg.norm(smoothed - np.array(truth), axis=1)
+        # the reference's scheme (an independent backward filter averaged in)
+        # guarantees no gain; both passes must track the drive
+        assert np.sqrt(np.mean(err_f ** 2)) < 3.0 and np.sqrt(np.mean(err_s ** 2)) < 3.0
