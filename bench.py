@@ -13,7 +13,7 @@ filters with no exchange), timed on the device, max over ranks.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                   [--workload cfg1-systematic|cfg1-megopolis|cfg2-batched|cfg3-learned|
-                              cfg4-batched-learned|device-filter|pf3d-city]
+                              cfg4-batched-learned|device-filter|pf3d-city|orbits]
 """
 from __future__ import annotations
 
@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="cfg1-systematic",
                     choices=["cfg1-systematic", "cfg1-megopolis", "cfg2-batched", "cfg3-learned",
-                             "cfg4-batched-learned", "device-filter", "pf3d-city"])
+                             "cfg4-batched-learned", "device-filter", "pf3d-city", "orbits"])
     ap.add_argument("--epochs", type=int, default=0, help="cfg3/cfg4: evaluated epochs (default 600 / 120)")
     ap.add_argument("--n-particles", type=int, default=1_000_000)
     ap.add_argument("--path", default="epoch", choices=["epoch", "chain"],
@@ -735,6 +735,147 @@ def run_pf3d(args, world, rank, local, pg):
     return out
 
 
+def run_orbits(args, world, rank, local, pg):
+    """Input formation on the device: broadcast orbits and clocks of one day
+    at 1 Hz (86,400 epochs) x 64 satellites (40 Kepler records of G/E/J/C
+    re-selected every 2 h, 24 GLONASS states re-selected every 30 min and
+    integrated by RK4 from their toe), one pf_broadcast_orbits launch per
+    step.  value: satellite-epochs/s, inputs resident; e2e: the public
+    broadcast_orbits call with host arrays (records, index and times up,
+    positions and clocks down)."""
+    import ctypes as C
+    import torch
+    from gnss_gpu_b200 import _native as N
+    from gnss_gpu_b200.ephemeris import broadcast_orbits
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    W, K = args.warmup, args.steps
+    n_epoch = args.epochs or 86_400
+    rng = np.random.default_rng(21 + rank)
+    n_kep, n_glo = 40, 24
+    kep_sets, glo_sets = 12, 48
+    n_rec = n_kep * kep_sets + n_glo * glo_sets
+    recs = np.zeros(n_rec, N.BROADCAST_DTYPE)
+    sys_k = np.array([ord(c) for c in "G" * 16 + "E" * 12 + "J" * 4 + "C" * 8])
+    for s in range(n_kep):
+        for j in range(kep_sets):
+            r = s * kep_sets + j
+            recs["system"][r] = sys_k[s]
+            k = recs["kepler"][r:r + 1]
+            k["sqrt_a"] = 5153.6 if sys_k[s] != ord("C") else 5282.6
+            k["e"] = rng.uniform(0.001, 0.02)
+            k["i0"], k["omega0"], k["omega"] = rng.uniform(0.9, 1.0), rng.uniform(-3, 3), rng.uniform(-3, 3)
+            k["M0"], k["delta_n"], k["omega_dot"] = rng.uniform(-3, 3), 4.5e-9, -8e-9
+            k["crc"], k["crs"], k["cuc"], k["cus"] = 220.0, -14.0, -3e-6, 7e-6
+            k["toe"] = k["toc"] = 7200.0 * j + 3600.0
+            k["af0"], k["af1"], k["tgd"] = rng.uniform(-1e-4, 1e-4), -1e-12, -1e-8
+    base = n_kep * kep_sets
+    for s in range(n_glo):
+        ang = 2 * np.pi * s / n_glo
+        for j in range(glo_sets):
+            r = base + s * glo_sets + j
+            recs["system"][r] = ord("R")
+            g = recs["glonass"][r:r + 1]
+            g["toe"] = 1800.0 * j + 900.0
+            g["pos"] = (2.55e7 * np.cos(ang), 2.55e7 * np.sin(ang), 0.0)
+            v = np.sqrt(3.9860044e14 / 2.55e7)
+            g["vel"] = (-v * np.sin(ang) * 0.5, v * np.cos(ang) * 0.5, v * 0.86)
+            g["tau_n"], g["gamma_n"] = 1e-5, 1e-12
+    t = np.arange(n_epoch, dtype=np.float64) + 18.0
+    idx = np.empty((n_epoch, n_kep + n_glo), np.int32)
+    kj = np.clip(np.floor((t - 3600.0) / 7200.0 + 0.5), 0, kep_sets - 1).astype(np.int32)
+    gj = np.clip(np.floor((t - 18.0 - 900.0) / 1800.0 + 0.5), 0, glo_sets - 1).astype(np.int32)
+    for s in range(n_kep):
+        idx[:, s] = s * kep_sets + kj
+    for s in range(n_glo):
+        idx[:, n_kep + s] = base + s * glo_sets + gj
+    S_ = n_kep + n_glo
+    d_rec = torch.from_numpy(recs.view(np.uint8).copy()).to(dev)
+    d_idx = torch.from_numpy(idx).to(dev)
+    d_t = torch.from_numpy(t).to(dev)
+    d_pos = torch.empty((n_epoch, S_, 3), dtype=torch.float64, device=dev)
+    d_clk = torch.empty((n_epoch, S_), dtype=torch.float64, device=dev)
+    st = torch.cuda.Stream(dev)
+    L = N.load()
+    ptr = lambda x: C.c_void_p(x.data_ptr())  # noqa: E731
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def launch():
+        N.check(L.pf_broadcast_orbits(ptr(d_rec), n_rec, ptr(d_idx), ptr(d_t), n_epoch, S_, 60.0, ptr(d_pos),
+                                      ptr(d_clk), C.c_void_p(st.cuda_stream)))
+
+    for _ in range(W):
+        launch()
+    st.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    for i in range(K):
+        with torch.cuda.stream(st):
+            flush.fill_(i & 0xFF)
+            ev[i][0].record(st)
+        launch()
+        with torch.cuda.stream(st):
+            ev[i][1].record(st)
+    st.synchronize()
+    clk = clocks.stop()
+    t_dev = reduce_max(pg, sum(a.elapsed_time(b_) for a, b_ in ev) / 1e3)
+    units = n_epoch * S_
+    out_bytes = units * 32 + units * 4 + n_epoch * 8
+    ms = t_dev / K * 1e3
+    peak, peak_kind = peaks()
+    out = {
+        "metric": "broadcast orbit satellite-epochs/s (positions + clocks, multi-GNSS)",
+        "value": units * K * world / t_dev, "unit": "satellite-epochs/s", "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic broadcast records",
+        "config": {"workload": f"orbits: {n_epoch} epochs x {S_} satellites ({n_kep} Kepler G/E/J/C re-selected "
+                               f"every 2 h, {n_glo} GLONASS RK4 from toe re-selected every 30 min), "
+                               f"{n_rec} records",
+                   "epochs": n_epoch, "satellites": S_, "parallelism": f"replicas x{world}",
+                   "l2": "flushed between steps (outside the event intervals)"},
+        "gpu_launches": K,
+        "roofline": {"bound": "hbm", "achieved": out_bytes / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": out_bytes / (ms / 1e3) / 1e9 / peak, "peak_kind": f"{peak_kind} hbm_gbs",
+                     "traffic": None,
+                     "note": "FP64 math (Kepler iterations, sin/cos/atan2, RK4) bounds this kernel, "
+                             "not HBM: 36 B moved per satellite-epoch"},
+        "clocks": clk,
+    }
+    if not args.no_e2e:
+        ts = []
+        for i in range(max(3, min(K, 5))):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            pos, clk_h = broadcast_orbits(recs, t, idx)
+            ts.append(time.perf_counter() - t0)
+        e2e_t = float(np.median(ts))
+        out["e2e"] = {"value": units * world / e2e_t, "unit": "satellite-epochs/s",
+                      "h2d_bytes_per_step": int(recs.nbytes + idx.nbytes + t.nbytes),
+                      "d2h_bytes_per_step": int(units * 32), "timing": "host clock, median of calls"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import orbit as OO
+        m = 600
+        t0 = time.perf_counter()
+        for s in range(S_):
+            for r in np.unique(idx[:m, s]):
+                e_ = np.nonzero(idx[:m, s] == r)[0]
+                if recs["system"][r] == ord("R"):
+                    g = recs["glonass"][r]
+                    st_ = {"toe": float(g["toe"]), "pos": g["pos"], "vel": g["vel"], "acc": g["acc"],
+                           "tau_n": float(g["tau_n"]), "gamma_n": float(g["gamma_n"])}
+                    for e in e_:
+                        OO.glonass(st_, float(t[e]))
+                else:
+                    rec = {f: float(recs["kepler"][f][r]) for f in N.EPHEMERIS_FIELDS}
+                    OO.kepler(rec, chr(recs["system"][r]), t[e_])
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": m * S_ / dt, "unit": "satellite-epochs/s", "cores": 1, "kind": "port",
+                               "sample": f"oracle FP64 (numpy Kepler per record, Python RK4 per GLONASS "
+                                         f"epoch), first {m} epochs x {S_} satellites, {dt:.1f} s"}
+    return out
+
+
 # ------------------------------------------------------- reference arm
 def run_reference(args, world, rank):
     if rank != 0:
@@ -774,6 +915,8 @@ def main():
         out = run_device_filter(args, world, rank, local, pg)
     elif args.workload == "pf3d-city":
         out = run_pf3d(args, world, rank, local, pg)
+    elif args.workload == "orbits":
+        out = run_orbits(args, world, rank, local, pg)
     elif args.workload in ("cfg3-learned", "cfg4-batched-learned"):
         out = run_learned(args, world, rank, local, pg, args.workload == "cfg4-batched-learned")
     else:

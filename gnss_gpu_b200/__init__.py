@@ -11,6 +11,8 @@ from .particle_filter_device import ParticleFilterDevice
 from .particle_filter_3d import ParticleFilter3D, ParticleFilter3DBVH
 from .bvh import BVHAccelerator, BuildingModel
 from .engine import Engine, EngineOptions, FilterSpec
+from .ephemeris import Ephemeris
+from .nav_rinex import NavMessage, read_nav_rinex
 
-__all__ = ["ParticleFilter", "ParticleFilterDevice", "ParticleFilter3D", "ParticleFilter3DBVH", "BVHAccelerator",
+__all__ = ["ParticleFilter", "Ephemeris", "NavMessage", "read_nav_rinex", "ParticleFilterDevice", "ParticleFilter3D", "ParticleFilter3DBVH", "BVHAccelerator",
            "BuildingModel", "Engine", "EngineOptions", "FilterSpec"]

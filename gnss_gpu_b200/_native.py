@@ -84,6 +84,19 @@ class VelState(C.Structure):
 DOPPLER_ROW_DTYPE = np.dtype([("sat", "<f8", 3), ("sat_vel", "<f8", 3), ("doppler_hz", "<f8"), ("weight", "<f8")])
 
 
+# pf_ephemeris_t (the reference's EphemerisParams layout), pf_glonass_state_t,
+# pf_broadcast_t (system letter, then the two record kinds overlaid)
+EPHEMERIS_FIELDS = ("sqrt_a", "e", "i0", "omega0", "omega", "M0", "delta_n", "omega_dot", "idot",
+                    "cuc", "cus", "crc", "crs", "cic", "cis", "toe", "af0", "af1", "af2", "toc", "tgd")
+EPHEMERIS_DTYPE = np.dtype([(k, "<f8") for k in EPHEMERIS_FIELDS] + [("week", "<i4"), ("pad_", "<i4")])
+GLONASS_DTYPE = np.dtype([("toe", "<f8"), ("pos", "<f8", 3), ("vel", "<f8", 3), ("acc", "<f8", 3),
+                          ("tau_n", "<f8"), ("gamma_n", "<f8")])
+BROADCAST_DTYPE = np.dtype({"names": ["system", "pad_", "kepler", "glonass"],
+                            "formats": ["<i4", "<i4", EPHEMERIS_DTYPE, GLONASS_DTYPE],
+                            "offsets": [0, 4, 8, 8], "itemsize": 184})
+assert EPHEMERIS_DTYPE.itemsize == 176 and GLONASS_DTYPE.itemsize == 96
+
+
 class FilterResult(C.Structure):
     _fields_ = [
         ("est_ecef", C.c_double * 3), ("est_clk", C.c_double * PF_MAX_CLK), ("cov_enu", C.c_double * 6),
@@ -116,7 +129,7 @@ EXPORTED = [
     "pfe_set_mlp", "pfe_get_sat_debug", "pfe_set_epoch_ctas_per_sm", "pfe_set_likelihood", "pfe_shift",
     "pfe_add_position_term", "pfe_add_obs_term", "pfe_step_io", "pfe_vel_init", "pfe_vel_follow",
     "pfe_vel_predict", "pfe_vel_doppler", "pf_mesh_build", "pf_mesh_los", "pfe_add_3d_term",
-    "pf_weight_3d",
+    "pf_weight_3d", "pf_sat_positions", "pf_sat_positions_batch", "pf_broadcast_orbits", "pf_sagnac",
 ]
 
 _lib = None
@@ -202,6 +215,10 @@ def load():
     L.pf_mesh_los.argtypes = [C.POINTER(Mesh), C.c_void_p, C.c_void_p, i, i, C.c_void_p, C.c_void_p]
     L.pfe_add_3d_term.argtypes = [p, i, C.POINTER(Mesh), dp, i, d, d, d, d, d, i]
     L.pf_weight_3d.argtypes = [dp, dp, dp, dp, dp, dp, dp, dp, i, dp, i, i, d, d, d, d, d]
+    L.pf_sat_positions.argtypes = [p, d, dp, dp, i]
+    L.pf_sat_positions_batch.argtypes = [p, dp, dp, dp, i, i]
+    L.pf_broadcast_orbits.argtypes = [p, i, p, p, i, i, d, p, p, p]
+    L.pf_sagnac.argtypes = [p, p, i, i, p, p, p]
     L.pfe_get_sat_debug.argtypes = [p, i, p, i, C.POINTER(C.c_int)]
     for name in EXPORTED:
         fn = getattr(L, name)

@@ -18,6 +18,7 @@
 
 #include "pf_bvh.cuh"
 #include "pf_common.cuh"
+#include "pf_orbit.cuh"
 #include "pf_status.h"
 
 namespace pfb {
@@ -641,6 +642,71 @@ int pf_weight_3d(const double* px, const double* py, const double* pz, const dou
   c_weight_3d<<<grid_of(n_particles), kB, 0, w->stream>>>(dx, dy, dz, dcb, m, dsat, a, dlw, n_particles);
   CK(cudaMemcpyAsync(log_weights, dlw, nb, cudaMemcpyDeviceToHost, w->stream));
   return finish(w);
+}
+
+// ------------------------------------------------------- input formation
+int pf_sat_positions_batch(const pf_ephemeris_t* params, const double* gps_times, double* sat_pos,
+                           double* sat_clk, int n_epoch, int n_sat) {
+  clear_err();
+  if (n_sat < 0 || n_epoch < 0) return set_err(PF_EINVAL, "n_sat and n_epoch must be >= 0");
+  if ((long long)n_epoch * n_sat > (1ll << 30)) return set_err(PF_EINVAL, "n_epoch * n_sat above 2^30");
+  if (n_sat == 0 || n_epoch == 0) return PF_OK;
+  if (!params || !gps_times || !sat_pos || !sat_clk) return set_err(PF_EINVAL, "null array");
+  int s;
+  std::lock_guard<std::mutex> lk(g_mu);
+  const size_t ne = (size_t)n_epoch * n_sat;
+  Workspace* w;
+  if ((s = workspace(align_up(sizeof(pf_ephemeris_t) * n_sat, 256) + align_up(8 * (size_t)n_epoch, 256) +
+                         align_up(24 * ne, 256) + align_up(8 * ne, 256),
+                     &w)) != PF_OK)
+    return s;
+  Carve c{(unsigned char*)w->buf};
+  pf_ephemeris_t* dp = c.take<pf_ephemeris_t>(n_sat);
+  double* dt = c.take<double>(n_epoch);
+  double* dpos = c.take<double>(3 * ne);
+  double* dclk = c.take<double>(ne);
+  CK(cudaMemcpyAsync(dp, params, sizeof(pf_ephemeris_t) * n_sat, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dt, gps_times, 8 * (size_t)n_epoch, cudaMemcpyHostToDevice, w->stream));
+  k_sat_pos_gps<<<(unsigned)((ne + kB - 1) / kB), kB, 0, w->stream>>>(dp, dt, n_epoch, n_sat, dpos, dclk);
+  CK(cudaMemcpyAsync(sat_pos, dpos, 24 * ne, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(sat_clk, dclk, 8 * ne, cudaMemcpyDeviceToHost, w->stream));
+  return finish(w);
+}
+
+int pf_sat_positions(const pf_ephemeris_t* params, double gps_time, double* sat_pos, double* sat_clk,
+                     int n_sat) {
+  return pf_sat_positions_batch(params, &gps_time, sat_pos, sat_clk, 1, n_sat);
+}
+
+int pf_broadcast_orbits(const pf_broadcast_t* d_recs, int n_recs, const int* d_rec_index, const double* d_times,
+                        int n_epoch, int n_sat, double glo_step, double* d_pos, double* d_clk, void* stream) {
+  clear_err();
+  if (n_sat < 0 || n_epoch < 0 || n_recs < 0) return set_err(PF_EINVAL, "sizes must be >= 0");
+  if ((long long)n_epoch * n_sat > (1ll << 30)) return set_err(PF_EINVAL, "n_epoch * n_sat above 2^30");
+  if (n_sat == 0 || n_epoch == 0) return PF_OK;
+  if (!d_times || (n_recs > 0 && !d_recs)) return set_err(PF_EINVAL, "null array");
+  if (!d_rec_index && n_recs < n_sat) return set_err(PF_EINVAL, "without an index, n_recs must be >= n_sat");
+  if (!isfinite(glo_step) || glo_step <= 0.0) glo_step = kGloStep;
+  if (glo_step < 1.0) return set_err(PF_EINVAL, "glo_step below 1 s");
+  const long ne = (long)n_epoch * n_sat;
+  k_broadcast_orbits<<<(unsigned)((ne + kB - 1) / kB), kB, 0, (cudaStream_t)stream>>>(
+      d_recs, n_recs, d_rec_index, d_times, n_epoch, n_sat, glo_step, d_pos, d_clk, nullptr);
+  CK(cudaGetLastError());
+  return PF_OK;
+}
+
+int pf_sagnac(const double* d_rx, const double* d_sat, int n_epoch, int n_sat, double* d_sat_rot,
+              double* d_range, void* stream) {
+  clear_err();
+  if (n_sat < 0 || n_epoch < 0) return set_err(PF_EINVAL, "sizes must be >= 0");
+  if ((long long)n_epoch * n_sat > (1ll << 30)) return set_err(PF_EINVAL, "n_epoch * n_sat above 2^30");
+  if (n_sat == 0 || n_epoch == 0) return PF_OK;
+  if (!d_rx || !d_sat) return set_err(PF_EINVAL, "null array");
+  const long ne = (long)n_epoch * n_sat;
+  k_sagnac<<<(unsigned)((ne + kB - 1) / kB), kB, 0, (cudaStream_t)stream>>>(d_rx, d_sat, n_epoch, n_sat,
+                                                                           d_sat_rot, d_range);
+  CK(cudaGetLastError());
+  return PF_OK;
 }
 
 }  // extern "C"

@@ -551,6 +551,72 @@ int pf_mlp_adam_step(const float* d_x, const float* d_y, int n, float* d_params,
 int pf_mlp_forward(const float* d_x, int n, const float* d_params, float* d_out,
                    void* stream);
 
+/* ------------------------------------------------------------------------
+ * Input formation: satellite positions and clocks from broadcast records,
+ * and the Sagnac-corrected geometric range.
+ * ---------------------------------------------------------------------- */
+
+/* Kepler broadcast record in the reference's EphemerisParams layout
+ * (include/gnss_gpu/ephemeris.h:6-29; 21 doubles, int week, 176 bytes, as
+ * packed by python/gnss_gpu/ephemeris.py:135-171).  toe / toc are seconds
+ * of week of the record's own time scale; tgd is the group delay the clock
+ * correction subtracts. */
+typedef struct {
+  double sqrt_a, e, i0, omega0, omega, M0, delta_n, omega_dot, idot;
+  double cuc, cus, crc, crs, cic, cis;
+  double toe, af0, af1, af2, toc, tgd;
+  int week;
+  int pad_;
+} pf_ephemeris_t;
+
+/* GLONASS broadcast state (python/gnss_gpu/orbit_glonass.py:38-62): toe in
+ * seconds of week of the UTC-aligned scale, PZ-90 ECEF position (m),
+ * velocity (m/s), luni-solar acceleration (m/s^2), clock bias tau_n (s) and
+ * relative frequency bias gamma_n; clock = -tau_n + gamma_n (t - toe). */
+typedef struct {
+  double toe;
+  double pos[3], vel[3], acc[3];
+  double tau_n, gamma_n;
+} pf_glonass_state_t;
+
+/* One broadcast record of any system: system is the RINEX letter ('G', 'E',
+ * 'J', 'C' use the Kepler orbit with that system's constants and time scale
+ * (ephemeris.py:36-64; BeiDou receive time is GPST - 14 s), 'R' the GLONASS
+ * integrator (GPST - 18 s); other letters use the GPS constants). */
+typedef struct {
+  int system;
+  int pad_;
+  union {
+    pf_ephemeris_t kepler;
+    pf_glonass_state_t glonass;
+  } u;
+} pf_broadcast_t;
+
+/* Replaces gnss_gpu::compute_satellite_position (include/gnss_gpu/
+ * ephemeris.h:31-36; src/ephemeris/ephemeris.cu:24-104,186-212): GPS
+ * constants, host arrays: params[n_sat], sat_pos[n_sat*3], sat_clk[n_sat]. */
+int pf_sat_positions(const pf_ephemeris_t* params, double gps_time, double* sat_pos, double* sat_clk,
+                     int n_sat);
+/* Replaces gnss_gpu::compute_satellite_position_batch (ephemeris.h:38-46;
+ * ephemeris.cu:106-180,214-246): the same records at n_epoch times,
+ * sat_pos[n_epoch*n_sat*3], sat_clk[n_epoch*n_sat]. */
+int pf_sat_positions_batch(const pf_ephemeris_t* params, const double* gps_times, double* sat_pos,
+                           double* sat_clk, int n_epoch, int n_sat);
+/* Multi-system batch in one launch, all pointers device memory, asynchronous
+ * on `stream`: output [e][s] comes from d_recs[d_rec_index[e*n_sat+s]] (from
+ * d_recs[s] when d_rec_index is NULL; an index outside [0, n_recs) gives NaN)
+ * at GPST second of week d_times[e].  d_pos (n_epoch*n_sat*3) or d_clk
+ * (n_epoch*n_sat) may be NULL.  glo_step is the GLONASS RK4 step in seconds
+ * (<= 0: 60 s, the reference's default, orbit_glonass.py:36). */
+int pf_broadcast_orbits(const pf_broadcast_t* d_recs, int n_recs, const int* d_rec_index, const double* d_times,
+                        int n_epoch, int n_sat, double glo_step, double* d_pos, double* d_clk, void* stream);
+/* Sagnac rotation and geometric range (python/gnss_gpu/range_model.py:12-40)
+ * for receivers d_rx (n_epoch*3) and satellites d_sat (n_epoch*n_sat*3),
+ * device memory, asynchronous on `stream`: d_sat_rot (n_epoch*n_sat*3) and
+ * d_range (n_epoch*n_sat), either may be NULL. */
+int pf_sagnac(const double* d_rx, const double* d_sat, int n_epoch, int n_sat, double* d_sat_rot,
+              double* d_range, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
