@@ -226,6 +226,7 @@ __device__ __forceinline__ void epoch_sys_assign(const EngineDev& e, unsigned* b
       unsigned long long P = 0, W = 0;
       {
         unsigned long long pre = 0, all = 0;
+#pragma unroll 4
         for (int i = threadIdx.x; i < nt; i += kThreads) {
           const unsigned long long v = __ldcg(e.lb_agg + tb + i);
           all += v;
@@ -280,12 +281,30 @@ __device__ __forceinline__ void epoch_sys_assign(const EngineDev& e, unsigned* b
               const bool run = i < n && hi > lo;
               if (run && hi - lo <= (uint32_t)kLightRun)
                 for (uint32_t j = lo; j < hi; ++j) e.anc[base + j] = i;
-              // long runs: the lane reserves its chunks, the warp writes them
+              // long runs: one reservation per warp, a lane writes its own
+              // one or two chunk descriptors, the warp writes longer lists
               const bool heavy = run && hi - lo > (uint32_t)kLightRun;
               const uint32_t nch = heavy ? (hi - lo + kRunChunk - 1) / kRunChunk : 0u;
-              const unsigned at = heavy ? atomicAdd(bar + kBarChunks, nch) : 0u;
+              if (__ballot_sync(0xffffffffu, heavy) == 0u) continue;  // warp-uniform
+              uint32_t incl = nch;
+#pragma unroll
+              for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+              }
+              unsigned at0 = 0u;
+              if (lane == 31) at0 = atomicAdd(bar + kBarChunks, incl);
+              const unsigned at = __shfl_sync(0xffffffffu, at0, 31) + incl - nch;
               if (heavy && at + nch > e.max_chunks) atomicOr(e.err, ERR_INTERNAL_CAP);  // cannot happen: bounded by the layout
-              unsigned todo = __ballot_sync(0xffffffffu, heavy);
+              if (heavy && nch <= 2u) {
+                const uint32_t si = (uint32_t)i;
+                for (uint32_t c = 0; c < nch && at + c < e.max_chunks; ++c) {
+                  const long long st = base + lo + (long long)c * kRunChunk;
+                  e.chunks[at + c] = make_uint4((uint32_t)st, (uint32_t)(st >> 32),
+                                                min((uint32_t)kRunChunk, hi - lo - c * (uint32_t)kRunChunk), si);
+                }
+              }
+              unsigned todo = __ballot_sync(0xffffffffu, heavy && nch > 2u);
               while (todo) {
                 const int src = __ffs(todo) - 1;
                 todo &= todo - 1u;
