@@ -12,7 +12,10 @@ from .particle_filter_3d import ParticleFilter3D, ParticleFilter3DBVH
 from .bvh import BVHAccelerator, BuildingModel
 from .engine import Engine, EngineOptions, FilterSpec
 from .ephemeris import Ephemeris
-from .nav_rinex import NavMessage, read_nav_rinex
+from .nav_rinex import NavMessage, read_nav_rinex, read_nav_rinex_multi
+from .nmea import NMEAWriter, ecef_to_nmea, parse_nmea, positions_to_nmea
+from .rinex_obs import read_rinex_obs
 
-__all__ = ["ParticleFilter", "Ephemeris", "NavMessage", "read_nav_rinex", "ParticleFilterDevice", "ParticleFilter3D", "ParticleFilter3DBVH", "BVHAccelerator",
+__all__ = ["ParticleFilter", "Ephemeris", "NavMessage", "read_nav_rinex", "read_nav_rinex_multi", "read_rinex_obs", "parse_nmea",
+           "NMEAWriter", "positions_to_nmea", "ecef_to_nmea", "ParticleFilterDevice", "ParticleFilter3D", "ParticleFilter3DBVH", "BVHAccelerator",
            "BuildingModel", "Engine", "EngineOptions", "FilterSpec"]

@@ -709,4 +709,28 @@ int pf_sagnac(const double* d_rx, const double* d_sat, int n_epoch, int n_sat, d
   return PF_OK;
 }
 
+int pf_ecef_to_lla(const double* ecef_x, const double* ecef_y, const double* ecef_z, double* lat, double* lon,
+                   double* alt, int n) {
+  clear_err();
+  if (n < 0) return set_err(PF_EINVAL, "n must be >= 0");
+  if (n == 0) return PF_OK;
+  if (!ecef_x || !ecef_y || !ecef_z || !lat || !lon || !alt) return set_err(PF_EINVAL, "null array");
+  int s;
+  std::lock_guard<std::mutex> lk(g_mu);
+  const size_t nb = (size_t)n * 8;
+  Workspace* w;
+  if ((s = workspace(6 * align_up(nb, 256), &w)) != PF_OK) return s;
+  Carve c{(unsigned char*)w->buf};
+  double *dx = c.take<double>(n), *dy = c.take<double>(n), *dz = c.take<double>(n);
+  double *dla = c.take<double>(n), *dlo = c.take<double>(n), *dal = c.take<double>(n);
+  CK(cudaMemcpyAsync(dx, ecef_x, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dy, ecef_y, nb, cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(dz, ecef_z, nb, cudaMemcpyHostToDevice, w->stream));
+  k_ecef_to_lla<<<grid_of(n), kB, 0, w->stream>>>(dx, dy, dz, dla, dlo, dal, n);
+  CK(cudaMemcpyAsync(lat, dla, nb, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(lon, dlo, nb, cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(alt, dal, nb, cudaMemcpyDeviceToHost, w->stream));
+  return finish(w);
+}
+
 }  // extern "C"

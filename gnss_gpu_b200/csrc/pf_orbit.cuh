@@ -254,4 +254,28 @@ __global__ void k_sagnac(const double* __restrict__ rx, const double* __restrict
   }
 }
 
+// WGS84 geodetic latitude, longitude (rad) and height of ECEF points by
+// Bowring's closed form (src/utils/coordinates.cu:7-27): one auxiliary
+// angle, no iteration.
+constexpr double kWgsA = 6378137.0;
+constexpr double kWgsF = 1.0 / 298.257223563;
+constexpr double kWgsB = kWgsA * (1.0 - kWgsF);
+constexpr double kWgsE2 = 2.0 * kWgsF - kWgsF * kWgsF;
+
+__global__ void k_ecef_to_lla(const double* __restrict__ x, const double* __restrict__ y,
+                              const double* __restrict__ z, double* __restrict__ lat, double* __restrict__ lon,
+                              double* __restrict__ alt, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double X = x[i], Y = y[i], Z = z[i];
+  const double p = sqrt(X * X + Y * Y);
+  const double th = atan2(Z * kWgsA, p * kWgsB);
+  const double st = sin(th), ct = cos(th);
+  const double la = atan2(Z + kWgsE2 / (1.0 - kWgsE2) * kWgsB * st * st * st, p - kWgsE2 * kWgsA * ct * ct * ct);
+  const double sl = sin(la);
+  lat[i] = la;
+  lon[i] = atan2(Y, X);
+  alt[i] = p / cos(la) - kWgsA / sqrt(1.0 - kWgsE2 * sl * sl);
+}
+
 }  // namespace pfb

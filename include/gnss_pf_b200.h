@@ -617,6 +617,12 @@ int pf_broadcast_orbits(const pf_broadcast_t* d_recs, int n_recs, const int* d_r
 int pf_sagnac(const double* d_rx, const double* d_sat, int n_epoch, int n_sat, double* d_sat_rot,
               double* d_range, void* stream);
 
+/* Replaces gnss_gpu::ecef_to_lla (src/utils/coordinates.cu:29-51): WGS84
+ * latitude / longitude (rad) and height (m) of n ECEF points, host arrays,
+ * Bowring's closed form.  Used by the NMEA writer (ecef_to_nmea). */
+int pf_ecef_to_lla(const double* ecef_x, const double* ecef_y, const double* ecef_z, double* lat, double* lon,
+                   double* alt, int n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,52 @@
+"""ECEF -> geodetic conversion on the device (pf_ecef_to_lla) and the NMEA
+text built from it (ecef_to_nmea), against the reference's outputs
+(tests/golden/io_golden.json).  Tolerance: Bowring's closed form in FP64 on
+both sides; 1e-12 rad in latitude / longitude, 1e-6 m in height, and the
+NMEA text (4 decimals of minutes, mm heights) equal."""
+from __future__ import annotations
+
+import json
+from datetime import datetime
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = Path(__file__).resolve().parents[1]
+GOLD = json.loads((ROOT / "tests" / "golden" / "io_golden.json").read_text())
+
+
+def test_ecef_to_lla_and_nmea_match_reference():
+    from gnss_gpu_b200.nmea import ecef_to_lla, ecef_to_nmea
+
+    g = GOLD["writer"]["ecef_to_nmea"]
+    ecef = np.array(g["ecef"])
+    lat, lon, alt = ecef_to_lla(ecef)
+    ref = np.array(g["lla"])
+    np.testing.assert_allclose(np.degrees(lat), ref[:, 0], rtol=0, atol=1e-10)
+    np.testing.assert_allclose(np.degrees(lon), ref[:, 1], rtol=0, atol=1e-10)
+    np.testing.assert_allclose(alt, ref[:, 2], rtol=0, atol=1e-6)
+    assert ecef_to_nmea(ecef, times=[datetime.fromisoformat(x) for x in g["times"]]) == g["text"]
+
+
+def test_ecef_to_lla_round_trip_many_points():
+    """10^5 points on and above the ellipsoid: geodetic -> ECEF (FP64 on the
+    host) -> device -> geodetic within the closed form's error."""
+    from gnss_gpu_b200.nmea import ecef_to_lla
+
+    rng = np.random.default_rng(0)
+    n = 100_000
+    la = rng.uniform(-np.pi / 2 + 1e-3, np.pi / 2 - 1e-3, n)
+    lo = rng.uniform(-np.pi, np.pi, n)
+    h = rng.uniform(-100.0, 10_000.0, n)
+    a, f = 6378137.0, 1.0 / 298.257223563
+    e2 = 2 * f - f * f
+    N = a / np.sqrt(1 - e2 * np.sin(la) ** 2)
+    x = np.stack([(N + h) * np.cos(la) * np.cos(lo), (N + h) * np.cos(la) * np.sin(lo),
+                  (N * (1 - e2) + h) * np.sin(la)], 1)
+    la2, lo2, h2 = ecef_to_lla(x)
+    assert np.abs(la2 - la).max() < 1e-9 and np.abs(lo2 - lo).max() < 1e-12 and np.abs(h2 - h).max() < 1e-3
+    e0 = ecef_to_lla(np.zeros((0, 3)))
+    assert all(v.shape == (0,) for v in e0)
