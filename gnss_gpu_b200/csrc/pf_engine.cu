@@ -38,8 +38,16 @@ struct pf_engine {
   unsigned char* pinned[2] = {nullptr, nullptr};
   cudaEvent_t pin_ev[2] = {nullptr, nullptr};
   int pin_cur = 0;
-  FilterCtrl* ctrl_host = nullptr;  // pinned mirror
-  unsigned* err_host = nullptr;     // pinned copy of the device error word
+  FilterCtrl* ctrl_host = nullptr;  // pinned mirror of the control blocks, then the error word
+  unsigned* err_host = nullptr;     // pinned copy of the device error word (inside ctrl_host's block)
+  size_t ctrl_span = 0;             // bytes from the first control block to the end of the error word
+  // pfe_step_io: per pinned staging buffer a graph of upload copy, epoch
+  // kernel and result copy, re-captured when the launch parameters change
+  cudaGraph_t io_graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t io_exec[2] = {nullptr, nullptr};
+  cudaGraphNode_t io_h2d[2] = {nullptr, nullptr};
+  size_t io_h2d_bytes[2] = {0, 0};
+  std::vector<unsigned char> io_key[2];
   size_t obs_slot_bytes = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -163,10 +171,11 @@ Layout make_layout(const pf_engine_config_t* cfg, const pf_filter_params_t* fp) 
   L.off_satdbg = take(mix ? (size_t)cfg->n_filters * cfg->max_sats * kSatDbg * 4 : 0);
   L.off_obsrows = take(sizeof(ObsRow) * kMaxObsRows);
   L.off_desc = take(sizeof(FilterDesc) * cfg->n_filters);
+  // the error word follows the control blocks, so one copy returns both
   L.off_ctrl = take(sizeof(FilterCtrl) * cfg->n_filters);
+  L.off_err = take(sizeof(unsigned) * 4);
   L.off_tf = take((size_t)T * 4);
   L.off_queue = take(sizeof(unsigned) * (2 * Q_COUNT + kBarFlags + kMaxEpochGrid));
-  L.off_err = take(sizeof(unsigned) * 4);
   L.obs_slot_bytes = align_up(sizeof(pf_filter_epoch_t) * cfg->n_filters +
                                   sizeof(pf_sat_t) * (size_t)cfg->n_filters * cfg->max_sats,
                               256);
@@ -386,17 +395,20 @@ int launch_epoch(pf_engine* eng, int t0, int count) {
 
 bool use_chain(const pf_engine* eng) { return (eng->cfg.flags & PF_FLAG_KERNEL_CHAIN) != 0; }
 
-int sync_and_check(pf_engine* eng) {
-  // the error word rides on the same stream as the caller's reads: one sync
-  CK(cudaMemcpyAsync(eng->err_host, eng->dev.err, sizeof(unsigned), cudaMemcpyDeviceToHost, eng->stream));
-  CK(cudaStreamSynchronize(eng->stream));
-  const unsigned w = *eng->err_host;
+int err_status(unsigned w) {
   if (w & ERR_LOOKBACK_TIMEOUT) return set_err(PF_ETIMEOUT, "device look-back spin limit reached (error word 0x%x)", w);
   if (w & ERR_BARRIER_TIMEOUT) return set_err(PF_ETIMEOUT, "device grid-barrier spin limit reached (error word 0x%x)", w);
   if (w & ERR_SAT_CAP) return set_err(PF_ECAP, "n_sat above max_sats (error word 0x%x)", w);
   if (w & ERR_BAD_WEIGHTS) return set_err(PF_EINVAL, "all log-weights non-finite (error word 0x%x)", w);
   if (w & ERR_INTERNAL_CAP) return set_err(PF_ECUDA, "internal capacity exceeded (error word 0x%x)", w);
   return PF_OK;
+}
+
+int sync_and_check(pf_engine* eng) {
+  // the error word rides on the same stream as the caller's reads: one sync
+  CK(cudaMemcpyAsync(eng->err_host, eng->dev.err, sizeof(unsigned), cudaMemcpyDeviceToHost, eng->stream));
+  CK(cudaStreamSynchronize(eng->stream));
+  return err_status(*eng->err_host);
 }
 
 int read_ctrl(pf_engine* eng) {
@@ -552,10 +564,10 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
     if (check_cuda(cudaEventCreateWithFlags(&eng->pin_ev[i], cudaEventDisableTiming), "event") != PF_OK)
       return fail(PF_ECUDA);
   }
-  if (check_cuda(cudaHostAlloc((void**)&eng->ctrl_host, sizeof(FilterCtrl) * cfg->n_filters, cudaHostAllocDefault),
-                 "pinned ctrl") != PF_OK ||
-      check_cuda(cudaHostAlloc((void**)&eng->err_host, 64, cudaHostAllocDefault), "pinned error word") != PF_OK)
+  eng->ctrl_span = (L.off_err - L.off_ctrl) + sizeof(unsigned) * 4;
+  if (check_cuda(cudaHostAlloc((void**)&eng->ctrl_host, eng->ctrl_span, cudaHostAllocDefault), "pinned ctrl") != PF_OK)
     return fail(PF_ENOMEM);
+  eng->err_host = (unsigned*)((unsigned char*)eng->ctrl_host + (L.off_err - L.off_ctrl));
 
   // Device tables and zeroed control blocks.
   std::vector<FilterCtrl> hc(cfg->n_filters);
@@ -594,8 +606,11 @@ int pfe_destroy(pf_engine_t* eng) {
     if (eng->pinned[i]) cudaFreeHost(eng->pinned[i]);
     if (eng->pin_ev[i]) cudaEventDestroy(eng->pin_ev[i]);
   }
+  for (int i = 0; i < 2; ++i) {
+    if (eng->io_exec[i]) cudaGraphExecDestroy(eng->io_exec[i]);
+    if (eng->io_graph[i]) cudaGraphDestroy(eng->io_graph[i]);
+  }
   if (eng->ctrl_host) cudaFreeHost(eng->ctrl_host);
-  if (eng->err_host) cudaFreeHost(eng->err_host);
   for (cudaEvent_t e : eng->tev) cudaEventDestroy(e);
   delete eng;
   return PF_OK;
@@ -702,11 +717,13 @@ int pfe_obs_slot_bytes(pf_engine_t* eng, size_t* bytes) {
   return PF_OK;
 }
 
-int pfe_upload_obs(pf_engine_t* eng, int slot, const pf_filter_epoch_t* fe, const pf_sat_t* sats,
-                   int n_sats_total) {
-  clear_err();
-  if (!eng || !fe) return set_err(PF_EINVAL, "null argument");
-  if (slot < 0 || slot >= eng->cfg.obs_slots) return set_err(PF_EINVAL, "slot %d out of range", slot);
+}  // extern "C"
+
+namespace {
+
+// Checks of one epoch's records before they are staged (pfe_upload_obs,
+// pfe_step_io).
+int validate_obs(pf_engine* eng, const pf_filter_epoch_t* fe, const pf_sat_t* sats, int n_sats_total) {
   const int F = eng->cfg.n_filters;
   const int cap = F * eng->cfg.max_sats;
   if (n_sats_total < 0 || n_sats_total > cap) return set_err(PF_ECAP, "n_sats_total %d above capacity %d", n_sats_total, cap);
@@ -729,6 +746,21 @@ int pfe_upload_obs(pf_engine_t* eng, int slot, const pf_filter_epoch_t* fe, cons
       }
     }
   }
+  return PF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pfe_upload_obs(pf_engine_t* eng, int slot, const pf_filter_epoch_t* fe, const pf_sat_t* sats,
+                   int n_sats_total) {
+  clear_err();
+  if (!eng || !fe) return set_err(PF_EINVAL, "null argument");
+  if (slot < 0 || slot >= eng->cfg.obs_slots) return set_err(PF_EINVAL, "slot %d out of range", slot);
+  const int F = eng->cfg.n_filters;
+  int vs = validate_obs(eng, fe, sats, n_sats_total);
+  if (vs != PF_OK) return vs;
   const int b = eng->pin_cur;
   eng->pin_cur ^= 1;
   CK(cudaEventSynchronize(eng->pin_ev[b]));
@@ -894,11 +926,11 @@ int pfe_graph_launch(pf_engine_t* eng, int n_epochs) {
   return PF_OK;
 }
 
-int pfe_read_results(pf_engine_t* eng, pf_filter_result_t* out) {
-  clear_err();
-  if (!eng || !out) return set_err(PF_EINVAL, "null argument");
-  int s = read_ctrl(eng);
-  if (s != PF_OK) return s;
+}  // extern "C"
+
+namespace {
+
+void fill_results(pf_engine* eng, pf_filter_result_t* out) {
   for (int f = 0; f < eng->cfg.n_filters; ++f) {
     const FilterCtrl& c = eng->ctrl_host[f];
     pf_filter_result_t& r = out[f];
@@ -913,6 +945,83 @@ int pfe_read_results(pf_engine_t* eng, pf_filter_result_t* out) {
     r.epoch = c.epoch;
     r.initialized = eng->initialized[f];
   }
+}
+
+// Everything the epoch launch of a step-io graph depends on: the kernel's
+// parameter block, the kernel chosen, the grid and its shared memory.
+std::vector<unsigned char> io_key(pf_engine* eng) {
+  struct Launch {
+    EpochKernel fn;
+    unsigned* bar;
+    int T, resident, cap;
+    size_t smem;
+  } x;
+  memset(&x, 0, sizeof(x));
+  x.fn = epoch_kernel(eng);
+  x.bar = eng->bar;
+  x.T = eng->T;
+  x.resident = eng->epoch_resident;
+  x.cap = eng->epoch_cap;
+  x.smem = eng->epoch_smem;
+  std::vector<unsigned char> k(sizeof(EngineDev) + sizeof(Launch));
+  memcpy(k.data(), &eng->dev, sizeof(EngineDev));
+  memcpy(k.data() + sizeof(EngineDev), &x, sizeof(Launch));
+  return k;
+}
+
+// (Re)capture staging buffer b's graph: upload copy of `bytes`, the epoch
+// kernel, one copy of the control blocks and the error word back.
+int io_capture(pf_engine* eng, int b, size_t bytes) {
+  if (eng->io_exec[b]) cudaGraphExecDestroy(eng->io_exec[b]);
+  if (eng->io_graph[b]) cudaGraphDestroy(eng->io_graph[b]);
+  eng->io_exec[b] = nullptr;
+  eng->io_graph[b] = nullptr;
+  eng->io_h2d[b] = nullptr;
+  eng->io_key[b].clear();
+  CK(cudaStreamBeginCapture(eng->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t ce = cudaMemcpyAsync((void*)eng->dev.obs, eng->pinned[b], bytes, cudaMemcpyHostToDevice, eng->stream);
+  int s = ce == cudaSuccess ? launch_epoch(eng, 0, eng->T) : set_err(PF_ECUDA, "capture upload: %s", cudaGetErrorString(ce));
+  if (s == PF_OK) {
+    ce = cudaMemcpyAsync(eng->ctrl_host, eng->ctrl_dev, eng->ctrl_span, cudaMemcpyDeviceToHost, eng->stream);
+    if (ce != cudaSuccess) s = set_err(PF_ECUDA, "capture result copy: %s", cudaGetErrorString(ce));
+  }
+  cudaGraph_t g = nullptr;
+  ce = cudaStreamEndCapture(eng->stream, &g);
+  if (s != PF_OK) {
+    if (g) cudaGraphDestroy(g);
+    return s;
+  }
+  CK(ce);
+  eng->io_graph[b] = g;
+  size_t n = 0;
+  CK(cudaGraphGetNodes(g, nullptr, &n));
+  std::vector<cudaGraphNode_t> nodes(n);
+  CK(cudaGraphGetNodes(g, nodes.data(), &n));
+  for (cudaGraphNode_t nd : nodes) {
+    cudaGraphNodeType t;
+    CK(cudaGraphNodeGetType(nd, &t));
+    if (t != cudaGraphNodeTypeMemcpy) continue;
+    cudaMemcpy3DParms mp;
+    CK(cudaGraphMemcpyNodeGetParams(nd, &mp));
+    if (mp.kind == cudaMemcpyHostToDevice) eng->io_h2d[b] = nd;
+  }
+  if (!eng->io_h2d[b]) return set_err(PF_ECUDA, "step-io graph: upload node not found");
+  CK(cudaGraphInstantiate(&eng->io_exec[b], g, 0));
+  eng->io_h2d_bytes[b] = bytes;
+  eng->io_key[b] = io_key(eng);
+  return PF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pfe_read_results(pf_engine_t* eng, pf_filter_result_t* out) {
+  clear_err();
+  if (!eng || !out) return set_err(PF_EINVAL, "null argument");
+  int s = read_ctrl(eng);
+  if (s != PF_OK) return s;
+  fill_results(eng, out);
   return PF_OK;
 }
 
@@ -921,10 +1030,40 @@ int pfe_step_io(pf_engine_t* eng, const pf_filter_epoch_t* fe, const pf_sat_t* s
   clear_err();
   if (!eng || !fe || !out) return set_err(PF_EINVAL, "null argument");
   if (eng->cfg.obs_slots != 1) return set_err(PF_EINVAL, "pfe_step_io needs an engine with obs_slots == 1");
-  int s = pfe_upload_obs(eng, 0, fe, sats, n_sats_total);
+  if (use_chain(eng) || eng->t_slots > 0 || !eng->stream) {
+    // kernel chain, timed steps or the legacy stream: separate calls
+    int s = pfe_upload_obs(eng, 0, fe, sats, n_sats_total);
+    if (s != PF_OK) return s;
+    if ((s = pfe_step(eng)) != PF_OK) return s;
+    return pfe_read_results(eng, out);
+  }
+  int s = validate_obs(eng, fe, sats, n_sats_total);
   if (s != PF_OK) return s;
-  if ((s = pfe_step(eng)) != PF_OK) return s;
-  return pfe_read_results(eng, out);
+  for (int f = 0; f < eng->cfg.n_filters; ++f)
+    if (!eng->initialized[f]) return set_err(PF_ENOTINIT, "filter %d not initialized", f);
+  if (eng->cfg.weight_mode == PF_WEIGHT_MIXTURE && !eng->mlp_set)
+    return set_err(PF_ENOTINIT, "mixture likelihood: network parameters not set (pfe_set_mlp)");
+  const int b = eng->pin_cur;
+  eng->pin_cur ^= 1;
+  CK(cudaEventSynchronize(eng->pin_ev[b]));
+  unsigned char* h = eng->pinned[b];
+  const size_t fe_bytes = sizeof(pf_filter_epoch_t) * eng->cfg.n_filters;
+  memcpy(h, fe, fe_bytes);
+  if (n_sats_total > 0) memcpy(h + fe_bytes, sats, sizeof(pf_sat_t) * n_sats_total);
+  const size_t bytes = fe_bytes + sizeof(pf_sat_t) * (size_t)n_sats_total;
+  if (!eng->io_exec[b] || eng->io_key[b] != io_key(eng)) {
+    if ((s = io_capture(eng, b, bytes)) != PF_OK) return s;
+  } else if (bytes != eng->io_h2d_bytes[b]) {
+    CK(cudaGraphExecMemcpyNodeSetParams1D(eng->io_exec[b], eng->io_h2d[b], (void*)eng->dev.obs, h, bytes,
+                                          cudaMemcpyHostToDevice));
+    eng->io_h2d_bytes[b] = bytes;
+  }
+  CK(cudaGraphLaunch(eng->io_exec[b], eng->stream));
+  CK(cudaStreamSynchronize(eng->stream));
+  eng->last_launches = 1;
+  if ((s = err_status(*eng->err_host)) != PF_OK) return s;
+  fill_results(eng, out);
+  return PF_OK;
 }
 
 int pfe_result_bytes(pf_engine_t* eng, size_t* bytes) {

@@ -319,3 +319,45 @@ def test_recentering_keeps_offsets_small_over_a_trajectory():
     x, _ = eng.state_f32(0)
     assert np.abs(x[:3]).max() < 200.0  # offsets stay near the anchor after 60 epochs (600 m travelled)
     assert np.median(errs[10:]) < 5.0
+
+
+def test_step_io_graph_tracks_sizes_and_parameters():
+    """pfe_step_io runs a captured graph per staging buffer: epochs with
+    different satellite counts (the upload node is resized) and a likelihood
+    change between calls (the graph is re-captured) give exactly the results
+    of separate upload / step / read calls."""
+    rng = np.random.RandomState(9)
+    d = rng.randn(8, 3)
+    sats = d / np.linalg.norm(d, axis=1, keepdims=True) * 20_000_000.0
+    pr = np.linalg.norm(sats, axis=1) + 100.0 + rng.randn(8)
+    from gnss_gpu_b200.engine import Engine, EngineOptions, FilterSpec
+
+    counts = [8, 5, 8, 6, 4, 7, 8, 5]
+    kinds = ["gaussian", "gaussian", "gaussian", "student_t", "student_t", "huber", "gaussian", "gmm"]
+
+    def run(io):
+        eng = Engine([FilterSpec(n_particles=30_000, seed=11, sigma_pos=(1.0, 1.0, 1.0), sigma_clk=3.0,
+                                 sigma_pr=5.0)],
+                     EngineOptions(n_clk=1, max_sats=8, obs_slots=1, weight_mode="generic"))
+        eng.initialize(0, np.zeros(3), 100.0, 20.0, 50.0)
+        out = []
+        for t, (k, kind) in enumerate(zip(counts, kinds)):
+            eng.set_likelihood(kind, nu=4.0)
+            fe, sv = eng.pack_epoch([{"disp": np.zeros(3), "sats": sats[:k], "pr": pr[:k],
+                                      "flags": N.PF_EP_PREDICT | N.PF_EP_WEIGHT | N.PF_EP_RESAMPLE_CHECK}])
+            if io:
+                r = eng.step_io(fe, sv)[0]
+                out.append((tuple(r.est_ecef), r.ess, r.resampled, r.epoch))
+            else:
+                eng.upload(0, fe, sv)
+                eng.step()
+                r = eng.results()[0]
+                out.append((tuple(r["est_ecef"]), r["ess"], int(r["resampled"]), r["epoch"]))
+        st = eng.state_f32(0)
+        eng.close()
+        return out, st
+
+    (oa, sa), (ob, sb) = run(True), run(False)
+    for a, b in zip(oa, ob):
+        assert np.array_equal(np.asarray(a[0]), np.asarray(b[0])) and a[1] == b[1] and a[2] == b[2] and a[3] == b[3]
+    assert np.array_equal(sa[0], sb[0]) and np.array_equal(sa[1], sb[1])
