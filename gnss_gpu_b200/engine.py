@@ -6,7 +6,7 @@ CUDA stream; every step runs the library's sm_100a kernels.
 from __future__ import annotations
 
 import ctypes as C
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 from typing import Sequence
 
 import numpy as np

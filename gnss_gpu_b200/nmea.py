@@ -6,7 +6,6 @@ GGA / RMC / GSA / GSV / VTG sentences from positioning results, and
 """
 from __future__ import annotations
 
-import ctypes as C
 import math
 from dataclasses import dataclass
 from datetime import date, datetime, timezone

@@ -6,7 +6,6 @@ import numpy as np
 
 from gnss_gpu_b200 import _native as N
 from gnss_gpu_b200.engine import Engine, EngineOptions, FilterSpec
-from gnss_gpu_b200 import scenario as S
 from oracle import oracle as O
 
 # Tolerances against the FP64 oracle (north-star precision gates):

@@ -4,7 +4,6 @@ contents, bounded depth; and the brute-force line-of-sight oracle."""
 import ctypes as C
 
 import numpy as np
-import pytest
 
 from gnss_gpu_b200 import _native as N
 from gnss_gpu_b200 import citysim as CS

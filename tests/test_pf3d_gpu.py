@@ -199,7 +199,6 @@ def test_engine_3d_term_matches_oracle(M):
 
 def test_bvh_filter_in_a_city(M):
     g, _, _ = M
-    from gnss_gpu_b200 import citysim as CS
     tri, anchor, rot, city = city_mesh(7, 800.0)
     bvh = g.BVHAccelerator(tri)
     rng = np.random.default_rng(8)
