@@ -739,8 +739,9 @@ def run_orbits(args, world, rank, local, pg):
     """Input formation on the device: broadcast orbits and clocks of one day
     at 1 Hz (86,400 epochs) x 64 satellites (40 Kepler records of G/E/J/C
     re-selected every 2 h, 24 GLONASS states re-selected every 30 min and
-    integrated by RK4 from their toe), one pf_broadcast_orbits launch per
-    step.  value: satellite-epochs/s, inputs resident; e2e: the public
+    integrated by RK4 from their toe), one pf_broadcast_orbits call per
+    step (three kernels: GLONASS steps needed, shared GLONASS states, the
+    orbits).  value: satellite-epochs/s, inputs resident; e2e: the public
     broadcast_orbits call with host arrays (records, index and times up,
     positions and clocks down)."""
     import ctypes as C
@@ -834,7 +835,7 @@ def run_orbits(args, world, rank, local, pg):
                                f"{n_rec} records",
                    "epochs": n_epoch, "satellites": S_, "parallelism": f"replicas x{world}",
                    "l2": "flushed between steps (outside the event intervals)"},
-        "gpu_launches": K,
+        "gpu_launches": 3 * K,  # k_glo_need, k_glo_table, k_broadcast_orbits
         "roofline": {"bound": "hbm", "achieved": out_bytes / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": out_bytes / (ms / 1e3) / 1e9 / peak, "peak_kind": f"{peak_kind} hbm_gbs",
                      "traffic": None,

@@ -13,6 +13,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -689,9 +690,39 @@ int pf_broadcast_orbits(const pf_broadcast_t* d_recs, int n_recs, const int* d_r
   if (!isfinite(glo_step) || glo_step <= 0.0) glo_step = kGloStep;
   if (glo_step < 1.0) return set_err(PF_EINVAL, "glo_step below 1 s");
   const long ne = (long)n_epoch * n_sat;
-  k_broadcast_orbits<<<(unsigned)((ne + kB - 1) / kB), kB, 0, (cudaStream_t)stream>>>(
-      d_recs, n_recs, d_rec_index, d_times, n_epoch, n_sat, glo_step, d_pos, d_clk, nullptr);
-  CK(cudaGetLastError());
+  cudaStream_t st = (cudaStream_t)stream;
+  const unsigned grid = (unsigned)((ne + kB - 1) / kB);
+  // GLONASS state table: the epochs of a record share its states at whole
+  // steps from toe, so they are integrated once per (record, direction)
+  int kc = 0;
+  if (n_recs > 0) {
+    const size_t per_state = (size_t)2 * n_recs * 6 * sizeof(double);
+    kc = (int)std::min<size_t>(kGloTable, kGloTableBytes / per_state);
+    if (kc < 4) kc = 0;  // too many records for the scratch: walk from toe
+  }
+  if (kc == 0) {
+    k_broadcast_orbits<<<grid, kB, 0, st>>>(d_recs, n_recs, d_rec_index, d_times, n_epoch, n_sat, glo_step,
+                                            nullptr, 0, d_pos, d_clk, nullptr);
+    CK(cudaGetLastError());
+    return PF_OK;
+  }
+  const size_t kmax_bytes = align_up(sizeof(int) * 2 * (size_t)n_recs, 256);
+  const size_t tbl_bytes = (size_t)2 * n_recs * kc * 6 * sizeof(double);
+  unsigned char* scratch = nullptr;
+  CK(cudaMallocAsync((void**)&scratch, kmax_bytes + tbl_bytes, st));
+  int* kmax = (int*)scratch;
+  double* tbl = (double*)(scratch + kmax_bytes);
+  cudaError_t ce = cudaMemsetAsync(kmax, 0, kmax_bytes, st);
+  if (ce == cudaSuccess) {
+    k_glo_need<<<grid, kB, 0, st>>>(d_recs, n_recs, d_rec_index, d_times, n_epoch, n_sat, glo_step, kc, kmax);
+    k_glo_table<<<(unsigned)((2 * n_recs + 127) / 128), 128, 0, st>>>(d_recs, n_recs, glo_step, kmax, kc, tbl);
+    k_broadcast_orbits<<<grid, kB, 0, st>>>(d_recs, n_recs, d_rec_index, d_times, n_epoch, n_sat, glo_step, tbl,
+                                            kc, d_pos, d_clk, nullptr);
+    ce = cudaGetLastError();
+  }
+  const cudaError_t fe = cudaFreeAsync(scratch, st);
+  CK(ce);
+  CK(fe);
   return PF_OK;
 }
 

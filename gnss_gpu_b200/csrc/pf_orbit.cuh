@@ -38,6 +38,10 @@ constexpr double kGloOmega = 7.292115e-5;
 constexpr double kGloStep = 60.0;
 // Integration steps one record may take: half a week at 1 s per step.
 constexpr long kGloMaxSteps = 1L << 20;
+// Stored GLONASS states per record and direction (k_glo_table) and the
+// scratch they may take per call.
+constexpr int kGloTable = 64;
+constexpr size_t kGloTableBytes = 64u << 20;
 
 struct OrbitConsts {
   double mu, omega_e, rel_f;
@@ -154,26 +158,50 @@ __device__ inline void glo_rk4(double h, double* x, const double* acc) {
   for (int i = 0; i < 6; ++i) x[i] += (k1[i] + 2.0 * k2[i] + 2.0 * k3[i] + k4[i]) * (h / 6.0);
 }
 
-// GLONASS position and clock at GPST second of week t: align to the record's
-// UTC-based scale, integrate from toe in steps of `step` seconds with one
-// residual step (orbit_glonass.py:122-170).  Returns false (outputs NaN) when
-// the integration would take more than kGloMaxSteps steps.
-__device__ inline bool glonass_orbit(const pf_glonass_state_t& g, double t, double step, double* pos,
-                                     double* clk) {
-  const double el = wrap_half_week(broadcast_rx_sow('R', t) - g.toe);
-  double x[6] = {g.pos[0], g.pos[1], g.pos[2], g.vel[0], g.vel[1], g.vel[2]};
-  const double base = el < 0.0 ? -step : step;
-  double rem = el;
-  long it = 0;
-  while (fabs(rem) > 1.0e-9) {
-    if (++it > kGloMaxSteps || !isfinite(rem)) {
-      pos[0] = pos[1] = pos[2] = *clk = nan("");
-      return false;
-    }
-    const double h = fabs(rem) >= fabs(base) ? base : rem;
-    glo_rk4(h, x, g.acc);
-    rem -= h;
+// Full steps of the GLONASS integration of a record at GPST second of
+// week t and what is left for the residual step: the loop of
+// orbit_glonass.py:122-150 without the arithmetic (rem decremented in the
+// same order, so it is bit-identical).  Returns false past kGloMaxSteps.
+__device__ inline bool glo_plan(const pf_glonass_state_t& g, double t, double step, double& el, double& base,
+                                long& k, double& rem) {
+  el = wrap_half_week(broadcast_rx_sow('R', t) - g.toe);
+  base = el < 0.0 ? -step : step;
+  rem = el;
+  k = 0;
+  // a NaN time takes no step (the reference returns the broadcast position
+  // with a NaN clock); an infinite one runs into the step bound
+  while (fabs(rem) >= fabs(base)) {  // |base| >= 1 s, so |rem| > 1e-9 here
+    if (++k > kGloMaxSteps) return false;
+    rem -= base;
   }
+  return true;
+}
+
+// GLONASS position and clock at GPST second of week t: align to the
+// record's UTC-based scale, integrate from toe in steps of `step` seconds
+// with one residual step (orbit_glonass.py:122-170).  `tbl` (may be null)
+// holds the states after 1..kc full steps from toe in this direction, shared
+// by every epoch of the record: the walk starts from the deepest stored
+// state instead of from toe, with the same RK4 steps in the same order, so
+// the result is the same bit for bit.  Returns false (outputs NaN) past
+// kGloMaxSteps steps.
+__device__ inline bool glonass_orbit(const pf_glonass_state_t& g, double t, double step, const double* tbl,
+                                     int kc, double* pos, double* clk) {
+  double el, base, rem;
+  long k;
+  if (!glo_plan(g, t, step, el, base, k, rem)) {
+    pos[0] = pos[1] = pos[2] = *clk = nan("");
+    return false;
+  }
+  double x[6] = {g.pos[0], g.pos[1], g.pos[2], g.vel[0], g.vel[1], g.vel[2]};
+  long done = 0;
+  if (tbl && k > 0 && kc > 0) {
+    done = k < kc ? k : kc;
+    const double* st = tbl + 6 * (done - 1);
+    for (int i = 0; i < 6; ++i) x[i] = st[i];
+  }
+  for (; done < k; ++done) glo_rk4(base, x, g.acc);
+  if (fabs(rem) > 1.0e-9) glo_rk4(rem, x, g.acc);
   pos[0] = x[0];
   pos[1] = x[1];
   pos[2] = x[2];
@@ -181,13 +209,62 @@ __device__ inline bool glonass_orbit(const pf_glonass_state_t& g, double t, doub
   return true;
 }
 
+// Record index of output i (idx null: record s); -1 when out of range.
+__device__ inline int orbit_record(const int* idx, long i, int s, int n_recs) {
+  const int r = idx ? idx[i] : s;
+  return (r < 0 || r >= n_recs) ? -1 : r;
+}
+
+// Deepest stored state each (GLONASS record, direction) needs: kmax[2r + d]
+// = max over its satellite-epochs of min(full steps, kc).
+__global__ void k_glo_need(const pf_broadcast_t* __restrict__ recs, int n_recs, const int* __restrict__ idx,
+                           const double* __restrict__ times, int n_epoch, int n_sat, double step, int kc,
+                           int* __restrict__ kmax) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int slot = -1, need = 0;
+  if (t < (long)n_epoch * n_sat) {
+    const int s = (int)(t / n_epoch), e = (int)(t - (long)s * n_epoch);
+    const int r = orbit_record(idx, (long)e * n_sat + s, s, n_recs);
+    double el, base, rem;
+    long k;
+    if (r >= 0 && recs[r].system == 'R' && glo_plan(recs[r].u.glonass, times[e], step, el, base, k, rem) && k > 0) {
+      slot = 2 * r + (base < 0.0 ? 1 : 0);
+      need = (int)(k < kc ? k : kc);
+    }
+  }
+  // satellite-major order: a warp's lanes are consecutive epochs of one
+  // satellite and mostly share a slot, so one atomic per group of lanes
+  const unsigned grp = __match_any_sync(0xffffffffu, slot);
+  const int m = (int)__reduce_max_sync(grp, (unsigned)need);
+  if (slot >= 0 && (threadIdx.x & 31) == __ffs(grp) - 1) atomicMax(kmax + slot, m);
+}
+
+// The stored states: one thread per (record, direction) integrates kmax
+// full steps from toe and keeps every state (6 doubles each, kc per slot).
+__global__ void k_glo_table(const pf_broadcast_t* __restrict__ recs, int n_recs, double step,
+                            const int* __restrict__ kmax, int kc, double* __restrict__ tbl) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2 * n_recs) return;
+  const int K = kmax[t];
+  if (K <= 0) return;
+  const pf_glonass_state_t& g = recs[t >> 1].u.glonass;
+  const double h = (t & 1) ? -step : step;
+  double x[6] = {g.pos[0], g.pos[1], g.pos[2], g.vel[0], g.vel[1], g.vel[2]};
+  double* out = tbl + (size_t)t * kc * 6;
+  for (int k = 0; k < K; ++k) {
+    glo_rk4(h, x, g.acc);
+    for (int c = 0; c < 6; ++c) out[6 * k + c] = x[c];
+  }
+}
+
 // Multi-system records: out[e][s] from recs[idx[e*S+s]] (or recs[s] when idx
 // is null) at times[e]; an index outside [0, n_recs) gives NaN, and so does a
 // GLONASS integration past kGloMaxSteps steps (also flagged in *err if given).
+// tbl / kc: the GLONASS state table of k_glo_table, or null / 0.
 __global__ void k_broadcast_orbits(const pf_broadcast_t* __restrict__ recs, int n_recs,
                                    const int* __restrict__ idx, const double* __restrict__ times,
-                                   int n_epoch, int n_sat, double glo_step, double* __restrict__ pos,
-                                   double* __restrict__ clk, int* __restrict__ err) {
+                                   int n_epoch, int n_sat, double glo_step, const double* __restrict__ tbl, int kc,
+                                   double* __restrict__ pos, double* __restrict__ clk, int* __restrict__ err) {
   // Satellite-major thread order: a warp covers 32 consecutive epochs of one
   // satellite, so its lanes run the same orbit model (Kepler or the longer
   // GLONASS integration) with similar step counts.
@@ -195,14 +272,16 @@ __global__ void k_broadcast_orbits(const pf_broadcast_t* __restrict__ recs, int 
   if (t >= (long)n_epoch * n_sat) return;
   const int s = (int)(t / n_epoch), e = (int)(t - (long)s * n_epoch);
   const long i = (long)e * n_sat + s;
-  const int r = idx ? idx[i] : s;
+  const int r = orbit_record(idx, i, s, n_recs);
   double p[3], c;
-  if (r < 0 || r >= n_recs) {
+  if (r < 0) {
     p[0] = p[1] = p[2] = c = nan("");
   } else {
     const pf_broadcast_t& rec = recs[r];
     if (rec.system == 'R') {
-      if (!glonass_orbit(rec.u.glonass, times[e], glo_step, p, &c) && err) atomicOr(err, 1);
+      const double el = wrap_half_week(broadcast_rx_sow('R', times[e]) - rec.u.glonass.toe);
+      const double* tb = tbl ? tbl + ((size_t)2 * r + (el < 0.0 ? 1 : 0)) * kc * 6 : nullptr;
+      if (!glonass_orbit(rec.u.glonass, times[e], glo_step, tb, kc, p, &c) && err) atomicOr(err, 1);
     } else {
       kepler_orbit(rec.u.kepler, rec.system, times[e], p, &c);
     }

@@ -190,3 +190,71 @@ def test_sagnac_matches_reference_and_batch():
         np.testing.assert_allclose(dist[e], d_o, rtol=0, atol=1e-7)
     r0, d0 = R.sagnac_batch(np.zeros((0, 3)), np.zeros((0, 4, 3)))
     assert r0.shape == (0, 4, 3) and d0.shape == (0, 4)
+
+
+def _glonass_records(n, rng):
+    from gnss_gpu_b200 import _native as N
+
+    recs = np.zeros(n, N.BROADCAST_DTYPE)
+    recs["system"] = ord("R")
+    g = recs["glonass"]
+    for r in range(n):
+        ang = rng.uniform(0, 2 * np.pi)
+        inc = rng.uniform(1.0, 1.2)
+        rad = rng.uniform(2.54e7, 2.56e7)
+        v = np.sqrt(3.9860044e14 / rad)
+        g["toe"][r] = rng.choice([900.0, 302400.0, 603900.0])
+        pos = np.array([rad * np.cos(ang), rad * np.sin(ang), 0.0])
+        v_in = np.array([-v * np.sin(ang) * np.cos(inc), v * np.cos(ang) * np.cos(inc), v * np.sin(inc)])
+        g["pos"][r] = pos
+        g["vel"][r] = v_in - np.cross([0.0, 0.0, 7.292115e-5], pos)  # earth-fixed velocity of a circular orbit
+        g["acc"][r] = rng.normal(0, 2e-6, 3)
+        g["tau_n"][r], g["gamma_n"][r] = rng.normal(0, 1e-5), rng.normal(0, 1e-12)
+    return recs
+
+
+def test_glonass_batch_matches_oracle():
+    """GLONASS states integrated from toe over up to +-2 h (more steps than the
+    device's state table holds, so walks continue past it), week crossover
+    included, against the oracle's RK4 walk from toe."""
+    from gnss_gpu_b200.ephemeris import broadcast_orbits
+
+    rng = np.random.default_rng(17)
+    recs = _glonass_records(6, rng)
+    n_epoch = 120
+    times = np.empty(n_epoch)
+    idx = np.empty((n_epoch, 6), np.int32)
+    for e in range(n_epoch):
+        times[e] = (recs["glonass"]["toe"][e % 6] + 18.0 + rng.uniform(-7200.0, 7200.0)) % 604800.0
+        idx[e] = (np.arange(6) + e) % 6
+    pos, clk = broadcast_orbits(recs, times, idx)
+    g = recs["glonass"]
+    for e in range(0, n_epoch, 3):
+        for s in range(6):
+            r = idx[e, s]
+            st = {"toe": float(g["toe"][r]), "pos": g["pos"][r], "vel": g["vel"][r], "acc": g["acc"][r],
+                  "tau_n": float(g["tau_n"][r]), "gamma_n": float(g["gamma_n"][r])}
+            p_o, c_o = O.glonass(st, float(times[e]))
+            # FP64 on both sides, the device contracting multiply-adds: up to
+            # 120 RK4 steps agree to 1e-12 of the orbit radius
+            assert np.abs(pos[e, s] - p_o).max() <= 1e-6 + 1e-12 * np.linalg.norm(p_o)
+            assert abs(clk[e, s] - c_o) <= 1e-15
+
+
+def test_glonass_state_table_equals_walk_from_toe():
+    """The shared state table changes nothing: with a record table too large
+    for it (the kernel then walks every epoch from toe) the positions are
+    the same bit for bit."""
+    from gnss_gpu_b200 import _native as N
+    from gnss_gpu_b200.ephemeris import broadcast_orbits
+
+    rng = np.random.default_rng(23)
+    recs = _glonass_records(8, rng)
+    times = (recs["glonass"]["toe"][0] + 18.0 + np.linspace(-5000.0, 5000.0, 257)) % 604800.0
+    idx = np.tile(np.arange(8, dtype=np.int32), (times.size, 1))
+    pos_a, clk_a = broadcast_orbits(recs, times, idx)
+    big = np.zeros(200_000, N.BROADCAST_DTYPE)  # 200K records: no room for the state table
+    big[:8] = recs
+    big["system"][8:] = ord("G")
+    pos_b, clk_b = broadcast_orbits(big, times, idx)
+    assert np.array_equal(pos_a, pos_b) and np.array_equal(clk_a, clk_b)
