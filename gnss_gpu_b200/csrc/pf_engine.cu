@@ -412,9 +412,10 @@ int sync_and_check(pf_engine* eng) {
 }
 
 int read_ctrl(pf_engine* eng) {
-  CK(cudaMemcpyAsync(eng->ctrl_host, eng->ctrl_dev, sizeof(FilterCtrl) * eng->cfg.n_filters,
-                     cudaMemcpyDeviceToHost, eng->stream));
-  return sync_and_check(eng);
+  // control blocks and the error word that follows them, in one copy
+  CK(cudaMemcpyAsync(eng->ctrl_host, eng->ctrl_dev, eng->ctrl_span, cudaMemcpyDeviceToHost, eng->stream));
+  CK(cudaStreamSynchronize(eng->stream));
+  return err_status(*eng->err_host);
 }
 
 int check_filter(pf_engine* eng, int f) {
