@@ -481,7 +481,8 @@ def run_learned(args, world, rank, local, pg, cfg4: bool):
         wall = time.perf_counter() - t0
         e = rr.err2d[:, 10:]
         out_runs[mode] = {"particle_steps_per_s": rr.steps_per_s, "e2e_particle_steps_per_s": float(n.sum()) * E / wall,
-                          "p50_2d_m": float(np.median(e)), "rms_2d_m": float(np.sqrt(np.mean(e ** 2)))}
+                          "p50_2d_m": float(np.median(e)), "rms_2d_m": float(np.sqrt(np.mean(e ** 2))),
+                          "h2d": rr.h2d_bytes, "d2h": rr.d2h_bytes}
     total = int(n.sum())
     # whole-job rate: every rank did the same work, the slowest sets the time
     value = -reduce_max(pg, -out_runs["mixture"]["particle_steps_per_s"])
@@ -503,9 +504,9 @@ def run_learned(args, world, rank, local, pg, cfg4: bool):
                      "epochs_scored": "all after the first 10"},
         "plain_particle_steps_per_s": pm["particle_steps_per_s"],
         "e2e": {"value": lm["e2e_particle_steps_per_s"], "unit": UNIT,
-                "h2d_bytes_per_step": "per epoch: filter records + satellites (56 B each)",
-                "d2h_bytes_per_step": "per epoch: results of every filter",
-                "api": "learned.run_filters: host ray trace of the prior, pack_epoch, upload, step, results"},
+                "h2d_bytes_per_step": int(lm["h2d"]), "d2h_bytes_per_step": int(lm["d2h"]),
+                "api": "learned.run_filters per epoch: prior geometry with the blocked flags ray-traced on the "
+                       "device (pf_city_los), pack_epoch, upload, step, results"},
         "training": training,
         "roofline": {"bound": "hbm", "kernel": "k_epoch<.., mixture, systematic>", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",

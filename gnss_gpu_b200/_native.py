@@ -130,7 +130,7 @@ EXPORTED = [
     "pfe_add_position_term", "pfe_add_obs_term", "pfe_step_io", "pfe_vel_init", "pfe_vel_follow",
     "pfe_vel_predict", "pfe_vel_doppler", "pf_mesh_build", "pf_mesh_los", "pfe_add_3d_term",
     "pf_weight_3d", "pf_sat_positions", "pf_sat_positions_batch", "pf_broadcast_orbits", "pf_sagnac",
-    "pf_ecef_to_lla",
+    "pf_ecef_to_lla", "pf_city_los",
 ]
 
 _lib = None
@@ -221,6 +221,7 @@ def load():
     L.pf_broadcast_orbits.argtypes = [p, i, p, p, i, i, d, p, p, p]
     L.pf_sagnac.argtypes = [p, p, i, i, p, p, p]
     L.pf_ecef_to_lla.argtypes = [dp, dp, dp, dp, dp, dp, i]
+    L.pf_city_los.argtypes = [p, p, p, i, d, d, i, p, p, i, p, p]
     L.pfe_get_sat_debug.argtypes = [p, i, p, i, C.POINTER(C.c_int)]
     for name in EXPORTED:
         fn = getattr(L, name)

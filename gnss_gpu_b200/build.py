@@ -17,7 +17,7 @@ LIB = LIBDIR / "libgnsspf_b200.so"
 SOURCES = ["pf_status.cu", "pf_engine.cu", "pf_compat.cu", "pf_noalloc.cu", "pf_mlp.cu"]
 HEADERS = ["pf_common.cuh", "pf_engine_dev.cuh", "pf_engine_kernels.cuh", "pf_epoch_kernel.cuh", "pf_mlp.cuh",
            "pf_learned.cuh", "pf_generic.cuh", "pf_obs_terms.cuh", "pf_velocity.cuh", "pf_bvh.cuh",
-           "pf_weight3d.cuh", "pf_orbit.cuh",
+           "pf_weight3d.cuh", "pf_orbit.cuh", "pf_city.cuh",
            "pf_status.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [

@@ -78,7 +78,7 @@ def los_blocked(city: City, p: np.ndarray, az: np.ndarray, el: np.ndarray) -> np
     blocked = np.zeros(len(p), bool)
     t_cur = np.zeros(len(p))
     alive = t_end > 0
-    steps = int(np.ceil(2.0 * (city.hmax / np.tan(np.radians(5.0))) / c)) + 4
+    steps = los_steps(city)
     for _ in range(steps):
         if not alive.any():
             break
@@ -118,6 +118,47 @@ def los_blocked(city: City, p: np.ndarray, az: np.ndarray, el: np.ndarray) -> np
         t_max_y = np.where(go_x, t_max_y, t_max_y + t_dy)
         alive = alive & ~blocked & (t_cur <= t_end)
     return blocked
+
+
+def los_steps(city: City) -> int:
+    """Cells a ray may cross in los_blocked before it is declared clear."""
+    return int(np.ceil(2.0 * (city.hmax / np.tan(np.radians(5.0))) / city.cell)) + 4
+
+
+def los_blocked_device(city: City, p: np.ndarray, az: np.ndarray, el: np.ndarray) -> np.ndarray:
+    """los_blocked on the GPU (pf_city_los): the same DDA in FP64 with the
+    same rounding, so the flags equal the host's.  The city's arrays stay on
+    the device (cached on the City object)."""
+    import ctypes as C
+
+    import torch
+
+    from . import _native as N
+
+    p = np.asarray(p, np.float64).reshape(-1, 3)
+    az = np.broadcast_to(np.asarray(az, np.float64), (len(p),))
+    el = np.broadcast_to(np.asarray(el, np.float64), (len(p),))
+    d = np.stack([np.cos(el) * np.sin(az), np.cos(el) * np.cos(az), np.sin(el)], axis=1)
+    out = np.zeros(len(p), bool)
+    if len(p) == 0:
+        return out
+    dev = torch.device("cuda", torch.cuda.current_device())
+    cache = getattr(city, "_dev", None)
+    if cache is None or cache[0] != dev:
+        cache = (dev, torch.from_numpy(np.ascontiguousarray(city.occ, dtype=np.uint8)).to(dev),
+                 torch.from_numpy(np.ascontiguousarray(city.box, dtype=np.float64)).to(dev),
+                 torch.from_numpy(np.ascontiguousarray(city.height, dtype=np.float64)).to(dev))
+        city._dev = cache
+    _, d_occ, d_box, d_h = cache
+    d_p = torch.from_numpy(np.ascontiguousarray(p)).to(dev)
+    d_d = torch.from_numpy(np.ascontiguousarray(d)).to(dev)
+    d_b = torch.empty(len(p), dtype=torch.uint8, device=dev)
+    ptr = lambda x: C.c_void_p(x.data_ptr())  # noqa: E731
+    N.check(N.load().pf_city_los(ptr(d_occ), ptr(d_box), ptr(d_h), int(city.n), float(city.cell),
+                                 float(city.hmax), los_steps(city), ptr(d_p), ptr(d_d), len(p), ptr(d_b),
+                                 C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
+    out[:] = d_b.cpu().numpy() != 0
+    return out
 
 
 @dataclass

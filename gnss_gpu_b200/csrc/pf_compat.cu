@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "pf_bvh.cuh"
+#include "pf_city.cuh"
 #include "pf_common.cuh"
 #include "pf_orbit.cuh"
 #include "pf_status.h"
@@ -762,6 +763,29 @@ int pf_ecef_to_lla(const double* ecef_x, const double* ecef_y, const double* ece
   CK(cudaMemcpyAsync(lon, dlo, nb, cudaMemcpyDeviceToHost, w->stream));
   CK(cudaMemcpyAsync(alt, dal, nb, cudaMemcpyDeviceToHost, w->stream));
   return finish(w);
+}
+
+int pf_city_los(const unsigned char* d_occ, const double* d_box, const double* d_height, int n, double cell,
+                double hmax, int steps, const double* d_p, const double* d_dir, int n_ray, unsigned char* d_blocked,
+                void* stream) {
+  clear_err();
+  if (n_ray < 0 || n < 0 || steps < 0) return set_err(PF_EINVAL, "sizes must be >= 0");
+  if (n_ray == 0) return PF_OK;
+  if (!d_p || !d_dir || !d_blocked || (n > 0 && (!d_occ || !d_box || !d_height)))
+    return set_err(PF_EINVAL, "null array");
+  if (!(cell > 0.0) || !isfinite(cell) || !isfinite(hmax)) return set_err(PF_EINVAL, "cell must be > 0, hmax finite");
+  if ((long long)n * n > (1ll << 28)) return set_err(PF_EINVAL, "city grid above 2^28 cells");
+  pfb::CityDev c;
+  c.occ = d_occ;
+  c.box = d_box;
+  c.height = d_height;
+  c.n = n;
+  c.cell = cell;
+  c.hmax = hmax;
+  c.steps = steps;
+  k_city_los<<<grid_of(n_ray), kB, 0, (cudaStream_t)stream>>>(c, d_p, d_dir, n_ray, d_blocked);
+  CK(cudaGetLastError());
+  return PF_OK;
 }
 
 }  // extern "C"

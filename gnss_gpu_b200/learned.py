@@ -80,7 +80,7 @@ def prior_geometry(tr: CS.CityTrajectory, t: int, prior_ecef: np.ndarray, prior_
     el = np.arcsin(np.clip(e[:, 2], -1.0, 1.0))
     p_enu = (prior_ecef - tr.anchor) @ tr.rot.T
     p_enu = np.array([p_enu[0], p_enu[1], CS.RX_HEIGHT])
-    blk = CS.los_blocked(tr.city, np.repeat(p_enu[None], len(sats), 0), az, el).astype(np.float32)
+    blk = CS.los_blocked_device(tr.city, np.repeat(p_enu[None], len(sats), 0), az, el).astype(np.float32)
     return e, res, blk
 
 
@@ -94,6 +94,8 @@ class RunResult:
     err2d: np.ndarray          # (F, E) horizontal error of the fused estimate, m
     priors: list               # per filter, per epoch (prior ECEF, prior clock)
     steps_per_s: float         # particle-steps/s of the device steps (event-timed)
+    h2d_bytes: float = 0.0     # mean host-to-device bytes per epoch (rays, records, satellites)
+    d2h_bytes: float = 0.0     # mean device-to-host bytes per epoch (blocked flags, results)
 
 
 def prior_geometry_many(trajs, t: int, priors):
@@ -119,7 +121,7 @@ def prior_geometry_many(trajs, t: int, priors):
             els.append(np.arcsin(np.clip(e[:, 2], -1.0, 1.0)))
             geo.append((e, res))
             spans.append(len(rng))
-        blk = CS.los_blocked(city, np.concatenate(pts), np.concatenate(azs), np.concatenate(els)).astype(np.float32)
+        blk = CS.los_blocked_device(city, np.concatenate(pts), np.concatenate(azs), np.concatenate(els)).astype(np.float32)
         o = 0
         for k, (e, res), m in zip(ks, geo, spans):
             out[k] = (e, res, blk[o:o + m])
@@ -151,6 +153,7 @@ def run_filters(trajs, n_particles, mode: str, params=None, seed: int = 0, keep_
         prior.append((start + tr.disp_enu[0] @ tr.rot, float(tr.truth_clk[0][0])))
     err = np.zeros((F, E))
     priors = [[] for _ in range(F)]
+    h2d = d2h = 0
     eng.enable_timing(E + 1)
     for t in range(E):
         geo = prior_geometry_many(trajs, t, prior)
@@ -163,6 +166,9 @@ def run_filters(trajs, n_particles, mode: str, params=None, seed: int = 0, keep_
         eng.upload(0, fe, sv)
         eng.step()
         res = eng.results()
+        # one ray per satellite (origin + direction, FP64) up and a flag back
+        h2d += fe.nbytes + sv.nbytes + 48 * len(sv)
+        d2h += eng.result_bytes() + len(sv)
         for k, tr in enumerate(trajs):
             est = res[k]["est_ecef"]
             d = (est - tr.truth_ecef[t]) @ tr.rot.T
@@ -172,7 +178,7 @@ def run_filters(trajs, n_particles, mode: str, params=None, seed: int = 0, keep_
     _, whole = eng.read_timing()
     eng.close()
     sps = float(np.sum(counts)) * len(whole) / max(float(np.sum(whole)) / 1e3, 1e-12)
-    return RunResult(err, priors, sps)
+    return RunResult(err, priors, sps, h2d / E, d2h / E)
 
 
 def training_set(trajs, priors):

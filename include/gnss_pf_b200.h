@@ -623,6 +623,18 @@ int pf_sagnac(const double* d_rx, const double* d_sat, int n_epoch, int n_sat, d
 int pf_ecef_to_lla(const double* ecef_x, const double* ecef_y, const double* ecef_z, double* lat, double* lon,
                    double* alt, int n);
 
+/* Line of sight through a box city (the learned likelihood's simulator
+ * cities: an n x n grid of cells of side `cell`, at most one axis-aligned
+ * box per cell; no counterpart in the reference, whose 3D path uses meshes).
+ * Device arrays: d_occ [n*n] (cell (ix, iy) at ix*n + iy), d_box [n*n*4]
+ * (x0, x1, y0, y1 in the city's local E/N, m), d_height [n*n]; rays from
+ * d_p [n_ray*3] (local E/N/U) along unit directions d_dir [n_ray*3] with
+ * positive up component; at most `steps` cells per ray; d_blocked [n_ray]
+ * 1 when a building is hit.  Asynchronous on `stream`. */
+int pf_city_los(const unsigned char* d_occ, const double* d_box, const double* d_height, int n, double cell,
+                double hmax, int steps, const double* d_p, const double* d_dir, int n_ray, unsigned char* d_blocked,
+                void* stream);
+
 #ifdef __cplusplus
 }
 #endif

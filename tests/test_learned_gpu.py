@@ -103,3 +103,26 @@ def test_trained_network_beats_plain_robust_filter():
     p50_plain, p50_learned = np.median(plain), np.median(learned)
     assert p50_learned < 0.8 * p50_plain, (p50_plain, p50_learned)
     assert np.sqrt(np.mean(learned ** 2)) < np.sqrt(np.mean(plain ** 2))
+
+
+def test_city_los_device_equals_host():
+    """pf_city_los restates the simulator's box-city DDA with the same FP64
+    rounding: flags equal to the host's, ray for ray, including rays along
+    the grid axes, from inside buildings and from outside the grid."""
+    from gnss_gpu_b200 import citysim as CS
+
+    rng = np.random.default_rng(8)
+    total = 0
+    for seed in (1, 2, 3):
+        city = CS.make_city(seed)
+        m = 20_000
+        p = np.column_stack([rng.uniform(-200.0, city.size + 200.0, m), rng.uniform(-200.0, city.size + 200.0, m),
+                             rng.uniform(0.0, 40.0, m)])
+        az = rng.uniform(0.0, 2 * np.pi, m)
+        el = rng.uniform(np.radians(2.0), np.radians(89.0), m)
+        az[:200] = rng.choice([0.0, np.pi / 2, np.pi, 3 * np.pi / 2], 200)  # along the grid axes
+        host = CS.los_blocked(city, p, az, el)
+        dev = CS.los_blocked_device(city, p, az, el)
+        assert np.array_equal(host, dev), int(np.sum(host != dev))
+        total += int(host.sum())
+    assert total > 1000  # the cases exercise blocked rays
