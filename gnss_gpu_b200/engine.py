@@ -135,34 +135,48 @@ class Engine:
     # ---------------------------------------------------------------- inputs
     def pack_epoch(self, per_filter):
         """per_filter: list of dicts with keys disp (3,), sats (S,3), pr (S,),
-        w (S,) [optional], clk (S,) [optional], flags (int)."""
+        w (S,) [optional], clk (S,) [optional], cn0 / blocked (S,)
+        [optional], flags (int).  One pass gathers the fields, then each
+        column is filled for all filters at once (an optional column given by
+        only some filters is filled filter by filter)."""
         F = len(self.filters)
         fe = np.zeros(F, N.FILTER_EPOCH_DTYPE)
-        chunks = []
+        opt = ("w", "clk", "cn0", "blocked")
+        sats_l, pr_l, counts = [], [], []
+        given = {k: [] for k in opt}
         off = 0
         for k, r in enumerate(per_filter):
-            fe["disp"][k] = np.asarray(r.get("disp", (0.0, 0.0, 0.0)), dtype=np.float64)
+            d = r.get("disp")
+            if d is not None:
+                fe["disp"][k] = d
             fe["flags"][k] = int(r.get("flags", N.PF_EP_PREDICT | N.PF_EP_WEIGHT))
-            sats = np.asarray(r.get("sats", np.zeros((0, 3))), dtype=np.float64).reshape(-1, 3)
-            s = len(sats)
+            sats = r.get("sats")
+            s = 0 if sats is None else len(sats)
             fe["n_sat"][k] = s
             fe["sat_offset"][k] = off
             if s:
-                rec = np.zeros(s, N.SAT_DTYPE)
-                rec["x"], rec["y"], rec["z"] = sats[:, 0], sats[:, 1], sats[:, 2]
-                rec["pr"] = np.asarray(r["pr"], dtype=np.float64).ravel()
-                w = r.get("w")
-                rec["w"] = 1.0 if w is None else np.asarray(w, dtype=np.float64).ravel()
-                clk = r.get("clk")
-                rec["clk"] = 0 if clk is None else np.asarray(clk, dtype=np.int32).ravel()
-                cn0 = r.get("cn0")
-                rec["cn0"] = 45.0 if cn0 is None else np.asarray(cn0, dtype=np.float32).ravel()
-                blk = r.get("blocked")
-                rec["blocked"] = 0.0 if blk is None else np.asarray(blk, dtype=np.float32).ravel()
-                chunks.append(rec)
-            off += s
-        sats_all = np.concatenate(chunks) if chunks else np.zeros(0, N.SAT_DTYPE)
-        return fe, sats_all
+                sats_l.append(sats)
+                pr_l.append(r["pr"])
+                for key in opt:
+                    v = r.get(key)
+                    if v is not None:
+                        given[key].append((off, s, v))
+                off += s
+        out = np.zeros(off, N.SAT_DTYPE)
+        if off:
+            xyz = np.concatenate([np.asarray(a, dtype=np.float64).reshape(-1, 3) for a in sats_l])
+            out["x"], out["y"], out["z"] = xyz[:, 0], xyz[:, 1], xyz[:, 2]
+            out["pr"] = np.concatenate([np.asarray(a, dtype=np.float64).ravel() for a in pr_l])
+            out["w"] = 1.0
+            out["cn0"] = 45.0
+            for key in opt:
+                g = given[key]
+                if len(g) == len(sats_l) and g:
+                    out[key] = np.concatenate([np.asarray(v).ravel() for _, _, v in g])
+                else:
+                    for a, n, v in g:
+                        out[key][a:a + n] = np.asarray(v).ravel()
+        return fe, out
 
     def upload(self, slot: int, fe: np.ndarray, sats: np.ndarray):
         fe = np.ascontiguousarray(fe, dtype=N.FILTER_EPOCH_DTYPE)
@@ -287,6 +301,13 @@ class Engine:
                 "resampled": bool(r.resampled), "epoch": r.epoch,
             })
         return out
+
+    def results_array(self) -> np.ndarray:
+        """The per-filter results as one structured array (fields est_ecef,
+        est_clk, cov_enu, ess, sum_w, max_lw, resampled, epoch, initialized),
+        a copy of pfe_read_results' records."""
+        N.check(self.lib.pfe_read_results(self.h, self._results))
+        return np.ctypeslib.as_array(self._results).copy()
 
     def result_bytes(self) -> int:
         b = C.c_size_t(0)

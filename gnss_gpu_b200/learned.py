@@ -99,32 +99,34 @@ class RunResult:
 
 
 def prior_geometry_many(trajs, t: int, priors):
-    """prior_geometry for many filters at once (one ray-trace call per
-    city)."""
+    """prior_geometry for many filters at once: per city, the satellites of
+    all its filters in one set of array operations and one device ray
+    trace."""
     out = [None] * len(trajs)
     by_city = {}
     for k, tr in enumerate(trajs):
         by_city.setdefault(id(tr.city), []).append(k)
     for ks in by_city.values():
         city = trajs[ks[0]].city
-        pts, azs, els, spans, geo = [], [], [], [], []
-        for k in ks:
-            tr = trajs[k]
-            pe, pc = priors[k]
-            v = tr.sats[t] - pe
-            rng = np.linalg.norm(v, axis=1)
-            e = (v / rng[:, None]) @ tr.rot.T
-            res = tr.pr[t] - rng - pc
-            p_enu = (pe - tr.anchor) @ tr.rot.T
-            pts.append(np.repeat(np.array([[p_enu[0], p_enu[1], CS.RX_HEIGHT]]), len(rng), 0))
-            azs.append(np.mod(np.arctan2(e[:, 0], e[:, 1]), 2 * np.pi))
-            els.append(np.arcsin(np.clip(e[:, 2], -1.0, 1.0)))
-            geo.append((e, res))
-            spans.append(len(rng))
-        blk = CS.los_blocked_device(city, np.concatenate(pts), np.concatenate(azs), np.concatenate(els)).astype(np.float32)
+        counts = [len(trajs[k].sats[t]) for k in ks]
+        sats = np.concatenate([trajs[k].sats[t] for k in ks])
+        pe = np.repeat(np.stack([priors[k][0] for k in ks]), counts, axis=0)
+        pc = np.repeat(np.array([priors[k][1] for k in ks], np.float64), counts)
+        rot = np.repeat(np.stack([trajs[k].rot for k in ks]), counts, axis=0)
+        anchor = np.repeat(np.stack([trajs[k].anchor for k in ks]), counts, axis=0)
+        pr = np.concatenate([trajs[k].pr[t] for k in ks])
+        v = sats - pe
+        rng = np.linalg.norm(v, axis=1)
+        e = np.einsum("nij,nj->ni", rot, v / rng[:, None])
+        res = pr - rng - pc
+        p_enu = np.einsum("nij,nj->ni", rot, pe - anchor)
+        p_enu[:, 2] = CS.RX_HEIGHT
+        az = np.mod(np.arctan2(e[:, 0], e[:, 1]), 2 * np.pi)
+        el = np.arcsin(np.clip(e[:, 2], -1.0, 1.0))
+        blk = CS.los_blocked_device(city, p_enu, az, el).astype(np.float32)
         o = 0
-        for k, (e, res), m in zip(ks, geo, spans):
-            out[k] = (e, res, blk[o:o + m])
+        for k, m in zip(ks, counts):
+            out[k] = (e[o:o + m], res[o:o + m], blk[o:o + m])
             o += m
     return out
 
@@ -154,6 +156,7 @@ def run_filters(trajs, n_particles, mode: str, params=None, seed: int = 0, keep_
     err = np.zeros((F, E))
     priors = [[] for _ in range(F)]
     h2d = d2h = 0
+    rots = np.stack([tr.rot for tr in trajs])
     eng.enable_timing(E + 1)
     for t in range(E):
         geo = prior_geometry_many(trajs, t, prior)
@@ -165,16 +168,16 @@ def run_filters(trajs, n_particles, mode: str, params=None, seed: int = 0, keep_
         fe, sv = eng.pack_epoch(recs)
         eng.upload(0, fe, sv)
         eng.step()
-        res = eng.results()
+        res = eng.results_array()
         # one ray per satellite (origin + direction, FP64) up and a flag back
         h2d += fe.nbytes + sv.nbytes + 48 * len(sv)
         d2h += eng.result_bytes() + len(sv)
-        for k, tr in enumerate(trajs):
-            est = res[k]["est_ecef"]
-            d = (est - tr.truth_ecef[t]) @ tr.rot.T
-            err[k, t] = np.hypot(d[0], d[1])
-            nxt = min(t + 1, E - 1)
-            prior[k] = (est + tr.disp_enu[nxt] @ tr.rot, float(res[k]["est_clk"][0]))
+        est = res["est_ecef"]
+        d = np.einsum("kij,kj->ki", rots, est - np.stack([tr.truth_ecef[t] for tr in trajs]))
+        err[:, t] = np.hypot(d[:, 0], d[:, 1])
+        nxt = min(t + 1, E - 1)
+        moved = est + np.einsum("kj,kji->ki", np.stack([tr.disp_enu[nxt] for tr in trajs]), rots)
+        prior = [(moved[k], float(res["est_clk"][k, 0])) for k in range(F)]
     _, whole = eng.read_timing()
     eng.close()
     sps = float(np.sum(counts)) * len(whole) / max(float(np.sum(whole)) / 1e3, 1e-12)
