@@ -409,6 +409,36 @@ def run_cfg2(args, world, rank, local, pg):
     t_pfg = timed(eng, lambda: eng.replay(1), len(n_part))
     eng.close()
     clk = clocks.stop()
+    # e2e: the same epochs from host records to host results through the
+    # public one-call API (pfe_step_io: pinned upload, the batched launch,
+    # one copy of every filter's results), host clock
+    e2e = None
+    if not args.no_e2e:
+        specs = [FilterSpec(n_particles=int(nf), seed=100 + k, sigma_pos=(1.0, 1.0, 0.5), sigma_clk=0.5,
+                            sigma_pr=3.0) for k, nf in enumerate(n_part)]
+        eng = Engine(specs, EngineOptions(n_clk=1, resampler="systematic", ess_threshold=0.5, max_sats=40,
+                                          obs_slots=1, covariance=True, recenter=True), device=local)
+        for k, tr in enumerate(trajs):
+            eng.initialize(k, tr.truth_ecef[0], tr.truth_clk[0], 10.0, 30.0)
+        host_in = [eng.pack_epoch([{"disp": tr.disp_enu[t], "sats": tr.sats[t], "pr": tr.pr[t], "flags": flags}
+                                   for tr in trajs]) for t in range(E)]
+        wall, h2d = [], 0
+        for t in range(W + K):
+            fe, sv = host_in[t]
+            with torch.cuda.stream(eng.stream):
+                flush.fill_(t & 0xFF)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eng.step_io(fe, sv)
+            wall.append(time.perf_counter() - t0)
+            h2d = max(h2d, fe.nbytes + sv.nbytes)
+        e2e_s = reduce_max(pg, float(np.sum(wall[W:])))
+        e2e = {"value": total_n * K * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(eng.result_bytes()), "ms_per_step": e2e_s / K * 1e3,
+               "api": "gnss_gpu_b200.Engine.step_io per epoch (all 256 filters)",
+               "timing": "host clock around each call; the L2 flush and a device synchronize run before each "
+                         "timer starts"}
+        eng.close()
     value = total_n * K * world / t_graph
     v_pf = total_n * K * world / t_pf
     peak, peak_kind = peaks()
@@ -430,6 +460,7 @@ def run_cfg2(args, world, rank, local, pg):
         "per_filter_launches_graph": {"value": total_n * K * world / t_pfg, "unit": UNIT,
                                       "ms_per_step": t_pfg / K * 1e3},
         "batched_over_per_filter": value / v_pf,
+        "e2e": e2e,
         "roofline": {"bound": "hbm", "kernel": "k_epoch (cooperative, all filters)", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",
                      "algorithmic_bytes_per_launch": b_alg * total_n, "traffic": committed_traffic("k_epoch:cfg2-batched")},
