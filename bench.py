@@ -706,6 +706,7 @@ def run_pf3d(args, world, rank, local, pg):
     eng = Engine([FilterSpec(n_particles=n, seed=7, sigma_pos=(0.5, 0.5, 0.5), sigma_clk=1.0, sigma_pr=3.0)],
                  EngineOptions(n_clk=1, max_sats=S_, ess_threshold=0.5))
     eng.initialize(0, truth, 80.0, 20.0, 5.0)
+    eng.sort_spatially(0)  # as ParticleFilter3DBVH.initialize does
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=torch.device("cuda", local))
     fe, sv = eng.pack_epoch([{"disp": np.zeros(3), "flags": N.PF_EP_PREDICT | N.PF_EP_RESAMPLE_CHECK}])
     eng.upload(0, fe, sv)

@@ -367,6 +367,27 @@ class Engine:
         lwa = None if lw is None else np.ascontiguousarray(lw, dtype=np.float32)
         N.check(self.lib.pfe_set_state_f32(self.h, k, N.vptr(st), None if lwa is None else N.vptr(lwa)))
 
+    def sort_spatially(self, k: int, cell: float = 1.0):
+        """Reorder filter k's particles (with their log-weights) by a Morton
+        code of their East/North offsets in cells of `cell` metres, stably
+        (ties keep their index order), so the order is deterministic.
+        Particles are exchangeable, so the filter's distribution does not
+        change; per-particle ray casts then run in spatially coherent
+        warps, and since systematic resampling keeps ancestors in index
+        order the population stays close to this order afterwards."""
+        st, lw = self.state_f32(k)
+        q = []
+        for a in (st[0], st[1]):
+            v = np.nan_to_num(a.astype(np.float64), nan=0.0)
+            q.append(np.clip(np.floor((v - v.min()) / cell), 0, 65535).astype(np.uint64))
+        key = np.zeros(len(lw), np.uint64)
+        for b in range(16):
+            one = np.uint64(1)
+            key |= ((q[0] >> np.uint64(b)) & one) << np.uint64(2 * b)
+            key |= ((q[1] >> np.uint64(b)) & one) << np.uint64(2 * b + 1)
+        order = np.argsort(key, kind="stable")
+        self.set_state_f32(k, np.ascontiguousarray(st[:, order]), np.ascontiguousarray(lw[order]))
+
     def ancestors(self, k: int) -> np.ndarray:
         out = np.zeros(self.filters[k].n_particles, np.int32)
         N.check(self.lib.pfe_get_ancestors(self.h, k, N.vptr(out)))

@@ -37,6 +37,13 @@ class ParticleFilter3D(ParticleFilter):
         self.blocked_nlos_prob = blocked_nlos_prob
         self.clear_nlos_prob = clear_nlos_prob
 
+    def initialize(self, position_ecef, clock_bias=0.0, spread_pos=100.0, spread_cb=1000.0):
+        """As ParticleFilter.initialize, then the particles are put in
+        spatial order (Engine.sort_spatially) so that the ray casts of
+        neighbouring threads take similar paths through the buildings."""
+        super().initialize(position_ecef, clock_bias, spread_pos, spread_cb)
+        self._engine.sort_spatially(0)
+
     def update(self, sat_ecef, pseudoranges, weights=None):
         """Building-aware weight update, ESS and ESS-triggered resampling."""
         if not self._initialized:

@@ -231,3 +231,30 @@ def test_bvh_filter_in_a_city(M):
     m3.pf_weight_3d(pts[:, 0].copy(), pts[:, 1].copy(), pts[:, 2].copy(), np.full(2, 80.0), sats.ravel(), pr,
                     np.ones(S_), tri, lw, 2, S_, 3.0, 30.0, 20.0)
     assert lw[0] > lw[1]
+
+
+def test_sort_spatially_is_a_deterministic_permutation():
+    """Engine.sort_spatially reorders the particles (a permutation of the
+    same states and log-weights), the same way every time, into Morton
+    order of their East/North cells."""
+    import numpy as np
+    from gnss_gpu_b200 import scenario as S
+    from gnss_gpu_b200.engine import Engine, EngineOptions, FilterSpec
+
+    tr = S.config0()
+    outs = []
+    for _ in range(2):
+        eng = Engine([FilterSpec(n_particles=50_000, seed=3, sigma_pos=(1.0, 1.0, 1.0), sigma_clk=3.0,
+                                 sigma_pr=5.0)], EngineOptions(n_clk=1, max_sats=8))
+        eng.initialize(0, tr.anchor, 100.0, 30.0, 50.0)
+        st0, lw0 = eng.state_f32(0)
+        eng.sort_spatially(0, cell=2.0)
+        st1, lw1 = eng.state_f32(0)
+        eng.close()
+        outs.append(st1)
+        a = np.lexsort(st0[::-1]); b = np.lexsort(st1[::-1])
+        assert np.array_equal(st0[:, a], st1[:, b])
+        # neighbours in the new order are close: median step between consecutive particles
+        step = np.hypot(np.diff(st1[0]), np.diff(st1[1]))
+        assert np.median(step) < 0.25 * np.median(np.hypot(np.diff(st0[0]), np.diff(st0[1])))
+    assert np.array_equal(outs[0], outs[1])
