@@ -261,7 +261,9 @@ __global__ void k_glo_table(const pf_broadcast_t* __restrict__ recs, int n_recs,
 // is null) at times[e]; an index outside [0, n_recs) gives NaN, and so does a
 // GLONASS integration past kGloMaxSteps steps (also flagged in *err if given).
 // tbl / kc: the GLONASS state table of k_glo_table, or null / 0.
-__global__ void k_broadcast_orbits(const pf_broadcast_t* __restrict__ recs, int n_recs,
+// Three CTAs of 256 per SM (80 registers): the walk is FP64-latency bound,
+// and the extra warps hide more of it than the few spilled values cost.
+__global__ void __launch_bounds__(256, 3) k_broadcast_orbits(const pf_broadcast_t* __restrict__ recs, int n_recs,
                                    const int* __restrict__ idx, const double* __restrict__ times,
                                    int n_epoch, int n_sat, double glo_step, const double* __restrict__ tbl, int kc,
                                    double* __restrict__ pos, double* __restrict__ clk, int* __restrict__ err) {
