@@ -44,6 +44,7 @@ struct Workspace {
 std::mutex g_mu;
 std::vector<Workspace> g_ws;  // indexed by device
 
+
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 int cuda_status(cudaError_t e, const char* what) {
@@ -73,6 +74,33 @@ int workspace(size_t bytes, Workspace** out) {
     w.bytes = want;
   }
   *out = &w;
+  return PF_OK;
+}
+
+// Stream-ordered scratch of the asynchronous entry points: the library's own
+// memory pool per device, which keeps freed memory (release threshold
+// unlimited), so a call does not wait on the driver for fresh memory and the
+// caller's default pool is left as it is.
+std::vector<cudaMemPool_t> g_pools;  // indexed by device
+
+int scratch_pool(cudaMemPool_t* out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_mu);
+  if ((int)g_pools.size() <= dev) g_pools.resize(dev + 1, nullptr);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    CK(cudaMemPoolCreate(&pool, &props));
+    unsigned long long keep = ~0ull;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_pools[dev] = pool;
+  }
+  *out = g_pools[dev];
   return PF_OK;
 }
 
@@ -710,7 +738,10 @@ int pf_broadcast_orbits(const pf_broadcast_t* d_recs, int n_recs, const int* d_r
   const size_t kmax_bytes = align_up(sizeof(int) * 2 * (size_t)n_recs, 256);
   const size_t tbl_bytes = (size_t)2 * n_recs * kc * 6 * sizeof(double);
   unsigned char* scratch = nullptr;
-  CK(cudaMallocAsync((void**)&scratch, kmax_bytes + tbl_bytes, st));
+  cudaMemPool_t pool = nullptr;
+  int ps = scratch_pool(&pool);
+  if (ps != PF_OK) return ps;
+  CK(cudaMallocFromPoolAsync((void**)&scratch, kmax_bytes + tbl_bytes, pool, st));
   int* kmax = (int*)scratch;
   double* tbl = (double*)(scratch + kmax_bytes);
   cudaError_t ce = cudaMemsetAsync(kmax, 0, kmax_bytes, st);
