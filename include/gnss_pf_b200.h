@@ -607,7 +607,10 @@ int pf_sat_positions_batch(const pf_ephemeris_t* params, const double* gps_times
  * d_recs[s] when d_rec_index is NULL; an index outside [0, n_recs) gives NaN)
  * at GPST second of week d_times[e].  d_pos (n_epoch*n_sat*3) or d_clk
  * (n_epoch*n_sat) may be NULL.  glo_step is the GLONASS RK4 step in seconds
- * (<= 0: 60 s, the reference's default, orbit_glonass.py:36). */
+ * (<= 0: 60 s, the reference's default, orbit_glonass.py:36).  Each call
+ * takes up to 64 MB of scratch (the shared GLONASS states) from the
+ * library's own stream-ordered memory pool on the current device; the pool
+ * keeps that memory until the process exits. */
 int pf_broadcast_orbits(const pf_broadcast_t* d_recs, int n_recs, const int* d_rec_index, const double* d_times,
                         int n_epoch, int n_sat, double glo_step, double* d_pos, double* d_clk, void* stream);
 /* Sagnac rotation and geometric range (python/gnss_gpu/range_model.py:12-40)
