@@ -1,9 +1,10 @@
 // pf_noalloc.cu -- ESS of device-resident log-weights with no allocation.
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA graph is
-// being captured (allocation is not allowed there), real-time loops such as
-// a receiver node that must not allocate after start-up, and hosts whose
-// device memory is owned by another allocator.  pf_compute_ess_noalloc
+// Some callers cannot call cudaMalloc: real-time loops such as a receiver
+// node that must not allocate (and risk a stall) after start-up, and host
+// applications whose device memory is all handed to another allocator, where
+// a cudaMalloc of ours could fail or fragment their arena.
+// pf_compute_ess_noalloc
 // serves them: the caller passes its own device input and output, and the
 // per-block partial sums live in a fixed file-scope device array instead of
 // an allocated workspace.

@@ -86,9 +86,9 @@ int pf_compute_ess(const double* log_weights, int n_particles,
                    double* ess_out);
 
 /* No counterpart in the reference.  ESS of log-weights already in device
- * memory, for callers that cannot allocate device memory (during CUDA graph
- * capture, in real-time loops that must not allocate after start-up, or when
- * another allocator owns the device memory).  d_log_weights and d_ess_out
+ * memory, for callers that cannot allocate device memory (real-time loops
+ * that must not allocate after start-up, or applications whose device memory
+ * is owned by another allocator).  d_log_weights and d_ess_out
  * are caller-owned device pointers; the work is queued on `stream` (a
  * cudaStream_t, NULL = legacy) and *d_ess_out is valid once that stream
  * reaches this point.  The function allocates nothing: its scratch is one

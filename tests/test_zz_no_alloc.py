@@ -1,7 +1,6 @@
 """pf_compute_ess_noalloc: the entry point for callers that cannot call
-cudaMalloc -- code running while a CUDA graph is captured, real-time loops
-that must not allocate after start-up, hosts whose device memory belongs to
-another allocator.  It takes caller-owned device input and output and keeps
+cudaMalloc -- real-time loops that must not allocate after start-up, hosts
+whose device memory belongs to another allocator.  It takes caller-owned device input and output and keeps
 its scratch in a fixed device array of the library.
 
 This file is collected last on purpose (its name sorts after the others), so
