@@ -51,6 +51,8 @@ def parse():
                     help="epoch: one cooperative kernel per step; chain: one kernel per phase")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default workload at one GPU: skip the cfg1-megopolis, cfg2 and cfg3 keys")
     return ap.parse_args()
 
 
@@ -910,6 +912,40 @@ def run_orbits(args, world, rank, local, pg):
     return out
 
 
+# ------------------------------------- the rest of the metric, one GPU
+def run_extras(args, world, rank, local, pg):
+    """The other halves of the headline metric, bounded to a few minutes, as
+    extra keys of the default line: cfg1 with 32 Megopolis iterations, the
+    256 batched filters against per-filter launches, and the learned
+    likelihood against the plain robust filter (P50 / RMS 2D error)."""
+    import copy
+    out = {}
+    a = copy.copy(args)
+    a.workload, a.no_e2e, a.no_cpu_baseline = "cfg1-megopolis", True, True
+    m = run_b200(a, world, rank, local, pg)
+    out["cfg1_megopolis"] = {"value": m["value"], "unit": UNIT, "ms_per_step": m["ms_per_step"],
+                             "steps": m["steps"], "resampled_fraction": m["resampled_fraction"],
+                             "roofline_frac_64B": m["value"] * 64 / 1e9 / m["roofline"]["peak"],
+                             "roofline": m["roofline"], "clocks": m["clocks"],
+                             "workload": m["config"]["workload"]}
+    a = copy.copy(args)
+    a.workload, a.no_e2e = "cfg2-batched", False
+    c2 = run_cfg2(a, world, rank, local, pg)
+    out["cfg2"] = {"value": c2["value"], "unit": UNIT, "ms_per_step": c2["ms_per_step"], "steps": c2["steps"],
+                   "per_filter_launches": c2["per_filter_launches"],
+                   "per_filter_launches_graph": c2["per_filter_launches_graph"],
+                   "batched_over_per_filter": c2["batched_over_per_filter"],
+                   "e2e": c2["e2e"], "roofline": c2["roofline"], "clocks": c2["clocks"],
+                   "workload": c2["config"]["workload"]}
+    a = copy.copy(args)
+    a.workload = "cfg3-learned"
+    c3 = run_learned(a, world, rank, local, pg, False)
+    out["cfg3"] = {"value": c3["value"], "unit": UNIT, "plain_particle_steps_per_s": c3["plain_particle_steps_per_s"],
+                   "accuracy": c3["accuracy"], "e2e": c3["e2e"], "training": c3["training"],
+                   "workload": c3["config"]["workload"]}
+    return out
+
+
 # ------------------------------------------------------- reference arm
 def run_reference(args, world, rank):
     if rank != 0:
@@ -955,6 +991,8 @@ def main():
         out = run_learned(args, world, rank, local, pg, args.workload == "cfg4-batched-learned")
     else:
         out = run_b200(args, world, rank, local, pg)
+        if args.workload == "cfg1-systematic" and world == 1 and not args.no_extras:
+            out.update(run_extras(args, world, rank, local, pg))
     if rank == 0 and out is not None:
         print(json.dumps(out), flush=True)
     if pg is not None:

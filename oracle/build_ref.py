@@ -8,7 +8,8 @@ from the reference: the sources are read where they lie and only the compiled
 module is written.  The module needs a GPU at run time; it serves as a second
 check of the oracle and as the reference's own GPU path on the same B200.
 
-Usage: python oracle/build_ref.py [/path/to/reference]
+Usage: python oracle/build_ref.py /path/to/reference
+       (or set GNSS_GPU_REFERENCE to the reference checkout)
 """
 from __future__ import annotations
 
@@ -22,7 +23,10 @@ HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref" / "gnss_gpu"
 
 
-def build(ref_root: str = "/root/reference", force: bool = False) -> Path | None:
+def build(ref_root: str | None = None, force: bool = False) -> Path | None:
+    ref_root = ref_root or os.environ.get("GNSS_GPU_REFERENCE")
+    if not ref_root:
+        return None
     ref = Path(ref_root)
     src = ref / "src" / "particle_filter"
     if not src.exists():
@@ -57,4 +61,4 @@ def build(ref_root: str = "/root/reference", force: bool = False) -> Path | None
 
 
 if __name__ == "__main__":
-    print(build(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", force=True))
+    print(build(sys.argv[1] if len(sys.argv) > 1 else None, force=True))

@@ -5,7 +5,7 @@ ECEF -> geodetic conversion).
 
 Run in a container that has the reference checkout:
 
-    python tests/golden/make_io_golden.py /root/reference
+    python tests/golden/make_io_golden.py /path/to/reference
 
 The RINEX and NMEA files are written here, in the RINEX 2.11 / 3.04 and NMEA
 0183 layouts, with the cases the parsers handle: multi-line observation-type
@@ -15,6 +15,7 @@ event records, bad checksums, empty NMEA fields and both hemispheres.
 from __future__ import annotations
 
 import json
+import os
 import sys
 import tempfile
 from datetime import date, datetime
@@ -188,4 +189,4 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ["GNSS_GPU_REFERENCE"])

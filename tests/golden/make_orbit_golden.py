@@ -6,7 +6,7 @@ selection, and RINEX 2/3 navigation parsing (io/nav_rinex).
 
 Run in a container that has the reference checkout:
 
-    python tests/golden/make_orbit_golden.py /root/reference
+    python tests/golden/make_orbit_golden.py /path/to/reference
 
 The GPS record is the reference test-suite's PRN 01 record
 (tests/test_ephemeris.py:32-57, loaded from that file); the Galileo, QZSS
@@ -20,6 +20,7 @@ import dataclasses
 import importlib.util
 import json
 import math
+import os
 import sys
 import tempfile
 from datetime import datetime
@@ -227,4 +228,4 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ["GNSS_GPU_REFERENCE"])

@@ -43,6 +43,36 @@ def test_noalloc_ess_matches_pf_compute_ess_on_two_calls_in_a_row():
         assert got == pytest.approx(want, rel=1e-12), (got, want)
 
 
+def test_noalloc_ess_at_its_limit_and_without_allocating():
+    """n = PF_NOALLOC_MAX_PARTICLES fills every row of the scratch array (the
+    last block writes the last row).  A warmed-up call must leave the
+    device's free memory unchanged: the entry point allocates nothing."""
+    import torch
+    from gnss_gpu_b200 import _native as N
+    from gnss_gpu_b200 import _gnss_gpu_pf as pfm
+
+    lib = N.load()
+    n = N.PF_NOALLOC_MAX_PARTICLES
+    lw = np.random.default_rng(7).normal(-3.0, 2.0, n)
+    d_lw = torch.from_numpy(lw).cuda()
+    d_out = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def call():
+        st = lib.pf_compute_ess_noalloc(C.c_void_p(d_lw.data_ptr()), n, C.c_void_p(d_out.data_ptr()),
+                                        C.c_void_p(stream.cuda_stream))
+        assert st == 0, lib.pf_last_error().decode()
+        stream.synchronize()
+
+    call()  # warm-up: module load and the one-time symbol lookup
+    free_before, _ = torch.cuda.mem_get_info()
+    call()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before, (free_before, free_after)
+    want = pfm.pf_compute_ess(lw, n)
+    assert float(d_out.item()) == pytest.approx(want, rel=1e-12)
+
+
 def test_noalloc_ess_rejects_sizes_beyond_its_scratch():
     import torch
     from gnss_gpu_b200 import _native as N
