@@ -144,6 +144,19 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
+def host_cpu():
+    """Host CPU model, logical CPUs and the CPUs this process may run on."""
+    model = ""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"cpu_model": model, "logical_cpus": os.cpu_count(), "affinity": len(os.sched_getaffinity(0))}
+
+
 # ------------------------------------------------------------- workloads
 def cfg1_inputs(n_epochs: int, seed: int):
     from gnss_gpu_b200 import scenario as S
@@ -343,7 +356,7 @@ def run_b200(args, world, rank, local, pg):
         v, cores, dt = cpu_baseline_cfg1(n, epochs, 7)
         out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                                "sample": f"oracle FP64 C port (OpenMP), {n} particles x 32 satellites, "
-                                         f"{epochs} epochs, {dt:.1f} s"}
+                                         f"{epochs} epochs, {dt:.1f} s", **host_cpu()}
     eng.close()
     return out
 
@@ -947,6 +960,51 @@ def run_extras(args, world, rank, local, pg):
 
 
 # ------------------------------------------------------- reference arm
+def reference_gpu_cfg1(n: int, steps: int):
+    """The reference's own GPU path on this GPU: its stock ParticleFilter
+    class (python/gnss_gpu/particle_filter.py) over its _gnss_gpu_pf module,
+    as installed unmodified into baseline/_ref (CUDA built for sm_100a).  A
+    step is predict + update (weight, ESS, systematic resampling when
+    ESS < N/2) + estimate, as in the reference's benchmarks/
+    bench_particle_filter.py:53-145.  Every call moves the full FP64 particle
+    arrays between host and device, which is the reference's design.  It has
+    one clock state, so the four constellations' clocks are one state here."""
+    import torch
+    ref = ROOT / "baseline" / "_ref"
+    if not (ref / "gnss_gpu" / "particle_filter.py").exists():
+        return {"unavailable": "baseline/_ref holds no reference install"}
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    sys.path.insert(0, str(ref))
+    try:
+        from gnss_gpu.particle_filter import ParticleFilter as RefPF
+    finally:
+        sys.path.remove(str(ref))
+    tr = cfg1_inputs(steps + 4, 21)
+    pf = RefPF(n_particles=n, sigma_pos=1.0, sigma_cb=0.5, sigma_pr=3.0, resampling="systematic",
+               ess_threshold=0.5, seed=42)
+    pf.initialize(tr.truth_ecef[0], clock_bias=float(tr.truth_clk[0][0]), spread_pos=10.0, spread_cb=30.0)
+
+    def step(t):
+        vel = tr.disp_enu[t] @ tr.rot  # ENU displacement per 1 s epoch -> ECEF velocity
+        pf.predict(velocity=vel, dt=1.0)
+        pf.update(tr.sats[t], tr.pr[t])
+        return pf.estimate()
+
+    for t in range(2):
+        step(t)
+    t0 = time.perf_counter()
+    k = 0
+    while k < steps and (k < 3 or time.perf_counter() - t0 < 20.0):
+        step(2 + k)
+        k += 1
+    dt = time.perf_counter() - t0
+    return {"value": n * k / dt, "unit": UNIT, "ms_per_step": dt / k * 1e3, "steps": k,
+            "api": "gnss_gpu.ParticleFilter predict + update + estimate (reference, baseline/_ref)",
+            "timing": "host clock; every reference call synchronises the device and copies to the host",
+            "config": f"{n} particles x 32 satellites, one clock state, systematic resampling when ESS<N/2"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
@@ -967,10 +1025,15 @@ def run_reference(args, world, rank):
                                "systematic resampling when ESS<N/2 (CPU restatement of the reference step)",
                    "parallelism": "host cores (OpenMP)"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{n} particles x {k_eff} epochs, {dt:.1f} s"},
+                         "sample": f"{n} particles x {k_eff} epochs, {dt:.1f} s", **host_cpu()},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "gpu_launches": 0,
     }
+    if args.workload == "cfg1-systematic":
+        try:
+            out["reference_gpu"] = reference_gpu_cfg1(n, max(3, K))
+        except Exception as exc:  # a stated extra, never the arm itself
+            out["reference_gpu"] = {"unavailable": f"{type(exc).__name__}: {exc}"[:200]}
     return out
 
 
