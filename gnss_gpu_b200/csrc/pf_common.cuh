@@ -82,10 +82,11 @@ enum : uint32_t {
 __device__ __forceinline__ float bm_log_u1(uint32_t a) {
   const float two_m32 = 2.3283064365386963e-10f;
   const float half_ulp = 1.1641532182693481e-10f;
-  const float u1 = fmaf((float)a, two_m32, half_ulp);
-  const float v = fmaf((float)(~a), two_m32, half_ulp);
-  const float near_one = -v * fmaf(v, fmaf(v, 1.0f / 3.0f, 0.5f), 1.0f);
-  return (a >= 0xFF000000u) ? near_one : __logf(u1);
+  if (a >= 0xFF000000u) {
+    const float v = fmaf((float)(~a), two_m32, half_ulp);
+    return -v * fmaf(v, fmaf(v, 1.0f / 3.0f, 0.5f), 1.0f);
+  }
+  return __logf(fmaf((float)a, two_m32, half_ulp));
 }
 
 // The angle uses the top 24 bits of b: u2 = (b >> 8) 2^-24 - 1/2 is exact in

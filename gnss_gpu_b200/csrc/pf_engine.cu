@@ -175,7 +175,7 @@ Layout make_layout(const pf_engine_config_t* cfg, const pf_filter_params_t* fp) 
   L.off_ctrl = take(sizeof(FilterCtrl) * cfg->n_filters);
   L.off_err = take(sizeof(unsigned) * 4);
   L.off_tf = take((size_t)T * 4);
-  L.off_queue = take(sizeof(unsigned) * (2 * Q_COUNT + kBarFlags + kMaxEpochGrid));
+  L.off_queue = take(sizeof(unsigned) * (2 * Q_COUNT + kBarWords));
   L.obs_slot_bytes = align_up(sizeof(pf_filter_epoch_t) * cfg->n_filters +
                                   sizeof(pf_sat_t) * (size_t)cfg->n_filters * cfg->max_sats,
                               256);
@@ -578,7 +578,7 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
     c.rs_seq = 1;
   }
   if (check_cuda(cudaMemsetAsync(w + L.off_flag, 0, (size_t)L.T * 4, eng->stream), "memset flags") != PF_OK ||
-      check_cuda(cudaMemsetAsync(w + L.off_queue, 0, sizeof(unsigned) * (2 * Q_COUNT + kBarFlags + kMaxEpochGrid),
+      check_cuda(cudaMemsetAsync(w + L.off_queue, 0, sizeof(unsigned) * (2 * Q_COUNT + kBarWords),
                                  eng->stream), "memset queue") != PF_OK ||
       check_cuda(cudaMemsetAsync(w + L.off_err, 0, sizeof(unsigned) * 4, eng->stream), "memset err") != PF_OK ||
       check_cuda(cudaMemsetAsync(w + L.off_fmax, 0, (size_t)cfg->n_filters * 4, eng->stream), "memset fmax") != PF_OK ||
@@ -1743,8 +1743,8 @@ int pfe_test_poison_lookback(pf_engine_t* eng, int on) {
   if (!on) {
     CK(cudaStreamSynchronize(eng->stream));
     CK(cudaMemset(eng->dev.err, 0, sizeof(unsigned)));
-    // timed-out barriers leave their generation and arrival flags behind: start clean
-    CK(cudaMemset(eng->bar, 0, sizeof(unsigned) * (kBarFlags + kMaxEpochGrid)));
+    // timed-out barriers leave their generation and arrival count behind: start clean
+    CK(cudaMemset(eng->bar, 0, sizeof(unsigned) * kBarWords));
   }
   return PF_OK;
 }

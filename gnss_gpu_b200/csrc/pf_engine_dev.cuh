@@ -17,7 +17,8 @@ constexpr int kSubTiles = kTile / kWarpTile;    // warp segments per tile
 constexpr int kLightRun = 32;                   // epoch kernel: longest offspring run written in phase 4
 constexpr int kRunChunk = 1024;                 // epoch kernel: slots per queued chunk of a longer run
 constexpr int kBarChunks = 3;                   // epoch kernel: queued-chunk counter in the barrier block
-constexpr int kBarFlags = 8;                    // epoch kernel: first arrival-flag word of the barrier block
+constexpr int kBarCount = 4;                    // epoch kernel: arrival counter in the barrier block
+constexpr int kBarWords = 8;                    // epoch kernel: words of the barrier block
 constexpr int kMaxEpochGrid = 2048;             // epoch kernel: most CTAs of one launch
 constexpr int kMaxD = 3 + PF_MAX_CLK;
 
