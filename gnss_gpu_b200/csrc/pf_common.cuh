@@ -7,7 +7,8 @@
 // * Box-Muller normals.
 // * Deterministic weight quantisation: exp(lw - max) evaluated with IEEE
 //   double-precision operations that round identically on host and device,
-//   then scaled to a 64-bit integer.  The systematic resampler's CDF is an
+//   then scaled to a 64-bit integer, and the exact rescaling of integer sums
+//   by such exponentials (scale_floor).  The systematic resampler's CDF is an
 //   exact integer prefix sum of these values, so the ancestor indices are a
 //   function of (log-weights, offset) alone, independent of scan order.
 // * The systematic predicate of resampling.cu:69-77,
@@ -17,6 +18,7 @@
 #pragma once
 #include <stdint.h>
 #include <math.h>
+#include <string.h>
 #include <cuda_runtime.h>
 
 #define PF_HD __host__ __device__ __forceinline__
@@ -150,18 +152,10 @@ PF_HD int quant_exponent(int n) {
   return k < 40 ? k : 40;
 }
 
-// q = floor(2^K * exp(d)) for a shifted log-weight d = lw - max <= 0.
-// x = d * log2(e), n = floor(x), f = x - n (exact), t = f * ln 2, and
-// e^t = 2^f from the Taylor series of the exponential (coefficients 1/j!,
-// degree 13, truncation error < 1e-13 for t in [0, ln 2)) in Horner form
-// with fma; 2^n scales exactly.  Weights below 2^-40 of the largest
-// quantise to zero.
-PF_HD uint64_t quantize_shifted(double d, int K) {
-  const double x = det_mul(d, 1.4426950408889634074);
-  if (!(x > -40.0)) return 0ull;  // also catches NaN
-  const double n = floor(x);
-  const double f = det_sub(x, n);  // exact: f in [0, 1)
-  const double t = det_mul(f, 0.69314718055994530942);
+// e^t for t in [0, ln 2): the Taylor series of the exponential
+// (coefficients 1/j!, degree 13, truncation error < 1e-13) in Horner form
+// with fma.
+PF_HD double exp_poly(double t) {
   double q = 1.6059043836821615e-10;  // 1/13!
   q = det_fma(q, t, 2.0876756987868099e-09);  // 1/12!
   q = det_fma(q, t, 2.5052108385441720e-08);  // 1/11!
@@ -176,8 +170,103 @@ PF_HD uint64_t quantize_shifted(double d, int K) {
   q = det_fma(q, t, 0.5);
   q = det_fma(q, t, 1.0);
   q = det_fma(q, t, 1.0);  // e^t = 2^f in [1, 2]
-  const double v = ldexp(q, K + (int)n);  // exact scaling, <= 2^(K+1)
-  return (uint64_t)v;                     // truncation
+  return q;
+}
+
+// q = floor(2^K * exp(d)) for a shifted log-weight d = lw - max <= 0.
+// x = d * log2(e), n = floor(x), f = x - n (exact), t = f * ln 2, and
+// e^t = 2^f from exp_poly; 2^n scales exactly.  Weights below 2^-40 of the
+// largest quantise to zero.
+PF_HD uint64_t quantize_shifted(double d, int K) {
+  const double x = det_mul(d, 1.4426950408889634074);
+  if (!(x > -40.0)) return 0ull;  // also catches NaN
+  const double n = floor(x);
+  const double f = det_sub(x, n);  // exact: f in [0, 1)
+  const double t = det_mul(f, 0.69314718055994530942);
+  const double v = ldexp(exp_poly(t), K + (int)n);  // exact scaling, <= 2^(K+1)
+  return (uint64_t)v;                               // truncation
+}
+
+// floor(v * r) for an integer v < 2^53 and 0 <= r <= 1: one rounded product
+// (exact conversion of v), then truncation.
+PF_HD uint64_t scale_floor(uint64_t v, double r) { return (uint64_t)det_mul((double)v, r); }
+// The same on an integer-valued double v < 2^53.
+PF_HD double scale_trunc(double v, double r) { return trunc(det_mul(v, r)); }
+
+// ------------------------------------- deterministic FP32 exponential
+// The engine's log-weights are FP32 (about 1e-7 relative), so its integer
+// CDF evaluates e^d in FP32 with round-to-nearest operations that neither
+// compiler may contract, identical on host and device: x = d log2(e) (one
+// rounded product), n = floor(x), f = x - n (one rounded difference), 2^f
+// from the Taylor series of e^(f ln 2) (coefficients (ln 2)^k / k! rounded to
+// FP32, degree 9, Horner with fma; within 2 ulp of 2^f), and 2^n applied
+// exactly.
+PF_HD float det_fmul(float a, float b) {
+#ifdef __CUDA_ARCH__
+  return __fmul_rn(a, b);
+#else
+  volatile float r = a * b;
+  return r;
+#endif
+}
+PF_HD float det_fsub(float a, float b) {
+#ifdef __CUDA_ARCH__
+  return __fsub_rn(a, b);
+#else
+  volatile float r = a - b;
+  return r;
+#endif
+}
+PF_HD float det_ffma(float a, float b, float c) {
+#ifdef __CUDA_ARCH__
+  return __fmaf_rn(a, b, c);
+#else
+  return fmaf(a, b, c);
+#endif
+}
+PF_HD float exp2_frac_f32(float f) {
+  float q = 0x1.b5253ep-24f;  // (ln 2)^9 / 9!
+  q = det_ffma(q, f, 0x1.62c022p-20f);  // (ln 2)^8 / 8!
+  q = det_ffma(q, f, 0x1.ffcbfcp-17f);  // (ln 2)^7 / 7!
+  q = det_ffma(q, f, 0x1.430912p-13f);  // (ln 2)^6 / 6!
+  q = det_ffma(q, f, 0x1.5d87fep-10f);  // (ln 2)^5 / 5!
+  q = det_ffma(q, f, 0x1.3b2ab6p-7f);  // (ln 2)^4 / 4!
+  q = det_ffma(q, f, 0x1.c6b08ep-5f);  // (ln 2)^3 / 3!
+  q = det_ffma(q, f, 0x1.ebfbep-3f);  // (ln 2)^2 / 2!
+  q = det_ffma(q, f, 0x1.62e43p-1f);  // ln 2
+  q = det_ffma(q, f, 0x1.0p+0f);
+  return q;
+}
+
+// 2^m as a float, exact for -126 <= m <= 127.
+PF_HD float pow2_f32(int m) {
+  const uint32_t b = (uint32_t)(127 + m) << 23;
+#ifdef __CUDA_ARCH__
+  return __uint_as_float(b);
+#else
+  float r;
+  memcpy(&r, &b, sizeof(r));
+  return r;
+#endif
+}
+
+// floor(2^K e^d) for a shifted FP32 log-weight d = lw - max <= 0, as an
+// integer-valued float (exact: 2^f 2^(K+n) < 2^41 is a float, its
+// truncation too); weights below 2^-40 of the maximum quantise to zero.
+PF_HD float quantize_f32(float d, int K) {
+  const float x = det_fmul(d, 0x1.715476p+0f /* log2(e) */);
+  if (!(x > -40.0f)) return 0.0f;  // also catches NaN
+  const float n = floorf(x);
+  const float p = exp2_frac_f32(det_fsub(x, n));
+  return truncf(p * pow2_f32(K + (int)n));
+}
+
+// e^d for d <= 0 (0 below 2^-126), the scale factors of the tiled CDF.
+PF_HD float det_expf(float d) {
+  const float x = det_fmul(d, 0x1.715476p+0f /* log2(e) */);
+  if (!(x > -126.0f)) return 0.0f;
+  const float n = floorf(x);
+  return exp2_frac_f32(det_fsub(x, n)) * pow2_f32((int)n);  // exact: a normal float
 }
 
 // ------------------------------------------------ 128-bit exact compare
@@ -245,6 +334,21 @@ PF_HD uint32_t offspring_end_scaled(uint64_t C, uint64_t W, uint32_t N, uint32_t
   const double fr = x - fl;
   if (fr > 0x1p-16 && fr < 1.0 - 0x1p-16) return (uint32_t)(k + 1);
   return offspring_end_settle(k, C, W, N, u);
+}
+
+// offspring_end_scaled for C = P + t2 with P exact (and Pd its double) and t2
+// an integer-valued double: the estimate uses (Pd + t2) (relative error
+// 2^-52, the same bound as above), the exact checks the 64-bit sum.
+PF_HD uint32_t offspring_end_split(uint64_t P, double Pd, double t2, uint64_t W, uint32_t N, uint32_t u,
+                                   double scale, double uf) {
+  const double x = (Pd + t2) * scale - uf;
+  const double fl = floor(x);
+  long long k = (long long)fl;
+  if (k < -1) k = -1;
+  if (k > (long long)N - 1) k = (long long)N - 1;
+  const double fr = x - fl;
+  if (fr > 0x1p-16 && fr < 1.0 - 0x1p-16) return (uint32_t)(k + 1);
+  return offspring_end_settle(k, P + (uint64_t)t2, W, N, u);
 }
 
 }  // namespace pfb

@@ -80,7 +80,7 @@ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
   size_t off_state0, off_state1, off_lw, off_anc, off_offs, off_mp, off_part, off_agg, off_inc,
-      off_flag, off_excl, off_wq, off_wsum, off_chunks, off_fmax, off_mlp, off_satdbg, off_obsrows, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
+      off_flag, off_excl, off_wq, off_seg_rho, off_seg_E, off_tile_S, off_tile_m, off_chunks, off_fmax, off_mlp, off_satdbg, off_obsrows, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
       total;
   size_t obs_slot_bytes;
   size_t max_chunks;
@@ -160,7 +160,10 @@ Layout make_layout(const pf_engine_config_t* cfg, const pf_filter_params_t* fp) 
   L.off_flag = take((size_t)T * 4);
   L.off_excl = take((size_t)T * 8);
   L.off_wq = take((size_t)P * 8);
-  L.off_wsum = take((size_t)T * kSubTiles * 8);
+  L.off_seg_rho = take((size_t)T * kSubTiles * 8);
+  L.off_seg_E = take((size_t)T * kSubTiles * 8);
+  L.off_tile_S = take((size_t)T * 8);
+  L.off_tile_m = take((size_t)T * 4);
   // a run longer than kLightRun slots needs ceil(len / kRunChunk) chunks:
   // at most P / (kLightRun + 1) runs and P / kRunChunk + T extra chunks
   L.max_chunks = (size_t)(P / kLightRun) + (size_t)T + 64;
@@ -504,8 +507,11 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
   e.lb_inc = (unsigned long long*)(w + L.off_inc);
   e.lb_flag = (unsigned*)(w + L.off_flag);
   e.tile_excl = (unsigned long long*)(w + L.off_excl);
-  e.wq = (unsigned long long*)(w + L.off_wq);
-  e.wsum = (unsigned long long*)(w + L.off_wsum);
+  e.seg_c = (double*)(w + L.off_wq);
+  e.seg_rho = (double*)(w + L.off_seg_rho);
+  e.seg_E = (double*)(w + L.off_seg_E);
+  e.tile_S = (double*)(w + L.off_tile_S);
+  e.tile_m = (float*)(w + L.off_tile_m);
   e.chunks = (uint4*)(w + L.off_chunks);
   e.max_chunks = (unsigned)L.max_chunks;
   e.fmax = (unsigned*)(w + L.off_fmax);

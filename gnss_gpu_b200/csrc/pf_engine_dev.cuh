@@ -64,6 +64,7 @@ struct FilterCtrl {
   float shift[8];         // pending re-centring, applied by the next predict
   float max_lw;
   uint32_t sys_u;
+  uint32_t sys_u_cur;     // systematic offset of the running step (written before its first grid barrier)
   unsigned epoch;
   unsigned ticket;
   unsigned est_ticket;
@@ -89,8 +90,18 @@ struct EngineDev {
   unsigned long long* lb_inc;
   unsigned* lb_flag;
   unsigned long long* tile_excl;
-  unsigned long long* wq;    // epoch kernel: quantised weight per particle
-  unsigned long long* wsum;  // epoch kernel: quantised weight sum per warp segment
+  // tiled integer CDF of the systematic resampler (written in the step's
+  // first phase; every value an integer below 2^53, held exactly as a
+  // double): per particle the inclusive prefix c_i of its quantised weight
+  // inside its 128-particle warp segment; per segment the scale rho_s =
+  // e^(wm_s - tm_t) to the tile maximum and the exclusive prefix E_s of the
+  // rescaled segment sums inside the tile; per tile their sum S_t and the
+  // tile maximum tm_t
+  double* seg_c;
+  double* seg_rho;
+  double* seg_E;
+  double* tile_S;
+  float* tile_m;
   uint4* chunks;             // epoch kernel: queued offspring-run chunks (first slot lo/hi, length, ancestor)
   unsigned max_chunks;
   unsigned* fmax;            // epoch kernel: per filter, order-preserving code of the max log-weight

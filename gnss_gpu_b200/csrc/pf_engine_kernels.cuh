@@ -3,15 +3,17 @@
 // One epoch of every filter is a short chain of persistent kernels, each a
 // loop over (filter, tile) work items taken from an atomic queue:
 //
-//   k_step   fused predict + likelihood + tile statistics; the last tile of a
-//            filter merges the tile statistics into max log-weight, ESS,
-//            weighted mean and covariance and decides on the device whether
-//            the filter resamples (reference: predict.cu:23-38,
-//            weight.cu:13-57,61-108,163-220, particle_filter.py:153-161).
-//   k_scan   quantised weights, tile sums and a decoupled look-back scan of
-//            the tile sums (systematic only).
-//   k_offs   in-tile scan, offspring end F(i) of every particle and the
-//            merge-path partition points.
+//   k_step   fused predict + likelihood + tile statistics (+ the segment
+//            and tile levels of the systematic resampler's tiled integer
+//            CDF); the last tile of a filter merges the tile statistics into
+//            max log-weight, ESS, weighted mean and covariance and decides
+//            on the device whether the filter resamples (reference:
+//            predict.cu:23-38, weight.cu:13-57,61-108,163-220,
+//            particle_filter.py:153-161).
+//   k_scan   tile sums scaled to the filter maximum and a decoupled
+//            look-back scan of them (systematic only).
+//   k_offs   filter-wide CDF of every particle, its offspring end F(i) and
+//            the merge-path partition points.
 //   k_merge  merge-path offspring assignment: ancestor index of every slot.
 //   k_mego   Megopolis chain per slot, ancestor in registers.
 //
@@ -395,6 +397,90 @@ __device__ __forceinline__ void load_particles(const EngineDev& e, const float* 
 }
 
 
+// The systematic offset u (a 32-bit slot fraction) of the step `epoch`:
+// the reference's fixed (seed % 1e6)/(1e6 N) (resampling.cu:152) or one
+// Philox draw per filter and step.
+__device__ __forceinline__ uint32_t sys_offset_u(const EngineDev& e, const FilterDesc* fd, unsigned epoch) {
+  if (e.sys_offset == PF_SYS_OFFSET_RANDOM)
+    return philox10(U4{0u, epoch, TAG_SYS_U, (uint32_t)fd->filter_id}, fd->key0, fd->key1).x;
+  return fd->sys_ref_u;
+}
+
+// Tiled integer CDF of the systematic resampler.  Every quantity below is
+// an integer smaller than 2^53 (K <= 40: q < 2^41, a segment sum < 2^48, a
+// tile sum < 2^51), so it is held exactly as a double and sums are exact.
+//
+// Segment level (one warp, 128 particles, four per lane): q = floor(2^K
+// e^(lw - wm)) against the warp maximum wm (quantize_f32), stored as
+// inclusive prefixes inside the segment; returns the segment sum in every
+// lane.  lwv is -inf past the filter's end.
+__device__ __forceinline__ double warp_incl_scan_f64(double v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  return v;
+}
+__device__ __forceinline__ double sys_segment_prefix(const EngineDev& e, long long base, int p0, bool active,
+                                                     const float (&lwv)[4], float wm, int K) {
+  double q[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) q[k] = (double)quantize_f32(det_fsub(lwv[k], wm), K);
+  const double ts = (q[0] + q[1]) + (q[2] + q[3]);
+  const double incl = warp_incl_scan_f64(ts);
+  const double c0 = (incl - ts) + q[0], c1 = c0 + q[1], c2 = c1 + q[2];
+  if (active) {  // the filter's slots are padded to a multiple of 4
+    double2* dst = reinterpret_cast<double2*>(e.seg_c + base + p0);
+    dst[0] = make_double2(c0, c1);
+    dst[1] = make_double2(c2, incl);
+  }
+  return __shfl_sync(0xffffffffu, incl, 31);
+}
+
+// Tile level (one warp; lane w < kThreads/32 holds segment w's sum S and
+// maximum mw, tm is the tile maximum): rho_w = e^(mw - tm) (det_expf), the
+// rescaled sums floor(S rho_w), their exclusive prefix E_w inside the tile,
+// the tile sum S_t and the tile maximum.
+__device__ __forceinline__ void sys_tile_scale(const EngineDev& e, int t, double S, float mw, float tm) {
+  constexpr int kWarps = kThreads / 32;
+  const int lane = threadIdx.x & 31;
+  const double rho = S > 0.0 ? (double)det_expf(det_fsub(mw, tm)) : 0.0;
+  const double Q = S > 0.0 ? scale_trunc(S, rho) : 0.0;
+  double inc = Q;
+#pragma unroll
+  for (int o = 1; o < kWarps; o <<= 1) {
+    const double v = __shfl_up_sync(0xffffffffu, inc, o, kWarps);
+    if ((lane & (kWarps - 1)) >= o) inc += v;
+  }
+  if (lane < kWarps) {
+    e.seg_rho[(size_t)t * kSubTiles + lane] = rho;
+    e.seg_E[(size_t)t * kSubTiles + lane] = inc - Q;
+  }
+  if (lane == kWarps - 1) {
+    e.tile_S[t] = inc;
+    e.tile_m[t] = tm;
+  }
+}
+
+// The filter-level scale of tile t: Q_t = floor(S_t e^(tm_t - M)) (r_t on
+// return) from its sum and maximum.
+__device__ __forceinline__ double sys_tile_total(double S, float tm, float M, double& r) {
+  r = S > 0.0 ? (double)det_expf(det_fsub(tm, M)) : 0.0;
+  return S > 0.0 ? scale_trunc(S, r) : 0.0;
+}
+__device__ __forceinline__ double sys_tile_total(const EngineDev& e, int t, float M, double& r) {
+  return sys_tile_total(__ldcg(e.tile_S + t), __ldcg(e.tile_m + t), M, r);
+}
+
+// Particle i of tile t, warp segment s: its filter-wide inclusive prefix is
+// C = P_t + floor((E_s + floor(c_i rho_s)) r_t); this returns the second
+// term (an integer-valued double).
+__device__ __forceinline__ double sys_inner(double E, double rho, double r, double c) {
+  return scale_trunc(E + scale_trunc(c, rho), r);
+}
+
 // The last tile of a filter: merged statistics -> estimate, covariance,
 // ESS, the device-side resample decision (particle_filter.py:159-161), the
 // next re-centring shift, the systematic offset, and the epoch/parity step.
@@ -453,12 +539,7 @@ __device__ __forceinline__ void finalize_filter(const EngineDev& e, const Filter
   fc->lw_zero = rs ? 1 : (do_weight ? 0 : (lw_zero ? 1 : 0));
   if (rs) {
     fc->rs_seq = fc->rs_seq + 1u;
-    uint32_t u = fd->sys_ref_u;
-    if (e.sys_offset == PF_SYS_OFFSET_RANDOM) {
-      const U4 r = philox10(U4{0u, epoch, TAG_SYS_U, (uint32_t)fd->filter_id}, fd->key0, fd->key1);
-      u = r.x;
-    }
-    fc->sys_u = u;
+    fc->sys_u = sys_offset_u(e, fd, epoch);
   }
   fc->parity = parity ^ 1;
   fc->epoch = epoch + 1u;
@@ -492,6 +573,7 @@ __global__ void __launch_bounds__(kThreads, PF_KSTEP_MINB) k_step(EngineDev e, i
   __shared__ int s_grp[PF_MAX_CLK + 1];
   __shared__ unsigned char s_clk[PF_MAX_SATS];
   __shared__ float s_wrow[kWarps][17];       // per-warp max + NV sums
+  __shared__ double s_wq[kWarps];            // per-warp quantised weight sums
   __shared__ float s_maxtmp[kWarps];
   __shared__ double s_dred[kWarps * 16];
   __shared__ int s_next, s_last;
@@ -525,6 +607,8 @@ __global__ void __launch_bounds__(kThreads, PF_KSTEP_MINB) k_step(EngineDev e, i
     if (n_sat < 0) n_sat = 0;
     const bool do_predict = (eflags & PF_EP_PREDICT) != 0;
     const bool do_weight = (eflags & PF_EP_WEIGHT) != 0;
+    const bool sys_q = e.resampler == PF_RESAMPLE_SYSTEMATIC &&
+                       (do_weight || (eflags & PF_EP_RESAMPLE_CHECK)) && !(eflags & PF_EP_NO_RESAMPLE);
 
     // ---- per-filter satellite geometry in FP64, stored as FP32 pairs in
     //      smem, grouped by clock state (stable order).
@@ -698,6 +782,10 @@ __global__ void __launch_bounds__(kThreads, PF_KSTEP_MINB) k_step(EngineDev e, i
       const int idx = warp_transpose_sum16(v);  // lane holds the warp total of value idx
       if ((lane & 1) == 0 && idx < NV) s_wrow[warp][1 + idx] = v[0];
       if (lane == 0) s_wrow[warp][0] = wm;
+      // tiled integer CDF of the systematic resampler, segment level
+      double seg_sum = 0.0;
+      if (sys_q) seg_sum = sys_segment_prefix(e, base, p0, active, lwv, wm, fd->K);
+      if (lane == 0) s_wq[warp] = seg_sum;
     }
     __syncthreads();
     if (warp == 0) {
@@ -719,6 +807,8 @@ __global__ void __launch_bounds__(kThreads, PF_KSTEP_MINB) k_step(EngineDev e, i
       float* row = e.part + (size_t)t * kPartStride;
       if (lane < NV) row[1 + lane] = acc;
       if (lane == 0) row[0] = tm;
+      if (sys_q)
+        sys_tile_scale(e, t, lane < kWarps ? s_wq[lane] : 0.0, lane < kWarps ? s_wrow[lane][0] : -INFINITY, tm);
       __syncwarp();
       if (lane == 0) {
         __threadfence();
@@ -763,7 +853,9 @@ __device__ __forceinline__ void load_q4(const EngineDev& e, long long base, int 
 }
 
 // -------------------------------------------------------------------------
-// k_scan: quantised weights, tile sums, decoupled look-back over tiles.
+// k_scan: tile sums of the integer CDF, decoupled look-back over tiles.  The
+// stateless API's FP64 log-weights (lw64) use the plain integer CDF against
+// the global maximum instead: quantised weights summed per tile here.
 __global__ void __launch_bounds__(kThreads) k_scan(EngineDev e, int t0, int count) {
   __shared__ unsigned long long s_u64[kThreads / 32];
   __shared__ int s_slot, s_first;
@@ -784,11 +876,15 @@ __global__ void __launch_bounds__(kThreads) k_scan(EngineDev e, int t0, int coun
     const int tb = fd->tile_begin, j = t - tb;
     const int p0 = j * kTile + (int)threadIdx.x * 4;
     const long long base = fd->p_off;
-    unsigned long long qv[4];
-    load_q4(e, base, p0, n, M, K, qv);
-    const unsigned long long qs = qv[0] + qv[1] + qv[2] + qv[3];
     unsigned long long tot;
-    block_excl_scan_u64(qs, s_u64, &tot);
+    if (e.lw64) {  // stateless API: the plain integer CDF of the FP64 log-weights
+      unsigned long long qv[4];
+      load_q4(e, base, p0, n, M, K, qv);
+      block_excl_scan_u64(qv[0] + qv[1] + qv[2] + qv[3], s_u64, &tot);
+    } else {  // engine: the tile's sum of the tiled integer CDF, scaled to the filter maximum
+      double r;
+      tot = (unsigned long long)sys_tile_total(e, t, M, r);
+    }
     unsigned long long excl = 0;
     if (j == 0) {
       if (threadIdx.x == 0) {
@@ -886,30 +982,52 @@ __global__ void __launch_bounds__(kThreads) k_offs(EngineDev e, int t0, int coun
     const int tb = fd->tile_begin, j = t - tb;
     const int p0 = j * kTile + (int)threadIdx.x * 4;
     const long long base = fd->p_off;
-    unsigned long long qv[4];
-    load_q4(e, base, p0, n, M, K, qv);
-    unsigned long long tot;
-    const unsigned long long texcl = block_excl_scan_u64(qv[0] + qv[1] + qv[2] + qv[3], s_u64, &tot);
+    // inclusive CDF before this thread's particles (Cp) and after each (Ck)
+    unsigned long long Cp = 0ull, Ck[4] = {0ull, 0ull, 0ull, 0ull};
+    const int lane = threadIdx.x & 31;
+    if (e.lw64) {  // stateless API: plain integer CDF
+      unsigned long long qv[4];
+      load_q4(e, base, p0, n, M, K, qv);
+      unsigned long long tot;
+      Cp = __ldcg(e.tile_excl + t) + block_excl_scan_u64(qv[0] + qv[1] + qv[2] + qv[3], s_u64, &tot);
+      unsigned long long C = Cp;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) Ck[k] = (C += qv[k]);
+    } else {  // engine: tiled integer CDF (segment prefixes written by k_step)
+      const int w = threadIdx.x >> 5;
+      double r;
+      (void)sys_tile_total(e, t, M, r);
+      const double rho = __ldcg(e.seg_rho + (size_t)t * kSubTiles + w);
+      const double E = __ldcg(e.seg_E + (size_t)t * kSubTiles + w);
+      const unsigned long long P = __ldcg(e.tile_excl + t);
+      double c[4] = {0.0, 0.0, 0.0, 0.0};
+      if (p0 < n) {
+        const double2* src = reinterpret_cast<const double2*>(e.seg_c + base + p0);
+        const double2 a = __ldcg(src), b = __ldcg(src + 1);
+        c[0] = a.x; c[1] = a.y; c[2] = b.x; c[3] = b.y;
+      }
+      double cprev = __shfl_up_sync(0xffffffffu, c[3], 1);
+      if (lane == 0) cprev = 0.0;
+      Cp = P + (unsigned long long)sys_inner(E, rho, r, cprev);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) Ck[k] = P + (unsigned long long)sys_inner(E, rho, r, c[k]);
+    }
     if (W == 0ull) {  // uniform over the CTA (one filter per tile)
       if (threadIdx.x == 0) atomicOr(e.err, ERR_BAD_WEIGHTS);
       continue;
     }
     uint32_t Fprev = 0u, Fk[4] = {0u, 0u, 0u, 0u};
     if (p0 < n) {
-      unsigned long long C = __ldcg(e.tile_excl + t) + texcl;
       const double scale = (double)n / (double)W, uf = (double)u * 2.3283064365386963e-10;
-      Fprev = (p0 == 0) ? 0u : offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf);
+      Fprev = (p0 == 0) ? 0u : offspring_end_scaled(Cp, W, (uint32_t)n, u, scale, uf);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        C += qv[k];
-        Fk[k] = (p0 + k < n) ? offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf) : (uint32_t)n;
-      }
+      for (int k = 0; k < 4; ++k)
+        Fk[k] = (p0 + k < n) ? offspring_end_scaled(Ck[k], W, (uint32_t)n, u, scale, uf) : (uint32_t)n;
       *reinterpret_cast<uint4*>(e.offs + base + p0) = make_uint4(Fk[0], Fk[1], Fk[2], Fk[3]);
     }
     // merge-path tile starts: tile c begins in particle i when
     // i - 1 + F(i-1) < c * kMergeDiag <= i + F(i); each lane's run of starts
     // is written by the whole warp (heavy particles start many tiles)
-    const int lane = threadIdx.x & 31;
 #pragma unroll 1
     for (int k = 0; k < 4; ++k) {
       long long c_lo = 0, c_hi = 0;

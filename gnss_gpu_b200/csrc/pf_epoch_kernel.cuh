@@ -7,7 +7,10 @@
 //   1  predict + likelihood + tile statistics (particles loaded straight
 //      into registers, gathered through the last resample's ancestors;
 //      measured faster than staging them through shared memory with
-//      cp.async).
+//      cp.async).  Systematic: also the segment and tile levels of the
+//      tiled integer CDF -- each warp quantises its 128 particles against
+//      its own maximum and stores their prefixes inside the segment, warp 0
+//      rescales the segment sums exactly to the tile maximum.
 //   -- barrier
 //   2  per-filter merge of the tile rows (filter f_first + j by CTA j mod G;
 //      one pass, the filter maximum having been collected in phase 1): ESS,
@@ -15,22 +18,20 @@
 //      At the same time, systematic only, on the CTAs that own no filter
 //      (when filters are fewer than a quarter of the CTAs; otherwise every
 //      CTA after its merges):
-//   3  quantised weights, one sum per 128-particle warp segment and
-//      (integer atomics) one per tile, for every filter that may resample.
-//   -- barrier (what follows only if some filter resamples)
-//   3' Megopolis: the chain per slot.   Systematic:
-//   4  exclusive prefix of every particle (filter prefix of the tile from
-//      the tile sums, segment prefix from the warp sums, warp scan),
-//      offspring ends F(i); slots [F(i-1), F(i)) get ancestor i, written
-//      here when the run is short, queued in chunks of 1024 slots when long.
+//   4  tile sums rescaled to the filter maximum, the filter prefix of each
+//      tile, then per particle its filter-wide CDF and offspring end F(i);
+//      slots [F(i-1), F(i)) get ancestor i, written here when the run is
+//      short, queued in chunks of kRunChunk slots when long (speculative for
+//      every filter that may resample: the decision is taken meanwhile).
 //   -- barrier
 //   5  the queued chunks, taken by all warps of the grid in turn.
+//   Megopolis instead: -- barrier, then the chain per slot for the filters
+//   that resample.
 //
 // Compared with one kernel per phase this removes the launch/drain gaps and
-// every per-tile queue atomic; the log-weights and quantised weights reread
-// in phases 3 and 4 come from L2 (the epoch just wrote them).  Phases 3-5
-// need no CTA barrier per tile: warps work on independent segments and
-// blocks.
+// every per-tile queue atomic; the prefixes reread in phase 4 come from L2
+// (the epoch just wrote them).  Phase 4 needs no CTA barrier per tile: warps
+// work on independent segments.
 #pragma once
 #include "pf_engine_kernels.cuh"
 #include "pf_learned.cuh"
@@ -141,16 +142,10 @@ __device__ __forceinline__ void block_sum2_u64(unsigned long long a, unsigned lo
   }
 }
 
-// Quantised weights of particles [p0, p0 + 4) (zero past the filter end).
-__device__ __forceinline__ void quantize4(float4 v, int p0, int n, float M, int K, unsigned long long (&q)[4]) {
-  const float l[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-  for (int k = 0; k < 4; ++k) q[k] = (p0 + k < n) ? quantize_shifted((double)l[k] - (double)M, K) : 0ull;
-}
 
 // The systematic resampler's phases walk a chunk of tiles filter segment by
 // filter segment (the tiles of one filter inside the chunk).  Every warp
-// works on its own 128-particle segment (phases 3, 4) or on queued chunks of
+// works on its own 128-particle segment (phase 4) or on queued chunks of
 // long offspring runs (phase 5) without CTA barriers; only the per-filter
 // prefix of phase 4 is a CTA reduction.  The loops are kept compact (not
 // unrolled over tiles): this code runs a few times per CTA and epoch, so
@@ -158,71 +153,49 @@ __device__ __forceinline__ void quantize4(float4 v, int p0, int n, float M, int 
 // exact, so the result does not depend on the order of the atomics or on
 // the chunking.
 
-// Phase 3, run while the filters' owners merge statistics and decide: the
-// quantised weights, one sum per warp segment and (integer atomics) one per
-// tile, for every filter that may resample this epoch (weights updated,
-// resampling not suppressed: its max-code word is set).  Whether it does
-// resample is known only after the next barrier; when it does not, this
-// work is unused.
-__device__ __forceinline__ void epoch_sys_quantise(const EngineDev& e, int cb, int ce) {
+// Phase 4, right after the first barrier and speculative (the filters'
+// owners decide at the same time whether they resample; when one does not,
+// this work is unused): for every filter whose weights may resample (its
+// max-code word is set), the filter prefix of each tile of the chunk from
+// the tile sums scaled to the filter maximum, then per particle its
+// filter-wide CDF C_i and offspring end F(i); slots [F(i-1), F(i)) get
+// ancestor i, written here when the run is short, queued in chunks of
+// kRunChunk slots when long.
+__device__ __forceinline__ void epoch_sys_offspring(const EngineDev& e, unsigned* bar, int cb, int ce,
+                                                    unsigned long long* s_u64) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int t = cb; t < ce;) {
-    const int f = __ldg(e.tile_filter + t);
-    const FilterDesc* fd = e.desc + f;
-    const int tb = fd->tile_begin, se = min(ce, tb + fd->n_tiles);
-    const unsigned mcode = __ldcg(e.fmax + f);
-    if (mcode != 0u) {
-      const int n = fd->n, K = fd->K;
-      const long long base = fd->p_off;
-      const float M = ord_decode(mcode);
-      int p0 = (t - tb) * kTile + warp * kWarpTile + lane * 4;
-      float4 v = (p0 < n) ? __ldcg(reinterpret_cast<const float4*>(e.lw + base + p0)) : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll 1
-      for (int g = t; g < se; ++g, p0 += kTile) {
-        const int pn = p0 + kTile;  // prefetch the next tile's log-weights
-        const float4 vn = (g + 1 < se && pn < n) ? __ldcg(reinterpret_cast<const float4*>(e.lw + base + pn))
-                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
-        if (p0 - lane * 4 < n) {  // warp-uniform: the segment holds particles
-          unsigned long long q[4];
-          quantize4(v, p0, n, M, K, q);
-          if (p0 < n) {  // the filter's slots are padded to a multiple of 4
-            ulonglong2* dst = reinterpret_cast<ulonglong2*>(e.wq + base + p0);
-            dst[0] = make_ulonglong2(q[0], q[1]);
-            dst[1] = make_ulonglong2(q[2], q[3]);
-          }
-          const unsigned long long sw = warp_sum_u64(q[0] + q[1] + q[2] + q[3]);
-          if (lane == 0) {
-            e.wsum[(size_t)g * kSubTiles + warp] = sw;
-            atomicAdd(e.lb_agg + g, sw);  // tile sum (zeroed in phase 1)
-          }
-        }
-        v = vn;
-      }
-    }
-    t = se;
-  }
-}
-
-// Phases 4 and 5 for the filters that resample.
-__device__ __forceinline__ void epoch_sys_assign(const EngineDev& e, unsigned* bar, unsigned& gen, int cb, int ce,
-                                                 unsigned long long* s_u64) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // ---------------------------------------------------------------- phase 4
   for (int t = cb; t < ce;) {
     const int f = __ldg(e.tile_filter + t);
     const FilterDesc* fd = e.desc + f;
     FilterCtrl* fc = e.ctrl + f;
     const int tb = fd->tile_begin, nt = fd->n_tiles, se = min(ce, tb + nt);
-    if (ld_cg_int(&fc->resample_flag)) {  // CTA-uniform
-      // prefix of tile t inside its filter and the filter total, from the tile sums
+    const unsigned mcode = __ldcg(e.fmax + f);
+    if (mcode != 0u) {  // CTA-uniform
+      const float M = ord_decode(mcode);
+      // prefix of tile t inside its filter and the filter total, from the
+      // tile sums scaled to the filter maximum
       unsigned long long P = 0, W = 0;
       {
+        // four tiles per thread and round, their loads issued together
+        constexpr int kB = 4;
         unsigned long long pre = 0, all = 0;
-#pragma unroll 4
-        for (int i = threadIdx.x; i < nt; i += kThreads) {
-          const unsigned long long v = __ldcg(e.lb_agg + tb + i);
-          all += v;
-          if (tb + i < t) pre += v;
+#pragma unroll 1
+        for (int i0 = threadIdx.x; i0 < nt; i0 += kB * kThreads) {
+          double S[kB];
+          float m[kB];
+#pragma unroll
+          for (int j = 0; j < kB; ++j) {
+            const int i = i0 + j * kThreads;
+            S[j] = i < nt ? __ldcg(e.tile_S + tb + i) : 0.0;
+            m[j] = i < nt ? __ldcg(e.tile_m + tb + i) : 0.0f;
+          }
+#pragma unroll
+          for (int j = 0; j < kB; ++j) {
+            double r;
+            const unsigned long long v = (unsigned long long)sys_tile_total(S[j], m[j], M, r);
+            all += v;
+            if (tb + i0 + j * kThreads < t) pre += v;
+          }
         }
         block_sum2_u64(pre, all, s_u64, P, W);
       }
@@ -233,33 +206,37 @@ __device__ __forceinline__ void epoch_sys_assign(const EngineDev& e, unsigned* b
       if (W > 0ull) {
         const int n = fd->n;
         const long long base = fd->p_off;
-        const uint32_t u = ld_cg_u(&fc->sys_u);
+        const uint32_t u = ld_cg_u(&fc->sys_u_cur);
         const double scale = (double)n / (double)W, uf = (double)u * 2.3283064365386963e-10;
 #pragma unroll 1
         for (int g = t; g < se; ++g) {
           const int pw = (g - tb) * kTile + warp * kWarpTile;
           const int p0 = pw + lane * 4;
-          const unsigned long long ts = __ldcg(e.lb_agg + g);
+          double r;
+          const unsigned long long ts = (unsigned long long)sys_tile_total(e, g, M, r);
           if (pw < n) {  // warp-uniform
-            const unsigned long long ws = (lane < warp) ? __ldcg(e.wsum + (size_t)g * kSubTiles + lane) : 0ull;
-            ulonglong2 qa = make_ulonglong2(0ull, 0ull), qb = qa;
+            const double rho = __ldcg(e.seg_rho + (size_t)g * kSubTiles + warp);
+            const double E = __ldcg(e.seg_E + (size_t)g * kSubTiles + warp);
+            double2 ca = make_double2(0.0, 0.0), cb2 = ca;
             if (p0 < n) {
-              const ulonglong2* src = reinterpret_cast<const ulonglong2*>(e.wq + base + p0);
-              qa = __ldcg(src);
-              qb = __ldcg(src + 1);
+              const double2* src = reinterpret_cast<const double2*>(e.seg_c + base + p0);
+              ca = __ldcg(src);
+              cb2 = __ldcg(src + 1);
             }
-            const unsigned long long seg_pre = warp_sum_u64(ws);  // earlier segments of the tile
-            const unsigned long long q[4] = {qa.x, qa.y, qb.x, qb.y};
-            const unsigned long long mine = q[0] + q[1] + q[2] + q[3];
-            unsigned long long C = P + seg_pre + warp_incl_scan_u64(mine) - mine;
+            // segment prefixes of this lane's particles and of the one before
+            const double c[4] = {ca.x, ca.y, cb2.x, cb2.y};
+            double cprev = __shfl_up_sync(0xffffffffu, c[3], 1);
+            if (lane == 0) cprev = 0.0;
+            const double Pd = (double)P;
             uint32_t Fprev = 0u, Fk[4] = {0u, 0u, 0u, 0u};
             if (p0 < n) {
-              Fprev = (p0 == 0) ? 0u : offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf);
+              Fprev = (p0 == 0) ? 0u
+                                : offspring_end_split(P, Pd, sys_inner(E, rho, r, cprev), W, (uint32_t)n, u, scale, uf);
 #pragma unroll
-              for (int k = 0; k < 4; ++k) {
-                C += q[k];
-                Fk[k] = (p0 + k < n) ? offspring_end_scaled(C, W, (uint32_t)n, u, scale, uf) : (uint32_t)n;
-              }
+              for (int k = 0; k < 4; ++k)
+                Fk[k] = (p0 + k < n)
+                            ? offspring_end_split(P, Pd, sys_inner(E, rho, r, c[k]), W, (uint32_t)n, u, scale, uf)
+                            : (uint32_t)n;
             }
             // Slots [F(i-1), F(i)) take ancestor i.  Runs of up to kLightRun
             // slots are written here by their lane; longer runs (heavy
@@ -318,11 +295,13 @@ __device__ __forceinline__ void epoch_sys_assign(const EngineDev& e, unsigned* b
     }
     t = se;
   }
-  grid_barrier(e, bar, gen);
+}
 
-  // ---------------------------------------------------------------- phase 5
-  // Heavy runs: chunk descriptors (first slot, length, ancestor), taken by
-  // the warps of the grid in turn, each written with coalesced stores.
+// Phase 5, after the next barrier: the heavy runs' chunk descriptors (first
+// slot, length, ancestor), taken by the warps of the grid in turn, each
+// written with coalesced stores.
+__device__ __forceinline__ void epoch_sys_chunks(const EngineDev& e, const unsigned* bar) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned nchunks = min(ld_cg_u(bar + kBarChunks), e.max_chunks);
   const int gw = (int)(blockIdx.x * (kThreads / 32)) + warp, nw = (int)(gridDim.x * (kThreads / 32));
 #pragma unroll 1
@@ -349,6 +328,7 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
   __shared__ float s_maxtmp[kWarps];
   __shared__ double s_dred[kWarps * 16];
   __shared__ unsigned long long s_u64[2 * kWarps];
+  __shared__ double s_wq[2][kWarps];  // per-warp sums of the tiled integer CDF
   __shared__ int s_any;
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -361,7 +341,6 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
   }
   int cb, ce;
   cta_chunk(t0, count, cb, ce);
-  for (int t = cb + (int)threadIdx.x; t < ce; t += kThreads) e.lb_agg[t] = 0ull;  // tile sums of phase 3
 
   // ---------------------------------------------------------------- phase 1
   int cached = -1;
@@ -385,6 +364,10 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
     if (n_sat < 0) n_sat = 0;
     const bool do_predict = (eflags & PF_EP_PREDICT) != 0;
     const bool do_weight = (eflags & PF_EP_WEIGHT) != 0;
+    // the filter may resample this epoch: systematic builds its tiled integer CDF
+    const bool may_rs = (do_weight || (eflags & PF_EP_RESAMPLE_CHECK)) && !(eflags & PF_EP_NO_RESAMPLE);
+    const bool sys_q = RESAMPLER == PF_RESAMPLE_SYSTEMATIC && may_rs;
+    if (sys_q && t == fd->tile_begin && threadIdx.x == 0) fc->sys_u_cur = sys_offset_u(e, fd, epoch);
 
     if constexpr (WMODE == PF_WEIGHT_MIXTURE) {
       if (f != cached) {
@@ -597,8 +580,13 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
         if (b) named_sync<4>();
         else named_sync<3>();
       }
+      // tiled integer CDF of the systematic resampler, segment level
+      const double seg_sum = sys_q ? sys_segment_prefix(e, base, p0, active, lwv, wm, fd->K) : 0.0;
       if ((lane & 1) == 0 && idx < NV) wr[warp][1 + idx] = v[0];
-      if (lane == 0) wr[warp][0] = wm;
+      if (lane == 0) {
+        wr[warp][0] = wm;
+        s_wq[b][warp] = seg_sum;
+      }
       if (warp != 0) {
         if (b) named_arrive<2>();
         else named_arrive<1>();
@@ -625,11 +613,12 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
         if (lane < NV) row[1 + lane] = acc;
         if (lane == 0) {
           row[0] = tm;
-          // filter maximum for the one-pass merge and the quantiser, kept
+          // filter maximum for the one-pass merge and the integer CDF, kept
           // only when the filter may resample this epoch
-          if (tm > -INFINITY && (do_weight || (eflags & PF_EP_RESAMPLE_CHECK)) && !(eflags & PF_EP_NO_RESAMPLE))
-            atomicMax(e.fmax + f, ord_code(tm));
+          if (tm > -INFINITY && may_rs) atomicMax(e.fmax + f, ord_code(tm));
         }
+        // tile level of the tiled integer CDF
+        if (sys_q) sys_tile_scale(e, t, lane < kWarps ? s_wq[b][lane] : 0.0, lane < kWarps ? wr[lane][0] : -INFINITY, tm);
         if (it + 2 < ce - cb) {  // buffer b is free again
           if (b) named_arrive<4>();
           else named_arrive<3>();
@@ -641,7 +630,7 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
 
   // ---------------------------------------------------------------- phase 2
   // Filter f_first + j is merged and decided by CTA j mod G.  With fewer
-  // filters than CTAs the other CTAs start phase 3 meanwhile.
+  // filters than CTAs the other CTAs start phase 4 (systematic) meanwhile.
   const int f_first = __ldg(e.tile_filter + t0), nf = __ldg(e.tile_filter + t0 + count - 1) - f_first + 1;
   for (int j = blockIdx.x; j < nf; j += gridDim.x) {
     const int f = f_first + j;
@@ -661,23 +650,28 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
     __syncthreads();
   }
   if constexpr (RESAMPLER == PF_RESAMPLE_SYSTEMATIC) {
-    // With few filters their owners sit phase 3 out (it overlaps their
-    // merges); with many, every CTA takes a share after its merges.
-    const int h0 = 4 * nf <= (int)gridDim.x ? nf : 0;  // first CTA of phase 3
+    // Phase 4 needs only the first barrier: the tiled integer CDF is
+    // complete once every tile is (speculative, as the owners decide at the
+    // same time).  With few filters their owners sit it out (it overlaps
+    // their merges); with many, every CTA takes a share after its merges.
+    const int h0 = 4 * nf <= (int)gridDim.x ? nf : 0;  // first CTA of phase 4
     if ((int)blockIdx.x >= h0) {
-      int b3, e3;
-      chunk_of(t0, count, (int)blockIdx.x - h0, (int)gridDim.x - h0, b3, e3);
-      epoch_sys_quantise(e, b3, e3);
+      int b4, e4;
+      chunk_of(t0, count, (int)blockIdx.x - h0, (int)gridDim.x - h0, b4, e4);
+      epoch_sys_offspring(e, bar, b4, e4, s_u64);
     }
-  }
-  grid_barrier(e, bar, gen);
-  for (int j = blockIdx.x; j < nf; j += gridDim.x)  // every reader of the max codes is past the barrier
-    if (threadIdx.x == 0) e.fmax[f_first + j] = 0u;
-  if (threadIdx.x == 0) s_any = (int)ld_cg_u(&bar[2]);
-  __syncthreads();
-  if (!s_any) return;  // uniform: no filter resamples this epoch
-
-  if constexpr (RESAMPLER == PF_RESAMPLE_MEGOPOLIS) {
+    grid_barrier(e, bar, gen);
+    for (int j = blockIdx.x; j < nf; j += gridDim.x)  // every reader of the max codes is past the barrier
+      if (threadIdx.x == 0) e.fmax[f_first + j] = 0u;
+    // ---------------------------------------------------------------- phase 5
+    epoch_sys_chunks(e, bar);
+  } else {
+    grid_barrier(e, bar, gen);
+    for (int j = blockIdx.x; j < nf; j += gridDim.x)  // every reader of the max codes is past the barrier
+      if (threadIdx.x == 0) e.fmax[f_first + j] = 0u;
+    if (threadIdx.x == 0) s_any = (int)ld_cg_u(&bar[2]);
+    __syncthreads();
+    if (!s_any) return;  // uniform: no filter resamples this epoch
     for (int t = cb; t < ce; ++t) {
       const int f = __ldg(e.tile_filter + t);
       const FilterDesc* fd = e.desc + f;
@@ -685,8 +679,6 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
       if (!ld_cg_int(&fc->resample_flag)) continue;
       mego_tile(e, fd, ld_cg_u(&fc->epoch) - 1u, t);
     }
-  } else {
-    epoch_sys_assign(e, bar, gen, cb, ce, s_u64);
   }
 }
 

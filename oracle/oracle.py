@@ -54,6 +54,12 @@ def lib():
         L.orc_systematic64.restype = i32
         L.orc_systematic.argtypes = [F32, i32, f32, u32, I32, C.POINTER(C.c_uint64)]
         L.orc_systematic.restype = i32
+        L.orc_systematic_tiled.argtypes = [F32, i32, u32, I32, C.POINTER(C.c_uint64), C.POINTER(C.c_float)]
+        L.orc_systematic_tiled.restype = i32
+        L.orc_det_expf.argtypes = [f32]
+        L.orc_det_expf.restype = f32
+        L.orc_quantize_f32.argtypes = [f32, i32]
+        L.orc_quantize_f32.restype = C.c_uint64
         L.orc_megopolis.argtypes = [F32, i32, i32, u32, u32, u32, u32, I32]
         L.orc_init.argtypes = [i32, i32, f32, f32, u32, u32, u32, F64]
         L.orc_predict.argtypes = [i32, i32, F64, P, F64, F64, F32, i32, u32, u32, u32, u32, F64]
@@ -121,6 +127,29 @@ def systematic(lw32, max_lw, u32):
     if r != 0:
         raise ValueError("all weights quantised to zero")
     return anc, int(w.value)
+
+
+def systematic_tiled(lw32, u32):
+    """The engine's systematic resampler: ancestor of every slot, the integer
+    weight total W and the filter maximum, from the tiled integer CDF (each
+    128-particle segment quantised against its own maximum and rescaled
+    exactly to the tile and filter maxima; pf_oracle.c)."""
+    lw32 = _f32(lw32)
+    anc = np.zeros(len(lw32), np.int32)
+    w = C.c_uint64(0)
+    m = C.c_float(0.0)
+    r = lib().orc_systematic_tiled(lw32, len(lw32), int(u32), anc, C.byref(w), C.byref(m))
+    if r == -2:
+        raise MemoryError("oracle allocation")
+    return anc, int(w.value)
+
+
+def det_expf(d: float) -> float:
+    return float(lib().orc_det_expf(float(d)))
+
+
+def quantize_f32(d: float, K: int) -> int:
+    return int(lib().orc_quantize_f32(float(d), int(K)))
 
 
 def megopolis(lw32, iters, seed, epoch, filter_id=0):

@@ -11,7 +11,7 @@
  *   pf_device.cu:19-26     Huber cost         -> orc_weight_* (mode 1)
  *   weight.cu:61-160       ESS                -> orc_stats, orc_pf_ess
  *   weight.cu:163-328      weighted mean      -> orc_stats, orc_pf_estimate
- *   resampling.cu:60-83,152 systematic search -> orc_systematic
+ *   resampling.cu:60-83,152 systematic search -> orc_systematic, orc_systematic_tiled
  *   resampling.cu:175-272  reference Megopolis -> orc_pf_megopolis_ref
  *   Chesser et al. arXiv:2109.13504, canonical Megopolis -> orc_megopolis
  *   particle_filter.py:129-175 update order   -> orc_epoch
@@ -115,12 +115,8 @@ int orc_quant_exponent(int n) {
   return k < 40 ? k : 40;
 }
 
-uint64_t orc_quantize(double d, int K) {
-  const double x = dmul(d, 1.4426950408889634074);
-  if (!(x > -40.0)) return 0;
-  const double n = floor(x);
-  const double f = dsub(x, n);
-  const double t = dmul(f, 0.69314718055994530942);
+/* e^t for t in [0, ln 2): Taylor series of degree 13 in Horner form. */
+static double exp_poly(double t) {
   double q = 1.6059043836821615e-10;
   q = fma(q, t, 2.0876756987868099e-09);
   q = fma(q, t, 2.5052108385441720e-08);
@@ -135,7 +131,61 @@ uint64_t orc_quantize(double d, int K) {
   q = fma(q, t, 0.5);
   q = fma(q, t, 1.0);
   q = fma(q, t, 1.0);
-  return (uint64_t)ldexp(q, K + (int)n);
+  return q;
+}
+
+uint64_t orc_quantize(double d, int K) {
+  const double x = dmul(d, 1.4426950408889634074);
+  if (!(x > -40.0)) return 0;
+  const double n = floor(x);
+  const double f = dsub(x, n);
+  const double t = dmul(f, 0.69314718055994530942);
+  return (uint64_t)ldexp(exp_poly(t), K + (int)n);
+}
+
+/* floor(v * r) for an integer v < 2^53 and 0 <= r <= 1, one rounded product. */
+static uint64_t scale_floor(uint64_t v, double r) { return (uint64_t)dmul((double)v, r); }
+
+/* Deterministic FP32 exponential of the engine's tiled CDF (the device's
+ * exp2_frac_f32 / quantize_f32 / det_expf): x = d log2(e) (one rounded
+ * product), n = floor(x), f = x - n (one rounded difference), 2^f from the
+ * Taylor series of e^(f ln 2) (coefficients (ln 2)^k / k! rounded to FP32,
+ * degree 9, Horner with fma), 2^n applied exactly. */
+static float fmul32(float a, float b) { volatile float r = a * b; return r; }
+static float fsub32(float a, float b) { volatile float r = a - b; return r; }
+static float exp2_frac32(float f) {
+  float q = 0x1.b5253ep-24f;
+  q = fmaf(q, f, 0x1.62c022p-20f);
+  q = fmaf(q, f, 0x1.ffcbfcp-17f);
+  q = fmaf(q, f, 0x1.430912p-13f);
+  q = fmaf(q, f, 0x1.5d87fep-10f);
+  q = fmaf(q, f, 0x1.3b2ab6p-7f);
+  q = fmaf(q, f, 0x1.c6b08ep-5f);
+  q = fmaf(q, f, 0x1.ebfbep-3f);
+  q = fmaf(q, f, 0x1.62e43p-1f);
+  q = fmaf(q, f, 0x1.0p+0f);
+  return q;
+}
+static float pow2f32(int m) {
+  const uint32_t b = (uint32_t)(127 + m) << 23;
+  float r;
+  memcpy(&r, &b, sizeof(r));
+  return r;
+}
+uint64_t orc_quantize_f32(float d, int K) {
+  const float x = fmul32(d, 0x1.715476p+0f);
+  if (!(x > -40.0f)) return 0;
+  const float n = floorf(x);
+  const float p = exp2_frac32(fsub32(x, n));
+  volatile float v = p * pow2f32(K + (int)n);
+  return (uint64_t)v;
+}
+float orc_det_expf(float d) {
+  const float x = fmul32(d, 0x1.715476p+0f);
+  if (!(x > -126.0f)) return 0.0f;
+  const float n = floorf(x);
+  volatile float v = exp2_frac32(fsub32(x, n)) * pow2f32((int)n);
+  return v;
 }
 
 /* FP32 log-weights of the engine: the shift lw - max is exact in FP64. */
@@ -194,6 +244,101 @@ int orc_systematic64(const double* lw, int n, double max_lw, uint32_t u32, int* 
   if (!C) return -2;
   orc_quantize_all64(lw, n, max_lw, C);
   int r = systematic_from_q(C, n, u32, anc, wq_out);
+  free(C);
+  return r;
+}
+
+/* ------------------------------------------- tiled integer CDF (engine)
+ * The engine quantises each 128-particle segment (one warp) against its own
+ * maximum wm_s and rescales exactly, with one rounded product and a floor
+ * per level (tiles of 1024 particles = 8 segments, then the filter):
+ *   q_i   = floor(2^K e^(lw_i - wm_s)),       c_i = prefix of q inside s
+ *   (e^ here the deterministic FP32 exponential orc_quantize_f32 /
+ *   orc_det_expf; products with it one rounded FP64 multiply)
+ *   S_s   = c at the segment's end,            rho_s = e^(wm_s - tm_t)
+ *   Q_s   = floor(S_s rho_s),                  E_s = prefix of Q over s in t
+ *   S_t   = sum of Q_s,                        r_t = e^(tm_t - M)
+ *   Q_t   = floor(S_t r_t),                    P_t = prefix of Q_t
+ *   C_i   = P_t + floor((E_s + floor(c_i rho_s)) r_t),  W = sum of Q_t
+ * (tm_t the tile maximum, M the filter maximum).  C is non-decreasing and ends at W; slot k's ancestor
+ * is the first i with (k 2^32 + u) W <= C_i N 2^32, the predicate of
+ * resampling.cu:69-77 as for the plain integer CDF. */
+int orc_systematic_tiled(const float* lw, int n, uint32_t u32, int* anc, uint64_t* wq_out, float* max_out) {
+  const int K = orc_quant_exponent(n);
+  const int nt = (n + 1023) / 1024;
+  uint64_t* C = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)n);
+  float* tm = (float*)malloc(sizeof(float) * (size_t)nt);
+  uint64_t* St = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)nt);
+  double* rho = (double*)malloc(sizeof(double) * (size_t)nt * 8);
+  uint64_t* E = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)nt * 8);
+  if (!C || !tm || !St || !rho || !E) {
+    free(C); free(tm); free(St); free(rho); free(E);
+    return -2;
+  }
+  float M = -INFINITY;
+#pragma omp parallel for schedule(static) reduction(max : M)
+  for (int t = 0; t < nt; ++t) {
+    float wm[8];
+    uint64_t S[8];
+    float tmax = -INFINITY;
+    for (int s = 0; s < 8; ++s) {
+      const int a = t * 1024 + s * 128, b = a + 128 < n ? a + 128 : n;
+      float m = -INFINITY;
+      for (int i = a; i < b; ++i) m = fmaxf(m, lw[i]);
+      uint64_t run = 0;
+      for (int i = a; i < b; ++i) {
+        run += orc_quantize_f32(fsub32(lw[i], m), K);
+        C[i] = run;
+      }
+      wm[s] = m;
+      S[s] = run;
+      tmax = fmaxf(tmax, m);
+    }
+    uint64_t acc = 0;
+    for (int s = 0; s < 8; ++s) {
+      const double r = S[s] ? (double)orc_det_expf(fsub32(wm[s], tmax)) : 0.0;
+      rho[t * 8 + s] = r;
+      E[t * 8 + s] = acc;
+      acc += S[s] ? scale_floor(S[s], r) : 0;
+    }
+    St[t] = acc;
+    tm[t] = tmax;
+    M = fmaxf(M, tmax);
+  }
+  if (max_out) *max_out = M;
+  uint64_t W = 0;
+  double* rt = (double*)malloc(sizeof(double) * (size_t)nt);
+  uint64_t* P = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)nt);
+  for (int t = 0; t < nt; ++t) {
+    rt[t] = St[t] ? (double)orc_det_expf(fsub32(tm[t], M)) : 0.0;
+    P[t] = W;
+    W += St[t] ? scale_floor(St[t], rt[t]) : 0;
+  }
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    const int t = i / 1024, s = (i % 1024) / 128;
+    const uint64_t inner = E[t * 8 + s] + scale_floor(C[i], rho[t * 8 + s]);
+    C[i] = P[t] + scale_floor(inner, rt[t]);
+  }
+  free(rt); free(P); free(tm); free(St); free(rho); free(E);
+  if (wq_out) *wq_out = W;
+  int r = 0;
+  if (W == 0) {
+    r = -1;
+  } else {
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < n; ++k) {
+      const unsigned __int128 rhs = (unsigned __int128)((((uint64_t)k) << 32) | u32) * W;
+      int lo = 0, hi = n - 1;
+      while (lo < hi) {
+        int mid = (lo + hi) / 2;
+        unsigned __int128 lhs = ((unsigned __int128)C[mid] * (uint64_t)n) << 32;
+        if (lhs < rhs) lo = mid + 1;
+        else hi = mid;
+      }
+      anc[k] = lo;
+    }
+  }
   free(C);
   return r;
 }

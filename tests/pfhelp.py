@@ -82,7 +82,7 @@ def check_step(eng: Engine, k: int, before_state, before_shift, rec, weight_mode
         out["resampled"] = res["resampled"]
         if check_resample and res["resampled"] and eng.cfg.resampler == N.PF_RESAMPLE_SYSTEMATIC:
             u, W, M = eng.resample_info(k)
-            anc_o, W_o = O.systematic(lw_raw, M, u)
+            anc_o, W_o = O.systematic_tiled(lw_raw, u)
             anc_g = eng.ancestors(k)
             out["anc_equal"] = bool(np.array_equal(anc_o, anc_g))
             out["wq_equal"] = W == W_o

@@ -274,7 +274,7 @@ def test_degenerate_weights_single_survivor():
     assert np.all(anc == 54_321)
     u, W, M = eng.resample_info(0)
     _, lw_raw = eng.state_f32(0, raw=True)
-    assert np.array_equal(O.systematic(lw_raw, M, u)[0], anc)
+    assert np.array_equal(O.systematic_tiled(lw_raw, u)[0], anc)
     x, _ = eng.state_f32(0)
     assert np.all(x == st[:, 54_321][:, None])
 
