@@ -1251,6 +1251,113 @@ int pfe_set_state_f32(pf_engine_t* eng, int filter, const float* state, const fl
   return PF_OK;
 }
 
+// Checkpoint of one filter: a header, the local frame fixed at initialize
+// (ECEF -> E/N/U rotation), the control block and the particle arrays the
+// next step reads (the current state buffer, the log-weights and the last
+// resample's ancestors).  The Philox counter is the control block's
+// step counter, so a restored filter draws the same numbers.
+namespace {
+struct CkptHeader {
+  uint32_t magic;      // 'PFCK'
+  uint32_t version;
+  int32_t D, n;
+  uint32_t key0, key1;  // the filter's Philox key (its seed)
+  uint32_t ctrl_bytes, pad;
+};
+constexpr uint32_t kCkptMagic = 0x4b434650u;  // "PFCK" little-endian
+constexpr uint32_t kCkptVersion = 1u;
+size_t ckpt_bytes(const pf_engine* eng, int n) {
+  return sizeof(CkptHeader) + sizeof(double) * 9 + sizeof(FilterCtrl) +
+         (size_t)n * (sizeof(float) * (size_t)(eng->D + 1) + sizeof(int));
+}
+}  // namespace
+
+int pfe_checkpoint_bytes(pf_engine_t* eng, int filter, size_t* bytes) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!bytes) return set_err(PF_EINVAL, "null bytes");
+  *bytes = ckpt_bytes(eng, eng->hdesc[filter].n);
+  return PF_OK;
+}
+
+int pfe_checkpoint_save(pf_engine_t* eng, int filter, void* host_buf, size_t bytes) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!host_buf) return set_err(PF_EINVAL, "null buffer");
+  if (!eng->initialized[filter]) return set_err(PF_ENOTINIT, "filter %d not initialized", filter);
+  int n, tb, nt;
+  long long base;
+  filter_dims(eng, filter, &n, &base, &tb, &nt);
+  if (bytes < ckpt_bytes(eng, n))
+    return set_err(PF_ENOMEM, "checkpoint buffer too small (%zu < %zu bytes)", bytes, ckpt_bytes(eng, n));
+  if ((s = read_ctrl(eng)) != PF_OK) return s;
+  const FilterCtrl& c = eng->ctrl_host[filter];
+  unsigned char* o = (unsigned char*)host_buf;
+  CkptHeader h{kCkptMagic, kCkptVersion, eng->D, n, eng->hdesc[filter].key0, eng->hdesc[filter].key1,
+               (uint32_t)sizeof(FilterCtrl), 0u};
+  memcpy(o, &h, sizeof(h));
+  o += sizeof(h);
+  memcpy(o, eng->hdesc[filter].rot, sizeof(double) * 9);
+  o += sizeof(double) * 9;
+  memcpy(o, &c, sizeof(FilterCtrl));
+  o += sizeof(FilterCtrl);
+  const float* src = c.parity ? eng->dev.state1 : eng->dev.state0;
+  for (int dd = 0; dd < eng->D; ++dd) {
+    CK(cudaMemcpy(o, src + (size_t)dd * eng->P + base, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    o += sizeof(float) * n;
+  }
+  CK(cudaMemcpy(o, eng->dev.lw + base, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  o += sizeof(float) * n;
+  CK(cudaMemcpy(o, eng->dev.anc + base, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  return PF_OK;
+}
+
+int pfe_checkpoint_load(pf_engine_t* eng, int filter, const void* host_buf, size_t bytes) {
+  clear_err();
+  int s = check_filter(eng, filter);
+  if (s != PF_OK) return s;
+  if (!host_buf) return set_err(PF_EINVAL, "null buffer");
+  int n, tb, nt;
+  long long base;
+  filter_dims(eng, filter, &n, &base, &tb, &nt);
+  if (bytes < sizeof(CkptHeader)) return set_err(PF_EINVAL, "checkpoint too short");
+  CkptHeader h;
+  memcpy(&h, host_buf, sizeof(h));
+  if (h.magic != kCkptMagic || h.version != kCkptVersion)
+    return set_err(PF_EINVAL, "not a checkpoint of this library (magic 0x%08x, version %u)", h.magic, h.version);
+  if (h.D != eng->D || h.n != n || h.ctrl_bytes != sizeof(FilterCtrl))
+    return set_err(PF_EINVAL, "checkpoint of D=%d, N=%d does not fit filter %d (D=%d, N=%d)", h.D, h.n, filter,
+                   eng->D, n);
+  if (h.key0 != eng->hdesc[filter].key0 || h.key1 != eng->hdesc[filter].key1)
+    return set_err(PF_EINVAL, "checkpoint was taken with another seed than filter %d's", filter);
+  if (bytes < ckpt_bytes(eng, n)) return set_err(PF_EINVAL, "checkpoint truncated");
+  if ((s = sync_and_check(eng)) != PF_OK) return s;
+  const unsigned char* in = (const unsigned char*)host_buf + sizeof(h);
+  FilterDesc& d = eng->hdesc[filter];
+  memcpy(d.rot, in, sizeof(double) * 9);
+  in += sizeof(double) * 9;
+  CK(cudaMemcpy(eng->desc_dev + filter, &d, sizeof(FilterDesc), cudaMemcpyHostToDevice));
+  FilterCtrl c;
+  memcpy(&c, in, sizeof(FilterCtrl));
+  in += sizeof(FilterCtrl);
+  float* dst = c.parity ? eng->dev.state1 : eng->dev.state0;
+  for (int dd = 0; dd < eng->D; ++dd) {
+    CK(cudaMemcpy(dst + (size_t)dd * eng->P + base, in, sizeof(float) * n, cudaMemcpyHostToDevice));
+    in += sizeof(float) * n;
+  }
+  CK(cudaMemcpy(eng->dev.lw + base, in, sizeof(float) * n, cudaMemcpyHostToDevice));
+  in += sizeof(float) * n;
+  CK(cudaMemcpy(eng->dev.anc + base, in, sizeof(int) * n, cudaMemcpyHostToDevice));
+  c.ticket = 0u;
+  c.est_ticket = 0u;
+  eng->ctrl_host[filter] = c;
+  CK(cudaMemcpy(eng->ctrl_dev + filter, &c, sizeof(FilterCtrl), cudaMemcpyHostToDevice));
+  eng->initialized[filter] = 1;
+  return PF_OK;
+}
+
 int pfe_get_ancestors(pf_engine_t* eng, int filter, int* out_host) {
   clear_err();
   int s = check_filter(eng, filter);

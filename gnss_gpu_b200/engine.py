@@ -367,6 +367,21 @@ class Engine:
         lwa = None if lw is None else np.ascontiguousarray(lw, dtype=np.float32)
         N.check(self.lib.pfe_set_state_f32(self.h, k, N.vptr(st), None if lwa is None else N.vptr(lwa)))
 
+    def checkpoint(self, k: int) -> bytes:
+        """Filter k's complete state (control block with the FP64 anchors and
+        the step counter of its random numbers, FP32 offsets, log-weights,
+        ancestors) as bytes; restore() continues the filter bit for bit in an
+        engine of the same configuration, particle count and seed."""
+        nb = C.c_size_t(0)
+        N.check(self.lib.pfe_checkpoint_bytes(self.h, k, C.byref(nb)))
+        buf = np.empty(int(nb.value), np.uint8)
+        N.check(self.lib.pfe_checkpoint_save(self.h, k, N.vptr(buf), buf.nbytes))
+        return buf.tobytes()
+
+    def restore(self, k: int, blob: bytes):
+        buf = np.frombuffer(blob, np.uint8).copy()
+        N.check(self.lib.pfe_checkpoint_load(self.h, k, N.vptr(buf), buf.nbytes))
+
     def sort_spatially(self, k: int, cell: float = 1.0):
         """Reorder filter k's particles (with their log-weights) by a Morton
         code of their East/North offsets in cells of `cell` metres, stably

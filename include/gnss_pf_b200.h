@@ -389,6 +389,26 @@ int pfe_get_anchor(pf_engine_t* eng, int filter, double anchor_ecef[3],
  * ParticleFilterDevice.set_particle_states / set_log_weights and tests. */
 int pfe_set_state_f32(pf_engine_t* eng, int filter, const float* state_DxN,
                       const float* lw_or_null);
+/* Checkpoint and resume of one filter.  The checkpoint holds the filter's
+ * local frame (the ECEF -> E/N/U rotation fixed at pfe_initialize), its
+ * control block (FP64 anchor and clock anchors, pending re-centring shift,
+ * the step counter that keys the Philox draws, state-buffer parity,
+ * resample and log-weight flags, systematic offset, last estimate) and the
+ * particle arrays the next step reads: the current FP32 offsets [D][N], the
+ * log-weights [N] and the last resample's ancestors [N].  Loading it into a
+ * filter of an engine created with the same configuration, particle count
+ * and seed continues the filter bit for bit.  Replaces, for one filter, the
+ * reference's pf_device_get/set_particle_states and get/set_log_weights
+ * (include/gnss_gpu/pf_device.h:211-222), which carry the particles and
+ * weights but not the anchor or the random-number position.
+ * pfe_checkpoint_bytes gives the buffer size; save returns PF_ENOMEM for a
+ * smaller buffer, PF_ENOTINIT for a filter never initialized; load returns
+ * PF_EINVAL for a foreign, truncated or mismatched (D, N, seed) buffer.
+ * Velocity states, observation terms and the network of the learned
+ * likelihood are not part of it. */
+int pfe_checkpoint_bytes(pf_engine_t* eng, int filter, size_t* bytes);
+int pfe_checkpoint_save(pf_engine_t* eng, int filter, void* host_buf, size_t bytes);
+int pfe_checkpoint_load(pf_engine_t* eng, int filter, const void* host_buf, size_t bytes);
 /* Ancestor indices written by the last resample (host copy, N ints). */
 int pfe_get_ancestors(pf_engine_t* eng, int filter, int* out_host);
 /* Systematic offset (u32 fraction of a slot) and quantised weight total
