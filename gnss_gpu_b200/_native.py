@@ -121,7 +121,7 @@ EXPORTED = [
     "pfe_initialize", "pfe_get_frame", "pfe_upload_obs", "pfe_obs_slot_bytes", "pfe_step",
     "pfe_step_per_filter", "pfe_graph_capture", "pfe_graph_launch", "pfe_read_results",
     "pfe_estimate", "pfe_get_ess", "pfe_current_ess", "pfe_position_spread", "pfe_get_particles",
-    "pfe_get_state_f32", "pfe_set_state_f32", "pfe_checkpoint_bytes", "pfe_checkpoint_save",
+    "pf_test_fail_alloc", "pfe_get_state_f32", "pfe_set_state_f32", "pfe_checkpoint_bytes", "pfe_checkpoint_save",
     "pfe_checkpoint_load",
     "pfe_get_ancestors", "pfe_get_resample_info", "pfe_error_word", "pfe_set_spin_limit",
     "pfe_last_launch_count", "pfe_get_anchor", "pfe_test_poison_lookback", "pfe_enable_timing",
@@ -188,6 +188,7 @@ def load():
     L.pfe_get_anchor.argtypes = [p, i, dp, dp, C.POINTER(C.c_float)]
     L.pfe_set_state_f32.argtypes = [p, i, p, p]
     L.pfe_checkpoint_bytes.argtypes = [p, i, C.POINTER(C.c_size_t)]
+    L.pf_test_fail_alloc.argtypes = [i]
     L.pfe_checkpoint_save.argtypes = [p, i, p, C.c_size_t]
     L.pfe_checkpoint_load.argtypes = [p, i, p, C.c_size_t]
     L.pfe_get_ancestors.argtypes = [p, i, p]

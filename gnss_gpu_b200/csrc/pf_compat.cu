@@ -70,7 +70,15 @@ int workspace(size_t bytes, Workspace** out) {
     w.buf = nullptr;
     w.bytes = 0;
     size_t want = align_up(bytes, 1 << 20);
-    CK(cudaMalloc(&w.buf, want));
+    if (pf_injected_alloc_failure())
+      return set_err(PF_ENOMEM, "workspace allocation of %zu bytes failed (injected by pf_test_fail_alloc)", want);
+    const cudaError_t e = cudaMalloc(&w.buf, want);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      w.buf = nullptr;
+      return set_err(e == cudaErrorMemoryAllocation ? PF_ENOMEM : PF_ECUDA, "workspace allocation of %zu bytes: %s",
+                     want, cudaGetErrorString(e));
+    }
     w.bytes = want;
   }
   *out = &w;

@@ -566,12 +566,20 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
   if ((st = occupancy(k_export<7>, eng->sm_count, &eng->resident[Q_EXPORT])) != PF_OK) return fail(st);
 
   for (int i = 0; i < 2; ++i) {
+    if (pf_injected_alloc_failure()) {
+      set_err(PF_ENOMEM, "pinned staging allocation failed (injected by pf_test_fail_alloc)");
+      return fail(PF_ENOMEM);
+    }
     if (check_cuda(cudaHostAlloc((void**)&eng->pinned[i], L.obs_slot_bytes, cudaHostAllocDefault), "pinned staging") != PF_OK)
       return fail(PF_ENOMEM);
     if (check_cuda(cudaEventCreateWithFlags(&eng->pin_ev[i], cudaEventDisableTiming), "event") != PF_OK)
       return fail(PF_ECUDA);
   }
   eng->ctrl_span = (L.off_err - L.off_ctrl) + sizeof(unsigned) * 4;
+  if (pf_injected_alloc_failure()) {
+    set_err(PF_ENOMEM, "pinned control-block allocation failed (injected by pf_test_fail_alloc)");
+    return fail(PF_ENOMEM);
+  }
   if (check_cuda(cudaHostAlloc((void**)&eng->ctrl_host, eng->ctrl_span, cudaHostAllocDefault), "pinned ctrl") != PF_OK)
     return fail(PF_ENOMEM);
   eng->err_host = (unsigned*)((unsigned char*)eng->ctrl_host + (L.off_err - L.off_ctrl));

@@ -1124,53 +1124,63 @@ __global__ void __launch_bounds__(kThreads) k_merge(EngineDev e, int t0, int cou
 // decided to resample.  Log-weights are read through L2 (another CTA of the
 // same launch may have written them).
 __device__ __forceinline__ void mego_tile(const EngineDev& e, const FilterDesc* fd, unsigned epoch, int t) {
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int n = fd->n;
   const int j = t - fd->tile_begin;
   const long long base = fd->p_off;
   const uint32_t fid = (uint32_t)fd->filter_id;
   const int B = e.mego_iters;
   const float* lw = e.lw + base;
-  // The warp's four 32-slot segments of the tile run their chains side by
-  // side (four independent dependency chains per lane).
+  // The warp's four 32-slot segments r (slots j*1024 + r*256 + warp*32 +
+  // lane) run their chains side by side (four independent dependency chains
+  // per lane).  Iteration b's offsets of all four come from one Philox call,
+  // counter (quad, epoch, TAG_MEGO_OFF | b, filter) with quad = j*8 + warp,
+  // word r for segment r, computed by lane b % 32; slot k's acceptance
+  // uniforms are 16-bit halves, eight per call with counter (k, epoch,
+  // TAG_MEGO_U | b/8, filter): word (b % 8)/2, low half for even b.
+  const uint32_t quad = (uint32_t)(j * kSubTiles + warp);
   int k[4], a[4];
   float la[4];
   bool valid[4];
-  U4 ol[4];
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
-    const int seg0 = j * kTile + r * kThreads + ((int)threadIdx.x & ~31);  // segment's first slot
-    const bool act = seg0 < n;                                           // warp-uniform
+    const int seg0 = j * kTile + r * kThreads + warp * 32;  // segment's first slot
+    const bool act = seg0 < n;                               // warp-uniform
     const int k_real = seg0 + lane;
     valid[r] = act && k_real < n;
     k[r] = valid[r] ? k_real : (act ? seg0 : 0);  // lanes past the end shadow a valid slot
-    // lane l draws the offsets of iterations 4l .. 4l+3 of this segment
-    ol[r] = philox10(U4{(uint32_t)(seg0 / 32), epoch, TAG_MEGO_OFF | (uint32_t)lane, fid}, fd->key0, fd->key1);
     a[r] = k[r];
     la[r] = __ldcg(lw + k[r]);
   }
 #pragma unroll 1
-  for (int b0 = 0; b0 < B; b0 += 4) {
-    U4 ur[4];
+  for (int c0 = 0; c0 < B; c0 += 32) {
+    const U4 ol = philox10(U4{quad, epoch, TAG_MEGO_OFF | (uint32_t)(c0 + lane), fid}, fd->key0, fd->key1);
+#pragma unroll 1
+    for (int b0 = c0; b0 < min(B, c0 + 32); b0 += 8) {
+      U4 ur[4];
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
-      ur[r] = philox10(U4{(uint32_t)k[r], epoch, TAG_MEGO_U | (uint32_t)(b0 >> 2), fid}, fd->key0, fd->key1);
+      for (int r = 0; r < 4; ++r)
+        ur[r] = philox10(U4{(uint32_t)k[r], epoch, TAG_MEGO_U | (uint32_t)(b0 >> 3), fid}, fd->key0, fd->key1);
 #pragma unroll
-    for (int bb = 0; bb < 4; ++bb) {
-      if (b0 + bb >= B) break;
-      const int src_lane = (b0 + bb) >> 2;
+      for (int bb = 0; bb < 8; ++bb) {
+        if (b0 + bb >= B) break;
+        const int src_lane = (b0 + bb) & 31;
+        const uint32_t o0 = __shfl_sync(0xffffffffu, ol.x, src_lane), o1 = __shfl_sync(0xffffffffu, ol.y, src_lane);
+        const uint32_t o2 = __shfl_sync(0xffffffffu, ol.z, src_lane), o3 = __shfl_sync(0xffffffffu, ol.w, src_lane);
+        const uint32_t ow[4] = {o0, o1, o2, o3};
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const uint32_t ow = (bb == 0) ? ol[r].x : (bb == 1) ? ol[r].y : (bb == 2) ? ol[r].z : ol[r].w;
-        const uint32_t uw = (bb == 0) ? ur[r].x : (bb == 1) ? ur[r].y : (bb == 2) ? ur[r].z : ur[r].w;
-        const uint32_t o = __umulhi(__shfl_sync(0xffffffffu, ow, src_lane), (uint32_t)n);
-        int cand = k[r] + (int)o;
-        if (cand >= n) cand -= n;
-        const float lc = __ldcg(lw + cand);
-        const float lu = __logf(fmaf((float)uw, 2.3283064365386963e-10f, 1.1641532182693481e-10f));
-        if (lc - la[r] > lu) {
-          a[r] = cand;
-          la[r] = lc;
+        for (int r = 0; r < 4; ++r) {
+          const uint32_t w32 = (bb >> 1) == 0 ? ur[r].x : (bb >> 1) == 1 ? ur[r].y : (bb >> 1) == 2 ? ur[r].z : ur[r].w;
+          const uint32_t h = (bb & 1) ? (w32 >> 16) : (w32 & 0xFFFFu);
+          const uint32_t o = __umulhi(ow[r], (uint32_t)n);
+          int cand = k[r] + (int)o;
+          if (cand >= n) cand -= n;
+          const float lc = __ldcg(lw + cand);
+          const float lu = __logf(fmaf((float)h, 1.52587890625e-05f, 7.62939453125e-06f));  // (h + 1/2) 2^-16
+          if (lc - la[r] > lu) {
+            a[r] = cand;
+            la[r] = lc;
+          }
         }
       }
     }

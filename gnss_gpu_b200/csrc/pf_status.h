@@ -21,3 +21,7 @@ inline int set_err(int status, const char* fmt, ...) {
 }
 
 inline void clear_err() { pfb::g_last_error[0] = '\0'; }
+
+// Test hook behind pf_test_fail_alloc: true when the library's allocation
+// about to be made is the one chosen to fail (counts down over calls).
+bool pf_injected_alloc_failure();

@@ -415,6 +415,12 @@ int pfe_get_ancestors(pf_engine_t* eng, int filter, int* out_host);
  * used by the last systematic resample. */
 int pfe_get_resample_info(pf_engine_t* eng, int filter, uint32_t* u32,
                           uint64_t* wq_total, float* max_lw);
+/* Test hook: make the library's nth next host or device allocation fail
+ * (pinned staging of pfe_create, the stateless functions' workspace) as if
+ * memory were exhausted: the call returns PF_ENOMEM, frees what it had
+ * allocated, and later calls work again.  0 switches it off.  The
+ * reference has no counterpart (its CUDA_CHECK throws on any CUDA error). */
+int pf_test_fail_alloc(int nth);
 /* Device error word (0 = fine); non-zero after a bounded spin gave up. */
 int pfe_error_word(pf_engine_t* eng, unsigned* word);
 /* Test hook: spin limit of the decoupled look-back (0 = default). */

@@ -347,27 +347,36 @@ int orc_systematic_tiled(const float* lw, int n, uint32_t u32, int* anc, uint64_
  * Chesser et al. (arXiv:2109.13504): for each slot k the chain starts at
  * ancestor k; iteration b proposes j = (k + o_{b,g}) mod N with an offset
  * shared by the 32-slot segment g = k / 32 and accepts with probability
- * min(1, w_j / w_ancestor). */
+ * min(1, w_j / w_ancestor).  Draws (the engine's layout): the offsets of
+ * iteration b for the four segments g = 32 t + 8 r + w (tile t, r = 0..3)
+ * are the words r of Philox (8 t + w, epoch, TAG_MEGO_OFF | b, filter); the
+ * acceptance uniform of slot k at iteration b is the 16-bit half (b even:
+ * low) of word (b % 8) / 2 of Philox (k, epoch, TAG_MEGO_U | b / 8, filter),
+ * as (h + 1/2) 2^-16. */
 void orc_megopolis(const float* lw, int n, int iters, uint32_t k0, uint32_t k1, uint32_t epoch,
                    uint32_t fid, int* anc) {
 #pragma omp parallel for schedule(static)
   for (int k = 0; k < n; ++k) {
     const uint32_t g = (uint32_t)(k / 32);
+    const uint32_t quad = (g / 32) * 8 + (g % 8), r = (g % 32) / 8;
     int a = k;
     double la = (double)lw[k];
-    uint32_t ow[4], uw[4];
+    uint32_t uw[4];
     for (int b = 0; b < iters; ++b) {
-      if ((b & 3) == 0) {
-        uint32_t co[4] = {g, epoch, TAG_MEGO_OFF | (uint32_t)(b >> 2), fid};
-        orc_philox10(co, k0, k1, ow);
-        uint32_t cu[4] = {(uint32_t)k, epoch, TAG_MEGO_U | (uint32_t)(b >> 2), fid};
+      uint32_t ow[4];
+      uint32_t co[4] = {quad, epoch, TAG_MEGO_OFF | (uint32_t)b, fid};
+      orc_philox10(co, k0, k1, ow);
+      if ((b & 7) == 0) {
+        uint32_t cu[4] = {(uint32_t)k, epoch, TAG_MEGO_U | (uint32_t)(b >> 3), fid};
         orc_philox10(cu, k0, k1, uw);
       }
-      const uint32_t o = (uint32_t)(((uint64_t)ow[b & 3] * (uint64_t)(uint32_t)n) >> 32);
+      const uint32_t w32 = uw[(b & 7) >> 1];
+      const uint32_t h = (b & 1) ? (w32 >> 16) : (w32 & 0xFFFFu);
+      const uint32_t o = (uint32_t)(((uint64_t)ow[r] * (uint64_t)(uint32_t)n) >> 32);
       int cand = k + (int)o;
       if (cand >= n) cand -= n;
       const double lc = (double)lw[cand];
-      const double u = ((double)uw[b & 3] + 0.5) * 2.3283064365386963e-10;
+      const double u = ((double)h + 0.5) * 1.52587890625e-05;
       if (log(u) < lc - la) {
         a = cand;
         la = lc;
