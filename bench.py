@@ -51,6 +51,10 @@ def parse():
                     help="epoch: one cooperative kernel per step; chain: one kernel per phase")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--sigma-pr", type=float, default=3.0,
+                    help="cfg1: pseudorange sigma of the likelihood (30 gives a wide posterior, ESS ~N/4, for traffic "
+                         "profiles; the benchmark is 3)")
+    ap.add_argument("--force-resample", action="store_true", help="cfg1: resample every epoch regardless of the ESS")
     ap.add_argument("--no-extras", action="store_true",
                     help="default workload at one GPU: skip the cfg1-megopolis, cfg2 and cfg3 keys")
     return ap.parse_args()
@@ -233,10 +237,11 @@ def run_b200(args, world, rank, local, pg):
     opts = EngineOptions(n_clk=4, resampler=resampler, megopolis_iters=32, ess_threshold=0.5,
                          sys_offset="random", max_sats=32, obs_slots=E, covariance=True, recenter=True,
                          kernel_chain=args.path == "chain")
-    spec = FilterSpec(n_particles=n, seed=1234 + rank, sigma_pos=(1.0, 1.0, 0.5), sigma_clk=0.5, sigma_pr=3.0)
+    spec = FilterSpec(n_particles=n, seed=1234 + rank, sigma_pos=(1.0, 1.0, 0.5), sigma_clk=0.5,
+                      sigma_pr=args.sigma_pr)
     eng = Engine([spec], opts, device=local)
     eng.initialize(0, tr.truth_ecef[0], tr.truth_clk[0], 10.0, 30.0)
-    flags = N.PF_EP_PREDICT | N.PF_EP_WEIGHT
+    flags = N.PF_EP_PREDICT | N.PF_EP_WEIGHT | (N.PF_EP_FORCE_RESAMPLE if args.force_resample else 0)
     for t in range(E):  # every input resident in HBM before timing
         fe, sv = eng.pack_epoch([epoch_record(tr, t, flags)])
         eng.upload(t, fe, sv)
@@ -310,10 +315,12 @@ def run_b200(args, world, rank, local, pg):
     peak, peak_kind = peaks()
     D = 7
     rs_frac = float(np.mean(resampled))
-    # algorithmic bytes per particle-step: state read + write (2*D*4), log-weight
-    # write (4), ancestor read by the gather (4, when the previous step
-    # resampled) and ancestor write (4, when this step resamples)
-    b_alg = 2 * D * 4 + 4 + 4 * rs_frac + 4 * rs_frac
+    # algorithmic bytes per particle-step (the scope table's B_alg = 2 D p + 2 q):
+    # state read + write (2*D*4) and log-weight write + read (2*4) = 64 B at
+    # D = 7.  Also reported: the same plus the ancestor write and the gather's
+    # ancestor read of a resampling step (68 B when every step resamples).
+    b_alg = 2 * D * 4 + 2 * 4
+    b_alg_anc = 2 * D * 4 + 4 + 4 * rs_frac + 4 * rs_frac
     if args.path == "chain":
         kname = "k_step (fused predict+weight+statistics)"
         alg_k1 = (2 * D * 4 + 4 + 4 * rs_frac) * n
@@ -324,10 +331,11 @@ def run_b200(args, world, rank, local, pg):
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": total_s / K * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 state / f64 anchor+scan-free int64 CDF", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f32 state and log-weights / f64 anchor / exact integer CDF", "data": "synthetic",
         "config": {"workload": f"{args.workload}: 1 filter x {n} particles x 32 satellites (4 constellations x 8), "
-                               f"D=7 (E,N,U + 4 clocks), sigma_pr 3 m, 25% NLOS Exp(15 m), ESS<N/2 "
-                               f"{resampler} resampling" + (" (32 iterations)" if resampler == "megopolis" else ""),
+                               f"D=7 (E,N,U + 4 clocks), sigma_pr {args.sigma_pr:g} m, 25% NLOS Exp(15 m), "
+                               + ("every epoch " if args.force_resample else "ESS<N/2 ")
+                               + f"{resampler} resampling" + (" (32 iterations)" if resampler == "megopolis" else ""),
                    "particles": n, "satellites": 32, "state_dim": D, "parallelism": f"replicas x{world}",
                    "path": args.path,
                    "l2": "flushed between steps (512 MiB device write outside the per-step event intervals)",
@@ -340,7 +348,9 @@ def run_b200(args, world, rank, local, pg):
         "step_roofline": {"b_alg_bytes_per_particle_step": b_alg,
                           "achieved_gbs": value / world * b_alg / 1e9,
                           "frac_of_measured_peak": value / world * b_alg / 1e9 / peak,
-                          "frac_of_nominal_8tbs": value / world * b_alg / 1e9 / 8000.0},
+                          "frac_of_nominal_8tbs": value / world * b_alg / 1e9 / 8000.0,
+                          "b_alg_with_ancestors": b_alg_anc,
+                          "frac_of_measured_peak_with_ancestors": value / world * b_alg_anc / 1e9 / peak},
         "path": args.path,
         "resampled_fraction": rs_frac,
         "p50_2d_error_m": float(np.median(errs)),
@@ -464,7 +474,7 @@ def run_cfg2(args, world, rank, local, pg):
         "metric": "PF particle-steps/s (256 batched uneven filters, 1 launch per epoch from a CUDA graph)",
         "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": t_graph / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 state / f64 anchor+scan-free int64 CDF", "data": "synthetic",
+        "dtype": "f32 state and log-weights / f64 anchor / exact integer CDF", "data": "synthetic",
         "config": {"workload": f"cfg2-batched: 256 filters, particles log-uniform 1K-100K (total {total_n}), "
                                "6-40 satellites per filter and epoch, D=4, ESS<N/2 systematic resampling",
                    "particles": total_n, "filters": 256, "parallelism": f"replicas x{world}",
