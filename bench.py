@@ -344,7 +344,11 @@ def run_b200(args, world, rank, local, pg):
         "roofline": {"bound": "hbm", "kernel": kname,
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": alg_k1,
-                     "kernel_ms": kern_ms, "traffic": committed_traffic(kname.split()[0] + ":" + args.workload)},
+                     "kernel_ms": kern_ms, "traffic": committed_traffic(kname.split()[0] + ":" + args.workload),
+                     "traffic_wide_posterior": committed_traffic(kname.split()[0] + ":" + args.workload + "-wide"),
+                     "traffic_note": "DRAM read + write per launch from one-pass ncu captures of the L2-flushed "
+                                     "step (profiles/k_epoch_cfg1_dram.md): the benchmark's peaked posterior and a "
+                                     "wide one (sigma_pr 30 m, ESS ~N/4, resampling every epoch)"},
         "step_roofline": {"b_alg_bytes_per_particle_step": b_alg,
                           "achieved_gbs": value / world * b_alg / 1e9,
                           "frac_of_measured_peak": value / world * b_alg / 1e9 / peak,
