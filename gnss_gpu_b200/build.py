@@ -1,4 +1,6 @@
-"""Build libgnsspf_b200.so in-tree with nvcc for sm_100a.
+"""Build libgnsspf_b200.so in-tree with nvcc for sm_100a, and its checked
+variant libgnsspf_b200_checked.so (-DPF_CHECKED: data-dependent indexes are
+tested before use and a bad one is reported through the error word).
 
 Usage: python -m gnss_gpu_b200.build [--force]
 """
@@ -14,6 +16,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIBDIR = PKG / "lib"
 LIB = LIBDIR / "libgnsspf_b200.so"
+LIB_CHECKED = LIBDIR / "libgnsspf_b200_checked.so"
 SOURCES = ["pf_status.cu", "pf_engine.cu", "pf_compat.cu", "pf_noalloc.cu", "pf_mlp.cu"]
 HEADERS = ["pf_common.cuh", "pf_engine_dev.cuh", "pf_engine_kernels.cuh", "pf_epoch_kernel.cuh", "pf_mlp.cuh",
            "pf_learned.cuh", "pf_generic.cuh", "pf_obs_terms.cuh", "pf_velocity.cuh", "pf_bvh.cuh",
@@ -33,34 +36,46 @@ def nvcc() -> str:
     return cand
 
 
-def _stale() -> bool:
-    if not LIB.exists():
+def _stale(lib: Path) -> bool:
+    if not lib.exists():
         return True
-    t = LIB.stat().st_mtime
+    t = lib.stat().st_mtime
     deps = [CSRC / s for s in SOURCES + HEADERS] + [PKG.parent / "include" / "gnss_pf_b200.h"]
     return any(p.stat().st_mtime > t for p in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    if not force and not _stale():
-        return LIB
+def _build_lib(lib: Path, objdir: Path, extra: list, verbose: bool) -> Path:
+    from concurrent.futures import ThreadPoolExecutor
+
     LIBDIR.mkdir(exist_ok=True)
-    objdir = PKG / "_build"
     objdir.mkdir(exist_ok=True)
-    objs = []
+    cmds, objs = [], []
     for src in SOURCES:
         obj = objdir / (Path(src).stem + ".o")
-        cmd = [nvcc()] + NVCC_FLAGS + ["-c", str(CSRC / src), "-o", str(obj)]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        cmds.append([nvcc()] + NVCC_FLAGS + extra + ["-c", str(CSRC / src), "-o", str(obj)])
         objs.append(str(obj))
-    tmp = LIB.with_suffix(".so.tmp")
+    if verbose:
+        for c in cmds:
+            print(" ".join(c), flush=True)
+    with ThreadPoolExecutor(max_workers=len(cmds)) as ex:  # independent translation units
+        for r in ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds):
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed:\n{r.stdout}\n{r.stderr}")
+    tmp = lib.with_suffix(".so.tmp")
     cmd = [nvcc()] + ARCH + ["-shared", "-o", str(tmp)] + objs + ["-lcudart"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
-    os.replace(tmp, LIB)
+    os.replace(tmp, lib)
+    return lib
+
+
+def build(force: bool = False, verbose: bool = False, checked: bool = True) -> Path:
+    """Build the library (and its checked variant) when a source is newer."""
+    if force or _stale(LIB):
+        _build_lib(LIB, PKG / "_build", [], verbose)
+    if checked and (force or _stale(LIB_CHECKED)):
+        _build_lib(LIB_CHECKED, PKG / "_build_checked", ["-DPF_CHECKED"], verbose)
     return LIB
 
 

@@ -404,6 +404,7 @@ int err_status(unsigned w) {
   if (w & ERR_SAT_CAP) return set_err(PF_ECAP, "n_sat above max_sats (error word 0x%x)", w);
   if (w & ERR_BAD_WEIGHTS) return set_err(PF_EINVAL, "all log-weights non-finite (error word 0x%x)", w);
   if (w & ERR_INTERNAL_CAP) return set_err(PF_ECUDA, "internal capacity exceeded (error word 0x%x)", w);
+  if (w & ERR_BOUNDS) return set_err(PF_ECUDA, "index out of bounds caught by the checked build (error word 0x%x)", w);
   return PF_OK;
 }
 
@@ -1357,6 +1358,11 @@ int pfe_checkpoint_load(pf_engine_t* eng, int filter, const void* host_buf, size
   }
   CK(cudaMemcpy(eng->dev.lw + base, in, sizeof(float) * n, cudaMemcpyHostToDevice));
   in += sizeof(float) * n;
+  for (int k = 0; k < n; ++k) {  // the next gather indexes the state with these
+    int a;
+    memcpy(&a, in + sizeof(int) * (size_t)k, sizeof(int));
+    if (a < 0 || a >= n) return set_err(PF_EINVAL, "checkpoint ancestor %d of slot %d out of range [0, %d)", a, k, n);
+  }
   CK(cudaMemcpy(eng->dev.anc + base, in, sizeof(int) * n, cudaMemcpyHostToDevice));
   c.ticket = 0u;
   c.est_ticket = 0u;

@@ -30,8 +30,21 @@ enum QueueSlot : int {
 
 // Error word bits.
 enum : unsigned {
-  ERR_LOOKBACK_TIMEOUT = 1u, ERR_BAD_WEIGHTS = 2u, ERR_SAT_CAP = 4u, ERR_BARRIER_TIMEOUT = 8u, ERR_INTERNAL_CAP = 16u
+  ERR_LOOKBACK_TIMEOUT = 1u, ERR_BAD_WEIGHTS = 2u, ERR_SAT_CAP = 4u, ERR_BARRIER_TIMEOUT = 8u, ERR_INTERNAL_CAP = 16u,
+  ERR_BOUNDS = 32u
 };
+
+// Checked build (-DPF_CHECKED, libgnsspf_b200_checked.so): indexes that come
+// from data (ancestors, offspring ends, queued chunks, satellite offsets) are
+// tested before use; a bad one sets ERR_BOUNDS in the error word and the
+// access is skipped or clamped, so the host reports the fault as an error
+// instead of the device faulting.  The release build clamps the same indexes
+// silently (or relies on invariants of the layout) and never sets the bit.
+#ifdef PF_CHECKED
+#define PF_BOUNDS_OK(e, cond) ((cond) ? true : (atomicOr((e).err, ERR_BOUNDS), false))
+#else
+#define PF_BOUNDS_OK(e, cond) true
+#endif
 
 struct FilterDesc {
   int n;

@@ -380,7 +380,7 @@ __device__ __forceinline__ void load_particles(const EngineDev& e, const float* 
     // slots past the filter's end hold no ancestor; keep every index in range
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-      if (p0 + k >= n || (unsigned)ai[k] >= (unsigned)n) ai[k] = p0;
+      if (p0 + k >= n || !PF_BOUNDS_OK(e, (unsigned)ai[k] < (unsigned)n)) ai[k] = p0;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
       const float* s = src + (size_t)d * e.p_total + base;

@@ -248,7 +248,7 @@ __device__ __forceinline__ void epoch_sys_offspring(const EngineDev& e, unsigned
               const uint32_t lo = (k == 0) ? Fprev : Fk[k - 1], hi = Fk[k];
               const int i = p0 + k;
               const bool run = i < n && hi > lo;
-              if (run && hi - lo <= (uint32_t)kLightRun)
+              if (run && hi - lo <= (uint32_t)kLightRun && PF_BOUNDS_OK(e, hi <= (uint32_t)n))
                 for (uint32_t j = lo; j < hi; ++j) e.anc[base + j] = i;
               // long runs: one reservation per warp, a lane writes its own
               // one or two chunk descriptors, the warp writes longer lists
@@ -307,7 +307,9 @@ __device__ __forceinline__ void epoch_sys_chunks(const EngineDev& e, const unsig
 #pragma unroll 1
   for (unsigned c = gw; c < nchunks; c += nw) {
     const uint4 d = __ldcg(e.chunks + c);
-    int* dst = e.anc + ((long long)d.y << 32 | d.x);
+    const long long first = (long long)d.y << 32 | d.x;
+    if (!PF_BOUNDS_OK(e, first >= 0 && first + (long long)d.z <= e.p_total && d.z <= (uint32_t)kRunChunk)) continue;
+    int* dst = e.anc + first;
     for (uint32_t j = lane; j < d.z; j += 32) dst[j] = (int)d.w;
   }
 }

@@ -403,7 +403,8 @@ int pfe_set_state_f32(pf_engine_t* eng, int filter, const float* state_DxN,
  * weights but not the anchor or the random-number position.
  * pfe_checkpoint_bytes gives the buffer size; save returns PF_ENOMEM for a
  * smaller buffer, PF_ENOTINIT for a filter never initialized; load returns
- * PF_EINVAL for a foreign, truncated or mismatched (D, N, seed) buffer.
+ * PF_EINVAL for a foreign, truncated or mismatched (D, N, seed) buffer or
+ * an ancestor outside [0, N).
  * Velocity states, observation terms and the network of the learned
  * likelihood are not part of it. */
 int pfe_checkpoint_bytes(pf_engine_t* eng, int filter, size_t* bytes);

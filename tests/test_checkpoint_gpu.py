@@ -68,5 +68,9 @@ def test_checkpoint_rejects_mismatched_filters():
         b.restore(0, b"\0" * len(blob))
     with pytest.raises(RuntimeError):
         b.checkpoint(0)  # never initialized
+    bad = bytearray(blob)
+    bad[-4:] = (4096 + 5).to_bytes(4, "little", signed=True)  # last slot's ancestor out of range
+    with pytest.raises(ValueError, match="ancestor"):
+        b.restore(0, bytes(bad))
     b.close()
     a.close()

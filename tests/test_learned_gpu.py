@@ -126,3 +126,46 @@ def test_city_los_device_equals_host():
         assert np.array_equal(host, dev), int(np.sum(host != dev))
         total += int(host.sum())
     assert total > 1000  # the cases exercise blocked rays
+
+
+def test_mixture_batched_uneven_filters_match_oracle():
+    """Several filters of uneven size (one tile shared by none of them, ragged
+    tails, 3 to 70,001 particles) and different cities and satellite counts
+    in one engine: every filter's in-kernel network outputs and log-weights
+    match the FP64 oracles, as for a single filter."""
+    ns = [3, 1500, 4096, 9000, 70_001]
+    prm = M.init_params(6)
+    specs = [FilterSpec(n_particles=n, seed=40 + k, sigma_pos=(1.0, 1.0, 0.5), sigma_clk=1.0, sigma_pr=3.0)
+             for k, n in enumerate(ns)]
+    eng = Engine(specs, EngineOptions(n_clk=1, weight_mode="mixture", huber_k=1.5, max_sats=40, obs_slots=1))
+    eng.set_mlp(prm)
+    trs, priors = [], []
+    for k, n in enumerate(ns):
+        tr = CS.drive(CS.make_city(30 + k), 4, seed=50 + k, n_sat=[6, 12, 24, 33, 40][k])
+        start = tr.truth_ecef[0] - tr.disp_enu[0] @ tr.rot
+        eng.initialize(k, start, tr.truth_clk[0], 5.0, 10.0)
+        trs.append(tr)
+        priors.append((start + tr.disp_enu[0] @ tr.rot, float(tr.truth_clk[0][0])))
+    for t in range(2):
+        recs = []
+        for k, tr in enumerate(trs):
+            _, _, blk = LR.prior_geometry(tr, t, *priors[k])
+            recs.append(LR.epoch_record(tr, t, blk))
+        fe, sv = eng.pack_epoch(recs)
+        eng.upload(0, fe, sv)
+        eng.step()
+        for k, tr in enumerate(trs):
+            rot, _ = eng.frame(k)
+            x_raw, lw_raw = eng.state_f32(k, raw=True)
+            anchor, clk, _ = eng.anchor(k)
+            d = eng.sat_debug(k)
+            p, mu = M.predict(prm, d[:, :12].astype(np.float64))
+            assert np.max(np.abs(d[:, 12] - np.clip(p, 1e-4, 1 - 1e-4))) < 2e-3
+            rows = H.sat_rows(recs[k]["sats"], recs[k]["pr"])
+            lw_o = O.weight_mixture(x_raw, anchor, clk, rot, rows, 3.0, d[:, 12].astype(np.float64),
+                                    d[:, 13].astype(np.float64), d[:, 14], huber_k=1.5)
+            ok, rel = H.lw_close(lw_raw, lw_o)
+            assert ok.all(), (k, float(rel.max()))
+            r = eng.results()[k]
+            priors[k] = (r["est_ecef"] + tr.disp_enu[t + 1] @ tr.rot, float(r["est_clk"][0]))
+    eng.close()
