@@ -80,10 +80,9 @@ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
   size_t off_state0, off_state1, off_lw, off_anc, off_offs, off_mp, off_part, off_agg, off_inc,
-      off_flag, off_excl, off_wq, off_seg_rho, off_seg_E, off_tile_S, off_tile_m, off_chunks, off_fmax, off_mlp, off_satdbg, off_obsrows, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
+      off_flag, off_excl, off_wq, off_seg_rho, off_seg_E, off_tile_S, off_tile_m, off_seg_anc, off_mlp, off_satdbg, off_obsrows, off_desc, off_ctrl, off_tf, off_queue, off_err, off_obs, off_export,
       total;
   size_t obs_slot_bytes;
-  size_t max_chunks;
   long long P;
   int T, D, max_n;
 };
@@ -164,11 +163,7 @@ Layout make_layout(const pf_engine_config_t* cfg, const pf_filter_params_t* fp) 
   L.off_seg_E = take((size_t)T * kSubTiles * 8);
   L.off_tile_S = take((size_t)T * 8);
   L.off_tile_m = take((size_t)T * 4);
-  // a run longer than kLightRun slots needs ceil(len / kRunChunk) chunks:
-  // at most P / (kLightRun + 1) runs and P / kRunChunk + T extra chunks
-  L.max_chunks = (size_t)(P / kLightRun) + (size_t)T + 64;
-  L.off_chunks = take(L.max_chunks * sizeof(uint4));
-  L.off_fmax = take((size_t)cfg->n_filters * 4);
+  L.off_seg_anc = take((size_t)T * kSubTiles * 4);
   const bool mix = cfg->weight_mode == PF_WEIGHT_MIXTURE;
   L.off_mlp = take(mix ? (size_t)kMlpParams * 4 : 0);
   L.off_satdbg = take(mix ? (size_t)cfg->n_filters * cfg->max_sats * kSatDbg * 4 : 0);
@@ -437,6 +432,33 @@ int filter_dims(pf_engine* eng, int f, int* n, long long* base, int* tb, int* nt
   return PF_OK;
 }
 
+// The ancestors of filter f's last resample, one per slot, on the host:
+// the slot array with every 128-slot segment that carries a marker
+// (systematic resampling in the epoch kernel) filled from it.
+int read_ancestors(pf_engine* eng, int f, int* out) {
+  int n, tb, nt;
+  long long base;
+  filter_dims(eng, f, &n, &base, &tb, &nt);
+  CK(cudaMemcpy(out, eng->dev.anc + base, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  if (eng->dev.anc_seg) {
+    std::vector<int> mk((size_t)nt * kSubTiles);
+    CK(cudaMemcpy(mk.data(), eng->dev.seg_anc + (size_t)tb * kSubTiles, sizeof(int) * mk.size(),
+                  cudaMemcpyDeviceToHost));
+    for (int k = 0; k < n; ++k)
+      if (mk[k / kWarpTile] >= 0) out[k] = mk[k / kWarpTile];
+  }
+  return PF_OK;
+}
+
+// After the host wrote every slot of filter f's ancestors: no segment marker
+// may override them.
+int clear_segment_markers(pf_engine* eng, int f) {
+  if (!eng->dev.anc_seg) return PF_OK;
+  const FilterDesc& d = eng->hdesc[f];
+  CK(cudaMemset(eng->dev.seg_anc + (size_t)d.tile_begin * kSubTiles, 0xFF, sizeof(int) * (size_t)d.n_tiles * kSubTiles));
+  return PF_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -513,9 +535,9 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
   e.seg_E = (double*)(w + L.off_seg_E);
   e.tile_S = (double*)(w + L.off_tile_S);
   e.tile_m = (float*)(w + L.off_tile_m);
-  e.chunks = (uint4*)(w + L.off_chunks);
-  e.max_chunks = (unsigned)L.max_chunks;
-  e.fmax = (unsigned*)(w + L.off_fmax);
+  e.seg_anc = (int*)(w + L.off_seg_anc);
+  // the epoch kernel's systematic resampler marks whole-segment runs there
+  e.anc_seg = (cfg->resampler == PF_RESAMPLE_SYSTEMATIC && !(cfg->flags & PF_FLAG_KERNEL_CHAIN)) ? 1 : 0;
   e.mlp = (const float*)(w + L.off_mlp);
   e.sat_dbg = (float*)(w + L.off_satdbg);
   eng->obs_rows = (ObsRow*)(w + L.off_obsrows);
@@ -596,7 +618,8 @@ int pfe_create(const pf_engine_config_t* cfg, const pf_filter_params_t* filters,
       check_cuda(cudaMemsetAsync(w + L.off_queue, 0, sizeof(unsigned) * (2 * Q_COUNT + kBarWords),
                                  eng->stream), "memset queue") != PF_OK ||
       check_cuda(cudaMemsetAsync(w + L.off_err, 0, sizeof(unsigned) * 4, eng->stream), "memset err") != PF_OK ||
-      check_cuda(cudaMemsetAsync(w + L.off_fmax, 0, (size_t)cfg->n_filters * 4, eng->stream), "memset fmax") != PF_OK ||
+      check_cuda(cudaMemsetAsync(w + L.off_seg_anc, 0xFF, (size_t)L.T * kSubTiles * 4, eng->stream),
+                 "memset segment markers") != PF_OK ||
       check_cuda(cudaMemsetAsync(w + L.off_obs, 0, L.obs_slot_bytes * cfg->obs_slots, eng->stream), "memset obs") != PF_OK ||
       check_cuda(cudaMemsetAsync(w + L.off_state0, 0, (size_t)L.D * L.P * 4, eng->stream), "memset state") != PF_OK ||
       check_cuda(cudaMemsetAsync(w + L.off_lw, 0, (size_t)L.P * 4, eng->stream), "memset lw") != PF_OK)
@@ -1211,7 +1234,7 @@ int pfe_get_state_f32(pf_engine_t* eng, int filter, float* out_state, float* out
   std::vector<int> anc;
   if (gather) {
     anc.resize(n);
-    CK(cudaMemcpy(anc.data(), eng->dev.anc + base, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    if ((s = read_ancestors(eng, filter, anc.data())) != PF_OK) return s;
   }
   if (out_state) {
     std::vector<float> tmp(n);
@@ -1319,7 +1342,9 @@ int pfe_checkpoint_save(pf_engine_t* eng, int filter, void* host_buf, size_t byt
   }
   CK(cudaMemcpy(o, eng->dev.lw + base, sizeof(float) * n, cudaMemcpyDeviceToHost));
   o += sizeof(float) * n;
-  CK(cudaMemcpy(o, eng->dev.anc + base, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  std::vector<int> anc(n);
+  if ((s = read_ancestors(eng, filter, anc.data())) != PF_OK) return s;
+  memcpy(o, anc.data(), sizeof(int) * n);
   return PF_OK;
 }
 
@@ -1364,6 +1389,7 @@ int pfe_checkpoint_load(pf_engine_t* eng, int filter, const void* host_buf, size
     if (a < 0 || a >= n) return set_err(PF_EINVAL, "checkpoint ancestor %d of slot %d out of range [0, %d)", a, k, n);
   }
   CK(cudaMemcpy(eng->dev.anc + base, in, sizeof(int) * n, cudaMemcpyHostToDevice));
+  if ((s = clear_segment_markers(eng, filter)) != PF_OK) return s;
   c.ticket = 0u;
   c.est_ticket = 0u;
   eng->ctrl_host[filter] = c;
@@ -1381,8 +1407,7 @@ int pfe_get_ancestors(pf_engine_t* eng, int filter, int* out_host) {
   int n, tb, nt;
   long long base;
   filter_dims(eng, filter, &n, &base, &tb, &nt);
-  CK(cudaMemcpy(out_host, eng->dev.anc + base, sizeof(int) * n, cudaMemcpyDeviceToHost));
-  return PF_OK;
+  return read_ancestors(eng, filter, out_host);
 }
 
 int pfe_get_resample_info(pf_engine_t* eng, int filter, uint32_t* u32, uint64_t* wq_total, float* max_lw) {

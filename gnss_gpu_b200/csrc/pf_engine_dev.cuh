@@ -14,9 +14,7 @@ constexpr int kMergeDiag = 2 * kTile;  // merge-path diagonals per tile
 constexpr int kPartStride = 16;        // floats per tile partial
 constexpr int kWarpTile = 32 * kPerThread;      // particles per warp segment (epoch kernel)
 constexpr int kSubTiles = kTile / kWarpTile;    // warp segments per tile
-constexpr int kLightRun = 32;                   // epoch kernel: longest offspring run written in phase 4
-constexpr int kRunChunk = 1024;                 // epoch kernel: slots per queued chunk of a longer run
-constexpr int kBarChunks = 3;                   // epoch kernel: queued-chunk counter in the barrier block
+constexpr int kLightRun = 128;                  // epoch kernel: longest offspring run written by one lane
 constexpr int kBarCount = 4;                    // epoch kernel: arrival counter in the barrier block
 constexpr int kBarWords = 8;                    // epoch kernel: words of the barrier block
 constexpr int kMaxEpochGrid = 2048;             // epoch kernel: most CTAs of one launch
@@ -35,7 +33,7 @@ enum : unsigned {
 };
 
 // Checked build (-DPF_CHECKED, libgnsspf_b200_checked.so): indexes that come
-// from data (ancestors, offspring ends, queued chunks, satellite offsets) are
+// from data (ancestors, offspring ends, segment markers, satellite offsets) are
 // tested before use; a bad one sets ERR_BOUNDS in the error word and the
 // access is skipped or clamped, so the host reports the fault as an error
 // instead of the device faulting.  The release build clamps the same indexes
@@ -78,6 +76,9 @@ struct FilterCtrl {
   float max_lw;
   uint32_t sys_u;
   uint32_t sys_u_cur;     // systematic offset of the running step (written before its first grid barrier)
+  int sys_q_cur;          // the running step builds the systematic CDF (written before its first grid barrier)
+  int eflags_cur;         // the running step's epoch flags and epoch (written before its first grid
+  unsigned epoch_cur;     // barrier; the owner advances `epoch` meanwhile)
   unsigned epoch;
   unsigned ticket;
   unsigned est_ticket;
@@ -115,9 +116,12 @@ struct EngineDev {
   double* seg_E;
   double* tile_S;
   float* tile_m;
-  uint4* chunks;             // epoch kernel: queued offspring-run chunks (first slot lo/hi, length, ancestor)
-  unsigned max_chunks;
-  unsigned* fmax;            // epoch kernel: per filter, order-preserving code of the max log-weight
+  // Systematic resampling in the epoch kernel: one word per 128-slot
+  // segment of the ancestor array (kSubTiles per tile, at the filter's
+  // tile_begin), >= 0 when every slot of the segment has that ancestor (the
+  // slots themselves are then not written), -1 when the slots hold theirs.
+  int* seg_anc;
+  int anc_seg;               // 1: readers of the ancestors consult seg_anc first
   const float* mlp;          // mixture mode: network parameters (FP32)
   int lk_type;               // generic mode: pf_likelihood_type_t and its parameters
   float lk_nu, lk_huber_k, lk_w_los, lk_mu_nlos, lk_sigma_nlos, lk_gate_m;

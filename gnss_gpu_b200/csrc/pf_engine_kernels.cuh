@@ -368,14 +368,45 @@ __device__ __forceinline__ void local_to_ecef(const double* rot, const double* a
 }
 
 // -------------------------------------------------------------------------
+// Ancestors after a resample.  When the engine keeps segment markers
+// (e.anc_seg), a 128-slot segment whose slots all share one ancestor holds
+// it in its marker and its slots are not written; other segments' markers
+// are -1 and their slots hold the ancestors.  seg_markers is null when every
+// slot is written.
+__device__ __forceinline__ const int* seg_markers(const EngineDev& e, const FilterDesc* fd) {
+  return e.anc_seg ? e.seg_anc + (size_t)fd->tile_begin * kSubTiles : nullptr;
+}
+__device__ __forceinline__ int ancestor_at(const EngineDev& e, const int* seg, long long base, int j) {
+  if (seg) {
+    const int u = __ldcg(seg + j / kWarpTile);
+    if (u >= 0) return u;
+  }
+  return __ldcg(e.anc + base + j);
+}
+
+// The ancestors of slots [p0, p0+4) (one 128-slot segment).  The marker and
+// the slots are loaded together (the slots of a marked segment are stale and
+// ignored): one memory latency.
+struct AncLoad {
+  int4 a;
+  int u;
+};
+__device__ __forceinline__ AncLoad issue_ancestors4(const EngineDev& e, const FilterDesc* fd, long long base, int p0) {
+  const int* seg = seg_markers(e, fd);
+  AncLoad r;
+  r.u = seg ? __ldcg(seg + p0 / kWarpTile) : -1;
+  r.a = __ldcg(reinterpret_cast<const int4*>(e.anc + base + p0));
+  return r;
+}
+
 // Load the 4 particles [p0, p0+4) of the current state (gathering through
-// the ancestor array when the last step resampled).
+// the ancestors when the last step resampled), with the ancestors' loads
+// already issued.
 template <int D>
-__device__ __forceinline__ void load_particles(const EngineDev& e, const float* src,
-                                               long long base, int p0, int n, bool gather,
-                                               float (&x)[D][4]) {
+__device__ __forceinline__ void load_particles_from(const EngineDev& e, const float* src, long long base, int p0,
+                                                    int n, bool gather, const AncLoad& al, float (&x)[D][4]) {
   if (gather) {
-    int4 a = __ldcg(reinterpret_cast<const int4*>(e.anc + base + p0));
+    const int4 a = al.u >= 0 ? make_int4(al.u, al.u, al.u, al.u) : al.a;
     int ai[4] = {a.x, a.y, a.z, a.w};
     // slots past the filter's end hold no ancestor; keep every index in range
 #pragma unroll
@@ -394,6 +425,14 @@ __device__ __forceinline__ void load_particles(const EngineDev& e, const float* 
       x[d][0] = v.x; x[d][1] = v.y; x[d][2] = v.z; x[d][3] = v.w;
     }
   }
+}
+template <int D>
+__device__ __forceinline__ void load_particles(const EngineDev& e, const FilterDesc* fd, const float* src,
+                                               long long base, int p0, int n, bool gather,
+                                               float (&x)[D][4]) {
+  AncLoad al{make_int4(0, 0, 0, 0), -1};
+  if (gather) al = issue_ancestors4(e, fd, base, p0);
+  load_particles_from<D>(e, src, base, p0, n, gather, al, x);
 }
 
 
@@ -485,12 +524,25 @@ __device__ __forceinline__ double sys_inner(double E, double rho, double r, doub
 // ESS, the device-side resample decision (particle_filter.py:159-161), the
 // next re-centring shift, the systematic offset, and the epoch/parity step.
 // Executed by one thread.
+// The device-side resample decision of particle_filter.py:159-161 (ESS
+// below threshold x N, or forced; never without finite weights) from the
+// merged statistics and the step's epoch flags.  A function of its inputs
+// alone, so any CTA holding the same merge reaches the same decision.
+__device__ __forceinline__ bool resample_decision(const EngineDev& e, const FilterDesc* fd, const MergedStats& ms,
+                                                  int eflags) {
+  const bool do_weight = (eflags & PF_EP_WEIGHT) != 0;
+  const double W = ms.w;
+  const double ess = (ms.w2 > 0.0) ? (W * W) / ms.w2 : 0.0;
+  if (!(W > 0.0) || !(ms.max_lw > -INFINITY)) return false;
+  return (do_weight || (eflags & PF_EP_RESAMPLE_CHECK)) && !(eflags & PF_EP_NO_RESAMPLE) &&
+         ((eflags & PF_EP_FORCE_RESAMPLE) || ess < (double)e.ess_threshold * (double)fd->n);
+}
+
 template <int D>
 __device__ __forceinline__ void finalize_filter(const EngineDev& e, const FilterDesc* fd, FilterCtrl* fc,
                                                 const MergedStats& ms, unsigned epoch, int parity,
                                                 bool lw_zero, int eflags, bool do_weight) {
   constexpr int NCLK = D - 3;
-  const int n = fd->n;
   const double W = ms.w;
   const double ess = (ms.w2 > 0.0) ? (W * W) / ms.w2 : 0.0;
   double mu[kMaxD];
@@ -529,12 +581,8 @@ __device__ __forceinline__ void finalize_filter(const EngineDev& e, const Filter
   const bool recenter = (e.flags & PF_FLAG_RECENTER) != 0 && W > 0.0;
 #pragma unroll
   for (int d = 0; d < 8; ++d) fc->shift[d] = (recenter && d < D) ? (float)mu[d] : 0.f;
-  bool rs = (do_weight || (eflags & PF_EP_RESAMPLE_CHECK)) && !(eflags & PF_EP_NO_RESAMPLE) &&
-            ((eflags & PF_EP_FORCE_RESAMPLE) || ess < (double)e.ess_threshold * (double)n);
-  if (!(W > 0.0) || !(ms.max_lw > -INFINITY)) {
-    if (do_weight) atomicOr(e.err, ERR_BAD_WEIGHTS);
-    rs = false;
-  }
+  const bool rs = resample_decision(e, fd, ms, eflags);
+  if ((!(W > 0.0) || !(ms.max_lw > -INFINITY)) && do_weight) atomicOr(e.err, ERR_BAD_WEIGHTS);
   fc->resample_flag = rs ? 1 : 0;
   fc->lw_zero = rs ? 1 : (do_weight ? 0 : (lw_zero ? 1 : 0));
   if (rs) {
@@ -669,7 +717,7 @@ __global__ void __launch_bounds__(kThreads, PF_KSTEP_MINB) k_step(EngineDev e, i
 #pragma unroll
       for (int k = 0; k < 4; ++k) x[d][k] = 0.f;
     if (active) {
-      load_particles<D>(e, src, base, p0, n, gather, x);
+      load_particles<D>(e, fd, src, base, p0, n, gather, x);
       float lw0[4] = {0.f, 0.f, 0.f, 0.f};
       const bool need_prev = !lw_zero && (!do_weight || e.lw_mode == PF_LW_ACCUMULATE);
       if (need_prev) {
@@ -1137,7 +1185,9 @@ __device__ __forceinline__ void mego_tile(const EngineDev& e, const FilterDesc* 
   // counter (quad, epoch, TAG_MEGO_OFF | b, filter) with quad = j*8 + warp,
   // word r for segment r, computed by lane b % 32; slot k's acceptance
   // uniforms are 16-bit halves, eight per call with counter (k, epoch,
-  // TAG_MEGO_U | b/8, filter): word (b % 8)/2, low half for even b.
+  // TAG_MEGO_U | b/8, filter): word (b % 8)/2, low half for even b.  The
+  // candidates do not depend on the chain, so a block of eight iterations
+  // loads its 32 candidate log-weights per lane before any comparison.
   const uint32_t quad = (uint32_t)(j * kSubTiles + warp);
   int k[4], a[4];
   float la[4];
@@ -1154,32 +1204,61 @@ __device__ __forceinline__ void mego_tile(const EngineDev& e, const FilterDesc* 
   }
 #pragma unroll 1
   for (int c0 = 0; c0 < B; c0 += 32) {
+    // lane b % 32 draws iteration b's four offsets and scales them to [0, n)
     const U4 ol = philox10(U4{quad, epoch, TAG_MEGO_OFF | (uint32_t)(c0 + lane), fid}, fd->key0, fd->key1);
+    const uint32_t osc[4] = {__umulhi(ol.x, (uint32_t)n), __umulhi(ol.y, (uint32_t)n), __umulhi(ol.z, (uint32_t)n),
+                             __umulhi(ol.w, (uint32_t)n)};
 #pragma unroll 1
     for (int b0 = c0; b0 < min(B, c0 + 32); b0 += 8) {
       U4 ur[4];
 #pragma unroll
       for (int r = 0; r < 4; ++r)
         ur[r] = philox10(U4{(uint32_t)k[r], epoch, TAG_MEGO_U | (uint32_t)(b0 >> 3), fid}, fd->key0, fd->key1);
+      const int nb = min(8, B - b0);
+      if (nb == 8) {
+        // a full block of eight iterations: every candidate's log-weight is
+        // loaded first (they do not depend on the chain), then the chains run
+        float lc[8][4];
+        int cand[8][4];
 #pragma unroll
-      for (int bb = 0; bb < 8; ++bb) {
-        if (b0 + bb >= B) break;
-        const int src_lane = (b0 + bb) & 31;
-        const uint32_t o0 = __shfl_sync(0xffffffffu, ol.x, src_lane), o1 = __shfl_sync(0xffffffffu, ol.y, src_lane);
-        const uint32_t o2 = __shfl_sync(0xffffffffu, ol.z, src_lane), o3 = __shfl_sync(0xffffffffu, ol.w, src_lane);
-        const uint32_t ow[4] = {o0, o1, o2, o3};
+        for (int bb = 0; bb < 8; ++bb)
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const uint32_t w32 = (bb >> 1) == 0 ? ur[r].x : (bb >> 1) == 1 ? ur[r].y : (bb >> 1) == 2 ? ur[r].z : ur[r].w;
-          const uint32_t h = (bb & 1) ? (w32 >> 16) : (w32 & 0xFFFFu);
-          const uint32_t o = __umulhi(ow[r], (uint32_t)n);
-          int cand = k[r] + (int)o;
-          if (cand >= n) cand -= n;
-          const float lc = __ldcg(lw + cand);
-          const float lu = __logf(fmaf((float)h, 1.52587890625e-05f, 7.62939453125e-06f));  // (h + 1/2) 2^-16
-          if (lc - la[r] > lu) {
-            a[r] = cand;
-            la[r] = lc;
+          for (int r = 0; r < 4; ++r) {
+            int c = k[r] + (int)__shfl_sync(0xffffffffu, osc[r], (b0 + bb) & 31);
+            if (c >= n) c -= n;
+            cand[bb][r] = c;
+            lc[bb][r] = __ldcg(lw + c);
+          }
+#pragma unroll
+        for (int bb = 0; bb < 8; ++bb)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const uint32_t w32 = (bb >> 1) == 0 ? ur[r].x : (bb >> 1) == 1 ? ur[r].y : (bb >> 1) == 2 ? ur[r].z : ur[r].w;
+            const uint32_t h = (bb & 1) ? (w32 >> 16) : (w32 & 0xFFFFu);
+            const float lu = __logf(fmaf((float)h, 1.52587890625e-05f, 7.62939453125e-06f));  // (h + 1/2) 2^-16
+            if (lc[bb][r] - la[r] > lu) {
+              a[r] = cand[bb][r];
+              la[r] = lc[bb][r];
+            }
+          }
+      } else {
+        for (int bb = 0; bb < nb; ++bb) {
+          const int src_lane = (b0 + bb) & 31;
+          uint32_t ow[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) ow[r] = __shfl_sync(0xffffffffu, osc[r], src_lane);
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const uint32_t w32 = (bb >> 1) == 0 ? ur[r].x : (bb >> 1) == 1 ? ur[r].y : (bb >> 1) == 2 ? ur[r].z : ur[r].w;
+            const uint32_t h = (bb & 1) ? (w32 >> 16) : (w32 & 0xFFFFu);
+            int cand = k[r] + (int)ow[r];
+            if (cand >= n) cand -= n;
+            const float lc = __ldcg(lw + cand);
+            const float lu = __logf(fmaf((float)h, 1.52587890625e-05f, 7.62939453125e-06f));
+            if (lc - la[r] > lu) {
+              a[r] = cand;
+              la[r] = lc;
+            }
           }
         }
       }
@@ -1288,7 +1367,7 @@ __global__ void __launch_bounds__(kThreads) k_estimate(EngineDev e, int t0, int 
 #pragma unroll
       for (int k = 0; k < 4; ++k) x[d][k] = 0.f;
     if (p0 < n) {
-      load_particles<D>(e, src, base, p0, n, fc->resample_flag != 0, x);
+      load_particles<D>(e, fd, src, base, p0, n, fc->resample_flag != 0, x);
       if (fc->lw_zero) {
         lwv[0] = lwv[1] = lwv[2] = lwv[3] = 0.f;
       } else {
@@ -1356,7 +1435,7 @@ __global__ void __launch_bounds__(kThreads) k_position_term(EngineDev e, int f, 
   const bool zero = fc->lw_zero != 0;
   for (int p0 = (blockIdx.x * kThreads + threadIdx.x) * 4; p0 < n; p0 += gridDim.x * kThreads * 4) {
     float x[D][4];
-    load_particles<D>(e, src, base, p0, n, fc->resample_flag != 0, x);
+    load_particles<D>(e, fd, src, base, p0, n, fc->resample_flag != 0, x);
     float4 l = zero ? make_float4(0.f, 0.f, 0.f, 0.f) : *reinterpret_cast<const float4*>(e.lw + base + p0);
     float lv[4] = {l.x, l.y, l.z, l.w};
 #pragma unroll
@@ -1401,7 +1480,7 @@ __global__ void __launch_bounds__(kThreads) k_export(EngineDev e, int t0, int co
     const long long base = fd->p_off;
     const float* src = fc->parity ? e.state1 : e.state0;
     float x[D][4];
-    load_particles<D>(e, src, base, p0, n, fc->resample_flag != 0, x);
+    load_particles<D>(e, fd, src, base, p0, n, fc->resample_flag != 0, x);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       if (p0 + k >= n) break;

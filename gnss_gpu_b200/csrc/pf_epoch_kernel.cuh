@@ -2,7 +2,7 @@
 //
 // All CTAs are co-resident (cooperative launch); each owns a contiguous
 // chunk of (filter, tile) work items and the phases of the epoch are
-// separated by grid barriers with bounded spins:
+// separated by one grid barrier with bounded spins:
 //
 //   1  predict + likelihood + tile statistics (particles loaded straight
 //      into registers, gathered through the last resample's ancestors;
@@ -12,21 +12,21 @@
 //      its own maximum and stores their prefixes inside the segment, warp 0
 //      rescales the segment sums exactly to the tile maximum.
 //   -- barrier
-//   2  per-filter merge of the tile rows (filter f_first + j by CTA j mod G;
-//      one pass, the filter maximum having been collected in phase 1): ESS,
-//      weighted mean / covariance, device-side resample decision.
+//   2  per-filter merge of the tile rows (filter f_first + j by CTA j mod G):
+//      ESS, weighted mean / covariance, device-side resample decision.
 //      At the same time, systematic only, on the CTAs that own no filter
 //      (when filters are fewer than a quarter of the CTAs; otherwise every
 //      CTA after its merges):
-//   4  tile sums rescaled to the filter maximum, the filter prefix of each
-//      tile, then per particle its filter-wide CDF and offspring end F(i);
-//      slots [F(i-1), F(i)) get ancestor i, written here when the run is
-//      short, queued in chunks of kRunChunk slots when long (speculative for
-//      every filter that may resample: the decision is taken meanwhile).
-//   -- barrier
-//   5  the queued chunks, taken by all warps of the grid in turn.
-//   Megopolis instead: -- barrier, then the chain per slot for the filters
-//   that resample.
+//   4  the filter maximum from the tile maxima, tile sums rescaled to it,
+//      the filter prefix of each tile, then per particle its filter-wide CDF
+//      and offspring end F(i); slots [F(i-1), F(i)) get ancestor i, written
+//      by the lane when the run is short and by the warp when it is long,
+//      where a 128-slot segment the run covers gets one marker word instead
+//      of 128 slots (speculative for every filter that may resample: the
+//      decision is taken meanwhile).  The kernel ends there.
+//   Megopolis instead: every CTA takes the resample decision for the
+//   filters of its tiles from the owner's merge (recomputed, bit-identical),
+//   then runs the chain per slot of its tiles.  The kernel ends there.
 //
 // Compared with one kernel per phase this removes the launch/drain gaps and
 // every per-tile queue atomic; the prefixes reread in phase 4 come from L2
@@ -41,11 +41,6 @@ namespace pfb {
 
 __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
 }
 
 __device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
@@ -143,52 +138,122 @@ __device__ __forceinline__ void block_sum2_u64(unsigned long long a, unsigned lo
 }
 
 
-// The systematic resampler's phases walk a chunk of tiles filter segment by
-// filter segment (the tiles of one filter inside the chunk).  Every warp
-// works on its own 128-particle segment (phase 4) or on queued chunks of
-// long offspring runs (phase 5) without CTA barriers; only the per-filter
-// prefix of phase 4 is a CTA reduction.  The loops are kept compact (not
-// unrolled over tiles): this code runs a few times per CTA and epoch, so
-// instruction fetch, not arithmetic, sets its speed.  Integer sums are
-// exact, so the result does not depend on the order of the atomics or on
-// the chunking.
+// The systematic resampler's phase 4 walks a chunk of tiles filter segment
+// by filter segment (the tiles of one filter inside the chunk).  Every warp
+// works on its own 128-particle segment without CTA barriers; only the
+// per-filter maximum and prefix are CTA reductions.  The loops are kept
+// compact (not unrolled over tiles): this code runs a few times per CTA and
+// epoch, so instruction fetch, not arithmetic, sets its speed.  Integer sums
+// are exact, so the result does not depend on the chunking.
+
+// Phase 4's inputs of one tile for one lane: the tile's integer sum and
+// maximum, its warp segment's scale and prefix, the lane's four in-segment
+// prefixes (zero past the filter's end).
+struct OffspringTileIn {
+  double S, rho, E;
+  double2 ca, cb;
+  float m;
+};
+__device__ __forceinline__ OffspringTileIn load_offspring_tile(const EngineDev& e, int g, int tb, int n,
+                                                               long long base, int warp, int lane) {
+  OffspringTileIn o;
+  o.S = __ldcg(e.tile_S + g);
+  o.m = __ldcg(e.tile_m + g);
+  o.rho = 0.0;
+  o.E = 0.0;
+  o.ca = make_double2(0.0, 0.0);
+  o.cb = o.ca;
+  const int pw = (g - tb) * kTile + warp * kWarpTile, p0 = pw + lane * 4;
+  if (pw < n) {
+    o.rho = __ldcg(e.seg_rho + (size_t)g * kSubTiles + warp);
+    o.E = __ldcg(e.seg_E + (size_t)g * kSubTiles + warp);
+    if (p0 < n) {
+      const double2* src = reinterpret_cast<const double2*>(e.seg_c + base + p0);
+      o.ca = __ldcg(src);
+      o.cb = __ldcg(src + 1);
+    }
+  }
+  return o;
+}
+
+// The run [lo, hi) of ancestor i, written by the whole warp (its values
+// broadcast from one lane): the marker of every 128-slot segment that starts
+// inside the run -- i when the run covers the segment, else -1 (only the
+// last one can be partial) -- and the slots of the segments the run covers
+// in part.  `seg` is the filter's marker array, n its slot count.
+__device__ __forceinline__ void write_heavy_run(const EngineDev& e, int* anc, int* seg, uint32_t lo, uint32_t hi,
+                                                int i, uint32_t n, int lane) {
+  if (!PF_BOUNDS_OK(e, lo < hi && hi <= n)) return;
+  const uint32_t s_first = (lo + kWarpTile - 1) / kWarpTile, s_last = (hi - 1) / kWarpTile;
+  const bool last_full = s_first <= s_last && min((s_last + 1) * (uint32_t)kWarpTile, n) <= hi;
+  for (uint32_t sg = s_first + lane; sg <= s_last; sg += 32) seg[sg] = (sg < s_last || last_full) ? i : -1;
+  const uint32_t head_end = min(hi, s_first * (uint32_t)kWarpTile);
+  for (uint32_t j = lo + lane; j < head_end; j += 32) anc[j] = i;
+  if (s_first <= s_last && !last_full)
+    for (uint32_t j = s_last * (uint32_t)kWarpTile + lane; j < hi; j += 32) anc[j] = i;
+}
 
 // Phase 4, right after the first barrier and speculative (the filters'
 // owners decide at the same time whether they resample; when one does not,
-// this work is unused): for every filter whose weights may resample (its
-// max-code word is set), the filter prefix of each tile of the chunk from
-// the tile sums scaled to the filter maximum, then per particle its
-// filter-wide CDF C_i and offspring end F(i); slots [F(i-1), F(i)) get
-// ancestor i, written here when the run is short, queued in chunks of
-// kRunChunk slots when long.
-__device__ __forceinline__ void epoch_sys_offspring(const EngineDev& e, unsigned* bar, int cb, int ce,
-                                                    unsigned long long* s_u64) {
+// this work is unused): for every filter that may resample this step (the
+// flag phase 1 left in its control block), the filter maximum from the tile
+// maxima, the filter prefix of each tile of the chunk from the tile sums
+// scaled to that maximum, then per particle its filter-wide CDF C_i and
+// offspring end F(i); slots [F(i-1), F(i)) get ancestor i.  A run of up to
+// kLightRun slots is written by its lane (with the marker of a segment
+// starting inside it); a longer one by the whole warp (write_heavy_run).
+// The marker of each segment is written by the run holding the segment's
+// first slot, so every resampling step rewrites all of them, and the step
+// needs no second grid barrier: the next step's gather is the first reader.
+__device__ __forceinline__ void epoch_sys_offspring(const EngineDev& e, int cb, int ce, unsigned long long* s_u64) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int t = cb; t < ce;) {
     const int f = __ldg(e.tile_filter + t);
     const FilterDesc* fd = e.desc + f;
     FilterCtrl* fc = e.ctrl + f;
     const int tb = fd->tile_begin, nt = fd->n_tiles, se = min(ce, tb + nt);
-    const unsigned mcode = __ldcg(e.fmax + f);
-    if (mcode != 0u) {  // CTA-uniform
-      const float M = ord_decode(mcode);
-      // prefix of tile t inside its filter and the filter total, from the
-      // tile sums scaled to the filter maximum
+    if (ld_cg_int(&fc->sys_q_cur)) {  // CTA-uniform
+      const int n = fd->n;
+      const long long base = fd->p_off;
+      // the first tile's inputs load while the filter prefix is formed; in
+      // the loop below the next tile's load while this one is worked on
+      // (every load is independent of the previous tile)
+      OffspringTileIn nxt{};
+      if (t < se) nxt = load_offspring_tile(e, t, tb, n, base, warp, lane);
+      // the filter maximum M (the largest tile maximum), then the prefix of
+      // tile t inside its filter and the filter total, from the tile sums
+      // scaled to M; four tiles per thread and round, their loads issued
+      // together, one round kept in registers for filters of up to
+      // kB * kThreads tiles
+      constexpr int kB = 4;
+      double S[kB];
+      float m[kB];
+      auto load_round = [&](int i0) {
+#pragma unroll
+        for (int j = 0; j < kB; ++j) {
+          const int i = i0 + j * kThreads;
+          S[j] = i < nt ? __ldcg(e.tile_S + tb + i) : 0.0;
+          m[j] = i < nt ? __ldcg(e.tile_m + tb + i) : -INFINITY;
+        }
+      };
+      float mx = -INFINITY;
+#pragma unroll 1
+      for (int i0 = threadIdx.x; i0 < nt; i0 += kB * kThreads) {
+        load_round(i0);
+#pragma unroll
+        for (int j = 0; j < kB; ++j) mx = fmaxf(mx, m[j]);
+      }
+      const float M = block_max(mx, reinterpret_cast<float*>(s_u64));
+      if (M == -INFINITY) {  // CTA-uniform: no finite weight (the owner reports it)
+        t = se;
+        continue;
+      }
       unsigned long long P = 0, W = 0;
       {
-        // four tiles per thread and round, their loads issued together
-        constexpr int kB = 4;
         unsigned long long pre = 0, all = 0;
 #pragma unroll 1
         for (int i0 = threadIdx.x; i0 < nt; i0 += kB * kThreads) {
-          double S[kB];
-          float m[kB];
-#pragma unroll
-          for (int j = 0; j < kB; ++j) {
-            const int i = i0 + j * kThreads;
-            S[j] = i < nt ? __ldcg(e.tile_S + tb + i) : 0.0;
-            m[j] = i < nt ? __ldcg(e.tile_m + tb + i) : 0.0f;
-          }
+          if (nt > kB * kThreads) load_round(i0);  // else the registers hold the only round
 #pragma unroll
           for (int j = 0; j < kB; ++j) {
             double r;
@@ -204,27 +269,22 @@ __device__ __forceinline__ void epoch_sys_offspring(const EngineDev& e, unsigned
         if (W == 0ull) atomicOr(e.err, ERR_BAD_WEIGHTS);
       }
       if (W > 0ull) {
-        const int n = fd->n;
-        const long long base = fd->p_off;
         const uint32_t u = ld_cg_u(&fc->sys_u_cur);
         const double scale = (double)n / (double)W, uf = (double)u * 2.3283064365386963e-10;
+        int* anc = e.anc + base;
+        int* seg = e.seg_anc + (size_t)tb * kSubTiles;
 #pragma unroll 1
         for (int g = t; g < se; ++g) {
           const int pw = (g - tb) * kTile + warp * kWarpTile;
           const int p0 = pw + lane * 4;
+          const OffspringTileIn cur = nxt;
+          if (g + 1 < se) nxt = load_offspring_tile(e, g + 1, tb, n, base, warp, lane);
           double r;
-          const unsigned long long ts = (unsigned long long)sys_tile_total(e, g, M, r);
+          const unsigned long long ts = (unsigned long long)sys_tile_total(cur.S, cur.m, M, r);
           if (pw < n) {  // warp-uniform
-            const double rho = __ldcg(e.seg_rho + (size_t)g * kSubTiles + warp);
-            const double E = __ldcg(e.seg_E + (size_t)g * kSubTiles + warp);
-            double2 ca = make_double2(0.0, 0.0), cb2 = ca;
-            if (p0 < n) {
-              const double2* src = reinterpret_cast<const double2*>(e.seg_c + base + p0);
-              ca = __ldcg(src);
-              cb2 = __ldcg(src + 1);
-            }
+            const double rho = cur.rho, E = cur.E;
             // segment prefixes of this lane's particles and of the one before
-            const double c[4] = {ca.x, ca.y, cb2.x, cb2.y};
+            const double c[4] = {cur.ca.x, cur.ca.y, cur.cb.x, cur.cb.y};
             double cprev = __shfl_up_sync(0xffffffffu, c[3], 1);
             if (lane == 0) cprev = 0.0;
             const double Pd = (double)P;
@@ -238,54 +298,24 @@ __device__ __forceinline__ void epoch_sys_offspring(const EngineDev& e, unsigned
                             ? offspring_end_split(P, Pd, sys_inner(E, rho, r, c[k]), W, (uint32_t)n, u, scale, uf)
                             : (uint32_t)n;
             }
-            // Slots [F(i-1), F(i)) take ancestor i.  Runs of up to kLightRun
-            // slots are written here by their lane; longer runs (heavy
-            // particles, which sit next to each other after a resample) are
-            // cut into chunks of kRunChunk slots and queued for phase 5,
-            // where every warp of the grid takes chunks.
 #pragma unroll 1
             for (int k = 0; k < 4; ++k) {
               const uint32_t lo = (k == 0) ? Fprev : Fk[k - 1], hi = Fk[k];
               const int i = p0 + k;
               const bool run = i < n && hi > lo;
-              if (run && hi - lo <= (uint32_t)kLightRun && PF_BOUNDS_OK(e, hi <= (uint32_t)n))
-                for (uint32_t j = lo; j < hi; ++j) e.anc[base + j] = i;
-              // long runs: one reservation per warp, a lane writes its own
-              // one or two chunk descriptors, the warp writes longer lists
               const bool heavy = run && hi - lo > (uint32_t)kLightRun;
-              const uint32_t nch = heavy ? (hi - lo + kRunChunk - 1) / kRunChunk : 0u;
-              if (__ballot_sync(0xffffffffu, heavy) == 0u) continue;  // warp-uniform
-              uint32_t incl = nch;
-#pragma unroll
-              for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += v;
+              if (run && !heavy && PF_BOUNDS_OK(e, hi <= (uint32_t)n)) {
+                for (uint32_t j = lo; j < hi; ++j) anc[j] = i;
+                const uint32_t sg = (lo + kWarpTile - 1) / kWarpTile;  // a segment starting inside the run
+                if (sg * (uint32_t)kWarpTile < hi)
+                  seg[sg] = min((sg + 1) * (uint32_t)kWarpTile, (uint32_t)n) <= hi ? i : -1;
               }
-              unsigned at0 = 0u;
-              if (lane == 31) at0 = atomicAdd(bar + kBarChunks, incl);
-              const unsigned at = __shfl_sync(0xffffffffu, at0, 31) + incl - nch;
-              if (heavy && at + nch > e.max_chunks) atomicOr(e.err, ERR_INTERNAL_CAP);  // cannot happen: bounded by the layout
-              if (heavy && nch <= 2u) {
-                const uint32_t si = (uint32_t)i;
-                for (uint32_t c = 0; c < nch && at + c < e.max_chunks; ++c) {
-                  const long long st = base + lo + (long long)c * kRunChunk;
-                  e.chunks[at + c] = make_uint4((uint32_t)st, (uint32_t)(st >> 32),
-                                                min((uint32_t)kRunChunk, hi - lo - c * (uint32_t)kRunChunk), si);
-                }
-              }
-              unsigned todo = __ballot_sync(0xffffffffu, heavy && nch > 2u);
-              while (todo) {
+              unsigned todo = __ballot_sync(0xffffffffu, heavy);
+              while (todo) {  // warp-uniform
                 const int src = __ffs(todo) - 1;
                 todo &= todo - 1u;
-                const uint32_t slo = __shfl_sync(0xffffffffu, lo, src), shi = __shfl_sync(0xffffffffu, hi, src);
-                const uint32_t snch = __shfl_sync(0xffffffffu, nch, src);
-                const unsigned sat = __shfl_sync(0xffffffffu, at, src);
-                const uint32_t si = (uint32_t)(pw + src * 4 + k);
-                for (uint32_t c = lane; c < snch && sat + c < e.max_chunks; c += 32) {
-                  const long long st = base + slo + (long long)c * kRunChunk;
-                  e.chunks[sat + c] = make_uint4((uint32_t)st, (uint32_t)(st >> 32),
-                                                 min((uint32_t)kRunChunk, shi - slo - c * (uint32_t)kRunChunk), si);
-                }
+                write_heavy_run(e, anc, seg, __shfl_sync(0xffffffffu, lo, src), __shfl_sync(0xffffffffu, hi, src),
+                                pw + src * 4 + k, (uint32_t)n, lane);
               }
             }
           }
@@ -294,23 +324,6 @@ __device__ __forceinline__ void epoch_sys_offspring(const EngineDev& e, unsigned
       }
     }
     t = se;
-  }
-}
-
-// Phase 5, after the next barrier: the heavy runs' chunk descriptors (first
-// slot, length, ancestor), taken by the warps of the grid in turn, each
-// written with coalesced stores.
-__device__ __forceinline__ void epoch_sys_chunks(const EngineDev& e, const unsigned* bar) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const unsigned nchunks = min(ld_cg_u(bar + kBarChunks), e.max_chunks);
-  const int gw = (int)(blockIdx.x * (kThreads / 32)) + warp, nw = (int)(gridDim.x * (kThreads / 32));
-#pragma unroll 1
-  for (unsigned c = gw; c < nchunks; c += nw) {
-    const uint4 d = __ldcg(e.chunks + c);
-    const long long first = (long long)d.y << 32 | d.x;
-    if (!PF_BOUNDS_OK(e, first >= 0 && first + (long long)d.z <= e.p_total && d.z <= (uint32_t)kRunChunk)) continue;
-    int* dst = e.anc + first;
-    for (uint32_t j = lane; j < d.z; j += 32) dst[j] = (int)d.w;
   }
 }
 
@@ -331,16 +344,15 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
   __shared__ double s_dred[kWarps * 16];
   __shared__ unsigned long long s_u64[2 * kWarps];
   __shared__ double s_wq[2][kWarps];  // per-warp sums of the tiled integer CDF
-  __shared__ int s_any;
+  __shared__ int s_dec_f, s_dec_rs;  // the filter this CTA owns in phase 2 and its decision
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // generation of the last barrier (every thread reads it before its CTA
-  // first arrives, so no CTA can have moved it on yet)
-  unsigned gen = ld_acquire(bar + 1);
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    bar[2] = 0u;           // any-filter-resamples flag of this epoch
-    bar[kBarChunks] = 0u;  // queued offspring-run chunks of this epoch
-  }
+  // first arrives, so no CTA can have moved it on yet).  A relaxed load: the
+  // kernel boundary already orders the previous launch's release, and an
+  // acquire here would hold every later load of the CTA behind it.
+  unsigned gen = ld_relaxed(bar + 1);
+  if (threadIdx.x == 0) s_dec_f = -1;
   int cb, ce;
   cta_chunk(t0, count, cb, ce);
 
@@ -369,8 +381,30 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
     // the filter may resample this epoch: systematic builds its tiled integer CDF
     const bool may_rs = (do_weight || (eflags & PF_EP_RESAMPLE_CHECK)) && !(eflags & PF_EP_NO_RESAMPLE);
     const bool sys_q = RESAMPLER == PF_RESAMPLE_SYSTEMATIC && may_rs;
-    if (sys_q && t == fd->tile_begin && threadIdx.x == 0) fc->sys_u_cur = sys_offset_u(e, fd, epoch);
+    if (t == fd->tile_begin && threadIdx.x == 0) {  // read after the barrier (phase 4, Megopolis)
+      fc->sys_q_cur = sys_q ? 1 : 0;
+      fc->eflags_cur = eflags;
+      fc->epoch_cur = epoch;
+      if (sys_q) fc->sys_u_cur = sys_offset_u(e, fd, epoch);
+    }
 
+    // the particles' loads are issued first: their memory latency overlaps the
+    // satellite table of a new filter (FP64 geometry, two CTA barriers)
+    const int n = fd->n;
+    const int p0 = (t - fd->tile_begin) * kTile + (int)threadIdx.x * 4;
+    const bool active = p0 < n;
+    const long long base = fd->p_off;
+    float* dst = fc->parity ? e.state0 : e.state1;
+    float x[D][4];
+    float lwv[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    if (active) {
+      load_particles<D>(e, fd, fc->parity ? e.state1 : e.state0, base, p0, n, fc->resample_flag != 0, x);
+    } else {
+#pragma unroll
+      for (int d = 0; d < D; ++d)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) x[d][k] = 0.f;
+    }
     if constexpr (WMODE == PF_WEIGHT_MIXTURE) {
       if (f != cached) {
         __shared__ MixSmem s_mix;
@@ -425,21 +459,6 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
       __syncthreads();
     }
 
-    const int n = fd->n;
-    const int p0 = (t - fd->tile_begin) * kTile + (int)threadIdx.x * 4;
-    const bool active = p0 < n;
-    const long long base = fd->p_off;
-    float* dst = fc->parity ? e.state0 : e.state1;
-    float x[D][4];
-    float lwv[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
-    if (active) {
-      load_particles<D>(e, fc->parity ? e.state1 : e.state0, base, p0, n, fc->resample_flag != 0, x);
-    } else {
-#pragma unroll
-      for (int d = 0; d < D; ++d)
-#pragma unroll
-        for (int k = 0; k < 4; ++k) x[d][k] = 0.f;
-    }
     if (active) {
       float lw0[4] = {0.f, 0.f, 0.f, 0.f};
       const bool need_prev = !lw_zero && (!do_weight || e.lw_mode == PF_LW_ACCUMULATE);
@@ -617,7 +636,6 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
           row[0] = tm;
           // filter maximum for the one-pass merge and the integer CDF, kept
           // only when the filter may resample this epoch
-          if (tm > -INFINITY && may_rs) atomicMax(e.fmax + f, ord_code(tm));
         }
         // tile level of the tiled integer CDF
         if (sys_q) sys_tile_scale(e, t, lane < kWarps ? s_wq[b][lane] : 0.0, lane < kWarps ? wr[lane][0] : -INFINITY, tm);
@@ -642,12 +660,11 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
     const unsigned char* ob = e.obs + (size_t)(epoch % (unsigned)e.obs_slots) * e.obs_slot_bytes;
     const pf_filter_epoch_t* fe = reinterpret_cast<const pf_filter_epoch_t*>(ob) + f;
     const int eflags = fe->flags;
-    const unsigned mcode = __ldcg(e.fmax + f);
-    const float M = mcode ? ord_decode(mcode) : rows_max(e.part, fd->tile_begin, fd->n_tiles, s_maxtmp);
-    MergedStats ms = merge_tiles_at<D>(e.part, fd->tile_begin, fd->n_tiles, M, s_dred);
+    MergedStats ms = merge_tiles<D>(e.part, fd->tile_begin, fd->n_tiles, s_maxtmp, s_dred);
     if (threadIdx.x == 0) {
       finalize_filter<D>(e, fd, fc, ms, epoch, fc->parity, fc->lw_zero != 0, eflags, (eflags & PF_EP_WEIGHT) != 0);
-      if (fc->resample_flag) atomicOr(&bar[2], 1u);
+      s_dec_f = f;
+      s_dec_rs = fc->resample_flag;
     }
     __syncthreads();
   }
@@ -660,26 +677,35 @@ __global__ void __launch_bounds__(kThreads, PF_EPOCH_MINB) k_epoch(EngineDev e, 
     if ((int)blockIdx.x >= h0) {
       int b4, e4;
       chunk_of(t0, count, (int)blockIdx.x - h0, (int)gridDim.x - h0, b4, e4);
-      epoch_sys_offspring(e, bar, b4, e4, s_u64);
+      epoch_sys_offspring(e, b4, e4, s_u64);
     }
-    grid_barrier(e, bar, gen);
-    for (int j = blockIdx.x; j < nf; j += gridDim.x)  // every reader of the max codes is past the barrier
-      if (threadIdx.x == 0) e.fmax[f_first + j] = 0u;
-    // ---------------------------------------------------------------- phase 5
-    epoch_sys_chunks(e, bar);
+    // no second barrier: the ancestors and segment markers are read first by
+    // the next step, after this kernel has ended
   } else {
-    grid_barrier(e, bar, gen);
-    for (int j = blockIdx.x; j < nf; j += gridDim.x)  // every reader of the max codes is past the barrier
-      if (threadIdx.x == 0) e.fmax[f_first + j] = 0u;
-    if (threadIdx.x == 0) s_any = (int)ld_cg_u(&bar[2]);
-    __syncthreads();
-    if (!s_any) return;  // uniform: no filter resamples this epoch
+    // Megopolis: no second barrier either.  A CTA decides for the filter of
+    // its tiles itself, with the owner's merge (the same function on the
+    // same rows gives the same bits, hence the same decision) or, for the
+    // filter it owns, with the owner's decision; epoch and flags come from
+    // the snapshot phase 1 left (the owner advances the epoch meanwhile).
+    int cf = -1;
+    bool crs = false;
     for (int t = cb; t < ce; ++t) {
       const int f = __ldg(e.tile_filter + t);
       const FilterDesc* fd = e.desc + f;
       const FilterCtrl* fc = e.ctrl + f;
-      if (!ld_cg_int(&fc->resample_flag)) continue;
-      mego_tile(e, fd, ld_cg_u(&fc->epoch) - 1u, t);
+      if (f != cf) {  // CTA-uniform
+        cf = f;
+        if (f == s_dec_f) {
+          crs = s_dec_rs != 0;
+        } else {
+          const MergedStats ms = merge_tiles<D>(e.part, fd->tile_begin, fd->n_tiles, s_maxtmp, s_dred);
+          if (threadIdx.x == 0) s_dec_rs = resample_decision(e, fd, ms, ld_cg_int(&fc->eflags_cur)) ? 1 : 0;
+          __syncthreads();
+          crs = s_dec_rs != 0;
+          __syncthreads();  // s_dec_rs is rewritten for the next filter
+        }
+      }
+      if (crs) mego_tile(e, fd, ld_cg_u(&fc->epoch_cur), t);
     }
   }
 }

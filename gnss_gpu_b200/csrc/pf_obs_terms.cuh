@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kThreads) k_obs_term(EngineDev e, int f, ObsBl
   const bool keep = b.accumulate && fc->lw_zero == 0;
   for (int p0 = (blockIdx.x * kThreads + threadIdx.x) * 4; p0 < n; p0 += gridDim.x * kThreads * 4) {
     float x[D][4];
-    load_particles<D>(e, src, base, p0, n, fc->resample_flag != 0, x);
+    load_particles<D>(e, fd, src, base, p0, n, fc->resample_flag != 0, x);
     const float4 l = keep ? *reinterpret_cast<const float4*>(e.lw + base + p0) : make_float4(0.f, 0.f, 0.f, 0.f);
     float lv[4] = {l.x, l.y, l.z, l.w};
 #pragma unroll 1

@@ -73,8 +73,9 @@ __global__ void __launch_bounds__(kThreads) k_vel_gather(EngineDev e, int f, con
   const FilterDesc* fd = e.desc + f;
   const int n = fd->n;
   const long long base = fd->p_off;
+  const int* seg = seg_markers(e, fd);
   for (int j = blockIdx.x * kThreads + threadIdx.x; j < n; j += gridDim.x * kThreads) {
-    int a = e.anc[base + j];
+    int a = ancestor_at(e, seg, base, j);
     a = a < 0 ? 0 : (a >= n ? n - 1 : a);
     for (int c = 0; c < kVelComp; ++c) vout[(size_t)c * n + j] = vin[(size_t)c * n + a];
   }
@@ -105,7 +106,7 @@ __global__ void __launch_bounds__(kThreads) k_vel_predict(EngineDev e, int f, do
   const double alpha = fmin(1.0, fmax(0.0, vp.alpha));
   for (int p0 = (blockIdx.x * kThreads + threadIdx.x) * 4; p0 < n; p0 += gridDim.x * kThreads * 4) {
     float x[D][4];
-    load_particles<D>(e, src, base, p0, n, fc->resample_flag != 0, x);
+    load_particles<D>(e, fd, src, base, p0, n, fc->resample_flag != 0, x);
 #pragma unroll 1
     for (int k = 0; k < 4; ++k) {
       const int j = p0 + k;
@@ -214,7 +215,7 @@ __global__ void __launch_bounds__(kThreads) k_doppler(EngineDev e, int f, double
   const double wl = a.wavelength;
   for (int p0 = (blockIdx.x * kThreads + threadIdx.x) * 4; p0 < n; p0 += gridDim.x * kThreads * 4) {
     float x[D][4];
-    load_particles<D>(e, src, base, p0, n, fc->resample_flag != 0, x);
+    load_particles<D>(e, fd, src, base, p0, n, fc->resample_flag != 0, x);
     const float4 l4 = keep ? *reinterpret_cast<const float4*>(e.lw + base + p0) : make_float4(0.f, 0.f, 0.f, 0.f);
     float lv[4] = {l4.x, l4.y, l4.z, l4.w};
 #pragma unroll 1

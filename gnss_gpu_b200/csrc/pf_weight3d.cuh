@@ -24,6 +24,7 @@ __global__ void __launch_bounds__(kThreads) k_weight_3d(EngineDev e, int f, Mesh
   const float* src = fc->parity ? e.state1 : e.state0;
   const bool keep = a.accumulate && fc->lw_zero == 0;
   const bool gather = fc->resample_flag != 0;
+  const int* seg = seg_markers(e, fd);
   // one particle per thread: the traversals are latency bound, so many
   // threads in flight matter more than per-thread reuse.  (A warp-wide walk
   // on a shared stack, one control path per warp, measured slower: 2.4 vs
@@ -31,7 +32,7 @@ __global__ void __launch_bounds__(kThreads) k_weight_3d(EngineDev e, int f, Mesh
   for (int j = blockIdx.x * kThreads + threadIdx.x; j < n; j += gridDim.x * kThreads) {
     int src_j = j;
     if (gather) {
-      src_j = __ldcg(e.anc + base + j);
+      src_j = ancestor_at(e, seg, base, j);
       if ((unsigned)src_j >= (unsigned)n) src_j = j;
     }
     const float* sp = src + base + src_j;
