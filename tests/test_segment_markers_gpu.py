@@ -67,7 +67,7 @@ def test_runs_around_segments_match_oracle_and_gather(n):
     assert np.array_equal(want, anc)
     assert W == w_want
     counts = np.bincount(anc, minlength=n)[owners]
-    assert (counts > 128).sum() >= 8 and (counts <= 128).sum() >= 8, counts  # both write paths ran
+    assert (counts > 128).sum() >= 8 and (counts <= 128).sum() >= 6, counts  # both write paths ran
 
     # the host export gathers through the merged ancestors
     x_host, _ = eng.state_f32(0)
