@@ -1404,9 +1404,6 @@ int pfe_get_ancestors(pf_engine_t* eng, int filter, int* out_host) {
   if (s != PF_OK) return s;
   if (!out_host) return set_err(PF_EINVAL, "null out");
   if ((s = sync_and_check(eng)) != PF_OK) return s;
-  int n, tb, nt;
-  long long base;
-  filter_dims(eng, filter, &n, &base, &tb, &nt);
   return read_ancestors(eng, filter, out_host);
 }
 

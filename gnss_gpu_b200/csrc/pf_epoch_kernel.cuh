@@ -193,7 +193,7 @@ __device__ __forceinline__ void write_heavy_run(const EngineDev& e, int* anc, in
     for (uint32_t j = s_last * (uint32_t)kWarpTile + lane; j < hi; j += 32) anc[j] = i;
 }
 
-// Phase 4, right after the first barrier and speculative (the filters'
+// Phase 4, right after the grid barrier and speculative (the filters'
 // owners decide at the same time whether they resample; when one does not,
 // this work is unused): for every filter that may resample this step (the
 // flag phase 1 left in its control block), the filter maximum from the tile
